@@ -1,0 +1,512 @@
+"""Host-side mirror of the reference's training-path interface over libcpx.so.
+
+The reference exposes its hot path as C++ static methods on structs passed by
+value (SparseVolumeRadianceField/RenderUtils.cuh:7-85, Optimizer.cuh:5-38,
+SceneUtils.cuh:4-98, Rays.cuh:8-57).  This module keeps those names and
+argument meanings -- ``ObjectScene``, ``Rays``, ``RenderUtils.renderRays``,
+``RenderUtils.renderRays_withGradients_RGB``, ``RenderUtils.addVarianceLoss``,
+``Optimizer.updateRGBScene`` -- and calls the C ABI of include/cpx.h.  Where the
+reference exits the process on a CUDA error (checkGPUStatus, Utils.cu:700-717)
+these raise ``CpxError`` carrying the status code.
+
+Device buffers that the reference takes as raw device pointers (the sample
+index table and the per-ray losses) are passed as CUDA tensors or integer
+device addresses.  There is no CPU fallback: importing this module fails
+loudly when the compiled library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+import numpy as np
+
+PKG_DIR = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "lib" / "libcpx.so"
+
+if not LIB_PATH.exists():
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}` (or __graft_entry__.build())"
+    )
+_lib = C.CDLL(str(LIB_PATH))
+
+STATUS = {
+    0: "CPX_OK",
+    1: "CPX_ERR_INVALID_ARGUMENT",
+    2: "CPX_ERR_OUT_OF_MEMORY",
+    3: "CPX_ERR_CUDA",
+    4: "CPX_ERR_ITERATION_CAP",
+    5: "CPX_ERR_NAN",
+    6: "CPX_ERR_NOT_READY",
+    7: "CPX_ERR_UNSUPPORTED",
+}
+
+# Exported symbols of include/cpx.h (checked by the CPU test suite).
+EXPORTED = [
+    "cpx_status_string", "cpx_last_error", "cpx_version", "cpx_grid_create", "cpx_grid_destroy",
+    "cpx_grid_info", "cpx_grid_upload_params", "cpx_grid_download_params", "cpx_grid_upload_grads",
+    "cpx_grid_download_grads", "cpx_grid_upload_moments", "cpx_grid_download_moments",
+    "cpx_grid_set_adaptive_lr", "cpx_grid_set_sample_offsets", "cpx_grid_set_optimize_step",
+    "cpx_occupancy_build", "cpx_grid_make_sparse", "cpx_rays_create", "cpx_rays_destroy",
+    "cpx_rays_upload", "cpx_rays_upload_packed", "cpx_rays_download", "cpx_rays_init_camera",
+    "cpx_render_forward", "cpx_render_backward", "cpx_render_forward_backward", "cpx_tv_grad",
+    "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_grid_check",
+    "cpx_last_sample_counts", "cpx_kernel_launches",
+]
+
+
+class CpxError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+        msg = _lib.cpx_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {self.name}: {msg}")
+
+
+class GridDesc(C.Structure):
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int), ("depth", C.c_int),
+        ("sh_dim", C.c_int), ("optimizing_band", C.c_int), ("hierarchy_strategy", C.c_int),
+        ("step_size", C.c_float), ("bbox", C.c_int * 6),
+    ]
+
+
+class Camera(C.Structure):
+    """Device fields of the reference's Camera that getBound reads (CameraUtils.cuh:16-26)."""
+    _fields_ = [
+        ("alpha", C.c_double * 2), ("principle", C.c_double * 2),
+        ("c2w", C.c_double * 16), ("centre", C.c_double * 4),
+    ]
+
+    @classmethod
+    def make(cls, alpha, principle, c2w, centre):
+        cam = cls()
+        cam.alpha[:] = [float(a) for a in alpha]
+        cam.principle[:] = [float(p) for p in principle]
+        cam.c2w[:] = [float(v) for v in np.asarray(c2w, dtype=np.float64).reshape(16)]
+        cam.centre[:] = [float(v) for v in np.asarray(centre, dtype=np.float64).reshape(4)]
+        return cam
+
+
+class StepArgs(C.Structure):
+    _fields_ = [
+        ("mask_coef", C.c_double), ("huber_delta", C.c_float), ("do_tv", C.c_int),
+        ("tv_type", C.c_int), ("tv_neighbours", C.c_int), ("lam_density", C.c_double),
+        ("lam_sh", C.c_double), ("lr", C.c_double), ("sh_lr", C.c_double), ("timestep", C.c_int),
+    ]
+
+
+_vp = C.c_void_p
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def _sig(name, args, res=C.c_int):
+    fn = getattr(_lib, name)
+    fn.argtypes = args
+    fn.restype = res
+    return fn
+
+
+_lib.cpx_last_error.restype = C.c_char_p
+_lib.cpx_status_string.restype = C.c_char_p
+_lib.cpx_status_string.argtypes = [C.c_int]
+_sig("cpx_version", [])
+_sig("cpx_kernel_launches", [], C.c_int64)
+_sig("cpx_grid_create", [C.POINTER(GridDesc), C.POINTER(_vp)])
+_sig("cpx_grid_destroy", [_vp])
+_sig("cpx_grid_info", [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int)])
+for _n in ("upload_params", "download_params", "upload_grads", "download_grads"):
+    _sig(f"cpx_grid_{_n}", [_vp, _f32p, C.c_int64])
+_sig("cpx_grid_upload_moments", [_vp, _f32p, _f32p, C.c_int64])
+_sig("cpx_grid_download_moments", [_vp, _f32p, _f32p, C.c_int64])
+_sig("cpx_grid_set_adaptive_lr", [_vp, _f32p, C.c_int64])
+_sig("cpx_grid_set_sample_offsets", [_vp, _vp, _vp, _vp, C.c_int])
+_sig("cpx_grid_set_optimize_step", [_vp, C.c_int])
+_sig("cpx_occupancy_build", [_vp, C.c_float, _vp, _vp, _vp, C.POINTER(C.c_uint32)])
+_sig("cpx_grid_make_sparse", [_vp])
+_sig("cpx_grid_check", [_vp])
+_sig("cpx_rays_create", [C.c_int64, C.c_int, C.POINTER(_vp)])
+_sig("cpx_rays_destroy", [_vp])
+_sig("cpx_rays_upload", [_vp, C.c_int64, C.c_int64] + [_vp] * 12 + [_vp])
+_sig("cpx_rays_upload_packed", [_vp, C.c_int64, C.c_int64, _vp, _vp])
+_sig("cpx_rays_download", [_vp, C.c_int64, C.c_int64] + [_vp] * 17)
+_sig("cpx_rays_init_camera", [_vp, _vp, C.POINTER(Camera), C.c_int, C.c_int, _u8p, _u8p, _u8p,
+                              _vp, _i32p, C.c_int64, C.c_int64])
+_sig("cpx_render_forward", [_vp, _vp, _vp, C.c_int, C.c_int, _vp])
+_sig("cpx_render_backward", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_double, C.c_float, _vp])
+_sig("cpx_render_forward_backward", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_double, C.c_float, _vp])
+_sig("cpx_tv_grad", [_vp, C.c_double, C.c_double, C.c_int, C.c_int, _vp])
+_sig("cpx_adam_step", [_vp, C.c_double, C.c_double, C.c_int, _vp])
+_sig("cpx_tv_adam_step", [_vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _vp])
+_sig("cpx_train_step", [_vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), _vp,
+                        C.POINTER(C.c_double), _vp])
+_sig("cpx_last_sample_counts", [_vp, _i32p, C.c_int])
+
+
+def _check(rc: int, where: str):
+    if rc != 0:
+        raise CpxError(rc, where)
+
+
+def _ptr(x) -> int | None:
+    """Device address of a CUDA tensor / integer, or None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if hasattr(x, "is_cuda") and not x.is_cuda:
+            raise ValueError("expected a CUDA tensor")
+        return x.data_ptr()
+    raise TypeError(f"cannot take a device address of {type(x)}")
+
+
+def _stream(stream) -> int | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def kernel_launches() -> int:
+    return int(_lib.cpx_kernel_launches())
+
+
+def version() -> int:
+    return int(_lib.cpx_version())
+
+
+class ObjectScene:
+    """Grid + optimizer state (objectScene, SceneUtils.cuh:4-98, and optimizer, Optimizer.cuh)."""
+
+    def __init__(self, width, height, depth, sh_dim=9, optimizing_band=None, step_size=0.5,
+                 hierarchy_strategy=False, bbox=None):
+        if optimizing_band is None:
+            optimizing_band = int(round(sh_dim ** 0.5)) - 1
+        if bbox is None:  # initSelf: bbox spans the grid (SceneUtils.cu:107-112)
+            bbox = (0, width - 1, 0, height - 1, 0, depth - 1)
+        d = GridDesc()
+        d.width, d.height, d.depth = int(width), int(height), int(depth)
+        d.sh_dim = int(sh_dim)
+        d.optimizing_band = int(optimizing_band)
+        d.hierarchy_strategy = 1 if hierarchy_strategy else 0
+        d.step_size = float(step_size)
+        d.bbox[:] = [int(b) for b in bbox]
+        self.desc = d
+        self.width, self.height, self.depth = d.width, d.height, d.depth
+        self.sh_dim = d.sh_dim
+        self.optimizing_band = d.optimizing_band
+        self.step_size = float(step_size)
+        self.bbox = tuple(bbox)
+        h = _vp()
+        _check(_lib.cpx_grid_create(C.byref(d), C.byref(h)), "cpx_grid_create")
+        self._h = h
+
+    # -- bookkeeping
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        n = C.c_int64()
+        a = C.c_int()
+        s = C.c_int()
+        _check(_lib.cpx_grid_info(self._h, C.byref(n), C.byref(a), C.byref(s)), "cpx_grid_info")
+        return n.value, a.value, bool(s.value)
+
+    @property
+    def actual_grid_nums(self) -> int:
+        return self.info()[0]
+
+    @property
+    def n_arrays(self) -> int:
+        return 1 + 3 * self.sh_dim
+
+    @property
+    def sparse(self) -> bool:
+        return self.info()[2]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cpx_grid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- parameter blocks (planar [n_arrays][n_active], reference layout)
+    def _planar(self, a):
+        n = self.actual_grid_nums
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        if a.size != self.n_arrays * n:
+            raise ValueError(f"expected {self.n_arrays}x{n} floats, got shape {a.shape}")
+        return a.reshape(self.n_arrays, n), n
+
+    def upload_params(self, planar):
+        a, n = self._planar(planar)
+        _check(_lib.cpx_grid_upload_params(self._h, a, n), "cpx_grid_upload_params")
+
+    def download_params(self):
+        n = self.actual_grid_nums
+        out = np.empty((self.n_arrays, n), np.float32)
+        _check(_lib.cpx_grid_download_params(self._h, out, n), "cpx_grid_download_params")
+        return out
+
+    def upload_grads(self, planar):
+        a, n = self._planar(planar)
+        _check(_lib.cpx_grid_upload_grads(self._h, a, n), "cpx_grid_upload_grads")
+
+    def download_grads(self):
+        n = self.actual_grid_nums
+        out = np.empty((self.n_arrays, n), np.float32)
+        _check(_lib.cpx_grid_download_grads(self._h, out, n), "cpx_grid_download_grads")
+        return out
+
+    def upload_moments(self, m, v):
+        a, n = self._planar(m)
+        b, _ = self._planar(v)
+        _check(_lib.cpx_grid_upload_moments(self._h, a, b, n), "cpx_grid_upload_moments")
+
+    def download_moments(self):
+        n = self.actual_grid_nums
+        m = np.empty((self.n_arrays, n), np.float32)
+        v = np.empty((self.n_arrays, n), np.float32)
+        _check(_lib.cpx_grid_download_moments(self._h, m, v, n), "cpx_grid_download_moments")
+        return m, v
+
+    def set_adaptive_lr(self, lr_mult):
+        a = np.ascontiguousarray(lr_mult, dtype=np.float32).reshape(-1)
+        _check(_lib.cpx_grid_set_adaptive_lr(self._h, a, a.size), "cpx_grid_set_adaptive_lr")
+
+    def set_sample_offsets(self, ox, oy, oz):
+        if ox is None or len(ox) == 0:
+            _check(_lib.cpx_grid_set_sample_offsets(self._h, None, None, None, 0), "offsets")
+            return
+        arrs = [np.ascontiguousarray(v, dtype=np.float64) for v in (ox, oy, oz)]
+        self._offsets_keep = arrs
+        _check(_lib.cpx_grid_set_sample_offsets(self._h, *[a.ctypes.data for a in arrs], len(arrs[0])),
+               "cpx_grid_set_sample_offsets")
+
+    def set_optimize_step(self, step: int):
+        _check(_lib.cpx_grid_set_optimize_step(self._h, int(step)), "cpx_grid_set_optimize_step")
+
+    # -- occupancy (pruneSelf + getCagedNums, SceneUtils.cu:883, 1081)
+    def prune_self(self, threshold: float):
+        W, H, D = self.width, self.height, self.depth
+        occ = np.empty((W - 1) * (H - 1) * (D - 1), np.uint8)
+        cage = np.empty(W * H * D, np.uint8)
+        idx = np.empty(W * H * D, np.uint32)
+        cnt = C.c_uint32()
+        _check(_lib.cpx_occupancy_build(self._h, float(threshold), occ.ctypes.data, cage.ctypes.data,
+                                        idx.ctypes.data, C.byref(cnt)), "cpx_occupancy_build")
+        return occ, cage, idx, int(cnt.value)
+
+    def make_sparse(self):
+        _check(_lib.cpx_grid_make_sparse(self._h), "cpx_grid_make_sparse")
+
+    def check(self):
+        _check(_lib.cpx_grid_check(self._h), "cpx_grid_check")
+
+    def last_sample_counts(self, n: int):
+        out = np.empty(n, np.int32)
+        _check(_lib.cpx_last_sample_counts(self._h, out, n), "cpx_last_sample_counts")
+        return out
+
+
+RAY_INPUTS = ("ox", "oy", "oz", "dx", "dy", "dz", "near", "far", "mask", "r", "g", "b")
+RAY_OUTPUTS = ("acc_density", "acc_weights", "acc_r", "acc_g", "acc_b")
+_FLOAT_FIELDS = set(RAY_INPUTS[:8]) | set(RAY_OUTPUTS)
+
+
+class Rays:
+    """Training-ray table (_rays, Rays.cuh:8-57)."""
+
+    def __init__(self, total_rays: int, white_bg: bool = True):
+        h = _vp()
+        _check(_lib.cpx_rays_create(int(total_rays), 1 if white_bg else 0, C.byref(h)), "cpx_rays_create")
+        self._h = h
+        self.total_rays = int(total_rays)
+        self.white_bg = bool(white_bg)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cpx_rays_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, offset: int = 0, stream=None, **fields):
+        count = None
+        keep = []
+        ptrs = []
+        for name in RAY_INPUTS:
+            if name in fields and fields[name] is not None:
+                dt = np.float32 if name in _FLOAT_FIELDS else np.uint8
+                a = np.ascontiguousarray(fields[name], dtype=dt).reshape(-1)
+                count = a.size if count is None else count
+                if a.size != count:
+                    raise ValueError("ray fields differ in length")
+                keep.append(a)
+                ptrs.append(a.ctypes.data)
+            else:
+                ptrs.append(None)
+        if count is None:
+            return
+        _check(_lib.cpx_rays_upload(self._h, int(offset), count, *ptrs, _stream(stream)), "cpx_rays_upload")
+
+    def upload_packed(self, packed, offset: int = 0, stream=None):
+        """packed: uint32 [count, 9] host array (pinned torch tensor or numpy)."""
+        if hasattr(packed, "data_ptr"):
+            count = packed.shape[0]
+            ptr = packed.data_ptr()
+        else:
+            packed = np.ascontiguousarray(packed, dtype=np.uint32)
+            count = packed.shape[0]
+            ptr = packed.ctypes.data
+        _check(_lib.cpx_rays_upload_packed(self._h, int(offset), int(count), ptr, _stream(stream)),
+               "cpx_rays_upload_packed")
+
+    def download(self, offset: int = 0, count: int | None = None, fields=None):
+        if count is None:
+            count = self.total_rays - offset
+        names = list(RAY_INPUTS) + list(RAY_OUTPUTS)
+        fields = names if fields is None else list(fields)
+        out = {}
+        ptrs = []
+        for name in names:
+            if name in fields:
+                a = np.empty(count, np.float32 if name in _FLOAT_FIELDS else np.uint8)
+                out[name] = a
+                ptrs.append(a.ctypes.data)
+            else:
+                ptrs.append(None)
+        _check(_lib.cpx_rays_download(self._h, int(offset), int(count), *ptrs), "cpx_rays_download")
+        return out
+
+    def initial_self(self, scene: ObjectScene, cameras, images, pixel_lists, img_w: int, img_h: int):
+        """_rays::initialSelf (Rays.cu:187-240): cameras[i] with images[i] = (r, g, b, mask)
+        planes of img_h*img_w bytes and pixel_lists[i] (row*img_w + col); rays of camera i
+        follow those of camera i-1."""
+        off = 0
+        for cam, img, pix in zip(cameras, images, pixel_lists):
+            r, g, b, m = (None if p is None else np.ascontiguousarray(p, np.uint8).reshape(-1) for p in img)
+            pix = np.ascontiguousarray(pix, np.int32).reshape(-1)
+            _check(_lib.cpx_rays_init_camera(self._h, scene.handle, C.byref(cam), int(img_w), int(img_h),
+                                             r, g, b, None if m is None else m.ctypes.data, pix,
+                                             pix.size, off), "cpx_rays_init_camera")
+            off += pix.size
+        return off
+
+
+def _len(rays: Rays, start: int, length):
+    return rays.total_rays - start if length is None else int(length)
+
+
+class RenderUtils:
+    """Per-batch march entry points (RenderUtils.cuh:7-85)."""
+
+    @staticmethod
+    def renderRays(rays: Rays, scene: ObjectScene, sampleIndex=None, startSampleIndex: int = 0,
+                   len: int | None = None, stream=None):
+        n = _len(rays, startSampleIndex, len)
+        _check(_lib.cpx_render_forward(scene.handle, rays.handle, _ptr(sampleIndex),
+                                       int(startSampleIndex), n, _stream(stream)), "renderRays")
+
+    @staticmethod
+    def renderRays_withGradients_RGB(scene: ObjectScene, rays: Rays, losses, sampleIndex=None,
+                                     startSampleIndex: int = 0, len: int | None = None,
+                                     maskRayLossCoefficient: float = 5.e-5, huberDelta: float = 0.01,
+                                     stream=None):
+        n = _len(rays, startSampleIndex, len)
+        _check(_lib.cpx_render_backward(scene.handle, rays.handle, _ptr(losses), _ptr(sampleIndex),
+                                        int(startSampleIndex), n, float(maskRayLossCoefficient),
+                                        float(huberDelta), _stream(stream)),
+               "renderRays_withGradients_RGB")
+
+    @staticmethod
+    def renderRays_forwardBackward(scene: ObjectScene, rays: Rays, losses, sampleIndex=None,
+                                   startSampleIndex: int = 0, len: int | None = None,
+                                   maskRayLossCoefficient: float = 5.e-5, huberDelta: float = 0.01,
+                                   stream=None):
+        n = _len(rays, startSampleIndex, len)
+        _check(_lib.cpx_render_forward_backward(scene.handle, rays.handle, _ptr(losses), _ptr(sampleIndex),
+                                                int(startSampleIndex), n, float(maskRayLossCoefficient),
+                                                float(huberDelta), _stream(stream)),
+               "renderRays_forwardBackward")
+
+    @staticmethod
+    def addVarianceLoss(scene: ObjectScene, varianceCoefficient: float = 0.001,
+                        shCoefficient: float = 0.001, varianceType: int = 0,
+                        neighboorNums: int = 6, stream=None):
+        _check(_lib.cpx_tv_grad(scene.handle, float(varianceCoefficient), float(shCoefficient),
+                                int(varianceType), int(neighboorNums), _stream(stream)), "addVarianceLoss")
+
+
+class Optimizer:
+    """Adam step (Optimizer::updateRGBScene, Optimizer.cu:451-479)."""
+
+    @staticmethod
+    def updateRGBScene(scene: ObjectScene, learningRate: float, shLearningRate: float, timeStep: int,
+                       stream=None):
+        _check(_lib.cpx_adam_step(scene.handle, float(learningRate), float(shLearningRate), int(timeStep),
+                                  _stream(stream)), "updateRGBScene")
+
+    @staticmethod
+    def varianceAndUpdate(scene: ObjectScene, varianceCoefficient: float, shCoefficient: float,
+                          learningRate: float, shLearningRate: float, timeStep: int, stream=None):
+        """TV type 0 / 6 neighbours fused with the Adam sweep."""
+        _check(_lib.cpx_tv_adam_step(scene.handle, float(varianceCoefficient), float(shCoefficient),
+                                     float(learningRate), float(shLearningRate), int(timeStep),
+                                     _stream(stream)), "varianceAndUpdate")
+
+
+def train_step(scene: ObjectScene, rays: Rays, losses, *, start: int = 0, length: int | None = None,
+               sample_index=None, mask_coef: float = 1.0, huber_delta: float = 0.1, do_tv: bool = True,
+               tv_type: int = 0, tv_neighbours: int = 6, lam_density: float = 1e-5,
+               lam_sh: float = 1e-6, lr: float = 0.3, sh_lr: float = 1.0, timestep: int = 1,
+               want_mse: bool = True, stream=None):
+    """One batch of the reference's training loop (Render.cu:407-500); returns the batch MSE."""
+    a = StepArgs()
+    a.mask_coef = float(mask_coef)
+    a.huber_delta = float(huber_delta)
+    a.do_tv = 1 if do_tv else 0
+    a.tv_type = int(tv_type)
+    a.tv_neighbours = int(tv_neighbours)
+    a.lam_density = float(lam_density)
+    a.lam_sh = float(lam_sh)
+    a.lr = float(lr)
+    a.sh_lr = float(sh_lr)
+    a.timestep = int(timestep)
+    n = _len(rays, start, length)
+    mse = C.c_double(0.0)
+    _check(_lib.cpx_train_step(scene.handle, rays.handle, _ptr(sample_index), int(start), n, C.byref(a),
+                               _ptr(losses), C.byref(mse) if want_mse else None, _stream(stream)),
+           "train_step")
+    return mse.value if want_mse else None
+
+
+def lr_decay(lr: float, batch_count: int, epoch: int) -> float:
+    """Per-batch learning-rate decay of the reference (Render.cu:499-500)."""
+    return lr / (2.0 ** (1.0 / batch_count / (epoch + 1.0)))
+
+
+def psnr_from_mse(mse: float) -> float:
+    """PSNR on the 255^2 scale of the per-ray loss (Render.cu:465)."""
+    return 10.0 * np.log10(65025.0 / mse)

@@ -1,0 +1,679 @@
+// api.cu -- the extern "C" entry points of libcpx (see include/cpx.h).
+//
+// Host-side logic only: argument checks, handle lifecycle, conversion between
+// the reference's planar host layout and the record layout on the device, and
+// the order of launches of one training batch (SVRF/Render.cu:407-500).
+#include "cpx_internal.cuh"
+
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <new>
+
+namespace cpx {
+
+static thread_local char g_last_error[512] = "";
+static std::atomic<long long> g_launches{0};
+
+void set_error(const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+}
+
+cpx_status cuda_status(cudaError_t e, const char* where)
+{
+    if (e == cudaSuccess) return CPX_OK;
+    set_error("%s: %s", where, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? CPX_ERR_OUT_OF_MEMORY : CPX_ERR_CUDA;
+}
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Column e of a record array <-> a packed float array.
+__global__ void k_set_column(float* aos, const float* col, int64_t n, int rec, int e,
+                             float* density_out)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = col[i];
+    aos[i * rec + e] = v;
+    if (density_out) density_out[i] = v;
+}
+
+__global__ void k_get_column(float* col, const float* aos, int64_t n, int rec, int e)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    col[i] = aos[i * rec + e];
+}
+
+__global__ void k_fill(float* p, int64_t n, float v)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// Packed ray records (9 words: 8 floats + rgba bytes) into the SoA ray table.
+__global__ void k_unpack_rays(const uint32_t* __restrict__ src, int64_t count, int64_t offset,
+                              RaysView rv)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint32_t* w = src + i * 9;
+    const int64_t ri = offset + i;
+    const_cast<float*>(rv.ox)[ri] = __uint_as_float(w[0]);
+    const_cast<float*>(rv.oy)[ri] = __uint_as_float(w[1]);
+    const_cast<float*>(rv.oz)[ri] = __uint_as_float(w[2]);
+    const_cast<float*>(rv.dx)[ri] = __uint_as_float(w[3]);
+    const_cast<float*>(rv.dy)[ri] = __uint_as_float(w[4]);
+    const_cast<float*>(rv.dz)[ri] = __uint_as_float(w[5]);
+    const_cast<float*>(rv.near_t)[ri] = __uint_as_float(w[6]);
+    const_cast<float*>(rv.far_t)[ri] = __uint_as_float(w[7]);
+    const uint32_t gt = w[8];
+    const_cast<uint8_t*>(rv.r)[ri] = (uint8_t)(gt & 0xff);
+    const_cast<uint8_t*>(rv.g)[ri] = (uint8_t)((gt >> 8) & 0xff);
+    const_cast<uint8_t*>(rv.b)[ri] = (uint8_t)((gt >> 16) & 0xff);
+    const_cast<uint8_t*>(rv.mask)[ri] = (uint8_t)(gt >> 24);
+}
+
+static unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+// Host planar [n_arrays][n] <-> device records, one array at a time through a staging column.
+static cpx_status planar_to_records(float* aos, const float* planar, int64_t n, int n_arrays,
+                                    int rec, float* density_out)
+{
+    if (n == 0) return CPX_OK;
+    float* col = nullptr;
+    cudaError_t e = cudaMalloc((void**)&col, n * sizeof(float));
+    if (e != cudaSuccess) return cuda_status(e, "upload staging");
+    for (int a = 0; a < n_arrays && e == cudaSuccess; a++) {
+        e = cudaMemcpy(col, planar + (int64_t)a * n, n * sizeof(float), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) break;
+        k_set_column<<<blocks_for(n), 256>>>(aos, col, n, rec, a, a == 0 ? density_out : nullptr);
+        count_launch();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(col);
+    return cuda_status(e, "upload");
+}
+
+static cpx_status records_to_planar(float* planar, const float* aos, int64_t n, int n_arrays,
+                                    int rec)
+{
+    if (n == 0) return CPX_OK;
+    float* col = nullptr;
+    cudaError_t e = cudaMalloc((void**)&col, n * sizeof(float));
+    if (e != cudaSuccess) return cuda_status(e, "download staging");
+    for (int a = 0; a < n_arrays && e == cudaSuccess; a++) {
+        k_get_column<<<blocks_for(n), 256>>>(col, aos, n, rec, a);
+        count_launch();
+        e = cudaMemcpy(planar + (int64_t)a * n, col, n * sizeof(float), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(col);
+    return cuda_status(e, "download");
+}
+
+static cpx_status check_grid(const cpx_grid* g)
+{
+    if (!g) {
+        set_error("null grid handle");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    return CPX_OK;
+}
+
+static cpx_status check_n(const cpx_grid* g, int64_t n)
+{
+    if (n != g->n_act) {
+        set_error("array length %lld does not match the grid's %lld active vertices", (long long)n,
+                  (long long)g->n_act);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    return CPX_OK;
+}
+
+static void free_grid(cpx_grid* g)
+{
+    cudaFree(g->params[0]);
+    cudaFree(g->params[1]);
+    cudaFree(g->grad);
+    cudaFree(g->m);
+    cudaFree(g->v);
+    cudaFree(g->density);
+    cudaFree(g->adaptive_lr);
+    cudaFree(g->occ_bytes);
+    cudaFree(g->occ_bits);
+    cudaFree(g->in_cage);
+    cudaFree(g->index_offsets);
+    cudaFree(g->compact_to_dense);
+    for (int i = 0; i < 3; i++) cudaFree(g->off[i]);
+    cudaFree(g->scratch.samples);
+    cudaFree(g->scratch.colours);
+    cudaFree(g->scratch.counts);
+    cudaFree(g->scratch.acc);
+    cudaFree(g->scratch.err);
+    cudaFree(g->scratch.mse);
+}
+
+}  // namespace cpx
+
+using namespace cpx;
+
+extern "C" {
+
+const char* cpx_status_string(cpx_status s)
+{
+    switch (s) {
+    case CPX_OK: return "ok";
+    case CPX_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case CPX_ERR_OUT_OF_MEMORY: return "out of memory";
+    case CPX_ERR_CUDA: return "CUDA error";
+    case CPX_ERR_ITERATION_CAP: return "march exceeded its sample bound";
+    case CPX_ERR_NAN: return "NaN detected";
+    case CPX_ERR_NOT_READY: return "not ready";
+    case CPX_ERR_UNSUPPORTED: return "unsupported";
+    }
+    return "unknown status";
+}
+
+const char* cpx_last_error(void) { return g_last_error; }
+int cpx_version(void) { return 100; }
+int64_t cpx_kernel_launches(void) { return g_launches.load(); }
+
+cpx_status cpx_grid_create(const cpx_grid_desc* d, cpx_grid** out)
+{
+    if (!d || !out) {
+        set_error("null argument");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    if (d->width < 2 || d->height < 2 || d->depth < 2) {
+        set_error("grid needs at least 2 vertices per axis");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    const int64_t n = (int64_t)d->width * d->height * d->depth;
+    if (n >= (int64_t)1 << 31) {
+        set_error("grid of %lld vertices exceeds the 32-bit index space", (long long)n);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (d->width > 65535 || d->height > 65535 || d->depth > 65535) {
+        set_error("axis longer than 65535 vertices");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (d->sh_dim != 1 && d->sh_dim != 4 && d->sh_dim != 9) {
+        set_error("sh_dim must be 1, 4 or 9 (got %d)", d->sh_dim);
+        return CPX_ERR_UNSUPPORTED;
+    }
+    if (d->optimizing_band < 0 || (d->optimizing_band + 1) * (d->optimizing_band + 1) > d->sh_dim) {
+        set_error("optimizing_band %d needs more than %d coefficients", d->optimizing_band, d->sh_dim);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (!(d->step_size > 0.f) || !std::isfinite(d->step_size)) {
+        set_error("step_size must be positive and finite");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    cpx_grid* g = new (std::nothrow) cpx_grid();
+    if (!g) return CPX_ERR_OUT_OF_MEMORY;
+    g->W = d->width;
+    g->H = d->height;
+    g->D = d->depth;
+    g->sh_dim = d->sh_dim;
+    g->band = d->optimizing_band;
+    g->hierarchy = d->hierarchy_strategy ? 1 : 0;
+    g->optimize_step = 0;
+    g->n_arrays = 1 + 3 * d->sh_dim;
+    g->rec = (g->n_arrays + 3) & ~3;
+    g->step = d->step_size;
+    for (int i = 0; i < 6; i++) g->bbox[i] = d->bbox[i];
+    g->n_dense = n;
+    g->n_act = n;
+    const size_t rb = (size_t)n * g->rec * sizeof(float);
+    cudaError_t e = cudaSuccess;
+    float** bufs[5] = {&g->params[0], &g->params[1], &g->grad, &g->m, &g->v};
+    for (auto b : bufs) {
+        if (e == cudaSuccess) e = cudaMalloc((void**)b, rb);
+        if (e == cudaSuccess) e = cudaMemset(*b, 0, rb);
+    }
+    if (e == cudaSuccess) e = cudaMalloc((void**)&g->density, n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(g->density, 0, n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&g->adaptive_lr, n * sizeof(float));
+    if (e == cudaSuccess) {
+        k_fill<<<blocks_for(n), 256>>>(g->adaptive_lr, n, 1.f);
+        count_launch();
+        e = cudaDeviceSynchronize();
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        free_grid(g);
+        delete g;
+        set_error("grid of %lld vertices could not be allocated: %s", (long long)n,
+                  cudaGetErrorString(e));
+        return CPX_ERR_OUT_OF_MEMORY;
+    }
+    *out = g;
+    return CPX_OK;
+}
+
+cpx_status cpx_grid_destroy(cpx_grid* g)
+{
+    if (!g) return CPX_OK;
+    cudaDeviceSynchronize();
+    free_grid(g);
+    delete g;
+    return CPX_OK;
+}
+
+cpx_status cpx_grid_info(const cpx_grid* g, int64_t* n_active, int* n_arrays, int* sparse)
+{
+    if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
+    if (n_active) *n_active = g->n_act;
+    if (n_arrays) *n_arrays = g->n_arrays;
+    if (sparse) *sparse = g->sparse;
+    return CPX_OK;
+}
+
+cpx_status cpx_grid_upload_params(cpx_grid* g, const float* planar, int64_t n)
+{
+    if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
+    return planar_to_records(g->params[g->cur], planar, n, g->n_arrays, g->rec, g->density);
+}
+
+cpx_status cpx_grid_download_params(const cpx_grid* g, float* planar, int64_t n)
+{
+    if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
+    cudaDeviceSynchronize();
+    return records_to_planar(planar, g->params[g->cur], n, g->n_arrays, g->rec);
+}
+
+cpx_status cpx_grid_upload_grads(cpx_grid* g, const float* planar, int64_t n)
+{
+    if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
+    return planar_to_records(g->grad, planar, n, g->n_arrays, g->rec, nullptr);
+}
+
+cpx_status cpx_grid_download_grads(const cpx_grid* g, float* planar, int64_t n)
+{
+    if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
+    cudaDeviceSynchronize();
+    return records_to_planar(planar, g->grad, n, g->n_arrays, g->rec);
+}
+
+cpx_status cpx_grid_upload_moments(cpx_grid* g, const float* m, const float* v, int64_t n)
+{
+    if (check_grid(g) || !m || !v) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
+    cpx_status s = planar_to_records(g->m, m, n, g->n_arrays, g->rec, nullptr);
+    if (s != CPX_OK) return s;
+    return planar_to_records(g->v, v, n, g->n_arrays, g->rec, nullptr);
+}
+
+cpx_status cpx_grid_download_moments(const cpx_grid* g, float* m, float* v, int64_t n)
+{
+    if (check_grid(g) || !m || !v) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
+    cudaDeviceSynchronize();
+    cpx_status s = records_to_planar(m, g->m, n, g->n_arrays, g->rec);
+    if (s != CPX_OK) return s;
+    return records_to_planar(v, g->v, n, g->n_arrays, g->rec);
+}
+
+cpx_status cpx_grid_set_adaptive_lr(cpx_grid* g, const float* lr_mult, int64_t n_dense)
+{
+    if (check_grid(g) || !lr_mult) return CPX_ERR_INVALID_ARGUMENT;
+    if (n_dense != g->n_dense) {
+        set_error("adaptive LR needs %lld entries", (long long)g->n_dense);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    return cuda_status(cudaMemcpy(g->adaptive_lr, lr_mult, n_dense * sizeof(float),
+                                  cudaMemcpyHostToDevice),
+                       "adaptive lr");
+}
+
+cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const double* oy,
+                                       const double* oz, int n)
+{
+    if (check_grid(g) || n < 0 || (n > 0 && (!ox || !oy || !oz))) return CPX_ERR_INVALID_ARGUMENT;
+    cudaDeviceSynchronize();
+    for (int i = 0; i < 3; i++) {
+        cudaFree(g->off[i]);
+        g->off[i] = nullptr;
+    }
+    g->n_off = 0;
+    if (n == 0) return CPX_OK;
+    const double* src[3] = {ox, oy, oz};
+    for (int i = 0; i < 3; i++) {
+        cudaError_t e = cudaMalloc((void**)&g->off[i], n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpy(g->off[i], src[i], n * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_status(e, "sample offsets");
+    }
+    g->n_off = n;
+    return CPX_OK;
+}
+
+cpx_status cpx_grid_set_optimize_step(cpx_grid* g, int optimize_step)
+{
+    if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
+    g->optimize_step = optimize_step;
+    return CPX_OK;
+}
+
+cpx_status cpx_occupancy_build(cpx_grid* g, float threshold, uint8_t* occupancy_out,
+                               uint8_t* in_cage_out, uint32_t* index_offsets_out,
+                               uint32_t* in_cage_count_out)
+{
+    if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
+    if (g->sparse) {
+        set_error("occupancy is built from a dense grid");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    cudaDeviceSynchronize();
+    cpx_status s = occupancy_launch(g, threshold);
+    if (s != CPX_OK) return s;
+    const int64_t C = (int64_t)(g->W - 1) * (g->H - 1) * (g->D - 1);
+    cudaError_t e = cudaSuccess;
+    if (occupancy_out) e = cudaMemcpy(occupancy_out, g->occ_bytes, C, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && in_cage_out)
+        e = cudaMemcpy(in_cage_out, g->in_cage, g->n_dense, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && index_offsets_out)
+        e = cudaMemcpy(index_offsets_out, g->index_offsets, g->n_dense * sizeof(uint32_t),
+                       cudaMemcpyDeviceToHost);
+    if (in_cage_count_out) *in_cage_count_out = g->in_cage_count;
+    return cuda_status(e, "occupancy download");
+}
+
+cpx_status cpx_grid_make_sparse(cpx_grid* g)
+{
+    if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
+    return make_sparse_launch(g);
+}
+
+cpx_status cpx_rays_create(int64_t n, int white_bg, cpx_rays** out)
+{
+    if (!out || n < 0) {
+        set_error("invalid ray count");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    cpx_rays* r = new (std::nothrow) cpx_rays();
+    if (!r) return CPX_ERR_OUT_OF_MEMORY;
+    r->n = n;
+    r->white_bg = white_bg ? 1 : 0;
+    const int64_t nn = n > 0 ? n : 1;
+    const size_t fbytes = (size_t)nn * sizeof(float);
+    const size_t total = 13 * fbytes + 4 * (size_t)nn + 64;
+    char* base = nullptr;
+    cudaError_t e = cudaMalloc((void**)&base, total);
+    if (e != cudaSuccess) {
+        delete r;
+        return cuda_status(e, "rays allocation");
+    }
+    cudaMemset(base, 0, total);
+    r->block = base;
+    float* f = reinterpret_cast<float*>(base);
+    float** fields[13] = {&r->ox, &r->oy, &r->oz, &r->dx, &r->dy, &r->dz, &r->near_t, &r->far_t,
+                          &r->acc_den, &r->acc_w, &r->acc_r, &r->acc_g, &r->acc_b};
+    for (int i = 0; i < 13; i++) *fields[i] = f + (size_t)i * nn;
+    uint8_t* u = reinterpret_cast<uint8_t*>(base + 13 * fbytes);
+    r->mask = u;
+    r->r = u + nn;
+    r->g = u + 2 * nn;
+    r->b = u + 3 * nn;
+    *out = r;
+    return CPX_OK;
+}
+
+cpx_status cpx_rays_destroy(cpx_rays* r)
+{
+    if (!r) return CPX_OK;
+    cudaDeviceSynchronize();
+    cudaFree(r->block);
+    cudaFree(r->staging);
+    delete r;
+    return CPX_OK;
+}
+
+static bool range_ok(const cpx_rays* r, int64_t offset, int64_t count)
+{
+    if (!r || offset < 0 || count < 0 || offset + count > r->n) {
+        set_error("ray range [%lld, %lld) outside the table", (long long)offset,
+                  (long long)(offset + count));
+        return false;
+    }
+    return true;
+}
+
+cpx_status cpx_rays_upload(cpx_rays* r, int64_t offset, int64_t count, const float* ox,
+                           const float* oy, const float* oz, const float* dx, const float* dy,
+                           const float* dz, const float* near_t, const float* far_t,
+                           const uint8_t* gt_mask, const uint8_t* gt_r, const uint8_t* gt_g,
+                           const uint8_t* gt_b, cpx_stream stream)
+{
+    if (!range_ok(r, offset, count)) return CPX_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    const float* fs[8] = {ox, oy, oz, dx, dy, dz, near_t, far_t};
+    float* fd[8] = {r->ox, r->oy, r->oz, r->dx, r->dy, r->dz, r->near_t, r->far_t};
+    const uint8_t* bs[4] = {gt_mask, gt_r, gt_g, gt_b};
+    uint8_t* bd[4] = {r->mask, r->r, r->g, r->b};
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 8 && e == cudaSuccess; i++)
+        if (fs[i]) e = cudaMemcpyAsync(fd[i] + offset, fs[i], count * sizeof(float), cudaMemcpyHostToDevice, st);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++)
+        if (bs[i]) e = cudaMemcpyAsync(bd[i] + offset, bs[i], count, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return cuda_status(e, "rays upload");
+}
+
+cpx_status cpx_rays_upload_packed(cpx_rays* r, int64_t offset, int64_t count,
+                                  const uint32_t* packed, cpx_stream stream)
+{
+    if (!range_ok(r, offset, count) || (!packed && count > 0)) return CPX_ERR_INVALID_ARGUMENT;
+    if (count == 0) return CPX_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (r->staging_cap < count) {
+        cudaStreamSynchronize(st);
+        cudaFree(r->staging);
+        r->staging = nullptr;
+        r->staging_cap = 0;
+        cudaError_t e = cudaMalloc((void**)&r->staging, (size_t)count * 9 * sizeof(uint32_t));
+        if (e != cudaSuccess) return cuda_status(e, "ray staging");
+        r->staging_cap = count;
+    }
+    cudaError_t e = cudaMemcpyAsync(r->staging, packed, (size_t)count * 9 * sizeof(uint32_t),
+                                    cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e, "packed upload");
+    k_unpack_rays<<<blocks_for(count), 256, 0, st>>>(r->staging, count, offset, rays_view(r));
+    count_launch();
+    return cuda_status(cudaGetLastError(), "packed upload");
+}
+
+cpx_status cpx_rays_download(const cpx_rays* r, int64_t offset, int64_t count, float* ox,
+                             float* oy, float* oz, float* dx, float* dy, float* dz,
+                             float* near_t, float* far_t, uint8_t* gt_mask, uint8_t* gt_r,
+                             uint8_t* gt_g, uint8_t* gt_b, float* acc_density,
+                             float* acc_weights, float* acc_r, float* acc_g, float* acc_b)
+{
+    if (!range_ok(r, offset, count)) return CPX_ERR_INVALID_ARGUMENT;
+    cudaDeviceSynchronize();
+    float* fd[13] = {ox, oy, oz, dx, dy, dz, near_t, far_t, acc_density, acc_weights, acc_r, acc_g, acc_b};
+    const float* fs[13] = {r->ox, r->oy, r->oz, r->dx, r->dy, r->dz, r->near_t, r->far_t,
+                           r->acc_den, r->acc_w, r->acc_r, r->acc_g, r->acc_b};
+    uint8_t* bd[4] = {gt_mask, gt_r, gt_g, gt_b};
+    const uint8_t* bs[4] = {r->mask, r->r, r->g, r->b};
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 13 && e == cudaSuccess; i++)
+        if (fd[i]) e = cudaMemcpy(fd[i], fs[i] + offset, count * sizeof(float), cudaMemcpyDeviceToHost);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++)
+        if (bd[i]) e = cudaMemcpy(bd[i], bs[i] + offset, count, cudaMemcpyDeviceToHost);
+    return cuda_status(e, "rays download");
+}
+
+cpx_status cpx_rays_init_camera(cpx_rays* r, const cpx_grid* g, const cpx_camera* cam,
+                                int img_w, int img_h, const uint8_t* red, const uint8_t* green,
+                                const uint8_t* blue, const uint8_t* gt_mask,
+                                const int32_t* pixel_index, int64_t n_pix, int64_t offset)
+{
+    if (check_grid(g) || !cam || !red || !green || !blue || (!pixel_index && n_pix > 0) ||
+        img_w <= 0 || img_h <= 0)
+        return CPX_ERR_INVALID_ARGUMENT;
+    if (!range_ok(r, offset, n_pix)) return CPX_ERR_INVALID_ARGUMENT;
+    const int64_t plane = (int64_t)img_w * img_h;
+    for (int64_t i = 0; i < n_pix; i++) {
+        if (pixel_index[i] < 0 || pixel_index[i] >= plane) {
+            set_error("pixel index %d outside the %dx%d image", pixel_index[i], img_w, img_h);
+            return CPX_ERR_INVALID_ARGUMENT;
+        }
+    }
+    if (n_pix == 0) return CPX_OK;
+    uint8_t* planes = nullptr;
+    int32_t* pix = nullptr;
+    cudaError_t e = cudaMalloc((void**)&planes, 4 * plane);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&pix, n_pix * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemcpy(planes, red, plane, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(planes + plane, green, plane, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(planes + 2 * plane, blue, plane, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && gt_mask) e = cudaMemcpy(planes + 3 * plane, gt_mask, plane, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(pix, pixel_index, n_pix * sizeof(int32_t), cudaMemcpyHostToDevice);
+    cpx_status s = cuda_status(e, "camera upload");
+    if (s == CPX_OK)
+        s = rays_camera_launch(r, g, cam, img_w, plane, planes, pix, n_pix, offset, gt_mask != nullptr,
+                               nullptr);
+    if (s == CPX_OK) s = cuda_status(cudaDeviceSynchronize(), "rays");
+    cudaFree(planes);
+    cudaFree(pix);
+    return s;
+}
+
+cpx_status cpx_render_forward(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                              cpx_stream stream)
+{
+    if (check_grid(g) || !r) return CPX_ERR_INVALID_ARGUMENT;
+    return march_launch(g, r, sidx, start, len, kForward, nullptr, 0., 0.f, (cudaStream_t)stream);
+}
+
+cpx_status cpx_render_backward(cpx_grid* g, cpx_rays* r, double* losses, const int32_t* sidx,
+                               int start, int len, double mask_coef, float huber,
+                               cpx_stream stream)
+{
+    if (check_grid(g) || !r) return CPX_ERR_INVALID_ARGUMENT;
+    return march_launch(g, r, sidx, start, len, kBackward, losses, mask_coef, huber,
+                        (cudaStream_t)stream);
+}
+
+cpx_status cpx_render_forward_backward(cpx_grid* g, cpx_rays* r, double* losses,
+                                       const int32_t* sidx, int start, int len,
+                                       double mask_coef, float huber, cpx_stream stream)
+{
+    if (check_grid(g) || !r) return CPX_ERR_INVALID_ARGUMENT;
+    return march_launch(g, r, sidx, start, len, kForwardBackward, losses, mask_coef, huber,
+                        (cudaStream_t)stream);
+}
+
+cpx_status cpx_tv_grad(cpx_grid* g, double lam_d, double lam_sh, int type, int nbrs,
+                       cpx_stream stream)
+{
+    if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
+    return tv_launch(g, lam_d, lam_sh, type, nbrs, (cudaStream_t)stream);
+}
+
+cpx_status cpx_adam_step(cpx_grid* g, double lr, double sh_lr, int timestep, cpx_stream stream)
+{
+    if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
+    if (timestep < 1) {
+        set_error("timestep starts at 1");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    return sweep_adam(g, false, 0., 0., lr, sh_lr, timestep, (cudaStream_t)stream);
+}
+
+cpx_status cpx_tv_adam_step(cpx_grid* g, double lam_d, double lam_sh, double lr, double sh_lr,
+                            int timestep, cpx_stream stream)
+{
+    if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
+    if (timestep < 1) {
+        set_error("timestep starts at 1");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (g->sparse && !g->have_occupancy) {
+        set_error("sparse grid without occupancy");
+        return CPX_ERR_NOT_READY;
+    }
+    return sweep_adam(g, true, lam_d, lam_sh, lr, sh_lr, timestep, (cudaStream_t)stream);
+}
+
+cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                          const cpx_step_args* a, double* losses, double* mse_out,
+                          cpx_stream stream)
+{
+    if (check_grid(g) || !r || !a) return CPX_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    cpx_status s = march_launch(g, r, sidx, start, len, kForwardBackward, losses, a->mask_coef,
+                                a->huber_delta, st);
+    if (s != CPX_OK) return s;
+    const bool fuse = a->do_tv && a->tv_type == 0 && a->tv_neighbours == 6;
+    if (a->do_tv && !fuse) {
+        s = tv_launch(g, a->lam_density, a->lam_sh, a->tv_type, a->tv_neighbours, st);
+        if (s != CPX_OK) return s;
+    }
+    if (a->timestep < 1) {
+        set_error("timestep starts at 1");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    s = sweep_adam(g, fuse, a->lam_density, a->lam_sh, a->lr, a->sh_lr, a->timestep, st);
+    if (s != CPX_OK) return s;
+    if (mse_out) {
+        s = mse_launch(losses, len, g->scratch.mse, st);
+        if (s != CPX_OK) return s;
+        cudaError_t e = cudaMemcpyAsync(mse_out, g->scratch.mse, sizeof(double),
+                                        cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_status(e, "mse");
+    }
+    return CPX_OK;
+}
+
+cpx_status cpx_grid_check(cpx_grid* g)
+{
+    if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_status(e, "check");
+    if (!g->scratch.err) return CPX_OK;
+    int flags[4] = {0, 0, 0, 0};
+    e = cudaMemcpy(flags, g->scratch.err, sizeof(flags), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "check");
+    cudaMemset(g->scratch.err, 0, sizeof(flags));
+    if (flags[0] & 2) {
+        set_error("a sample index pointed outside the ray table");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (flags[0] & 1) {
+        set_error("a ray's march exceeded its sample bound (near/far beyond the grid box?)");
+        return CPX_ERR_ITERATION_CAP;
+    }
+    return CPX_OK;
+}
+
+cpx_status cpx_last_sample_counts(const cpx_grid* g, int32_t* counts_host, int len)
+{
+    if (check_grid(g) || !counts_host || len < 0 || len > g->last_len) {
+        set_error("counts of %d rays requested, last batch had %d", len, g ? g->last_len : 0);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (len == 0) return CPX_OK;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess)
+        e = cudaMemcpy(counts_host, g->scratch.counts, len * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    for (int i = 0; i < len; i++)
+        if (counts_host[i] < 0) counts_host[i] = 0;
+    return cuda_status(e, "counts");
+}
+
+}  // extern "C"

@@ -1,0 +1,206 @@
+// cpx_internal.cuh -- handles, device views and shared helpers of libcpx.
+//
+// Data layout in HBM (plain FP32 form):
+//   * parameters: array-of-records, one record of `rec` floats per active vertex
+//     ([density, R0..R(s-1), G0.., B0..], padded to a multiple of 4 floats: 28 floats
+//     = 112 B at SH band 2), so a trilinear corner is 7 aligned 16-byte loads and the
+//     optimizer sweep streams whole records.  Two parameter buffers alternate (the
+//     fused TV+Adam sweep reads one and writes the other, so TV sees pre-step values).
+//   * gradients, Adam first and second moments: same record layout.
+//   * density mirror: the density of every active vertex again as a packed float
+//     array, read by the sample-placement march (4 B per corner instead of a record).
+//   * sparse tables: occupancy as one bit per cell, index_offsets u32 per dense vertex
+//     (the reference's compact-index table), compact->dense u32 per active vertex.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/cpx.h"
+
+namespace cpx {
+
+constexpr int kMaxShDim = 9;  // SH coefficients per channel supported by the kernels (band <= 2)
+
+// Record of one evaluated sample, written by the placement march, read by the shading pass.
+struct __align__(16) SampleRec {
+    uint16_t bx, by, bz, pad;  // base vertex of the sample's cell (unsigned-truncated position)
+    float fx, fy, fz;          // fractional position in the cell (computed in double)
+    float raw;                 // interpolated raw density
+    float w;                   // compositing weight T_i (1 - exp(-sigma step))
+    float tn;                  // transmittance after the sample, exp(-sum sigma step)
+};
+static_assert(sizeof(SampleRec) == 32, "SampleRec must be 32 bytes");
+
+// Per-kernel view of a grid (passed by value).
+struct GridView {
+    int W, H, D;
+    int sh_dim, band, n_sh_fwd, hierarchy;
+    int n_arrays, rec;  // rec = floats per record (multiple of 4)
+    float step;
+    int sparse;
+    int64_t n_act;
+    const float* __restrict__ params;   // [n_act][rec]
+    const float* __restrict__ density;  // [n_act]
+    float* grad;                        // [n_act][rec]
+    const uint32_t* __restrict__ occ_bits;       // [(C + 31) / 32]
+    const uint32_t* __restrict__ index_offsets;  // [W*H*D]
+    const double* __restrict__ off_x;
+    const double* __restrict__ off_y;
+    const double* __restrict__ off_z;
+    int n_off;
+};
+
+struct RaysView {
+    const float* __restrict__ ox;
+    const float* __restrict__ oy;
+    const float* __restrict__ oz;
+    const float* __restrict__ dx;
+    const float* __restrict__ dy;
+    const float* __restrict__ dz;
+    const float* __restrict__ near_t;
+    const float* __restrict__ far_t;
+    const uint8_t* __restrict__ mask;
+    const uint8_t* __restrict__ r;
+    const uint8_t* __restrict__ g;
+    const uint8_t* __restrict__ b;
+    float* acc_den;
+    float* acc_w;
+    float* acc_r;
+    float* acc_g;
+    float* acc_b;
+    int white_bg;
+};
+
+// Scratch of the two-stage march (sized for `cap_rays` rays of `maxs` samples).
+struct MarchScratch {
+    int maxs = 0;
+    int cap_rays = 0;
+    SampleRec* samples = nullptr;  // [cap_rays][maxs]
+    float4* colours = nullptr;     // [cap_rays][maxs]: sigmoid colour of each sample
+    int* counts = nullptr;         // [cap_rays]
+    double* acc = nullptr;         // [cap_rays]: sum of weights (double, for the background)
+    int* err = nullptr;            // [4] device error flags
+    double* mse = nullptr;         // [1]
+};
+
+}  // namespace cpx
+
+struct cpx_grid {
+    int W, H, D;
+    int sh_dim, band, hierarchy, optimize_step;
+    int n_arrays, rec;
+    float step;
+    int bbox[6];
+    int64_t n_dense, n_act;
+    int sparse = 0;
+    float* params[2] = {nullptr, nullptr};
+    int cur = 0;
+    float* grad = nullptr;
+    float* m = nullptr;
+    float* v = nullptr;
+    float* density = nullptr;
+    float* adaptive_lr = nullptr;  // [n_dense]
+    // occupancy (built by cpx_occupancy_build)
+    int have_occupancy = 0;
+    uint32_t in_cage_count = 0;
+    uint8_t* occ_bytes = nullptr;       // [C]
+    uint32_t* occ_bits = nullptr;       // [(C+31)/32]
+    uint8_t* in_cage = nullptr;         // [n_dense]
+    uint32_t* index_offsets = nullptr;  // [n_dense]
+    uint32_t* compact_to_dense = nullptr;  // [n_act] when sparse
+    // jitter
+    double* off[3] = {nullptr, nullptr, nullptr};
+    int n_off = 0;
+    cpx::MarchScratch scratch;
+    int last_len = 0;
+};
+
+struct cpx_rays {
+    int64_t n;
+    int white_bg;
+    void* block = nullptr;
+    float *ox, *oy, *oz, *dx, *dy, *dz, *near_t, *far_t;
+    uint8_t *mask, *r, *g, *b;
+    float *acc_den, *acc_w, *acc_r, *acc_g, *acc_b;
+    uint32_t* staging = nullptr;  // device copy of the last packed upload
+    int64_t staging_cap = 0;
+};
+
+namespace cpx {
+
+void set_error(const char* fmt, ...);
+cpx_status cuda_status(cudaError_t e, const char* where);
+void count_launch(int n = 1);
+
+inline GridView grid_view(cpx_grid* g)
+{
+    GridView v;
+    v.W = g->W;
+    v.H = g->H;
+    v.D = g->D;
+    v.sh_dim = g->sh_dim;
+    v.band = g->band;
+    v.n_sh_fwd = (g->band + 1) * (g->band + 1);
+    v.hierarchy = g->hierarchy;
+    v.n_arrays = g->n_arrays;
+    v.rec = g->rec;
+    v.step = g->step;
+    v.sparse = g->sparse;
+    v.n_act = g->n_act;
+    v.params = g->params[g->cur];
+    v.density = g->density;
+    v.grad = g->grad;
+    v.occ_bits = g->occ_bits;
+    v.index_offsets = g->index_offsets;
+    v.off_x = g->off[0];
+    v.off_y = g->off[1];
+    v.off_z = g->off[2];
+    v.n_off = g->n_off;
+    return v;
+}
+
+inline RaysView rays_view(cpx_rays* r)
+{
+    RaysView v;
+    v.ox = r->ox;
+    v.oy = r->oy;
+    v.oz = r->oz;
+    v.dx = r->dx;
+    v.dy = r->dy;
+    v.dz = r->dz;
+    v.near_t = r->near_t;
+    v.far_t = r->far_t;
+    v.mask = r->mask;
+    v.r = r->r;
+    v.g = r->g;
+    v.b = r->b;
+    v.acc_den = r->acc_den;
+    v.acc_w = r->acc_w;
+    v.acc_r = r->acc_r;
+    v.acc_g = r->acc_g;
+    v.acc_b = r->acc_b;
+    v.white_bg = r->white_bg;
+    return v;
+}
+
+// Launch helpers implemented in the kernel files.
+cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                        int mode, double* losses, double mask_coef, float huber,
+                        cudaStream_t s);
+cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
+                      double sh_lr, int timestep, cudaStream_t s);
+cpx_status tv_launch(cpx_grid* g, double lam_d, double lam_sh, int type, int nbrs,
+                     cudaStream_t s);
+cpx_status occupancy_launch(cpx_grid* g, float threshold);
+cpx_status make_sparse_launch(cpx_grid* g);
+cpx_status rays_camera_launch(cpx_rays* r, const cpx_grid* g, const cpx_camera* cam,
+                              int img_w, int64_t plane_bytes, const uint8_t* planes_dev,
+                              const int32_t* pix_dev, int64_t n_pix, int64_t offset,
+                              int has_mask, cudaStream_t s);
+cpx_status mse_launch(const double* losses, int len, double* out, cudaStream_t s);
+
+enum MarchMode { kForward = 1, kBackward = 2, kForwardBackward = 3 };
+
+}  // namespace cpx

@@ -1,0 +1,590 @@
+// march.cu -- forward and backward volume march on sm_100a.
+//
+// The reference marches each ray in one thread and interleaves everything
+// (RenderUtils.cu:1582-1718 forward, 2051-2256 backward): at every sample it
+// gathers 8 corners x 28 parameters from 28 planar arrays and, backward, issues
+// 224 float atomics.  Sample placement is the only part that is inherently
+// sequential -- t advances by |step - w| and w depends on the transmittance --
+// and it needs only the density.  So the march is split:
+//
+//  1. place (thread per ray): replays the reference's placement recurrence with
+//     the same FP64/FP32 operations in the same order (t, transmittance and
+//     weights in double, the trilinear density rounded to float after every
+//     corner, softplus and exp in float), reading only the packed density
+//     mirror.  Sample positions, counts, weights and accumulated density are
+//     therefore the reference's bit for bit.  Each evaluated sample is stored
+//     as a 32-byte record.
+//  2. shade (warp per ray, lane per sample): gathers the SH records of the
+//     samples in parallel (7 aligned 16-byte loads per corner), evaluates the
+//     colour, reduces the forward colour over the warp, then runs the backward
+//     with warp prefix scans for the running colour/weight sums and scatters the
+//     gradients with 16-byte vector atomics (7 per corner instead of 28).
+//
+// Reference citations: file:line in SparseVolumeRadianceField/.
+#include "cpx_internal.cuh"
+
+namespace cpx {
+
+// getSceneIndex (RenderUtils.cu:3-13).
+__device__ __forceinline__ int scene_index(int col, int row, int depth, int W, int H, int D)
+{
+    col = col < 0 ? 0 : (col > W - 1 ? W - 1 : col);
+    row = row < 0 ? 0 : (row > H - 1 ? H - 1 : row);
+    depth = depth < 0 ? 0 : (depth > D - 1 ? D - 1 : depth);
+    return depth * W * H + row * W + col;
+}
+
+__device__ __forceinline__ bool cell_occupied(const GridView& g, unsigned b0, unsigned b1,
+                                              unsigned b2)
+{
+    const int ci = scene_index((int)b0, (int)b1, (int)b2, g.W - 1, g.H - 1, g.D - 1);
+    return (g.occ_bits[ci >> 5] >> (ci & 31)) & 1u;
+}
+
+__device__ __forceinline__ unsigned corner_vertex(const GridView& g, unsigned b0, unsigned b1,
+                                                  unsigned b2, int q)
+{
+    const int ox = (q >> 1) & 1;  // corner order 000,010,100,110,001,011,101,111 (x,y,z)
+    const int oy = q & 1;
+    const int oz = (q >> 2) & 1;
+    unsigned idx = (unsigned)scene_index((int)(b0 + ox), (int)(b1 + oy), (int)(b2 + oz), g.W,
+                                         g.H, g.D);
+    if (g.sparse) idx = g.index_offsets[idx];
+    return idx;
+}
+
+// ---------------------------------------------------------------------------
+// Stage 1: sample placement (exact).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int32_t* sidx,
+                                               int start, int len, int64_t n_rays,
+                                               SampleRec* samples, int maxs, int* counts,
+                                               double* acc_out, int* err)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= len) return;
+    const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
+    if (ri < 0 || ri >= n_rays) {
+        atomicOr(err, 2);
+        counts[b] = -2;  // invalid ray index: nothing is read or written for it
+        return;
+    }
+    // renderRaysGPU zeroes the outputs first (RenderUtils.cu:1927-1941)
+    r.acc_den[ri] = 0.f;
+    r.acc_w[ri] = 0.f;
+    const float near_t = r.near_t[ri];
+    const float far_t = r.far_t[ri];
+    if (near_t > far_t) {  // RenderUtils.cu:1943-1946: no samples, no background
+        counts[b] = -1;
+        acc_out[b] = 0.;
+        return;
+    }
+    const float ox = r.ox[ri], oy = r.oy[ri], oz = r.oz[ri];
+    const float dx = r.dx[ri], dy = r.dy[ri], dz = r.dz[ri];
+    const float step = g.step;
+    // Provable bound on loop trips: every step is >= step - w and the weights sum to <= 1.
+    // maxs bounds every ray inside the grid box; longer (or non-finite) rays stop there with
+    // the error flag set instead of marching on.
+    const double bound = floor(((double)far_t - (double)near_t + 2.0) / (double)step) + 4.0;
+    const int it_cap = bound < (double)(maxs + 16) ? (int)bound : maxs + 16;
+
+    SampleRec* out = samples + (size_t)b * maxs;
+    double t = near_t;
+    double Ti = 1.0;
+    double acc = 0.;
+    double accD = 0.;
+    float accDen = 0.f;
+    int intT = 0, n = 0, it = 0;
+    while (t < far_t) {
+        if (++it > it_cap || n >= maxs) {
+            atomicOr(err, 1);
+            break;
+        }
+        double ofx = 0., ofy = 0., ofz = 0.;
+        if (intT < g.n_off) {
+            ofx = g.off_x[intT];
+            ofy = g.off_y[intT];
+            ofz = g.off_z[intT];
+        }
+        // RenderUtils.cu:1676-1678
+        const double bc0 = ox + t * dx + ofx;
+        const double bc1 = oy + t * dy + ofy;
+        const double bc2 = oz + t * dz + ofz;
+        const unsigned b0 = (unsigned int)bc0;
+        const unsigned b1 = (unsigned int)bc1;
+        const unsigned b2 = (unsigned int)bc2;
+        if (g.sparse && !cell_occupied(g, b0, b1, b2)) {  // RenderUtils.cu:1681-1686
+            t += step;
+            ++intT;
+            continue;
+        }
+        const double x = bc0 - b0;
+        const double y = bc1 - b1;
+        const double z = bc2 - b2;
+        // trilerpRGB density term (RenderUtils.cu:855-990), corners in the reference's order
+        float tri0 = 0.f;
+        double c;
+        c = (1. - x) * (1. - y) * (1. - z);
+        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 0)];
+        c = (1. - x) * y * (1. - z);
+        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 1)];
+        c = x * (1. - y) * (1. - z);
+        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 2)];
+        c = x * y * (1. - z);
+        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 3)];
+        c = (1. - x) * (1. - y) * z;
+        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 4)];
+        c = (1. - x) * y * z;
+        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 5)];
+        c = x * (1. - y) * z;
+        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 6)];
+        c = x * y * z;
+        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 7)];
+        // density_activation (RenderUtils.cu:491) and the weight (RenderUtils.cu:1693-1704)
+        const float sigma = logf(1.f + expf(tri0 - 13.f));
+        const double w = Ti * (1. - expf(-sigma * step));
+        acc += w;
+        accDen += sigma;
+        accD += sigma * step;
+        const double Tn = exp(-accD);
+        SampleRec rec;
+        rec.bx = (uint16_t)(b0 < 65535u ? b0 : 65535u);
+        rec.by = (uint16_t)(b1 < 65535u ? b1 : 65535u);
+        rec.bz = (uint16_t)(b2 < 65535u ? b2 : 65535u);
+        rec.pad = 0;
+        rec.fx = (float)x;
+        rec.fy = (float)y;
+        rec.fz = (float)z;
+        rec.raw = tri0;
+        rec.w = (float)w;
+        rec.tn = (float)Tn;
+        out[n] = rec;
+        Ti = Tn;
+        t += fabs(step - w);
+        ++intT;
+        ++n;
+    }
+    r.acc_den[ri] = accDen;
+    r.acc_w[ri] = (float)acc;
+    acc_out[b] = acc;
+    counts[b] = n;
+}
+
+// ---------------------------------------------------------------------------
+// Stage 2: shading and gradients (warp per ray, lane per sample).
+// ---------------------------------------------------------------------------
+
+// The reference's unnormalised SH basis on the float direction (RenderUtils.cu:1646-1656).
+template <int NSH>
+__device__ __forceinline__ void sh_basis(float dx, float dy, float dz, float* shs)
+{
+    const float dir[3] = {dx, dy, dz};
+    shs[0] = 1.f;
+    if (NSH > 1) {
+        shs[1] = dir[1];
+        shs[2] = dir[2];
+        shs[3] = dir[0];
+    }
+    if (NSH > 4) {
+        shs[4] = dir[0] * dir[1];
+        shs[5] = dir[1] * dir[2];
+        shs[6] = (3.f * dir[2] * dir[2] - 1.f);
+        shs[7] = dir[0] * dir[2];
+        shs[8] = (dir[0] * dir[0] - dir[1] * dir[1]);
+    }
+}
+
+// sigmoid / sigmoid_derivative (RenderUtils.cu:480-489), evaluated in double as there.
+__device__ __forceinline__ float colour_act(float x) { return 1.f / (1.f + exp(-0.1 * x)); }
+__device__ __forceinline__ float colour_deriv_from_act(float s)
+{
+    return 0.1 * s * (1.f - s);
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_inclusive_scan(double v, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    return v;
+}
+
+struct Corners {
+    unsigned idx[8];
+    float w[8];
+};
+
+__device__ __forceinline__ void sample_corners(const GridView& g, const SampleRec& s, Corners& c)
+{
+    const float x = s.fx, y = s.fy, z = s.fz;
+    const float x0 = 1.f - x, y0 = 1.f - y, z0 = 1.f - z;
+    c.w[0] = x0 * y0 * z0;
+    c.w[1] = x0 * y * z0;
+    c.w[2] = x * y0 * z0;
+    c.w[3] = x * y * z0;
+    c.w[4] = x0 * y0 * z;
+    c.w[5] = x0 * y * z;
+    c.w[6] = x * y0 * z;
+    c.w[7] = x * y * z;
+#pragma unroll
+    for (int q = 0; q < 8; q++) c.idx[q] = corner_vertex(g, s.bx, s.by, s.bz, q);
+}
+
+template <int NSH>
+struct RecShape {
+    static constexpr int NA = 1 + 3 * NSH;
+    static constexpr int REC = (NA + 3) & ~3;
+    static constexpr int NV4 = REC / 4;
+};
+
+// Trilinear SH (raw, before the basis product) of one sample.
+template <int NSH>
+__device__ __forceinline__ void gather_sh(const GridView& g, const Corners& c, float* sh)
+{
+    using RS = RecShape<NSH>;
+#pragma unroll
+    for (int e = 0; e < 3 * NSH; e++) sh[e] = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const float4* rec = reinterpret_cast<const float4*>(g.params + (size_t)c.idx[q] * RS::REC);
+        const float wq = c.w[q];
+#pragma unroll
+        for (int v = 0; v < RS::NV4; v++) {
+            const float4 p = __ldg(rec + v);
+            const float pv[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int e = 4 * v + k;
+                if (e >= 1 && e < RS::NA) sh[e - 1] = fmaf(wq, pv[k], sh[e - 1]);
+            }
+        }
+    }
+}
+
+template <int NSH, int MODE>
+__global__ void __launch_bounds__(128) k_shade(GridView g, RaysView r, const int32_t* sidx,
+                                                int start, int len, const SampleRec* samples,
+                                                float4* colours, int maxs, const int* counts,
+                                                const double* acc_in, double* losses,
+                                                double mask_coef, float huber)
+{
+    using RS = RecShape<NSH>;
+    const int lane = threadIdx.x & 31;
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (b >= len) return;  // warp-uniform
+    const int cnt = counts[b];  // -1: ray misses the box, -2: invalid ray index
+    if (cnt == -2) {
+        if ((MODE & kBackward) && lane == 0) losses[b] = 0.;
+        return;
+    }
+    const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
+    const bool miss = cnt < 0;
+    const int n = miss ? 0 : cnt;
+    float shs[NSH];
+    sh_basis<NSH>(r.dx[ri], r.dy[ri], r.dz[ri], shs);
+    const SampleRec* S = samples + (size_t)b * maxs;
+    float4* C = colours + (size_t)b * maxs;
+
+    // ---- forward colour ----
+    double s0 = 0., s1 = 0., s2 = 0.;
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        if (i < n) {
+            const SampleRec s = S[i];
+            Corners cr;
+            sample_corners(g, s, cr);
+            float sh[3 * NSH];
+            gather_sh<NSH>(g, cr, sh);
+            float col[3];
+#pragma unroll
+            for (int ch = 0; ch < 3; ch++) {
+                float a = 0.f;
+#pragma unroll
+                for (int k = 0; k < NSH; k++)
+                    if (k < g.n_sh_fwd) a = fmaf(sh[ch * NSH + k], shs[k], a);
+                col[ch] = colour_act(a);
+            }
+            C[i] = make_float4(col[0], col[1], col[2], 0.f);
+            const double w = (double)s.w;
+            s0 += w * col[0];
+            s1 += w * col[1];
+            s2 += w * col[2];
+        }
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    float pred[3];
+    if (MODE & kForward) {
+        if (miss) {
+            pred[0] = pred[1] = pred[2] = 0.f;
+        } else {
+            const double bg = r.white_bg ? 1. - acc_in[b] : 0.;  // RenderUtils.cu:1709-1716
+            pred[0] = (float)(s0 + bg);
+            pred[1] = (float)(s1 + bg);
+            pred[2] = (float)(s2 + bg);
+        }
+        if (lane == 0) {
+            r.acc_r[ri] = pred[0];
+            r.acc_g[ri] = pred[1];
+            r.acc_b[ri] = pred[2];
+        }
+    } else {
+        pred[0] = r.acc_r[ri];
+        pred[1] = r.acc_g[ri];
+        pred[2] = r.acc_b[ri];
+    }
+    if (!(MODE & kBackward)) return;
+
+    // ---- backward (renderRays_withGradients_RGBGPU, RenderUtils.cu:2145-2256) ----
+    if (miss) {
+        if (lane == 0) losses[b] = 0.;
+        return;
+    }
+    double res[3] = {
+        pred[0] - r.r[ri] / 255.,
+        pred[1] - r.g[ri] / 255.,
+        pred[2] - r.b[ri] / 255.,
+    };
+    double loss = (fabs(res[0]) + fabs(res[1]) + fabs(res[2])) * 255. / 3.;
+    if (isnan(loss)) {
+        if (lane == 0) losses[b] = 255.;
+        return;
+    }
+    if (lane == 0) losses[b] = loss;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        if (res[i] > huber)
+            res[i] = huber - 0.5 * huber * huber;
+        else if (res[i] < -huber)
+            res[i] = 0.5 * huber * huber - huber;
+    }
+    const float accw_f = r.acc_w[ri];
+    float mask_loss = 0.f;
+    const uint8_t gm = r.mask[ri];
+    if (gm && accw_f < 1.) mask_loss = (gm / 255.0 - accw_f) * mask_coef;
+    float wpre = fmax(1e-6, (double)accw_f);
+    wpre = fmin(1 - 1e-6, (double)wpre);
+    mask_loss += (logf(wpre) - log(1. - wpre)) * 1e-3;
+    const float step = g.step;
+
+    double carry_w = 0., carry_c0 = 0., carry_c1 = 0., carry_c2 = 0.;
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        const bool valid = i < n;
+        SampleRec s;
+        float4 col = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (valid) {
+            s = S[i];
+            col = C[i];
+        } else {
+            s.w = 0.f;
+        }
+        const double w = valid ? (double)s.w : 0.;
+        double aw = warp_inclusive_scan(w, lane);
+        double a0 = warp_inclusive_scan(w * col.x, lane);
+        double a1 = warp_inclusive_scan(w * col.y, lane);
+        double a2 = warp_inclusive_scan(w * col.z, lane);
+        const double acc_i = carry_w + aw;
+        const double acc_rgb0 = carry_c0 + a0;
+        const double acc_rgb1 = carry_c1 + a1;
+        const double acc_rgb2 = carry_c2 + a2;
+        carry_w += __shfl_sync(0xffffffffu, aw, 31);
+        carry_c0 += __shfl_sync(0xffffffffu, a0, 31);
+        carry_c1 += __shfl_sync(0xffffffffu, a1, 31);
+        carry_c2 += __shfl_sync(0xffffffffu, a2, 31);
+        if (!valid) continue;
+
+        float grad[4];
+        grad[1] = 0.6667f * w * res[0] * colour_deriv_from_act(col.x);
+        grad[2] = 0.6667f * w * res[1] * colour_deriv_from_act(col.y);
+        grad[3] = 0.6667f * w * res[2] * colour_deriv_from_act(col.z);
+        const double Ti = (double)s.tn;
+        grad[0] = res[0] * (Ti * col.x - (pred[0] - acc_rgb0));
+        grad[0] += res[1] * (Ti * col.y - (pred[1] - acc_rgb1));
+        grad[0] += res[2] * (Ti * col.z - (pred[2] - acc_rgb2));
+        const float dd = 1.f / (1.f + expf(13.f - s.raw));  // density_derivation (RenderUtils.cu:497)
+        grad[0] *= 0.6667 * step * dd;
+        grad[0] += step * dd * (accw_f - acc_i - Ti) * mask_loss;
+
+        // scatter: corner q receives grad[0]*w_q and grad[1+ch]*w_q*basis[k]
+        Corners cr;
+        sample_corners(g, s, cr);
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const float wq = cr.w[q];
+            const float a = grad[0] * wq;
+            const float bch[3] = {grad[1] * wq, grad[2] * wq, grad[3] * wq};
+            float4* dst = reinterpret_cast<float4*>(g.grad + (size_t)cr.idx[q] * RS::REC);
+#pragma unroll
+            for (int v = 0; v < RS::NV4; v++) {
+                float e4[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int e = 4 * v + k;
+                    float val = 0.f;
+                    if (e == 0) {
+                        val = a;
+                    } else if (e < RS::NA) {
+                        const int ch = (e - 1) / NSH;
+                        const int kk = (e - 1) % NSH;
+                        bool on = true;
+                        if (g.hierarchy) on = kk >= g.band * g.band && kk < g.n_sh_fwd;
+                        val = on ? bch[ch] * shs[kk] : 0.f;
+                    }
+                    e4[k] = val;
+                }
+                atomicAdd(dst + v, make_float4(e4[0], e4[1], e4[2], e4[3]));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batch MSE of the per-ray losses (getMSEError, Utils.cu:311-320), one block.
+// ---------------------------------------------------------------------------
+__global__ void k_mse(const double* losses, int len, double* out)
+{
+    __shared__ double part[32];
+    double s = 0.;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) s += losses[i] * losses[i];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) *out = len > 0 ? v / len : 0.;
+    }
+}
+
+cpx_status mse_launch(const double* losses, int len, double* out, cudaStream_t s)
+{
+    k_mse<<<1, 1024, 0, s>>>(losses, len, out);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "mse");
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+static int max_samples_per_ray(const cpx_grid* g)
+{
+    const double ex = (double)g->bbox[1] - g->bbox[0];
+    const double ey = (double)g->bbox[3] - g->bbox[2];
+    const double ez = (double)g->bbox[5] - g->bbox[4];
+    const double diag = sqrt(ex * ex + ey * ey + ez * ez);
+    return (int)ceil((diag + 2.0) / g->step) + 8;
+}
+
+static cpx_status ensure_scratch(cpx_grid* g, int len)
+{
+    MarchScratch& s = g->scratch;
+    const int maxs = max_samples_per_ray(g);
+    if (s.err == nullptr) {
+        if (cudaMalloc((void**)&s.err, sizeof(int) * 4) != cudaSuccess ||
+            cudaMalloc((void**)&s.mse, sizeof(double)) != cudaSuccess) {
+            set_error("scratch allocation failed");
+            return CPX_ERR_OUT_OF_MEMORY;
+        }
+        cudaMemset(s.err, 0, sizeof(int) * 4);
+    }
+    if (s.cap_rays >= len && s.maxs == maxs) return CPX_OK;
+    cudaFree(s.samples);
+    cudaFree(s.colours);
+    cudaFree(s.counts);
+    cudaFree(s.acc);
+    s.samples = nullptr;
+    s.colours = nullptr;
+    s.counts = nullptr;
+    s.acc = nullptr;
+    s.cap_rays = 0;
+    const int cap = len > 0 ? len : 1;
+    const size_t ns = (size_t)cap * maxs;
+    if (cudaMalloc((void**)&s.samples, ns * sizeof(SampleRec)) != cudaSuccess ||
+        cudaMalloc((void**)&s.colours, ns * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc((void**)&s.counts, (size_t)cap * sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&s.acc, (size_t)cap * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("march scratch of %zu samples could not be allocated", ns);
+        return CPX_ERR_OUT_OF_MEMORY;
+    }
+    s.cap_rays = cap;
+    s.maxs = maxs;
+    return CPX_OK;
+}
+
+template <int NSH>
+static void launch_shade(int mode, dim3 grid, dim3 block, cudaStream_t st, GridView gv,
+                         RaysView rv, const int32_t* sidx, int start, int len,
+                         const MarchScratch& s, double* losses, double mask_coef, float huber)
+{
+    if (mode == kForward)
+        k_shade<NSH, kForward><<<grid, block, 0, st>>>(gv, rv, sidx, start, len, s.samples,
+                                                       s.colours, s.maxs, s.counts, s.acc,
+                                                       losses, mask_coef, huber);
+    else if (mode == kBackward)
+        k_shade<NSH, kBackward><<<grid, block, 0, st>>>(gv, rv, sidx, start, len, s.samples,
+                                                        s.colours, s.maxs, s.counts, s.acc,
+                                                        losses, mask_coef, huber);
+    else
+        k_shade<NSH, kForwardBackward><<<grid, block, 0, st>>>(gv, rv, sidx, start, len,
+                                                               s.samples, s.colours, s.maxs,
+                                                               s.counts, s.acc, losses,
+                                                               mask_coef, huber);
+}
+
+cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                        int mode, double* losses, double mask_coef, float huber,
+                        cudaStream_t st)
+{
+    if (len < 0 || start < 0) {
+        set_error("negative start/len");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (!sidx && (int64_t)start + len > r->n) {
+        set_error("batch [%d, %d) exceeds the %lld rays", start, start + len, (long long)r->n);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if ((mode & kBackward) && !losses && len > 0) {
+        set_error("losses buffer is required for the backward");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (g->sparse && !g->have_occupancy) {
+        set_error("sparse grid without occupancy");
+        return CPX_ERR_NOT_READY;
+    }
+    g->last_len = len;
+    if (len == 0) return CPX_OK;
+    cpx_status rc = ensure_scratch(g, len);
+    if (rc != CPX_OK) return rc;
+    const GridView gv = grid_view(g);
+    const RaysView rv = rays_view(r);
+    const MarchScratch& s = g->scratch;
+    k_place<<<(len + 31) / 32, 32, 0, st>>>(gv, rv, sidx, start, len, r->n, s.samples, s.maxs,
+                                            s.counts, s.acc, s.err);
+    count_launch();
+    const dim3 block(128);
+    const dim3 grid((unsigned)(((int64_t)len * 32 + 127) / 128));
+    switch (g->sh_dim) {
+    case 1: launch_shade<1>(mode, grid, block, st, gv, rv, sidx, start, len, s, losses, mask_coef, huber); break;
+    case 4: launch_shade<4>(mode, grid, block, st, gv, rv, sidx, start, len, s, losses, mask_coef, huber); break;
+    case 9: launch_shade<9>(mode, grid, block, st, gv, rv, sidx, start, len, s, losses, mask_coef, huber); break;
+    default:
+        set_error("sh_dim %d unsupported", g->sh_dim);
+        return CPX_ERR_UNSUPPORTED;
+    }
+    count_launch();
+    return cuda_status(cudaGetLastError(), "march");
+}
+
+}  // namespace cpx

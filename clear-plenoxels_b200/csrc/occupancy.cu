@@ -1,0 +1,280 @@
+// occupancy.cu -- occupancy, in-cage flags, compact index table and compaction.
+//
+// The reference builds these with a kernel per (x,y) column (pruneScene,
+// SceneUtils.cu:831-881) followed by a host loop over every vertex for the
+// compact index (getCagedNums, SceneUtils.cu:1081-1120) and a host compaction
+// of the parameters (SceneUtils.cu:585-602).  Here all three run on the
+// device: a thread per cell sets the occupancy byte/bit and the in-cage flags,
+// a three-phase prefix scan turns the flags into the index table, and a
+// thread per vertex moves in-cage records to their compact slots.  The index
+// lists are identical to the reference's, including its quirks: the flag for
+// the x = W-1 face is written at depth*W*H + H*W + col + 1 (SceneUtils.cu:872),
+// and non-caged vertices get index 0.  The one write the reference makes past
+// the end of the flag array (cells at x = W-2, z = D-2) is dropped.
+#include "cpx_internal.cuh"
+
+namespace cpx {
+
+__device__ __forceinline__ int64_t grid_index_upper(int x, int y, int z, int W, int H, int D)
+{
+    x = x < W ? x : W - 1;
+    y = y < H ? y : H - 1;
+    z = z < D ? z : D - 1;
+    return (int64_t)z * W * H + (int64_t)y * W + x;
+}
+
+// occupiedVoxel + pruneScene; one thread per cell, cells in z-y-x order.
+__global__ void k_prune(const float* __restrict__ dens, int W, int H, int D, float thr,
+                        uint8_t* occ, uint32_t* occ_bits, uint8_t* in_cage, int64_t n_cells,
+                        unsigned long long* dropped)
+{
+    const int64_t ci = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int Wc = W - 1, Hc = H - 1;
+    bool occupied = false;
+    if (ci < n_cells) {
+        const int x = (int)(ci % Wc);
+        const int y = (int)((ci / Wc) % Hc);
+        const int z = (int)(ci / ((int64_t)Wc * Hc));
+        for (int dz = 0; dz <= 1 && !occupied; dz++)
+            for (int dy = 0; dy <= 1 && !occupied; dy++)
+                for (int dx = 0; dx <= 1 && !occupied; dx++)
+                    if (dens[grid_index_upper(x + dx, y + dy, z + dz, W, H, D)] > thr) occupied = true;
+        occ[ci] = occupied ? 1 : 0;
+        if (occupied) {
+            const int64_t N = (int64_t)W * H * D;
+            in_cage[(int64_t)z * W * H + (int64_t)y * W + x] = 1;
+            if (z == D - 2) in_cage[(int64_t)(D - 1) * W * H + (int64_t)y * W + x] = 1;
+            if (y == H - 2) in_cage[(int64_t)z * W * H + (int64_t)(H - 1) * W + x] = 1;
+            if (x == W - 2) {
+                const int64_t v = (int64_t)z * W * H + (int64_t)H * W + x + 1;
+                if (v < N)
+                    in_cage[v] = 1;
+                else
+                    atomicAdd(dropped, 1ull);
+            }
+        }
+    }
+    // one occupancy bit per cell: the warp covers 32 consecutive cells
+    const unsigned bits = __ballot_sync(0xffffffffu, occupied);
+    if ((threadIdx.x & 31) == 0) {
+        const int64_t word = ci >> 5;
+        if (word * 32 < n_cells) occ_bits[word] = bits;
+    }
+}
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums,
+                                                         uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) warp_sums[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0u;
+        uint32_t si = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, si, o);
+            if (lane >= o) si += u;
+        }
+        warp_sums[lane] = si - s;
+        if (lane == 31) *total = si;
+    }
+    __syncthreads();
+    return warp_sums[wid] + inc - v;
+}
+
+// Phase 1: in-cage count of each tile.
+__global__ void __launch_bounds__(kScanThreads) k_scan_count(const uint8_t* flags, int64_t n,
+                                                              uint32_t* tile_sums)
+{
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t total;
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+        if (base + k < n) c += flags[base + k] ? 1u : 0u;
+    block_exclusive_scan(c, ws, &total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// Phase 2: exclusive scan of the tile counts (single block, loops over chunks).
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(uint32_t* tile_sums, int n_tiles,
+                                                              uint32_t* grand_total)
+{
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t total;
+    uint32_t carry = 0;
+    for (int base = 0; base < n_tiles; base += kScanThreads) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < n_tiles ? tile_sums[i] : 0u;
+        const uint32_t ex = block_exclusive_scan(v, ws, &total);
+        if (i < n_tiles) tile_sums[i] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *grand_total = carry;
+}
+
+// Phase 3: index table (getCagedNums: running count for caged vertices, 0 otherwise).
+__global__ void __launch_bounds__(kScanThreads) k_scan_write(const uint8_t* flags, int64_t n,
+                                                              const uint32_t* tile_offsets,
+                                                              uint32_t* index_offsets)
+{
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t total;
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t f[kScanItems];
+    uint32_t c = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        f[k] = (base + k < n && flags[base + k]) ? 1u : 0u;
+        c += f[k];
+    }
+    uint32_t run = tile_offsets[blockIdx.x] + block_exclusive_scan(c, ws, &total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < n) index_offsets[base + k] = f[k] ? run : 0u;
+        run += f[k];
+    }
+}
+
+cpx_status occupancy_launch(cpx_grid* g, float threshold)
+{
+    const int64_t N = g->n_dense;
+    const int64_t C = (int64_t)(g->W - 1) * (g->H - 1) * (g->D - 1);
+    if (g->W < 2 || g->H < 2 || g->D < 2) {
+        set_error("occupancy needs at least 2 vertices per axis");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (!g->occ_bytes) {
+        const int64_t words = (C + 31) / 32;
+        if (cudaMalloc((void**)&g->occ_bytes, C) != cudaSuccess ||
+            cudaMalloc((void**)&g->occ_bits, (words + 1) * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc((void**)&g->in_cage, N) != cudaSuccess ||
+            cudaMalloc((void**)&g->index_offsets, N * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("occupancy tables could not be allocated");
+            return CPX_ERR_OUT_OF_MEMORY;
+        }
+    }
+    const int n_tiles = (int)((N + kScanTile - 1) / kScanTile);
+    uint32_t* tile_sums = nullptr;
+    unsigned long long* dropped = nullptr;
+    uint32_t* total = nullptr;
+    if (cudaMalloc((void**)&tile_sums, (size_t)n_tiles * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc((void**)&dropped, sizeof(unsigned long long) + sizeof(uint32_t) * 2) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(tile_sums);
+        set_error("occupancy scratch could not be allocated");
+        return CPX_ERR_OUT_OF_MEMORY;
+    }
+    total = reinterpret_cast<uint32_t*>(dropped + 1);
+    cudaMemset(dropped, 0, sizeof(unsigned long long) + sizeof(uint32_t) * 2);
+    cudaMemset(g->in_cage, 0, N);
+    const int64_t words = (C + 31) / 32;
+    cudaMemset(g->occ_bits, 0, (words + 1) * sizeof(uint32_t));
+    const int64_t prune_threads = words * 32;
+    k_prune<<<(unsigned)((prune_threads + 255) / 256), 256>>>(g->density, g->W, g->H, g->D,
+                                                               threshold, g->occ_bytes,
+                                                               g->occ_bits, g->in_cage, C,
+                                                               dropped);
+    k_scan_count<<<n_tiles, kScanThreads>>>(g->in_cage, N, tile_sums);
+    k_scan_tiles<<<1, kScanThreads>>>(tile_sums, n_tiles, total);
+    k_scan_write<<<n_tiles, kScanThreads>>>(g->in_cage, N, tile_sums, g->index_offsets);
+    count_launch(4);
+    uint32_t cnt = 0;
+    cudaError_t e = cudaMemcpy(&cnt, total, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    cudaFree(tile_sums);
+    cudaFree(dropped);
+    if (e != cudaSuccess) return cuda_status(e, "occupancy");
+    g->in_cage_count = cnt;
+    g->have_occupancy = 1;
+    return cuda_status(cudaGetLastError(), "occupancy");
+}
+
+// Move in-cage records to their compact slots (SceneUtils.cu:585-602).
+__global__ void k_compact(const float4* __restrict__ src, float4* dst, float* dens_out,
+                          const uint8_t* __restrict__ in_cage,
+                          const uint32_t* __restrict__ index_offsets, uint32_t* c2d, int64_t N,
+                          int S)
+{
+    const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (v >= N || !in_cage[v]) return;
+    const uint32_t c = index_offsets[v];
+    for (int j = 0; j < S; j++) dst[(int64_t)c * S + j] = src[v * S + j];
+    dens_out[c] = src[v * S].x;
+    c2d[c] = (uint32_t)v;
+}
+
+cpx_status make_sparse_launch(cpx_grid* g)
+{
+    if (!g->have_occupancy) {
+        set_error("cpx_occupancy_build must run before cpx_grid_make_sparse");
+        return CPX_ERR_NOT_READY;
+    }
+    if (g->sparse) {
+        set_error("grid is already sparse");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    const int64_t n = g->in_cage_count;
+    const int64_t nalloc = n > 0 ? n : 1;
+    const size_t rec_bytes = (size_t)g->rec * sizeof(float);
+    float *p0 = nullptr, *p1 = nullptr, *gr = nullptr, *m = nullptr, *v = nullptr, *dens = nullptr;
+    uint32_t* c2d = nullptr;
+    if (cudaMalloc((void**)&p0, nalloc * rec_bytes) != cudaSuccess ||
+        cudaMalloc((void**)&p1, nalloc * rec_bytes) != cudaSuccess ||
+        cudaMalloc((void**)&gr, nalloc * rec_bytes) != cudaSuccess ||
+        cudaMalloc((void**)&m, nalloc * rec_bytes) != cudaSuccess ||
+        cudaMalloc((void**)&v, nalloc * rec_bytes) != cudaSuccess ||
+        cudaMalloc((void**)&dens, nalloc * sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&c2d, nalloc * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p0); cudaFree(p1); cudaFree(gr); cudaFree(m); cudaFree(v); cudaFree(dens); cudaFree(c2d);
+        set_error("sparse buffers for %lld vertices could not be allocated", (long long)n);
+        return CPX_ERR_OUT_OF_MEMORY;
+    }
+    cudaMemset(p0, 0, nalloc * rec_bytes);
+    cudaMemset(p1, 0, nalloc * rec_bytes);
+    cudaMemset(gr, 0, nalloc * rec_bytes);
+    cudaMemset(m, 0, nalloc * rec_bytes);
+    cudaMemset(v, 0, nalloc * rec_bytes);
+    const int S = g->rec / 4;
+    k_compact<<<(unsigned)((g->n_dense + 255) / 256), 256>>>(
+        reinterpret_cast<const float4*>(g->params[g->cur]), reinterpret_cast<float4*>(p0), dens,
+        g->in_cage, g->index_offsets, c2d, g->n_dense, S);
+    count_launch();
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_status(e, "compaction");
+    cudaFree(g->params[0]);
+    cudaFree(g->params[1]);
+    cudaFree(g->grad);
+    cudaFree(g->m);
+    cudaFree(g->v);
+    cudaFree(g->density);
+    cudaFree(g->compact_to_dense);
+    g->params[0] = p0;
+    g->params[1] = p1;
+    g->cur = 0;
+    g->grad = gr;
+    g->m = m;
+    g->v = v;
+    g->density = dens;
+    g->compact_to_dense = c2d;
+    g->n_act = n;
+    g->sparse = 1;
+    return CPX_OK;
+}
+
+}  // namespace cpx

@@ -1,0 +1,416 @@
+// sweep.cu -- TV gradient and Adam over the grid (HBM-bound sweeps).
+//
+// The reference runs the TV term (RenderUtils.cu:2577-2813, a thread per (x,y)
+// column walking z over 28 planar arrays) and then Adam (Optimizer.cu:359-415,
+// a thread per vertex over the same 28 arrays) as two passes.  Here the
+// default pair -- TV type 0 with 6 neighbours, then Adam -- is one pass: a
+// thread owns one 16-byte slot (4 parameters) of one vertex record, reads the
+// slot from the current parameter buffer, its 6 neighbours' slots (L1/L2
+// resident: the sweep walks z-y-x rows in order, so rows y+-1 and planes z+-1
+// are recent), the gradient and both moments, and writes the updated slot to
+// the other parameter buffer.  Per vertex that is the algorithmic minimum:
+// params r+w, grad r + zero-w, m r+w, v r+w (+4 B density mirror write).
+//
+// TV and Adam arithmetic is FP32 (the reference mixes double into the TV
+// division and the Adam update; the FP32 results differ from it by a few ulp).
+#include "cpx_internal.cuh"
+
+namespace cpx {
+
+struct SweepArgs {
+    int W, H, D;
+    int S;  // float4 slots per record
+    int n_arrays, sh_dim, band, hierarchy;
+    int64_t n_act;
+    int sparse;
+    const float4* __restrict__ p_in;
+    float4* p_out;
+    float4* grad;
+    float4* m;
+    float4* v;
+    float* density_out;
+    const float* __restrict__ adaptive_lr;
+    const uint32_t* __restrict__ index_offsets;
+    const uint32_t* __restrict__ compact_to_dense;
+    float lam_d, lam_sh;
+    float lr, sh_lr;
+    int timestep;
+};
+
+// Which parameter of a record the Adam step updates (Optimizer.cu:380-413).
+__device__ __forceinline__ bool adam_applies(const SweepArgs& a, int e)
+{
+    if (e == 0) return true;
+    if (e >= a.n_arrays) return false;
+    if (!a.hierarchy) return true;
+    const int k = (e - 1) % a.sh_dim;
+    return k >= a.band * a.band && k < (a.band + 1) * (a.band + 1);
+}
+
+// Which parameter the TV term touches (RenderUtils.cu:2743-2746).
+__device__ __forceinline__ bool tv_applies(const SweepArgs& a, int e)
+{
+    if (e == 0) return true;
+    if (e >= a.n_arrays) return false;
+    const int k = (e - 1) % a.sh_dim;
+    const int lo = a.hierarchy ? a.band * a.band : 0;
+    return k >= lo && k < (a.band + 1) * (a.band + 1);
+}
+
+__device__ __forceinline__ float f4get(const float4& v, int c)
+{
+    return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void f4set(float4& v, int c, float x)
+{
+    if (c == 0) v.x = x;
+    else if (c == 1) v.y = x;
+    else if (c == 2) v.z = x;
+    else v.w = x;
+}
+
+// The six-neighbour TV term for one parameter (RenderUtils.cu:2672-2757); neighbours in
+// the reference's order z-1, y-1, x-1, x+1, y+1, z+1.
+__device__ __forceinline__ float tv6(float self, const float* nb, float lam)
+{
+    float sum = 0.f, disp = 0.f;
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+        const float d = self - nb[j];
+        sum += d * d;
+        disp = (j == 0) ? d : disp + d;
+    }
+    sum = sqrtf(sum) / 6.f;
+    return lam / (sum + 1.e-6f) * disp;
+}
+
+template <bool TV, bool SPARSE>
+__global__ void __launch_bounds__(256) k_sweep(SweepArgs a)
+{
+    __shared__ float s_bc[2];
+    if (threadIdx.x == 0) {
+        // bias corrections exactly as the reference forms them (powf of float beta)
+        s_bc[0] = 1.f / (float)(1. - powf(0.9f, a.timestep));
+        s_bc[1] = 1.f / (float)(1. - powf(0.999f, a.timestep));
+    }
+    __syncthreads();
+    const float inv_bc1 = s_bc[0], inv_bc2 = s_bc[1];
+    const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
+    const int S = a.S;
+    const int64_t WH = (int64_t)a.W * a.H;
+
+    // Dense: one block per (y,z) row; sparse: blocks tile the compact slots.
+    int64_t slot_begin, slot_end;
+    int y = 0, z = 0;
+    if (!SPARSE) {
+        const int row = blockIdx.x;
+        y = row % a.H;
+        z = row / a.H;
+        slot_begin = ((int64_t)z * WH + (int64_t)y * a.W) * S;
+        slot_end = slot_begin + (int64_t)a.W * S;
+    } else {
+        const int64_t per_block = (int64_t)blockDim.x * 8;
+        slot_begin = (int64_t)blockIdx.x * per_block;
+        slot_end = min(slot_begin + per_block, a.n_act * S);
+    }
+    const bool row_interior = !SPARSE && y >= 1 && y <= a.H - 2 && z >= 1 && z <= a.D - 2;
+
+    for (int64_t sl = slot_begin + threadIdx.x; sl < slot_end; sl += blockDim.x) {
+        const int64_t v = sl / S;
+        const int j = (int)(sl - v * S);
+        float4 p = a.p_in[sl];
+        float4 g = a.grad[sl];
+        float4 m = a.m[sl];
+        float4 vv = a.v[sl];
+        if (TV) {
+            bool interior;
+            int64_t nb_slot[6];
+            bool nb_self[6] = {false, false, false, false, false, false};
+            if (!SPARSE) {
+                const int x = (int)(v - ((int64_t)z * WH + (int64_t)y * a.W));
+                interior = row_interior && x >= 1 && x <= a.W - 2;
+                const int64_t off[6] = {-WH, -(int64_t)a.W, -1, 1, (int64_t)a.W, WH};
+#pragma unroll
+                for (int k = 0; k < 6; k++) nb_slot[k] = (v + off[k]) * S + j;
+            } else {
+                const int64_t dv = a.compact_to_dense[v];
+                const int x = (int)(dv % a.W);
+                const int yy = (int)((dv / a.W) % a.H);
+                const int zz = (int)(dv / WH);
+                interior = x >= 1 && x <= a.W - 2 && yy >= 1 && yy <= a.H - 2 && zz >= 1 &&
+                           zz <= a.D - 2;
+                if (interior) {
+                    const int64_t off[6] = {-WH, -(int64_t)a.W, -1, 1, (int64_t)a.W, WH};
+#pragma unroll
+                    for (int k = 0; k < 6; k++) {
+                        const uint32_t ci = a.index_offsets[dv + off[k]];
+                        nb_self[k] = ci == 0;  // compact index 0 reads as the vertex itself
+                        nb_slot[k] = (int64_t)ci * S + j;
+                    }
+                }
+            }
+            if (interior) {
+                float4 nbv[6];
+#pragma unroll
+                for (int k = 0; k < 6; k++) nbv[k] = nb_self[k] ? p : a.p_in[nb_slot[k]];
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int e = 4 * j + c;
+                    if (!tv_applies(a, e)) continue;
+                    float nb[6];
+#pragma unroll
+                    for (int k = 0; k < 6; k++) nb[k] = f4get(nbv[k], c);
+                    const float lam = e == 0 ? a.lam_d : a.lam_sh;
+                    f4set(g, c, f4get(g, c) + tv6(f4get(p, c), nb, lam));
+                }
+            }
+        }
+        // Adam (Optimizer.cu:374-413)
+        float4 pn = p;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int e = 4 * j + c;
+            if (!adam_applies(a, e)) continue;
+            const float gc = f4get(g, c);
+            const float mc = fmaf(1.f - beta1, gc, beta1 * f4get(m, c));
+            const float vc = fmaf((1.f - beta2) * gc, gc, beta2 * f4get(vv, c));
+            f4set(m, c, mc);
+            f4set(vv, c, vc);
+            const float cm = mc * inv_bc1;
+            const float cv = vc * inv_bc2;
+            float lr = a.sh_lr;
+            if (e == 0) lr = (!SPARSE && a.adaptive_lr) ? a.lr * a.adaptive_lr[v] : a.lr;
+            float np = f4get(p, c) - lr * cm / (sqrtf(cv) + eps);
+            if (e == 0) np = np < 0.f ? 0.f : np;  // density clamp (Optimizer.cu:384)
+            f4set(pn, c, np);
+            f4set(g, c, 0.f);
+        }
+        a.p_out[sl] = pn;
+        a.m[sl] = m;
+        a.v[sl] = vv;
+        a.grad[sl] = g;
+        if (j == 0) a.density_out[v] = pn.x;
+    }
+}
+
+cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
+                      double sh_lr, int timestep, cudaStream_t st)
+{
+    if (g->n_act == 0) return CPX_OK;
+    SweepArgs a;
+    a.W = g->W;
+    a.H = g->H;
+    a.D = g->D;
+    a.S = g->rec / 4;
+    a.n_arrays = g->n_arrays;
+    a.sh_dim = g->sh_dim;
+    a.band = g->band;
+    a.hierarchy = g->hierarchy;
+    a.n_act = g->n_act;
+    a.sparse = g->sparse;
+    a.p_in = reinterpret_cast<const float4*>(g->params[g->cur]);
+    a.p_out = reinterpret_cast<float4*>(g->params[g->cur ^ 1]);
+    a.grad = reinterpret_cast<float4*>(g->grad);
+    a.m = reinterpret_cast<float4*>(g->m);
+    a.v = reinterpret_cast<float4*>(g->v);
+    a.density_out = g->density;
+    a.adaptive_lr = g->adaptive_lr;
+    a.index_offsets = g->index_offsets;
+    a.compact_to_dense = g->compact_to_dense;
+    a.lam_d = (float)lam_d;
+    a.lam_sh = (float)lam_sh;
+    a.lr = (float)lr;
+    a.sh_lr = (float)sh_lr;
+    a.timestep = timestep;
+    if (!g->sparse) {
+        const unsigned rows = (unsigned)((int64_t)g->H * g->D);
+        if (fused_tv)
+            k_sweep<true, false><<<rows, 256, 0, st>>>(a);
+        else
+            k_sweep<false, false><<<rows, 256, 0, st>>>(a);
+    } else {
+        const int64_t slots = g->n_act * a.S;
+        const unsigned blocks = (unsigned)((slots + 256 * 8 - 1) / (256 * 8));
+        if (fused_tv)
+            k_sweep<true, true><<<blocks, 256, 0, st>>>(a);
+        else
+            k_sweep<false, true><<<blocks, 256, 0, st>>>(a);
+    }
+    count_launch();
+    g->cur ^= 1;
+    return cuda_status(cudaGetLastError(), "adam sweep");
+}
+
+// ---------------------------------------------------------------------------
+// Standalone TV gradient (RenderUtils::addVarianceLoss, RenderUtils.cu:2815-2851).
+// ---------------------------------------------------------------------------
+struct TvArgs {
+    int W, H, D, rec, n_arrays, sh_dim, band, hierarchy, sparse, optimize_step;
+    const float* __restrict__ p;
+    float* grad;
+    const uint32_t* __restrict__ index_offsets;
+    const uint8_t* __restrict__ in_cage;
+    const uint8_t* __restrict__ occ;
+    float lam_d, lam_sh;
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ uint32_t nb_index(const TvArgs& a, int x, int y, int z)
+{
+    x = clampi(x, 0, a.W - 1);
+    y = clampi(y, 0, a.H - 1);
+    z = clampi(z, 0, a.D - 1);
+    uint32_t v = (uint32_t)(z * a.W * a.H + y * a.W + x);
+    return a.sparse ? a.index_offsets[v] : v;
+}
+
+// Type 0: one thread per vertex (x,y interior, z in the reference's range), all
+// parameters of the vertex, 3 / 6 / 26 neighbours with the reference's quirks.
+__global__ void k_tv_type0(TvArgs a, int nbrs)
+{
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nplane = (int64_t)a.W * a.H;
+    if (tid >= nplane * a.D) return;
+    const int z = (int)(tid / nplane);
+    const int y = (int)((tid / a.W) % a.H);
+    const int x = (int)(tid % a.W);
+    if (y == 0 || y == a.H - 1 || x == 0 || x == a.W - 1) return;
+    if (nbrs == 3) {
+        if (z > a.D - 2) return;  // depth 0 .. D-2 (RenderUtils.cu:2608)
+    } else if (z < 1 || z > a.D - 2) {
+        return;
+    }
+    uint32_t ix[27];
+    for (int dz = -1; dz < 2; dz++)
+        for (int dy = -1; dy < 2; dy++)
+            for (int dx = -1; dx < 2; dx++)
+                ix[(dz + 1) * 9 + (dy + 1) * 3 + dx + 1] = nb_index(a, x + dx, y + dy, z + dz);
+    if (a.sparse) {
+        const uint32_t dv = (uint32_t)(z * a.W * a.H + y * a.W + x);
+        if (!a.in_cage[dv]) return;
+    }
+    const int startSH = a.hierarchy ? a.band * a.band : 0;
+    const int endSH = (a.band + 1) * (a.band + 1);
+    float slot4 = 0.f;  // neighbour array slot 4 as left by the previous parameter (26 case)
+    for (int e = 0; e < a.n_arrays; e++) {
+        if (e > 0) {
+            const int k = (e - 1) % a.sh_dim;
+            if (k < startSH || k >= endSH) continue;
+        }
+        const float lam = e == 0 ? a.lam_d : a.lam_sh;
+        auto val = [&](uint32_t i) { return a.p[(size_t)i * a.rec + e]; };
+        const float self = val(ix[13]);
+        float sum = 0.f, disp = 0.f, sd;
+        if (nbrs == 3) {
+            const float n14 = ix[14] != 0 ? val(ix[14]) : self;
+            sum += (self - n14) * (self - n14);
+            const float n16 = ix[16] != 0 ? val(ix[16]) : self;
+            sum += (self - n16) * (self - n16);
+            const bool have22 = e == 0 ? ix[22] != 0 : ix[4] != 0;  // RenderUtils.cu:2650
+            const float n22 = have22 ? val(ix[22]) : self;
+            disp = self - n22;
+            sum += (self - n22) * (self - n22);
+            sd = sqrtf(sum) / 3.f;
+        } else if (nbrs == 6) {
+            const int nb[6] = {4, 10, 12, 14, 16, 22};
+            for (int j = 0; j < 6; j++) {
+                const float nv = ix[nb[j]] != 0 ? val(ix[nb[j]]) : self;
+                sum += (self - nv) * (self - nv);
+                disp = j == 0 ? self - nv : disp + (self - nv);
+            }
+            sd = sqrtf(sum) / 6.f;
+        } else {
+            for (int j = 0; j < 27; j++) {
+                if (j == 13) continue;
+                const float nv = ix[j] != 0 ? val(ix[j]) : self;
+                if (j == 4) slot4 = nv;
+                sum += (self - nv) * (self - nv);
+                disp += e == 0 ? self - nv : self - slot4;
+            }
+            sd = sqrtf(sum) / 26.f;
+        }
+        float* gp = a.grad + (size_t)ix[13] * a.rec + e;
+        *gp = *gp + lam / (sd + 1.e-6f) * disp;
+    }
+}
+
+// Type 1 voxel disparity (RenderUtils.cu:2469-2547): one thread per cell; the shared
+// corners are accumulated with atomics (the reference's unsynchronised += is racy).
+__global__ void k_tv_type1(TvArgs a)
+{
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int Wc = a.W - 1, Hc = a.H - 1, Dc = a.D - 1;
+    if (tid >= (int64_t)Wc * Hc * Dc) return;
+    const int x = (int)(tid % Wc);
+    const int y = (int)((tid / Wc) % Hc);
+    const int z = (int)(tid / ((int64_t)Wc * Hc));
+    if (a.sparse && !a.occ[tid]) return;
+    uint32_t ix[8];
+    for (int dz = 0; dz < 2; dz++)
+        for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) ix[dz * 4 + dy * 2 + dx] = nb_index(a, x + dx, y + dy, z + dz);
+    const int startSH = a.hierarchy ? a.band * a.band : 0;
+    const int endSH = (a.band + 1) * (a.band + 1);
+    for (int e = 0; e < a.n_arrays; e++) {
+        float lam = a.lam_d;
+        if (e > 0) {
+            if (a.optimize_step > 1) continue;
+            const int k = (e - 1) % a.sh_dim;
+            if (k < startSH || k >= endSH) continue;
+            lam = a.lam_sh;
+        }
+        float mean = 0.f;
+        for (int i = 0; i < 8; i++) {
+            const float pv = a.p[(size_t)ix[i] * a.rec + e];
+            mean += e == 0 ? pv : pv / 8.f;
+        }
+        if (e == 0) mean /= 8.f;
+        for (int i = 0; i < 8; i++)
+            atomicAdd(a.grad + (size_t)ix[i] * a.rec + e, lam * (a.p[(size_t)ix[i] * a.rec + e] - mean));
+    }
+}
+
+cpx_status tv_launch(cpx_grid* g, double lam_d, double lam_sh, int type, int nbrs,
+                     cudaStream_t st)
+{
+    if (type < 0 || type > 2 || (type != 1 && nbrs != 3 && nbrs != 6 && nbrs != 26)) {
+        set_error("TV type %d with %d neighbours is not defined", type, nbrs);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (g->sparse && !g->have_occupancy) {
+        set_error("sparse grid without occupancy");
+        return CPX_ERR_NOT_READY;
+    }
+    TvArgs a;
+    a.W = g->W;
+    a.H = g->H;
+    a.D = g->D;
+    a.rec = g->rec;
+    a.n_arrays = g->n_arrays;
+    a.sh_dim = g->sh_dim;
+    a.band = g->band;
+    a.hierarchy = g->hierarchy;
+    a.sparse = g->sparse;
+    a.optimize_step = g->optimize_step;
+    a.p = g->params[g->cur];
+    a.grad = g->grad;
+    a.index_offsets = g->index_offsets;
+    a.in_cage = g->in_cage;
+    a.occ = g->occ_bytes;
+    a.lam_d = (float)lam_d;
+    a.lam_sh = (float)lam_sh;
+    if (type == 0 || type == 2) {
+        const int64_t n = g->n_dense;
+        k_tv_type0<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, nbrs);
+        count_launch();
+    }
+    if (type == 1 || type == 2) {
+        const int64_t c = (int64_t)(g->W - 1) * (g->H - 1) * (g->D - 1);
+        k_tv_type1<<<(unsigned)((c + 255) / 256), 256, 0, st>>>(a);
+        count_launch();
+    }
+    return cuda_status(cudaGetLastError(), "tv");
+}
+
+}  // namespace cpx

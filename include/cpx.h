@@ -1,0 +1,215 @@
+/*
+ * cpx.h -- C ABI of the B200-native Clear-plenoxels training hot path.
+ *
+ * A drop-in for the reference's per-batch entry points (citations are
+ * file:line in the reference project, SVRF = SparseVolumeRadianceField/):
+ *
+ *   cpx_render_forward           RenderUtils::renderRays                     SVRF/RenderUtils.cuh:37, .cu:1961
+ *   cpx_render_backward          RenderUtils::renderRays_withGradients_RGB   SVRF/RenderUtils.cuh:51, .cu:2258
+ *   cpx_tv_grad                  RenderUtils::addVarianceLoss                SVRF/RenderUtils.cuh:76, .cu:2815
+ *   cpx_adam_step                Optimizer::updateRGBScene                   SVRF/Optimizer.cuh:35, .cu:451
+ *   cpx_grid_create/upload       objectScene::initSelf, optimizer::initialSelf/initialAll
+ *                                                                            SVRF/SceneUtils.cu:60, Optimizer.cu:81,163
+ *   cpx_occupancy_build          objectScene::pruneSelf + getCagedNums       SVRF/SceneUtils.cu:883, 1081
+ *   cpx_grid_make_sparse         sparse compaction of initSelfByUpsample     SVRF/SceneUtils.cu:520-600
+ *   cpx_rays_init_camera         _rays::initialSelf / initialRays            SVRF/Rays.cu:187, 77
+ *
+ * Conventions.  Every call returns a cpx_status instead of exiting the
+ * process.  Work is enqueued on the caller's stream (a cudaStream_t passed as
+ * void*, NULL = legacy default stream) with no implicit device synchronisation;
+ * only the host upload/download calls block.  Grid and ray buffers are owned
+ * by the library behind opaque handles; host arrays are copied.  Arrays named
+ * *_dev are device pointers, exactly where the reference takes device
+ * pointers (sample index table, per-ray losses).  A handle is used by one host
+ * thread at a time.
+ *
+ * Parameter order follows the reference's totalVariableGPUPtrs table
+ * (SVRF/SceneUtils.cu:148-166): array 0 is density, arrays 1+c*sh_dim+i are
+ * SH coefficient i of colour channel c (R, G, B).  Host parameter blocks are
+ * planar float [n_arrays][n_active], the layout the reference keeps on device.
+ */
+#ifndef CPX_H
+#define CPX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cpx_status {
+    CPX_OK = 0,
+    CPX_ERR_INVALID_ARGUMENT = 1,
+    CPX_ERR_OUT_OF_MEMORY = 2,
+    CPX_ERR_CUDA = 3,
+    CPX_ERR_ITERATION_CAP = 4, /* a ray's march exceeded its provable sample bound */
+    CPX_ERR_NAN = 5,           /* reserved: NaN detected where a caller asked for a check */
+    CPX_ERR_NOT_READY = 6,     /* e.g. sparse call before cpx_occupancy_build */
+    CPX_ERR_UNSUPPORTED = 7
+} cpx_status;
+
+typedef void* cpx_stream; /* cudaStream_t */
+typedef struct cpx_grid cpx_grid;
+typedef struct cpx_rays cpx_rays;
+
+typedef struct cpx_grid_desc {
+    int width, height, depth; /* vertices per axis (sceneWidth/Height/Depth) */
+    int sh_dim;               /* SH coefficients per channel: 1, 4 or 9 */
+    int optimizing_band;      /* ObjectScene::optimizingBand; forward uses (band+1)^2 <= sh_dim */
+    int hierarchy_strategy;   /* Optimizer::hierarchyStrategy (band-restricted grads/updates) */
+    float step_size;          /* ObjectScene::stepSize, > 0 */
+    int bbox[6];              /* ray AABB in voxel space: wmin,wmax,hmin,hmax,dmin,dmax */
+} cpx_grid_desc;
+
+/* Pinhole camera as the reference's getBound reads it (SVRF/CameraUtils.cuh:16-26):
+ * focal lengths, principal point, camera-to-world 4x4 (row-major) and centre. */
+typedef struct cpx_camera {
+    double alpha[2];
+    double principle[2];
+    double c2w[16];
+    double centre[4];
+} cpx_camera;
+
+/* ------------------------------------------------------------------ status */
+const char* cpx_status_string(cpx_status s);
+/* Text of the last error raised on the calling thread ("" if none). */
+const char* cpx_last_error(void);
+/* Library version as major*10000 + minor*100 + patch. */
+int cpx_version(void);
+
+/* ------------------------------------------------------------------ grid */
+/* Dense grid, every parameter zero, Adam moments zero, adaptive LR one, no jitter.
+ * Replaces objectScene::initSelf(solid) + optimizer::initialSelf/initialAll. */
+cpx_status cpx_grid_create(const cpx_grid_desc* desc, cpx_grid** out);
+cpx_status cpx_grid_destroy(cpx_grid* g);
+/* n_active: W*H*D (dense) or the in-cage count (sparse); n_arrays = 1 + 3*sh_dim. */
+cpx_status cpx_grid_info(const cpx_grid* g, int64_t* n_active, int* n_arrays, int* sparse);
+
+/* Planar [n_arrays][n_active] host copies of parameters, gradients and moments. */
+cpx_status cpx_grid_upload_params(cpx_grid* g, const float* planar, int64_t n_active);
+cpx_status cpx_grid_download_params(const cpx_grid* g, float* planar, int64_t n_active);
+cpx_status cpx_grid_upload_grads(cpx_grid* g, const float* planar, int64_t n_active);
+cpx_status cpx_grid_download_grads(const cpx_grid* g, float* planar, int64_t n_active);
+cpx_status cpx_grid_upload_moments(cpx_grid* g, const float* m, const float* v, int64_t n_active);
+cpx_status cpx_grid_download_moments(const cpx_grid* g, float* m, float* v, int64_t n_active);
+/* Density LR multiplier (ObjectScene::adaptiveLRDevice), [W*H*D]; dense Adam only. */
+cpx_status cpx_grid_set_adaptive_lr(cpx_grid* g, const float* lr_mult, int64_t n_dense);
+/* Per-sample jitter offsets (ObjectScene::offset{X,Y,Z}Device, filled by setSelfSampleOffset,
+ * SVRF/SceneUtils.cu:792); entries past n read as zero.  n = 0 clears them. */
+cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const double* oy,
+                                       const double* oz, int n);
+/* ObjectScene::optimizeStep (hierarchy level); gates SH in the type-1 TV term. */
+cpx_status cpx_grid_set_optimize_step(cpx_grid* g, int optimize_step);
+
+/* ------------------------------------------------------------------ occupancy */
+/* From the dense density: occupancy per cell ((W-1)(H-1)(D-1) bytes), in-cage flag per
+ * vertex and the in-cage prefix index (0 when not in cage), exactly as pruneScene
+ * (SVRF/SceneUtils.cu:831) and getCagedNums (SVRF/SceneUtils.cu:1081).  Optional host
+ * outputs may be NULL.  The grid stays dense until cpx_grid_make_sparse. */
+cpx_status cpx_occupancy_build(cpx_grid* g, float threshold, uint8_t* occupancy_out,
+                               uint8_t* in_cage_out, uint32_t* index_offsets_out,
+                               uint32_t* in_cage_count_out);
+/* Switch to the sparse layout of the last cpx_occupancy_build: parameters compacted in
+ * z-y-x order of the in-cage flags, optimizer state reset to zero. */
+cpx_status cpx_grid_make_sparse(cpx_grid* g);
+
+/* ------------------------------------------------------------------ rays */
+cpx_status cpx_rays_create(int64_t n_rays, int white_bg, cpx_rays** out);
+cpx_status cpx_rays_destroy(cpx_rays* r);
+/* Rays [offset, offset+count) from host SoA arrays (the 12 input fields of _rays). */
+cpx_status cpx_rays_upload(cpx_rays* r, int64_t offset, int64_t count, const float* ox,
+                           const float* oy, const float* oz, const float* dx, const float* dy,
+                           const float* dz, const float* near_t, const float* far_t,
+                           const uint8_t* gt_mask, const uint8_t* gt_r, const uint8_t* gt_g,
+                           const uint8_t* gt_b, cpx_stream stream);
+/* Rays [offset, offset+count) from one packed host array of 9 32-bit words per ray:
+ * ox, oy, oz, dx, dy, dz, near, far (float) and the ground truth r, g, b, mask bytes
+ * packed little-endian into the ninth word.  One host-to-device copy per call. */
+cpx_status cpx_rays_upload_packed(cpx_rays* r, int64_t offset, int64_t count,
+                                  const uint32_t* packed, cpx_stream stream);
+/* Download any subset of the 17 fields (NULL skips a field). */
+cpx_status cpx_rays_download(const cpx_rays* r, int64_t offset, int64_t count, float* ox,
+                             float* oy, float* oz, float* dx, float* dy, float* dz,
+                             float* near_t, float* far_t, uint8_t* gt_mask, uint8_t* gt_r,
+                             uint8_t* gt_g, uint8_t* gt_b, float* acc_density,
+                             float* acc_weights, float* acc_r, float* acc_g, float* acc_b);
+/* Rays of one camera for the listed pixels (row*img_w+col), written at [offset, offset+n_pix):
+ * getBound + initialRays (SVRF/Rays.cu:22-144) on the device.  Image planes are host
+ * arrays of img_w*img_h bytes; gt_mask may be NULL (treated as 255). */
+cpx_status cpx_rays_init_camera(cpx_rays* r, const cpx_grid* g, const cpx_camera* cam,
+                                int img_w, int img_h, const uint8_t* red, const uint8_t* green,
+                                const uint8_t* blue, const uint8_t* gt_mask,
+                                const int32_t* pixel_index, int64_t n_pix, int64_t offset);
+
+/* ------------------------------------------------------------------ per-batch path */
+/* Batch = rays sample_index_dev[start .. start+len) (identity when NULL).
+ * Forward march: accumulated density, weight and RGB (+white background) per ray. */
+cpx_status cpx_render_forward(cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev,
+                              int start, int len, cpx_stream stream);
+/* Backward: per-ray loss into losses_dev[0..len) and gradients accumulated into the grid. */
+cpx_status cpx_render_backward(cpx_grid* g, cpx_rays* r, double* losses_dev,
+                               const int32_t* sample_index_dev, int start, int len,
+                               double mask_coef, float huber_delta, cpx_stream stream);
+/* Forward and backward of one batch in one pass over the samples (same results as the
+ * two calls above in sequence). */
+cpx_status cpx_render_forward_backward(cpx_grid* g, cpx_rays* r, double* losses_dev,
+                                       const int32_t* sample_index_dev, int start, int len,
+                                       double mask_coef, float huber_delta, cpx_stream stream);
+/* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,
+ * type 2 both. */
+cpx_status cpx_tv_grad(cpx_grid* g, double lam_density, double lam_sh, int type,
+                       int neighbours, cpx_stream stream);
+/* Adam over every active vertex (beta 0.9/0.999, eps 1e-6), density clamped at 0,
+ * gradients zeroed. */
+cpx_status cpx_adam_step(cpx_grid* g, double lr, double sh_lr, int timestep, cpx_stream stream);
+/* TV type 0 (6 neighbours) fused into the Adam sweep: each vertex record is read once.
+ * Same results as cpx_tv_grad(type 0, 6) followed by cpx_adam_step. */
+cpx_status cpx_tv_adam_step(cpx_grid* g, double lam_density, double lam_sh, double lr,
+                            double sh_lr, int timestep, cpx_stream stream);
+
+/* One training batch as the reference's loop runs it (SVRF/Render.cu:407-500):
+ * forward+backward, TV (when do_tv; fused into Adam for type 0 / 6 neighbours),
+ * Adam at `timestep`.  losses_dev receives the per-ray losses; when mse_out is
+ * non-NULL the losses are reduced on the device to the batch MSE (Utils.cu:311) and
+ * copied to *mse_out (this synchronises the stream). */
+typedef struct cpx_step_args {
+    double mask_coef;
+    float huber_delta;
+    int do_tv;
+    int tv_type;
+    int tv_neighbours;
+    double lam_density;
+    double lam_sh;
+    double lr;
+    double sh_lr;
+    int timestep;
+} cpx_step_args;
+cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev, int start,
+                          int len, const cpx_step_args* args, double* losses_dev,
+                          double* mse_out, cpx_stream stream);
+
+/* Synchronise the grid's work and report (then clear) the sticky device-side errors of
+ * earlier asynchronous calls: CPX_ERR_ITERATION_CAP when a ray's march exceeded its
+ * sample bound, CPX_ERR_INVALID_ARGUMENT when a sample index was out of range. */
+cpx_status cpx_grid_check(cpx_grid* g);
+
+/* Per-ray sample counts of the last forward/backward batch (device int32[len], or a
+ * host copy) -- the march's sample sequence, for bit-exact checks. */
+cpx_status cpx_last_sample_counts(const cpx_grid* g, int32_t* counts_host, int len);
+
+/* Number of kernels this library launched since load (for launch accounting). */
+int64_t cpx_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#endif /* CPX_H */

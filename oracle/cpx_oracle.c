@@ -1,0 +1,861 @@
+/*
+ * cpx_oracle.c -- CPU restatement of the Clear-plenoxels training hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA product path and the
+ * timed CPU baseline.  See cpx_oracle.h for the contract.  Citations are
+ * file:line in the reference project (SVRF = SparseVolumeRadianceField/).
+ *
+ * Parity pins: ray/AABB hits, occupancy and index lists are compared bit for
+ * bit against the reference's own kernels run on a B200 (tests/golden/);
+ * float results that pass through exp/log/pow agree to a few ulp.
+ */
+#include "cpx_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+static unsigned g_contract = ORC_CONTRACT_DEFAULT;
+static int g_threads = 0;
+
+void orc_set_contract_mode(unsigned mode) { g_contract = mode; }
+unsigned orc_get_contract_mode(void) { return g_contract; }
+void orc_set_threads(int n) { g_threads = n; }
+int orc_get_threads(void)
+{
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ---------------------------------------------------------------- helpers */
+
+/* (unsigned int)double as the GPU converts it (cvt.rzi.u32.f64 saturates;
+ * NaN -> 0).  The reference relies on this at RenderUtils.cu:830-833. */
+static inline uint32_t sat_u32(double v)
+{
+    if (!(v > 0.0)) return 0u;              /* negatives, -0, NaN */
+    if (v >= 4294967295.0) return 0xFFFFFFFFu;
+    return (uint32_t)v;
+}
+
+/* getSceneIndex (RenderUtils.cu:3-13): clamp to the grid, z-y-x linear index. */
+static inline int scene_index(int col, int row, int depth, int W, int H, int D)
+{
+    col = col < 0 ? 0 : (col > W - 1 ? W - 1 : col);
+    row = row < 0 ? 0 : (row > H - 1 ? H - 1 : row);
+    depth = depth < 0 ? 0 : (depth > D - 1 ? D - 1 : depth);
+    return depth * W * H + row * W + col;
+}
+
+/* getIndex (SceneUtils.cu:250-260): upper clamp only. */
+static inline int64_t grid_index_upper(int col, int row, int depth, int W, int H, int D)
+{
+    col = col < W ? col : W - 1;
+    row = row < H ? row : H - 1;
+    depth = depth < D ? depth : D - 1;
+    return (int64_t)depth * W * H + (int64_t)row * W + col;
+}
+
+static inline double offset_at(const double* o, int n, int i)
+{
+    return (o && i >= 0 && i < n) ? o[i] : 0.0;
+}
+
+static inline double minf_d(double a, double b) { return a > b ? b : a; }
+static inline double maxf_d(double a, double b) { return a > b ? a : b; }
+
+/* ------------------------------------------------------ R4 activations */
+
+/* density_activation: log(1 + exp(x - 13)) in float (RenderUtils.cu:491-495). */
+float orc_density_activation(float x) { return logf(1.f + expf(x - 13.f)); }
+
+/* density_derivation: 1 / (1 + exp(13 - x)) in float (RenderUtils.cu:497-501). */
+float orc_density_derivation(float x) { return 1.f / (1.f + expf(13.f - x)); }
+
+/* sigmoid: 1 / (1 + exp(-0.1 x)) evaluated in double (RenderUtils.cu:480-483). */
+float orc_sigmoid(float x) { return (float)(1.0 / (1.0 + exp(-0.1 * (double)x))); }
+
+/* sigmoid_derivative: 0.1 s (1 - s) (RenderUtils.cu:485-489). */
+float orc_sigmoid_derivative(float x)
+{
+    float s = orc_sigmoid(x);
+    return (float)(0.1 * (double)s * (double)(1.f - s));
+}
+
+/* ------------------------------------------------------ R5 SH basis */
+
+/* The unnormalised basis the reference uses (RenderUtils.cu:1646-1670); entries
+ * beyond band 2 are kept for completeness. */
+void orc_sh_basis(const float d[3], float shs[25])
+{
+    const float x = d[0], y = d[1], z = d[2];
+    shs[0] = 1.f;
+    shs[1] = y;
+    shs[2] = z;
+    shs[3] = x;
+    shs[4] = x * y;
+    shs[5] = y * z;
+    shs[6] = fmaf(3.f * z, z, -1.f);
+    shs[7] = x * z;
+    shs[8] = fmaf(x, x, -(y * y));
+    shs[9] = y * (fmaf(3.f * x, x, -(y * y)));
+    shs[10] = x * y * z;
+    shs[11] = y * (fmaf(5.f * z, z, -1.f));
+    shs[12] = fmaf(5.f * z * z, z, -(3.f * z));
+    shs[13] = x * (fmaf(5.f * z, z, -1.f));
+    shs[14] = (fmaf(x, x, -(y * y))) * z;
+    shs[15] = x * (fmaf(x, x, -(3.f * y * y)));
+    shs[16] = x * y * (fmaf(x, x, -(y * y)));
+    shs[17] = y * (fmaf(3.f * x, x, -(y * y))) * z;
+    shs[18] = x * y * (fmaf(7.f * z, z, -1.f));
+    shs[19] = y * (fmaf(7.f * z * z, z, -(3.f * z)));
+    shs[20] = fmaf(35.f * z * z * z, z, -(30.f * z * z)) + 3.f;
+    shs[21] = x * (fmaf(7.f * z * z, z, -(3.f * z)));
+    shs[22] = (float)((double)fmaf(x, x, -(y * y)) * ((double)(7.f * z * z) - 1.0));
+    shs[23] = x * (fmaf(x, x, -(3.f * y * y))) * z;
+    shs[24] = x * x * (fmaf(x, x, -(3.f * y * y))) - y * y * (fmaf(3.f * x, x, -(y * y)));
+}
+
+/* ------------------------------------------------------ R1 rays */
+
+/* getBound (Rays.cu:22-75) + initialRays (Rays.cu:77-144) for one pixel list. */
+void orc_rays_from_camera(const double* alpha, const double* principle,
+                          const double* c2w, const double* centre, const int* bbox,
+                          int img_w, const uint8_t* red, const uint8_t* green,
+                          const uint8_t* blue, const uint8_t* mask, int white_bg,
+                          const int* pix_index, int n_pix, orc_rays* out, int64_t out_start)
+{
+    for (int i = 0; i < n_pix; i++) {
+        const int pixel = pix_index[i];
+        const int row = pixel / img_w;
+        const int col = pixel % img_w;
+
+        float xin[4];
+        xin[0] = (float)(((double)col + 0.5 - principle[0]) / alpha[0]);
+        xin[1] = (float)(((double)row + 0.5 - principle[1]) / alpha[1]);
+        xin[2] = 1.0f;
+        xin[3] = 1.0f;
+
+        float sp[4];
+        for (int rr = 0; rr < 4; rr++) {
+            sp[rr] = 0.f;
+            for (int cc = 0; cc < 4; cc++) {
+                if (g_contract & ORC_CONTRACT_RAYDIR)
+                    sp[rr] = (float)fma(c2w[rr * 4 + cc], (double)xin[cc], (double)sp[rr]);
+                else
+                    sp[rr] = (float)((double)sp[rr] + c2w[rr * 4 + cc] * (double)xin[cc]);
+            }
+            sp[rr] = (float)((double)sp[rr] - centre[rr]);
+        }
+
+        /* normalizePoint (Rays.cu:13-20): float sum of squares, double sqrt. */
+        float fs;
+        if (g_contract & ORC_CONTRACT_NORM_P0)
+            fs = fmaf(sp[2], sp[2], fmaf(sp[0], sp[0], sp[1] * sp[1]));
+        else if (g_contract & ORC_CONTRACT_NORM_P1)
+            fs = fmaf(sp[2], sp[2], fmaf(sp[1], sp[1], sp[0] * sp[0]));
+        else
+            fs = (sp[0] * sp[0] + sp[1] * sp[1]) + sp[2] * sp[2];
+        double sum = sqrt((double)fs);
+        sp[0] = (float)((double)sp[0] / sum);
+        sp[1] = (float)((double)sp[1] / sum);
+        sp[2] = (float)((double)sp[2] / sum);
+
+        double t[6] = {
+            ((double)bbox[1] - centre[0]) / (double)sp[0],
+            ((double)bbox[0] - centre[0]) / (double)sp[0],
+            ((double)bbox[3] - centre[1]) / (double)sp[1],
+            ((double)bbox[2] - centre[1]) / (double)sp[1],
+            ((double)bbox[5] - centre[2]) / (double)sp[2],
+            ((double)bbox[4] - centre[2]) / (double)sp[2],
+        };
+        double t_min = minf_d(t[0], t[1]);
+        double t_max = maxf_d(t[0], t[1]);
+        t_min = maxf_d(t_min, minf_d(t[2], t[3]));
+        t_max = minf_d(t_max, maxf_d(t[2], t[3]));
+        t_min = maxf_d(t_min, minf_d(t[4], t[5]));
+        t_max = minf_d(t_max, maxf_d(t[4], t[5]));
+
+        const int64_t ri = out_start + i;
+        out->ox[ri] = (float)centre[0];
+        out->oy[ri] = (float)centre[1];
+        out->oz[ri] = (float)centre[2];
+        out->near_t[ri] = (float)t_min;
+        out->far_t[ri] = (float)t_max;
+        out->dx[ri] = sp[0];
+        out->dy[ri] = sp[1];
+        out->dz[ri] = sp[2];
+        const uint8_t m = mask ? mask[pixel] : 255;
+        out->mask[ri] = m;
+        if (white_bg) {
+            /* u8(r*m/255.f + 255 - m) (Rays.cu:128-133) */
+            out->r[ri] = (uint8_t)((float)(red[pixel] * m) / 255.f + 255.f - (float)m);
+            out->g[ri] = (uint8_t)((float)(green[pixel] * m) / 255.f + 255.f - (float)m);
+            out->b[ri] = (uint8_t)((float)(blue[pixel] * m) / 255.f + 255.f - (float)m);
+        } else {
+            out->r[ri] = red[pixel];
+            out->g[ri] = green[pixel];
+            out->b[ri] = blue[pixel];
+        }
+    }
+}
+
+/* ------------------------------------------------------ R6 trilinear */
+
+static inline int n_active_sh(const orc_scene* s) { return (s->band + 1) * (s->band + 1); }
+
+/* Corner offsets in the reference's visiting order (RenderUtils.cu:855-990). */
+static const int k_corner[8][3] = {
+    {0, 0, 0}, {0, 1, 0}, {1, 0, 0}, {1, 1, 0},
+    {0, 0, 1}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1},
+};
+
+static inline double corner_weight(int q, double x, double y, double z)
+{
+    switch (q) {
+    case 0: return (1. - x) * (1. - y) * (1. - z);
+    case 1: return (1. - x) * y * (1. - z);
+    case 2: return x * (1. - y) * (1. - z);
+    case 3: return x * y * (1. - z);
+    case 4: return (1. - x) * (1. - y) * z;
+    case 5: return (1. - x) * y * z;
+    case 6: return x * (1. - y) * z;
+    default: return x * y * z;
+    }
+}
+
+/* Sample position (RenderUtils.cu:1676-1678). */
+static inline void sample_position(const orc_scene* s, const orc_rays* r, int ri, double t,
+                                   int intT, double bc[3])
+{
+    const double o[3] = {(double)r->ox[ri], (double)r->oy[ri], (double)r->oz[ri]};
+    const double d[3] = {(double)r->dx[ri], (double)r->dy[ri], (double)r->dz[ri]};
+    const double off[3] = {offset_at(s->off_x, s->n_off, intT),
+                           offset_at(s->off_y, s->n_off, intT),
+                           offset_at(s->off_z, s->n_off, intT)};
+    for (int a = 0; a < 3; a++) {
+        if (g_contract & ORC_CONTRACT_POS)
+            bc[a] = fma(t, d[a], o[a]) + off[a];
+        else
+            bc[a] = (o[a] + t * d[a]) + off[a];
+    }
+}
+
+/* Cell index of a sample, -1 when the sparse occupancy says skip. */
+static inline int occupied(const orc_scene* s, const uint32_t bi[3])
+{
+    if (!s->sparse) return 1;
+    int ci = scene_index((int)bi[0], (int)bi[1], (int)bi[2], s->W - 1, s->H - 1, s->D - 1);
+    return s->occ[ci] != 0;
+}
+
+static inline int64_t corner_index(const orc_scene* s, const uint32_t bi[3], int q)
+{
+    int idx = scene_index((int)(bi[0] + (uint32_t)k_corner[q][0]),
+                          (int)(bi[1] + (uint32_t)k_corner[q][1]),
+                          (int)(bi[2] + (uint32_t)k_corner[q][2]), s->W, s->H, s->D);
+    if (s->sparse) return (int64_t)s->index_offsets[(uint32_t)idx];
+    return (int64_t)(uint32_t)idx;
+}
+
+/* trilerpRGB (RenderUtils.cu:826-1004): raw density and raw colours. */
+static int trilerp_rgb(const orc_scene* s, const double bc[3], const float* shs, float tri[4])
+{
+    uint32_t bi[3] = {sat_u32(bc[0]), sat_u32(bc[1]), sat_u32(bc[2])};
+    if (!occupied(s, bi)) return 0;
+    const double x = bc[0] - (double)bi[0];
+    const double y = bc[1] - (double)bi[1];
+    const double z = bc[2] - (double)bi[2];
+    const int nsh = n_active_sh(s);
+    const int64_t n = s->n_act;
+    const float* rho = s->params;
+    float sh_tri[75];
+    for (int i = 0; i < s->sh_dim * 3; i++) sh_tri[i] = 0.f;
+    tri[0] = tri[1] = tri[2] = tri[3] = 0.f;
+    for (int q = 0; q < 8; q++) {
+        const int64_t idx = corner_index(s, bi, q);
+        const double c = corner_weight(q, x, y, z);
+        tri[0] = (float)fma(c, (double)rho[idx], (double)tri[0]);
+        for (int i = 0; i < nsh; i++) {
+            for (int ch = 0; ch < 3; ch++) {
+                const float* a = s->params + (int64_t)(1 + ch * s->sh_dim + i) * n;
+                sh_tri[ch * s->sh_dim + i] =
+                    (float)fma(c, (double)a[idx], (double)sh_tri[ch * s->sh_dim + i]);
+            }
+        }
+    }
+    for (int ch = 0; ch < 3; ch++) {
+        float acc = 0.f;
+        for (int i = 0; i < nsh; i++) acc = fmaf(sh_tri[ch * s->sh_dim + i], shs[i], acc);
+        tri[1 + ch] = acc;
+    }
+    return 1;
+}
+
+/* accumulatedDensity += sigma * stepSize (RenderUtils.cu:1701). */
+static inline double accd_add(double accd, float sigma, float step)
+{
+    if (g_contract & ORC_CONTRACT_ACCD) return fma((double)sigma, (double)step, accd);
+    return accd + (double)(sigma * step);
+}
+
+/* ------------------------------------------------------ R7 forward */
+
+static void forward_ray(const orc_scene* s, orc_rays* r, int ri, int* count)
+{
+    r->acc_den[ri] = 0.f;
+    r->acc_w[ri] = 0.f;
+    r->acc_r[ri] = 0.f;
+    r->acc_g[ri] = 0.f;
+    r->acc_b[ri] = 0.f;
+    int n = 0;
+    if (r->near_t[ri] > r->far_t[ri]) { /* RenderUtils.cu:1943-1946: no background */
+        if (count) *count = 0;
+        return;
+    }
+    const float dir[3] = {r->dx[ri], r->dy[ri], r->dz[ri]};
+    float shs[25];
+    orc_sh_basis(dir, shs);
+    double t = (double)r->near_t[ri];
+    const double far_t = (double)r->far_t[ri];
+    double acc = 0., accd = 0.;
+    float tri[4];
+    int intT = 0;
+    float acc_den = 0.f, acc_r = 0.f, acc_g = 0.f, acc_b = 0.f;
+    while (t < far_t) {
+        double bc[3];
+        sample_position(s, r, ri, t, intT, bc);
+        if (!trilerp_rgb(s, bc, shs, tri)) {
+            t += (double)s->step;
+            ++intT;
+            continue;
+        }
+        const float sigma = orc_density_activation(tri[0]);
+        const float c0 = orc_sigmoid(tri[1]);
+        const float c1 = orc_sigmoid(tri[2]);
+        const float c2 = orc_sigmoid(tri[3]);
+        const double Ti = exp(-accd);
+        const double w = Ti * (1. - (double)expf(-sigma * s->step));
+        acc += w;
+        acc_den += sigma;
+        acc_r = (float)fma(w, (double)c0, (double)acc_r);
+        acc_g = (float)fma(w, (double)c1, (double)acc_g);
+        acc_b = (float)fma(w, (double)c2, (double)acc_b);
+        accd = accd_add(accd, sigma, s->step);
+        t += fabs((double)s->step - w);
+        ++intT;
+        ++n;
+    }
+    r->acc_den[ri] = acc_den;
+    r->acc_w[ri] = (float)acc;
+    if (r->white_bg) {
+        acc_r = (float)((double)acc_r + (1. - acc));
+        acc_g = (float)((double)acc_g + (1. - acc));
+        acc_b = (float)((double)acc_b + (1. - acc));
+    }
+    r->acc_r[ri] = acc_r;
+    r->acc_g[ri] = acc_g;
+    r->acc_b[ri] = acc_b;
+    if (count) *count = n;
+}
+
+void orc_render_forward(const orc_scene* s, orc_rays* r, const int* sample_index, int start,
+                        int len, int* counts)
+{
+#pragma omp parallel for schedule(dynamic, 16) num_threads(orc_get_threads())
+    for (int tid = 0; tid < len; tid++) {
+        const int ri = sample_index ? sample_index[tid + start] : tid + start;
+        forward_ray(s, r, ri, counts ? &counts[tid] : NULL);
+    }
+}
+
+/* ------------------------------------------------------ R8 backward */
+
+static inline void grad_add(double* p, double v)
+{
+#pragma omp atomic
+    *p += v;
+}
+
+/* trilerpGradientsRGB (RenderUtils.cu:1074-1364): scatter one sample. */
+static void scatter_sample(const orc_scene* s, const double bc[3], const float* shs,
+                           const float g[4], double* grad)
+{
+    uint32_t bi[3] = {sat_u32(bc[0]), sat_u32(bc[1]), sat_u32(bc[2])};
+    const double x = bc[0] - (double)bi[0];
+    const double y = bc[1] - (double)bi[1];
+    const double z = bc[2] - (double)bi[2];
+    if (!occupied(s, bi)) return;
+    const int64_t n = s->n_act;
+    for (int q = 0; q < 8; q++) {
+        const int64_t idx = corner_index(s, bi, q);
+        const double c = corner_weight(q, x, y, z);
+        grad_add(&grad[idx], (double)(float)((double)g[0] * c));
+        for (int ch = 0; ch < 3; ch++) {
+            int startk = ch * s->sh_dim + 1;
+            int endk = startk + s->sh_dim;
+            int shIdx = 0;
+            if (s->hierarchy) {
+                startk += s->band * s->band;
+                endk -= (s->sh_dim - (s->band + 1) * (s->band + 1));
+                shIdx += s->band * s->band;
+            }
+            for (int k = startk; k < endk; k++) {
+                const float v = (float)((double)g[1 + ch] * c * (double)shs[shIdx]);
+                grad_add(&grad[(int64_t)k * n + idx], (double)v);
+                ++shIdx;
+            }
+        }
+    }
+}
+
+static void backward_ray(const orc_scene* s, const orc_rays* r, int tid, int ri,
+                         double mask_coef, float huber, double* losses, double* grad, int* count)
+{
+    const float dir[3] = {r->dx[ri], r->dy[ri], r->dz[ri]};
+    float shs[25];
+    orc_sh_basis(dir, shs);
+    int n = 0;
+    if (r->near_t[ri] > r->far_t[ri]) {
+        losses[tid] = 0.;
+        if (count) *count = 0;
+        return;
+    }
+    double res[3] = {
+        (double)r->acc_r[ri] - (double)r->r[ri] / 255.,
+        (double)r->acc_g[ri] - (double)r->g[ri] / 255.,
+        (double)r->acc_b[ri] - (double)r->b[ri] / 255.,
+    };
+    losses[tid] = (fabs(res[0]) + fabs(res[1]) + fabs(res[2])) * 255. / 3.;
+    if (isnan(losses[tid])) {
+        losses[tid] = 255.;
+        if (count) *count = 0;
+        return;
+    }
+    const double hd = (double)huber;
+    for (int i = 0; i < 3; i++) {
+        if (res[i] > hd)
+            res[i] = fma(-(0.5 * hd), hd, hd);
+        else if (res[i] < -hd)
+            res[i] = fma(0.5 * hd, hd, -hd);
+    }
+    double t = (double)r->near_t[ri];
+    const double far_t = (double)r->far_t[ri];
+    double accd = 0., accw = 0.;
+    double acc_rgb[3] = {0., 0., 0.};
+    float tri[4], act[4], g[4];
+    float mask_loss = 0.f;
+    const float accw_f = r->acc_w[ri];
+    if (r->mask[ri] && accw_f < 1.) {
+        mask_loss = (float)(((double)r->mask[ri] / 255.0 - (double)accw_f) * mask_coef);
+    }
+    float wpre = (float)maxf_d(1e-6, (double)accw_f);
+    wpre = (float)minf_d(1 - 1e-6, (double)wpre);
+    mask_loss = (float)fma((double)logf(wpre) - log(1. - (double)wpre), 1e-3, (double)mask_loss);
+    int intT = 0;
+    const double pred[3] = {(double)r->acc_r[ri], (double)r->acc_g[ri], (double)r->acc_b[ri]};
+    while (t < far_t) {
+        double bc[3];
+        sample_position(s, r, ri, t, intT, bc);
+        if (!trilerp_rgb(s, bc, shs, tri)) {
+            t += (double)s->step;
+            ++intT;
+            continue;
+        }
+        act[0] = orc_density_activation(tri[0]);
+        act[1] = orc_sigmoid(tri[1]);
+        act[2] = orc_sigmoid(tri[2]);
+        act[3] = orc_sigmoid(tri[3]);
+        double Ti = exp(-accd);
+        const double w = Ti * (1. - (double)expf(-act[0] * s->step));
+        accw += w;
+        for (int c = 0; c < 3; c++) acc_rgb[c] = fma(w, (double)act[1 + c], acc_rgb[c]);
+        for (int c = 0; c < 3; c++)
+            g[1 + c] = (float)((double)0.6667f * w * res[c] * (double)orc_sigmoid_derivative(tri[1 + c]));
+        accd = accd_add(accd, act[0], s->step);
+        Ti = exp(-accd);
+        g[0] = (float)(res[0] * fma(Ti, (double)act[1], -(pred[0] - acc_rgb[0])));
+        g[0] = (float)fma(res[1], fma(Ti, (double)act[2], -(pred[1] - acc_rgb[1])), (double)g[0]);
+        g[0] = (float)fma(res[2], fma(Ti, (double)act[3], -(pred[2] - acc_rgb[2])), (double)g[0]);
+        const float dd = orc_density_derivation(tri[0]);
+        g[0] = (float)((double)g[0] * (0.6667 * (double)s->step * (double)dd));
+        g[0] = (float)fma((double)(s->step * dd) * (((double)accw_f - accw) - Ti), (double)mask_loss,
+                          (double)g[0]);
+        scatter_sample(s, bc, shs, g, grad);
+        t += fabs((double)s->step - w);
+        ++intT;
+        ++n;
+    }
+    if (count) *count = n;
+}
+
+void orc_render_backward(const orc_scene* s, const orc_rays* r, const int* sample_index,
+                         int start, int len, double mask_coef, float huber_delta,
+                         double* losses, double* grad, int* counts)
+{
+#pragma omp parallel for schedule(dynamic, 16) num_threads(orc_get_threads())
+    for (int tid = 0; tid < len; tid++) {
+        const int ri = sample_index ? sample_index[tid + start] : tid + start;
+        backward_ray(s, r, tid, ri, mask_coef, huber_delta, losses, grad,
+                     counts ? &counts[tid] : NULL);
+    }
+}
+
+/* ------------------------------------------------------ R9 TV */
+
+/* getNeighboorGridIndexes (RenderUtils.cu:2549-2575). */
+static void neighbour_indexes(const orc_scene* s, int cx, int cy, int cz, uint32_t res[27])
+{
+    for (int dz = -1; dz < 2; dz++)
+        for (int dy = -1; dy < 2; dy++)
+            for (int dx = -1; dx < 2; dx++) {
+                uint32_t v = (uint32_t)scene_index(cx + dx, cy + dy, cz + dz, s->W, s->H, s->D);
+                if (s->sparse) v = s->index_offsets[v];
+                res[(dz + 1) * 9 + (dy + 1) * 3 + dx + 1] = v;
+            }
+}
+
+/* One TV term (RenderUtils.cu:2755-2757): grad += coef / (sd + 1e-6) * disparity. */
+static inline float tv_apply(float g, double coef, float sd, float disparity)
+{
+    return (float)fma(coef / ((double)sd + 1.e-6), (double)disparity, (double)g);
+}
+
+/* Six-neighbour term for one parameter array (RenderUtils.cu:2663-2757). */
+static float tv6_value(const float* a, const uint32_t* ix, double coef, float g)
+{
+    static const int nb[6] = {4, 10, 12, 14, 16, 22};
+    const float self = a[ix[13]];
+    float sum = 0.f, disp = 0.f;
+    for (int j = 0; j < 6; j++) {
+        const float nv = ix[nb[j]] != 0 ? a[ix[nb[j]]] : self;
+        const float d = self - nv;
+        sum = fmaf(d, d, sum);
+        disp = (j == 0) ? d : disp + d;
+    }
+    sum = sqrtf(sum) / 6.f;
+    return tv_apply(g, coef, sum, disp);
+}
+
+static void tv_type0(const orc_scene* s, float* grad, double lam_d, double lam_sh, int nbrs)
+{
+    const int W = s->W, H = s->H, D = s->D;
+    const int64_t n = s->n_act;
+    const int startSH = s->hierarchy ? s->band * s->band : 0;
+    const int endSH = (s->band + 1) * (s->band + 1);
+#pragma omp parallel for schedule(static) num_threads(orc_get_threads())
+    for (int pos = 0; pos < W * H; pos++) {
+        const int row = pos / W, col = pos % W;
+        if (row == 0 || row == H - 1 || col == 0 || col == W - 1) continue;
+        uint32_t ix[27];
+        if (nbrs == 3) {
+            /* RenderUtils.cu:2606-2661 (depth from 0; disparity keeps the last term) */
+            for (int depth = 0; depth < D - 1; depth++) {
+                neighbour_indexes(s, col, row, depth, ix);
+                if (s->sparse && !s->in_cage[ix[13]]) continue;
+                {
+                    const float* a = s->params;
+                    const float self = a[ix[13]];
+                    float sum = 0.f;
+                    const float n14 = ix[14] != 0 ? a[ix[14]] : self;
+                    sum = fmaf(self - n14, self - n14, sum);
+                    const float n16 = ix[16] != 0 ? a[ix[16]] : self;
+                    sum = fmaf(self - n16, self - n16, sum);
+                    const float n22 = ix[22] != 0 ? a[ix[22]] : self;
+                    const float disp = self - n22;
+                    sum = fmaf(self - n22, self - n22, sum);
+                    sum = sqrtf(sum) / 3.f;
+                    grad[ix[13]] = tv_apply(grad[ix[13]], lam_d, sum, disp);
+                }
+                for (int ch = 0; ch < 3; ch++)
+                    for (int k = ch * s->sh_dim + startSH; k < ch * s->sh_dim + endSH; k++) {
+                        const float* a = s->params + (int64_t)(1 + k) * n;
+                        float* gk = grad + (int64_t)(1 + k) * n;
+                        const float self = a[ix[13]];
+                        float sum = 0.f;
+                        const float n14 = ix[14] != 0 ? a[ix[14]] : self;
+                        sum = fmaf(self - n14, self - n14, sum);
+                        const float n16 = ix[16] != 0 ? a[ix[16]] : self;
+                        sum = fmaf(self - n16, self - n16, sum);
+                        const float n22 = ix[4] != 0 ? a[ix[22]] : self;
+                        const float disp = self - n22;
+                        sum = fmaf(self - n22, self - n22, sum);
+                        sum = sqrtf(sum) / 3.f;
+                        gk[ix[13]] = tv_apply(gk[ix[13]], lam_sh, sum, disp);
+                    }
+            }
+        } else if (nbrs == 6) {
+            for (int depth = 1; depth < D - 1; depth++) {
+                neighbour_indexes(s, col, row, depth, ix);
+                if (s->sparse && !s->in_cage[ix[13]]) continue;
+                grad[ix[13]] = tv6_value(s->params, ix, lam_d, grad[ix[13]]);
+                for (int ch = 0; ch < 3; ch++)
+                    for (int k = ch * s->sh_dim + startSH; k < ch * s->sh_dim + endSH; k++) {
+                        const float* a = s->params + (int64_t)(1 + k) * n;
+                        float* gk = grad + (int64_t)(1 + k) * n;
+                        gk[ix[13]] = tv6_value(a, ix, lam_sh, gk[ix[13]]);
+                    }
+            }
+        } else {
+            /* 26 neighbours (RenderUtils.cu:2766-2812).  The SH disparity always reads
+             * slot 4 of the neighbour array, which for the first four neighbours still
+             * holds the previous array's value (density for the first SH array). */
+            for (int depth = 1; depth < D - 1; depth++) {
+                neighbour_indexes(s, col, row, depth, ix);
+                if (s->sparse && !s->in_cage[ix[13]]) continue;
+                float slot4 = 0.f;
+                {
+                    const float* a = s->params;
+                    const float self = a[ix[13]];
+                    float sum = 0.f, disp = 0.f;
+                    for (int j = 0; j < 27; j++) {
+                        if (j == 13) continue;
+                        const float nv = ix[j] != 0 ? a[ix[j]] : self;
+                        if (j == 4) slot4 = nv;
+                        sum = fmaf(self - nv, self - nv, sum);
+                        disp += self - nv;
+                    }
+                    sum = sqrtf(sum) / 26.f;
+                    grad[ix[13]] = tv_apply(grad[ix[13]], lam_d, sum, disp);
+                }
+                for (int ch = 0; ch < 3; ch++)
+                    for (int k = ch * s->sh_dim + startSH; k < ch * s->sh_dim + endSH; k++) {
+                        const float* a = s->params + (int64_t)(1 + k) * n;
+                        float* gk = grad + (int64_t)(1 + k) * n;
+                        const float self = a[ix[13]];
+                        float sum = 0.f, disp = 0.f;
+                        for (int j = 0; j < 27; j++) {
+                            if (j == 13) continue;
+                            const float nv = ix[j] != 0 ? a[ix[j]] : self;
+                            if (j == 4) slot4 = nv;
+                            sum = fmaf(self - nv, self - nv, sum);
+                            disp += self - slot4;
+                        }
+                        sum = sqrtf(sum) / 26.f;
+                        gk[ix[13]] = tv_apply(gk[ix[13]], lam_sh, sum, disp);
+                    }
+            }
+        }
+    }
+}
+
+/* getVoxelGridIndexes (RenderUtils.cu:2442-2467). */
+static void cell_corner_indexes(const orc_scene* s, int qx, int qy, int qz, uint32_t res[8])
+{
+    for (int dz = 0; dz < 2; dz++)
+        for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+                uint32_t v = (uint32_t)scene_index(qx + dx, qy + dy, qz + dz, s->W, s->H, s->D);
+                if (s->sparse) v = s->index_offsets[v];
+                res[dz * 4 + dy * 2 + dx] = v;
+            }
+}
+
+/* Voxel-disparity term, VarianceType 1 (RenderUtils.cu:2469-2547).  The reference
+ * updates shared corners with unsynchronised += from neighbouring threads; the
+ * oracle applies every update once, in column order (the race-free sum). */
+static void tv_type1(const orc_scene* s, float* grad, double lam_d, double lam_sh)
+{
+    const int W = s->W, H = s->H, D = s->D;
+    const int64_t n = s->n_act;
+    const int startSH = s->hierarchy ? s->band * s->band : 0;
+    const int endSH = (s->band + 1) * (s->band + 1);
+    for (int pos = 0; pos < (W - 1) * (H - 1); pos++) {
+        const int row = pos / (W - 1), col = pos % (W - 1);
+        uint32_t ix[8];
+        for (int depth = 0; depth < D - 1; depth++) {
+            const int vi = scene_index(col, row, depth, W - 1, H - 1, D - 1);
+            if (s->sparse && !s->occ[vi]) continue;
+            cell_corner_indexes(s, col, row, depth, ix);
+            if (s->optimize_step <= 1) {
+                float mean[3][25];
+                for (int k = startSH; k < endSH; k++) mean[0][k] = mean[1][k] = mean[2][k] = 0.f;
+                for (int i = 0; i < 8; i++)
+                    for (int k = startSH; k < endSH; k++)
+                        for (int ch = 0; ch < 3; ch++) {
+                            const float* a = s->params + (int64_t)(1 + ch * s->sh_dim + k) * n;
+                            mean[ch][k] += a[ix[i]] / 8.f;
+                        }
+                for (int i = 0; i < 8; i++)
+                    for (int k = startSH; k < endSH; k++)
+                        for (int ch = 0; ch < 3; ch++) {
+                            const int64_t arr = 1 + (int64_t)s->sh_dim * ch + k;
+                            const float* a = s->params + arr * n;
+                            float* gk = grad + arr * n;
+                            gk[ix[i]] = (float)fma(lam_sh, (double)(a[ix[i]] - mean[ch][k]),
+                                                   (double)gk[ix[i]]);
+                        }
+            }
+            float sum = 0.f;
+            for (int i = 0; i < 8; i++) sum += s->params[ix[i]];
+            sum /= 8.f;
+            for (int i = 0; i < 8; i++)
+                grad[ix[i]] = (float)fma(lam_d, (double)(s->params[ix[i]] - sum), (double)grad[ix[i]]);
+        }
+    }
+}
+
+void orc_tv_grad(const orc_scene* s, float* grad, double lam_density, double lam_sh, int type,
+                 int nbrs)
+{
+    if (type == 0) {
+        tv_type0(s, grad, lam_density, lam_sh, nbrs);
+    } else if (type == 1) {
+        tv_type1(s, grad, lam_density, lam_sh);
+    } else if (type == 2) {
+        tv_type0(s, grad, lam_density, lam_sh, nbrs);
+        tv_type1(s, grad, lam_density, lam_sh);
+    }
+}
+
+/* ------------------------------------------------------ R10 Adam */
+
+void orc_adam(orc_scene* s, float* grad, float* m, float* v, double lr, double sh_lr,
+              int timestep)
+{
+    const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
+    const int64_t n = s->n_act;
+    const double bc1 = 1. - (double)powf(beta1, (float)timestep);
+    const double bc2 = 1. - (double)powf(beta2, (float)timestep);
+#pragma omp parallel for schedule(static) num_threads(orc_get_threads())
+    for (int64_t p = 0; p < n; p++) {
+        double lr_p = lr;
+        if (!s->sparse && s->adaptive_lr) lr_p = lr * (double)s->adaptive_lr[p];
+        {
+            const float g = grad[p];
+            m[p] = (float)fma(1. - (double)beta1, (double)g, (double)(beta1 * m[p]));
+            v[p] = (float)fma((1. - (double)beta2) * (double)g, (double)g, (double)(beta2 * v[p]));
+            const float cm = (float)((double)m[p] / bc1);
+            const float cv = (float)((double)v[p] / bc2);
+            const double temp = (double)s->params[p] - lr_p * (double)cm / (double)(sqrtf(cv) + eps);
+            s->params[p] = temp < 0. ? 0.f : (float)temp;
+            grad[p] = 0.f;
+        }
+        for (int ch = 0; ch < 3; ch++) {
+            int startk = ch * s->sh_dim + 1;
+            int endk = startk + s->sh_dim;
+            if (s->hierarchy) {
+                startk += s->band * s->band;
+                endk -= (s->sh_dim - (s->band + 1) * (s->band + 1));
+            }
+            for (int k = startk; k < endk; k++) {
+                const int64_t e = (int64_t)k * n + p;
+                const float g = grad[e];
+                m[e] = (float)fma(1. - (double)beta1, (double)g, (double)(beta1 * m[e]));
+                v[e] = (float)fma((1. - (double)beta2) * (double)g, (double)g, (double)(beta2 * v[e]));
+                const float cm = (float)((double)m[e] / bc1);
+                const float cv = (float)((double)v[e] / bc2);
+                s->params[e] = (float)((double)s->params[e] - sh_lr * (double)cm / (double)(sqrtf(cv) + eps));
+                grad[e] = 0.f;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------ R3 occupancy */
+
+/* occupiedVoxel (SceneUtils.cu:800-829): any corner density strictly above thresh. */
+static int occupied_voxel(const float* dens, int W, int H, int D, int x, int y, int z, float thr)
+{
+    for (int dz = 0; dz <= 1; dz++)
+        for (int dy = 0; dy <= 1; dy++)
+            for (int dx = 0; dx <= 1; dx++)
+                if (dens[grid_index_upper(x + dx, y + dy, z + dz, W, H, D)] > thr) return 1;
+    return 0;
+}
+
+uint32_t orc_occupancy(const float* density, int W, int H, int D, float threshold,
+                       uint8_t* occ, uint8_t* in_cage, uint32_t* index_offsets,
+                       int64_t* dropped_writes)
+{
+    const int64_t N = (int64_t)W * H * D;
+    int64_t dropped = 0;
+    memset(in_cage, 0, (size_t)N);
+    /* pruneScene (SceneUtils.cu:831-881) */
+    for (int row = 0; row < H - 1; row++)
+        for (int col = 0; col < W - 1; col++)
+            for (int depth = 0; depth < D - 1; depth++) {
+                const int64_t ci = (int64_t)depth * (W - 1) * (H - 1) + (int64_t)row * (W - 1) + col;
+                if (!occupied_voxel(density, W, H, D, col, row, depth, threshold)) {
+                    occ[ci] = 0;
+                    continue;
+                }
+                occ[ci] = 1;
+                in_cage[(int64_t)depth * W * H + (int64_t)row * W + col] = 1;
+                if (depth == D - 2) in_cage[(int64_t)(D - 1) * W * H + (int64_t)row * W + col] = 1;
+                if (row == H - 2) in_cage[(int64_t)depth * W * H + (int64_t)(H - 1) * W + col] = 1;
+                if (col == W - 2) {
+                    /* the reference writes depth*W*H + H*W + col + 1 here (SceneUtils.cu:872) */
+                    const int64_t v = (int64_t)depth * W * H + (int64_t)H * W + col + 1;
+                    if (v < N) in_cage[v] = 1;
+                    else dropped++;
+                }
+            }
+    /* getCagedNums (SceneUtils.cu:1081-1120) */
+    uint32_t k = 0;
+    for (int64_t v = 0; v < N; v++) index_offsets[v] = in_cage[v] ? k++ : 0u;
+    if (dropped_writes) *dropped_writes = dropped;
+    return k;
+}
+
+void orc_compact(const float* dense, int n_arrays, int64_t n_dense, const uint8_t* in_cage,
+                 float* compact, int64_t n_compact)
+{
+    int64_t c = 0;
+    for (int64_t v = 0; v < n_dense && c < n_compact; v++) {
+        if (!in_cage[v]) continue;
+        for (int a = 0; a < n_arrays; a++) compact[(int64_t)a * n_compact + c] = dense[(int64_t)a * n_dense + v];
+        c++;
+    }
+}
+
+/* ------------------------------------------------------ R11 */
+
+double orc_mse(const double* losses, int n)
+{
+    double res = 0.0;
+    for (int i = 0; i < n; i++) res += losses[i] * losses[i];
+    return res / n;
+}
+
+/* ------------------------------------------------------ testRender KAT */
+
+void orc_composite_kat(const double* opacity, const double* colour, int n, const double* gt,
+                       double* render_res, double* weights, double* opacity_grad,
+                       double* colour_grad)
+{
+    double acc_op = 0., Ti;
+    for (int c = 0; c < 3; c++) render_res[c] = 0.;
+    for (int i = 0; i < n; i++) {
+        Ti = exp(-acc_op);
+        weights[i] = Ti * (1. - exp(-opacity[i] * 1.));
+        acc_op += opacity[i] * 1.;
+        for (int c = 0; c < 3; c++) render_res[c] += weights[i] * colour[c * n + i];
+    }
+    double acc_rr[3] = {0., 0., 0.};
+    acc_op = 0.;
+    for (int i = 0; i < n; i++) {
+        opacity_grad[i] = 0.;
+        for (int c = 0; c < 3; c++) colour_grad[c * n + i] = 0.;
+    }
+    for (int i = 0; i < n; i++) {
+        Ti = exp(-acc_op);
+        weights[i] = Ti * (1. - exp(-opacity[i] * 1.));
+        acc_op += opacity[i] * 1.;
+        for (int c = 0; c < 3; c++) {
+            acc_rr[c] += weights[i] * colour[c * n + i];
+            colour_grad[c * n + i] += 0.667 * (render_res[c] - gt[c]) * weights[i];
+        }
+        Ti = exp(-acc_op);
+        for (int c = 0; c < 3; c++) {
+            opacity_grad[i] += 0.667 * (render_res[c] - gt[c]) * 1. * Ti * colour[c * n + i];
+            opacity_grad[i] -= 0.667 * (render_res[c] - gt[c]) * 1. * (render_res[c] - acc_rr[c]);
+        }
+    }
+}

@@ -1,0 +1,137 @@
+/*
+ * cpx_oracle.h -- CPU restatement of the Clear-plenoxels training hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker that the CUDA
+ * product path (libcpx.so) is compared against, and the timed CPU baseline
+ * of bench.py.  Nothing in the product links, loads or calls it.
+ *
+ * Every function follows the reference line by line (file:line citations are
+ * relative to the reference project root; SVRF = SparseVolumeRadianceField).
+ * Types follow the reference exactly: where the reference computes in double
+ * and stores float, so does the oracle, and the multiply-add pairs that nvcc
+ * contracts into one fused operation are written as fma() (see the
+ * ORC_CONTRACT_* switches, pinned against the reference's own kernels run on
+ * a B200).  Transcendentals come from the host libm, so results that pass
+ * through exp/log/pow agree with the GPU to a few ulp, not bit for bit;
+ * everything built from +,-,*,/,sqrt alone (ray/AABB hits, occupancy and
+ * index lists) is bit-exact.
+ */
+#ifndef CPX_ORACLE_H
+#define CPX_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Scene: the fields of ObjectScene (SVRF/SceneUtils.cuh:4-98) the path reads. */
+typedef struct orc_scene {
+    int W, H, D;              /* vertices per axis (sceneWidth/Height/Depth) */
+    int sh_dim;               /* SH coefficients per channel in storage */
+    int band;                 /* optimizingBand: forward uses (band+1)^2 coefficients */
+    int hierarchy;            /* Optimizer::hierarchyStrategy */
+    int optimize_step;        /* ObjectScene::optimizeStep (TV type 1 colour gate) */
+    float step;               /* stepSize */
+    int sparse;
+    int64_t n_act;            /* actualGridNums: length of every parameter array */
+    float* params;            /* planar [(1 + 3*sh_dim)][n_act]: k=0 density, 1+c*sh_dim+i SH */
+    const uint8_t* occ;       /* [(W-1)(H-1)(D-1)] occupancy bytes (sparse) */
+    const uint32_t* index_offsets; /* [W*H*D] vertex -> compact index (sparse) */
+    const uint8_t* in_cage;   /* [W*H*D] (sparse) */
+    const float* adaptive_lr; /* [n_act] density LR multiplier (dense Adam); NULL = 1 */
+    const double* off_x;      /* per-sample jitter offsets [n_off]; NULL or beyond n_off = 0 */
+    const double* off_y;
+    const double* off_z;
+    int n_off;
+} orc_scene;
+
+/* Rays: the SoA of _rays (SVRF/Rays.cuh:8-57), RGB only. */
+typedef struct orc_rays {
+    int64_t n;
+    int white_bg;
+    float *ox, *oy, *oz, *dx, *dy, *dz, *near_t, *far_t;
+    uint8_t *mask, *r, *g, *b;
+    float *acc_den, *acc_w, *acc_r, *acc_g, *acc_b;
+} orc_rays;
+
+/* Contraction switches (which mul+add pairs nvcc fuses); default ORC_CONTRACT_DEFAULT. */
+#define ORC_CONTRACT_RAYDIR      1u  /* secondPoint += c2w*x as one fma (Rays.cu:40) */
+#define ORC_CONTRACT_NORM_P0     2u  /* normalize: fma(p2,p2, fma(p0,p0, p1*p1)) */
+#define ORC_CONTRACT_NORM_P1     4u  /* normalize: fma(p2,p2, fma(p1,p1, p0*p0)) */
+#define ORC_CONTRACT_POS         8u  /* o + t*d as one fma (RenderUtils.cu:1676) */
+#define ORC_CONTRACT_ACCD       16u  /* accD += sigma*step with the float product fused */
+#define ORC_CONTRACT_DEFAULT (ORC_CONTRACT_RAYDIR | ORC_CONTRACT_NORM_P0 | ORC_CONTRACT_POS)
+
+void orc_set_contract_mode(unsigned mode);
+unsigned orc_get_contract_mode(void);
+void orc_set_threads(int n);
+int orc_get_threads(void);
+
+/* R4 activations (RenderUtils.cu:480-515). */
+float orc_density_activation(float x);
+float orc_density_derivation(float x);
+float orc_sigmoid(float x);
+float orc_sigmoid_derivative(float x);
+
+/* R5: unnormalised SH basis on the float direction (RenderUtils.cu:1646-1670). */
+void orc_sh_basis(const float dir[3], float shs[25]);
+
+/* R1: rays of one camera (Rays.cu:22-144).  pix_index lists the pixels (row*w+col);
+ * rays are written at out->*[out_start + i].  Camera fields are the device copies
+ * getBound reads: alpha[2], principle[2], c2w[16] (row-major), centre[4]. */
+void orc_rays_from_camera(const double* alpha, const double* principle,
+                          const double* c2w, const double* centre,
+                          const int* bbox /* wmin,wmax,hmin,hmax,dmin,dmax */,
+                          int img_w, const uint8_t* red, const uint8_t* green,
+                          const uint8_t* blue, const uint8_t* mask, int white_bg,
+                          const int* pix_index, int n_pix,
+                          orc_rays* out, int64_t out_start);
+
+/* R7: forward march of the rays sample_index[start .. start+len) (RenderUtils.cu:1582-1718,
+ * 1919-1959).  counts[tid] (optional) receives the number of evaluated samples. */
+void orc_render_forward(const orc_scene* s, orc_rays* r, const int* sample_index,
+                        int start, int len, int* counts);
+
+/* R8: backward (RenderUtils.cu:2051-2256, 1074-1364).  losses[tid] as the reference;
+ * grad is planar [(1+3 sh_dim)][n_act] in double (each per-sample contribution is
+ * rounded to float as the reference's atomicAdd operand, then summed in double). */
+void orc_render_backward(const orc_scene* s, const orc_rays* r, const int* sample_index,
+                         int start, int len, double mask_coef, float huber_delta,
+                         double* losses, double* grad, int* counts);
+
+/* R9: TV / voxel-disparity gradient added into the float grad (RenderUtils.cu:2442-2851). */
+void orc_tv_grad(const orc_scene* s, float* grad, double lam_density, double lam_sh,
+                 int type, int nbrs);
+
+/* R10: Adam over every parameter slot, params updated in place, grad zeroed
+ * (Optimizer.cu:359-415). */
+void orc_adam(orc_scene* s, float* grad, float* m, float* v, double lr, double sh_lr,
+              int timestep);
+
+/* R3: occupancy bytes, in-cage flags and index offsets from a dense density
+ * (SceneUtils.cu:800-881, 1081-1120).  Returns the in-cage count; *dropped_writes
+ * counts the reference's out-of-range in-cage write (SceneUtils.cu:872) that the
+ * oracle drops instead of performing. */
+uint32_t orc_occupancy(const float* density, int W, int H, int D, float threshold,
+                       uint8_t* occ, uint8_t* in_cage, uint32_t* index_offsets,
+                       int64_t* dropped_writes);
+
+/* Compaction of a dense planar parameter block into in-cage order (SceneUtils.cu:585-602). */
+void orc_compact(const float* dense, int n_arrays, int64_t n_dense, const uint8_t* in_cage,
+                 float* compact, int64_t n_compact);
+
+/* R11: batch MSE of the per-ray losses (Utils.cu:311-320). */
+double orc_mse(const double* losses, int n);
+
+/* Compositing known-answer test: the arithmetic of testRender
+ * (SVRF/VolumeFieldRender.cu:111-183), FP64. */
+void orc_composite_kat(const double* opacity, const double* colour /*[3][n]*/, int n,
+                       const double* gt /*[3]*/, double* render_res /*[3]*/,
+                       double* weights /*[n]*/, double* opacity_grad /*[n]*/,
+                       double* colour_grad /*[3][n]*/);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
