@@ -9,8 +9,8 @@
 // thread per vertex moves in-cage records to their compact slots.  The index
 // lists are identical to the reference's, including its quirks: the flag for
 // the x = W-1 face is written at depth*W*H + H*W + col + 1 (SceneUtils.cu:872),
-// and non-caged vertices get index 0.  The one write the reference makes past
-// the end of the flag array (cells at x = W-2, z = D-2) is dropped.
+// i.e. at vertex (W-1, 0, depth+1) -- always inside the array since depth <= D-2
+// -- and non-caged vertices get index 0.
 #include "cpx_internal.cuh"
 
 namespace cpx {

@@ -791,7 +791,8 @@ uint32_t orc_occupancy(const float* density, int W, int H, int D, float threshol
                 if (depth == D - 2) in_cage[(int64_t)(D - 1) * W * H + (int64_t)row * W + col] = 1;
                 if (row == H - 2) in_cage[(int64_t)depth * W * H + (int64_t)(H - 1) * W + col] = 1;
                 if (col == W - 2) {
-                    /* the reference writes depth*W*H + H*W + col + 1 here (SceneUtils.cu:872) */
+                    /* the reference writes depth*W*H + H*W + col + 1 here (SceneUtils.cu:872):
+                     * vertex (W-1, 0, depth+1), at most (D-1)*W*H + W-1 < N */
                     const int64_t v = (int64_t)depth * W * H + (int64_t)H * W + col + 1;
                     if (v < N) in_cage[v] = 1;
                     else dropped++;

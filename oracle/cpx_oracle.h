@@ -110,9 +110,9 @@ void orc_adam(orc_scene* s, float* grad, float* m, float* v, double lr, double s
               int timestep);
 
 /* R3: occupancy bytes, in-cage flags and index offsets from a dense density
- * (SceneUtils.cu:800-881, 1081-1120).  Returns the in-cage count; *dropped_writes
- * counts the reference's out-of-range in-cage write (SceneUtils.cu:872) that the
- * oracle drops instead of performing. */
+ * (SceneUtils.cu:800-881, 1081-1120).  Returns the in-cage count.  The x = W-1
+ * face flag is written where the reference writes it (SceneUtils.cu:872); that
+ * index is always inside the array, *dropped_writes (bounds check) stays 0. */
 uint32_t orc_occupancy(const float* density, int W, int H, int D, float threshold,
                        uint8_t* occ, uint8_t* in_cage, uint32_t* index_offsets,
                        int64_t* dropped_writes);

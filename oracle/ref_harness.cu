@@ -12,13 +12,10 @@
 // It is the parity pin for the CUDA product path and the reference arm of the
 // benchmark; nothing in the product links it.
 //
-// Two guards keep the reference's kernels inside their buffers:
-//  * the per-sample jitter arrays are re-allocated zero-padded beyond
-//    maxSamplePoint, because the march index can pass it (the loop count is
-//    bounded by (far - near + 1) / step + 2);
-//  * pruneSelf writes one in-cage flag past the end of its array when a cell
-//    at x = W-2, z = D-2 is occupied (SVRF/SceneUtils.cu:872); such inputs are
-//    refused before the reference kernel runs.
+// One guard keeps the reference's kernels inside their buffers: the per-sample
+// jitter arrays are re-allocated zero-padded beyond maxSamplePoint, because the
+// march index can pass it (the loop count is bounded by (far - near + 1) / step
+// + 2, RenderUtils.cu:1674-1705).
 
 #include "RenderUtils.cuh"
 #include "Optimizer.cuh"
@@ -74,20 +71,6 @@ int pad_offsets(ObjectScene& s)
     return 0;
 }
 
-// True when pruneScene would write past the in-cage array (SVRF/SceneUtils.cu:870-873).
-bool prune_would_overflow(const float* dens, int W, int H, int D, float thr)
-{
-    const int x = W - 2, z = D - 2;
-    for (int y = 0; y < H - 1; y++)
-        for (int dz = 0; dz < 2; dz++)
-            for (int dy = 0; dy < 2; dy++)
-                for (int dx = 0; dx < 2; dx++) {
-                    int xx = x + dx, yy = y + dy, zz = z + dz;
-                    if (dens[(int64_t)zz * W * H + (int64_t)yy * W + xx] > thr) return true;
-                }
-    return false;
-}
-
 }  // namespace
 
 extern "C" {
@@ -123,7 +106,6 @@ int ref_scene_create_sparse(int W, int H, int D, int sh_dim, int band, float ste
                             const float* dense_planar, float threshold, void** out,
                             uint32_t* n_in_cage)
 {
-    if (prune_would_overflow(dense_planar, W, H, D, threshold)) return 3;
     const int64_t N = (int64_t)W * H * D;
     const int n_arrays = 1 + 3 * sh_dim;
     ObjectScene temp;
