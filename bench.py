@@ -1,0 +1,503 @@
+#!/usr/bin/env python
+"""Training throughput of the plain-FP32 Clear-plenoxels hot path on B200.
+
+A step is one batch of the reference's training loop (SparseVolumeRadianceField/
+Render.cu:407-500): forward march, backward march with gradient scatter, TV
+(type 0, 6 neighbours) and Adam over every vertex.  Workload (the plain FP32
+training-at-scale configuration): 256^3 grid, SH band 2, initialised to density
+0.1 and SH 0, fitted to pixels of 100 800x800 views rendered by the same plain
+forward from a hidden 512^3 grid of 64 seeded Gaussian blobs (SH ~ N(0, 0.5));
+cameras uniform on the upper hemisphere at r = 4, fov 40 deg; 8192-ray batches.
+Seeded synthetic data stands in for the NeRF-Blender images.
+
+  value   rays/s with the ray pool resident in HBM (device time, CUDA events)
+  e2e     rays/s through the public API from pinned host memory: per step the
+          batch's packed rays go host->device and the batch MSE comes back
+  roofline  the fused TV+Adam sweep (the dominant kernel): algorithmic bytes per
+          launch / its average launch time, against the measured HBM copy peak
+  cpu_baseline  the oracle (C restatement of the reference's path, OpenMP) on the
+          host cores, on a bounded sample of the same workload
+
+`--impl reference` runs the reference's own CUDA kernels (the unmodified
+SparseVolumeRadianceField sources built for sm_100a, oracle/_ref) through its
+public entry points on the same workload.  Multi-GPU: independent replicas, one
+per rank (the path does not shard), max-over-ranks device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "clear-plenoxels_b200"))
+
+METRIC = "train rays/s fwd+bwd+Adam; mixed+proposal vs plain FP32 at ΔPSNR≤0.05 dB"
+UNIT = "rays/s"
+
+WORKLOADS = {
+    # plain FP32 training at scale (the configuration the metric is quoted on)
+    "plain256": dict(n=256, gt_n=512, n_blobs=64, gt_sh_std=0.5, cams=100, img=800, batch=8192,
+                     pool_batches=32, init_density=0.1, seed=0),
+    # CPU-runnable plain case shape, for quick runs
+    "small128": dict(n=128, gt_n=128, n_blobs=8, gt_sh_std=0.3, cams=16, img=200, batch=4096,
+                     pool_batches=8, init_density=0.1, seed=0),
+}
+# the reference's shipped training constants (SparseVolumeRadianceField/config_linux.txt)
+STEP = dict(mask_coef=1.0, huber=0.1, lam_density=1e-5, lam_sh=1e-6, lr=0.3, sh_lr=1.0)
+SH_DIM = 9
+RAY_BYTES = 9 * 4  # packed ray record: 8 floats + rgba bytes
+
+
+# --------------------------------------------------------------------------- workload
+def camera_set(wl):
+    import cpx_scenes as S
+
+    rng = np.random.default_rng(wl["seed"] + 1)
+    eyes = S.upper_hemisphere(wl["cams"], 4.0, rng)
+    pix = S.sample_pixels(rng, wl["cams"], wl["img"], wl["img"], wl["batch"] * wl["pool_batches"])
+    # interleave cameras so every batch mixes views (the reference shuffles its ray table)
+    order = np.random.default_rng(wl["seed"] + 2).permutation(sum(len(p) for p in pix))
+    return eyes, pix, order
+
+
+def gt_params_device(wl, device):
+    """Hidden ground-truth grid, planar [28][gt_n^3] on the device (seeded)."""
+    import torch
+
+    import cpx_scenes as S
+
+    rng = np.random.default_rng(wl["seed"])
+    c, s, p = S.random_blobs(rng, wl["n_blobs"])
+    n = wl["gt_n"]
+    params = torch.empty((1 + 3 * SH_DIM, n ** 3), dtype=torch.float32, device=device)
+    params[0] = S.blob_density(n, n, n, c, s, p, device=device)
+    g = torch.Generator(device=device)
+    g.manual_seed(wl["seed"] + 7)
+    params[1:].normal_(0.0, wl["gt_sh_std"], generator=g)
+    return params
+
+
+def to_gt_bytes(acc_r, acc_g, acc_b, acc_w):
+    q = lambda a: np.clip(np.rint(np.asarray(a, np.float64) * 255.0), 0, 255).astype(np.uint8)
+    return q(acc_r), q(acc_g), q(acc_b), q(acc_w)
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path).read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------- distributed
+def dist_setup(use_cuda):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        if use_cuda:
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if use_cuda else "gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x, world, use_cuda):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if use_cuda else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------- peaks / profiles
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic_per_vertex():
+    """DRAM bytes per vertex of the fused sweep from the committed ncu summary, if any."""
+    p = REPO / "profiles" / "sweep_tv_adam_256.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_vertex:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+# --------------------------------------------------------------------------- our arm
+def run_ours(args, wl, world, rank, local):
+    import torch
+
+    import cpx
+    import cpx_scenes as S
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n, R, P = wl["n"], wl["batch"], wl["batch"] * wl["pool_batches"]
+    eyes, pix, order = camera_set(wl)
+
+    # ---- ground truth: render the pool pixels from the hidden grid with our forward
+    gt_n = wl["gt_n"]
+    gt_scene = cpx.ObjectScene(gt_n, gt_n, gt_n, SH_DIM)
+    gp = gt_params_device(wl, dev)
+    gt_scene.upload_params_device(gp)
+    del gp
+    torch.cuda.empty_cache()
+    blank = [(np.zeros(wl["img"] ** 2, np.uint8),) * 3 + (None,) for _ in range(wl["cams"])]
+    gt_rays = cpx.Rays(P, white_bg=True)
+    gt_rays.initial_self(gt_scene, [cpx.Camera.make(**S.look_at_camera(e, gt_n, wl["img"], wl["img"])) for e in eyes],
+                         blank, pix, wl["img"], wl["img"])
+    chunk = 65536
+    for s in range(0, P, chunk):
+        cpx.RenderUtils.renderRays(gt_rays, gt_scene, startSampleIndex=s, len=min(chunk, P - s))
+    gt_scene.check()
+    go = gt_rays.download(fields=("acc_r", "acc_g", "acc_b", "acc_weights"))
+    gr, gg, gb, gm = to_gt_bytes(go["acc_r"], go["acc_g"], go["acc_b"], go["acc_weights"])
+    gt_scene.close()
+    gt_rays.close()
+    torch.cuda.empty_cache()
+
+    # ---- training grid and the ray pool in its voxel space
+    scene = cpx.ObjectScene(n, n, n, SH_DIM)
+    init = torch.zeros((1 + 3 * SH_DIM, n ** 3), dtype=torch.float32, device=dev)
+    init[0] = wl["init_density"]
+    scene.upload_params_device(init)
+    del init
+    pool = cpx.Rays(P, white_bg=True)
+    pool.initial_self(scene, [cpx.Camera.make(**S.look_at_camera(e, n, wl["img"], wl["img"])) for e in eyes],
+                      blank, pix, wl["img"], wl["img"])
+    geo = pool.download(fields=("ox", "oy", "oz", "dx", "dy", "dz", "near", "far"))
+    packed = S.pack_rays(*[geo[k][order] for k in ("ox", "oy", "oz", "dx", "dy", "dz", "near", "far")],
+                         gr[order], gg[order], gb[order], gm[order])
+    pool.upload_packed(packed)  # pool in batch order, ground truth attached
+    host_pool = torch.from_numpy(packed).pin_memory()
+    batch_rays = cpx.Rays(R, white_bg=True)
+    losses = torch.zeros(R, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    lr = [STEP["lr"], STEP["sh_lr"]]
+    K, W = args.steps, args.warmup
+
+    def step(k, ev=None):
+        b = k % wl["pool_batches"]
+        cpx.RenderUtils.renderRays_forwardBackward(scene, pool, losses, None, b * R, R, STEP["mask_coef"],
+                                                   STEP["huber"], stream=stream)
+        if ev is not None:
+            ev[1].record(stream)
+        cpx.Optimizer.varianceAndUpdate(scene, STEP["lam_density"], STEP["lam_sh"], lr[0], lr[1], k + 1,
+                                        stream=stream)
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    for k in range(W):
+        step(k)
+    torch.cuda.synchronize()
+    scene.check()
+
+    # ---- timed: device-resident pool
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = cpx.kernel_launches()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(K):
+        evs[k][0].record(stream)
+        step(W + k, evs[k])
+        evs[k][2].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    launches = cpx.kernel_launches() - launches0
+    clk = clocks.stop()
+    dist_barrier(world)
+    scene.check()
+    ms_local = t0.elapsed_time(t1)
+    ms = dist_max(ms_local, world, True)
+    march_ms = float(np.mean([evs[k][0].elapsed_time(evs[k][1]) for k in range(K)]))
+    sweep_ms = float(np.mean([evs[k][1].elapsed_time(evs[k][2]) for k in range(K)]))
+    value = world * R * K / (ms / 1e3)
+
+    # ---- e2e: host buffers through the public API (H2D batch, step, MSE back)
+    mses = []
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(K):
+        b = k % wl["pool_batches"]
+        batch_rays.upload_packed(host_pool[b * R:(b + 1) * R], stream=stream)
+        mses.append(cpx.train_step(scene, batch_rays, losses, start=0, length=R, mask_coef=STEP["mask_coef"],
+                                   huber_delta=STEP["huber"], lam_density=STEP["lam_density"],
+                                   lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1], timestep=W + K + k + 1,
+                                   want_mse=True, stream=stream))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    scene.check()
+    e2e_ms = dist_max(e0.elapsed_time(e1), world, True)
+    e2e_value = world * R * K / (e2e_ms / 1e3)
+
+    # ---- roofline of the fused TV+Adam sweep
+    N = n ** 3
+    rec = 28 * 4
+    alg_bytes = N * (8 * rec + 4 + 4)  # params r+w, grad r+zero-w, m r+w, v r+w, density mirror w, LR mult r
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
+    tpv = profiled_traffic_per_vertex()
+    roofline = {"bound": "hbm", "kernel": "k_sweep<TV,dense> (fused TV type0/6 + Adam)", "achieved": round(achieved, 1),
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "alg_bytes_per_launch": int(alg_bytes), "traffic": None if tpv is None else int(tpv * N),
+                "launch_ms": round(sweep_ms, 4)}
+
+    result = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic: seeded 64-blob 512^3 hidden grid rendered by the plain forward; no dataset",
+        "config": {
+            "workload": "plain FP32 training at scale: %d^3 grid SH band 2 (density 0.1, SH 0 init), %d-ray "
+                        "batches from %d %dx%d views of a hidden %d^3 64-blob grid, TV type 0/6 + Adam every batch"
+                        % (n, R, wl["cams"], wl["img"], wl["img"], wl["gt_n"]),
+            "grid": n, "sh_dim": SH_DIM, "batch_rays": R, "pool_rays": P, "step_constants": STEP,
+            "l2": "inputs larger than L2: the sweep streams %.1f GB of grid state per step" % (alg_bytes / 1e9),
+            "parallelism": "replicas" if world > 1 else "single GPU",
+        },
+        "roofline": roofline,
+        "kernels_ms": {"march_fwd_bwd": round(march_ms, 4), "tv_adam_sweep": round(sweep_ms, 4)},
+        "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": R * RAY_BYTES,
+                "d2h_bytes_per_step": 8, "last_mse": mses[-1]},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    return result, (scene, pool, R, wl)
+
+
+def cpu_baseline(wl, scene, pool, R, args):
+    """The oracle on the host cores: forward+backward of a sample of one batch's rays (scaled
+    to the batch) plus TV(6)+Adam over the full grid, from the same grid state."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import orc
+
+    import cpx
+
+    n = wl["n"]
+    params = scene.download_params()
+    sample = min(args.cpu_rays, R)
+    d = pool.download(0, sample)
+    rays = orc.RaySet(sample, True, ox=d["ox"], oy=d["oy"], oz=d["oz"], dx=d["dx"], dy=d["dy"], dz=d["dz"],
+                      near=d["near"], far=d["far"], mask=d["mask"], r=d["r"], g=d["g"], b=d["b"])
+    osc = orc.Scene(n, n, n, SH_DIM, params, step=0.5)
+    t0 = time.perf_counter()
+    orc.render_forward(osc, rays)
+    _, grad, _ = orc.render_backward(osc, rays, STEP["mask_coef"], STEP["huber"])
+    t1 = time.perf_counter()
+    g = grad.astype(np.float32)
+    del grad
+    m = np.zeros_like(g)
+    v = np.zeros_like(g)
+    orc.tv_grad(osc, g, STEP["lam_density"], STEP["lam_sh"], 0, 6)
+    orc.adam(osc, g, m, v, STEP["lr"], STEP["sh_lr"], 1)
+    t2 = time.perf_counter()
+    step_s = (t1 - t0) * (R / sample) + (t2 - t1)
+    return {"value": round(R / step_s, 1), "unit": UNIT, "cores": orc.threads(), "kind": "port",
+            "sample": "oracle (C, OpenMP): forward+backward of %d of the %d batch rays (scaled x%.1f) + "
+                      "TV(6)+Adam over the full %d^3 grid; %.1f s measured" % (sample, R, R / sample, n, t2 - t0)}
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args, wl):
+    """The reference's own kernels (oracle/_ref/libcpxref.so) through its entry points."""
+    import torch
+
+    sys.path.insert(0, str(REPO / "oracle"))
+    import orc
+    import refharness as RH
+
+    import cpx_scenes as S
+
+    if not RH.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcpxref.so (reference built for sm_100a) missing"}
+    n, R, P = wl["n"], wl["batch"], wl["batch"] * wl["pool_batches"]
+    eyes, pix, order = camera_set(wl)
+    img = wl["img"]
+    zeros = np.zeros(img * img, np.uint8)
+
+    def host_rays(nv):
+        rays = orc.RaySet(P, True)
+        off = 0
+        for e, p in zip(eyes, pix):
+            cam = S.look_at_camera(e, nv, img, img)
+            orc.rays_from_camera(cam, (0, nv - 1, 0, nv - 1, 0, nv - 1), img, zeros, zeros, zeros, None, True, p,
+                                 rays, off)
+            off += len(p)
+        return rays
+
+    # ground truth with the reference's renderRays on the hidden grid
+    gt_n = wl["gt_n"]
+    gp = gt_params_device(wl, torch.device("cuda")).cpu().numpy()
+    torch.cuda.empty_cache()
+    gt = RH.RefScene(gt_n, gt_n, gt_n, SH_DIM, 2, 0.5, gp)
+    del gp
+    hr = host_rays(gt_n)
+    gt.rays_create(True, *[hr[k] for k in ("ox", "oy", "oz", "dx", "dy", "dz", "near_t", "far_t", "mask", "r", "g", "b")])
+    for s in range(0, P, 65536):
+        gt.render_forward(s, min(65536, P - s))
+    out = gt.rays_download()
+    gt.close()
+    gr, gg, gb, gm = to_gt_bytes(out["acc_r"], out["acc_g"], out["acc_b"], out["acc_weights"])
+    # training scene and ray table in batch order
+    init = np.zeros((1 + 3 * SH_DIM, n ** 3), np.float32)
+    init[0] = wl["init_density"]
+    sc = RH.RefScene(n, n, n, SH_DIM, 2, 0.5, init)
+    del init
+    sc.optimizer_init()
+    tr = host_rays(n)
+    f = {k: tr[k][order] for k in ("ox", "oy", "oz", "dx", "dy", "dz", "near_t", "far_t")}
+    sc.rays_create(True, *[f[k] for k in ("ox", "oy", "oz", "dx", "dy", "dz", "near_t", "far_t")],
+                   gm[order], gr[order], gg[order], gb[order])
+    losses = np.zeros(R, np.float64)
+    K, W = args.steps, args.warmup
+    for k in range(W):
+        sc.train_step((k % wl["pool_batches"]) * R, R, STEP["mask_coef"], STEP["huber"], STEP["lam_density"],
+                      STEP["lam_sh"], 0, 6, True, STEP["lr"], STEP["sh_lr"], k + 1, losses)
+    sc.sync()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for k in range(K):
+        mse = sc.train_step(((W + k) % wl["pool_batches"]) * R, R, STEP["mask_coef"], STEP["huber"],
+                            STEP["lam_density"], STEP["lam_sh"], 0, 6, True, STEP["lr"], STEP["sh_lr"], W + k + 1,
+                            losses)
+    t1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    value = R * K / (ms / 1e3)
+    sc.close()
+    return {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "impl": "reference",
+        "data": "synthetic: seeded 64-blob 512^3 hidden grid rendered by the reference's forward; no dataset",
+        "config": {"workload": "same as --impl ours", "grid": n, "batch_rays": R, "step_constants": STEP,
+                   "entry_points": "RenderUtils::renderRays, renderRays_withGradients_RGB, losses D2H + "
+                                   "getMSEError, addVarianceLoss(type 0, 6), Optimizer::updateRGBScene"},
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": 0, "kind": "reference",
+                         "sample": "the reference's own implementation is CUDA: its kernels built for sm_100a, "
+                                   "run on the same GPU over the full workload (no host cores used)"},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "last_mse": mse,
+        "clocks": clk,
+    }
+
+
+# --------------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="plain256")
+    ap.add_argument("--cpu-rays", type=int, default=512, help="rays in the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    wl = WORKLOADS[args.workload]
+    world, rank, local = dist_setup(use_cuda=True)
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, wl)), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    result, state = run_ours(args, wl, world, rank, local)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(wl, *state[:3], args)
+        else:
+            result["cpu_baseline"] = None
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

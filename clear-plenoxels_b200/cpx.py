@@ -23,7 +23,8 @@ import pathlib
 import numpy as np
 
 PKG_DIR = pathlib.Path(__file__).resolve().parent
-LIB_PATH = PKG_DIR / "lib" / "libcpx.so"
+# CPX_LIBRARY selects another build of the same ABI (e.g. a profiling variant)
+LIB_PATH = pathlib.Path(os.environ.get("CPX_LIBRARY", PKG_DIR / "lib" / "libcpx.so"))
 
 if not LIB_PATH.exists():
     raise ImportError(
@@ -45,7 +46,7 @@ STATUS = {
 # Exported symbols of include/cpx.h (checked by the CPU test suite).
 EXPORTED = [
     "cpx_status_string", "cpx_last_error", "cpx_version", "cpx_grid_create", "cpx_grid_destroy",
-    "cpx_grid_info", "cpx_grid_upload_params", "cpx_grid_download_params", "cpx_grid_upload_grads",
+    "cpx_grid_info", "cpx_grid_upload_params", "cpx_grid_upload_params_device", "cpx_grid_download_params", "cpx_grid_upload_grads",
     "cpx_grid_download_grads", "cpx_grid_upload_moments", "cpx_grid_download_moments",
     "cpx_grid_set_adaptive_lr", "cpx_grid_set_sample_offsets", "cpx_grid_set_optimize_step",
     "cpx_occupancy_build", "cpx_grid_make_sparse", "cpx_rays_create", "cpx_rays_destroy",
@@ -122,6 +123,7 @@ _sig("cpx_grid_destroy", [_vp])
 _sig("cpx_grid_info", [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.POINTER(C.c_int)])
 for _n in ("upload_params", "download_params", "upload_grads", "download_grads"):
     _sig(f"cpx_grid_{_n}", [_vp, _f32p, C.c_int64])
+_sig("cpx_grid_upload_params_device", [_vp, _vp, C.c_int64])
 _sig("cpx_grid_upload_moments", [_vp, _f32p, _f32p, C.c_int64])
 _sig("cpx_grid_download_moments", [_vp, _f32p, _f32p, C.c_int64])
 _sig("cpx_grid_set_adaptive_lr", [_vp, _f32p, C.c_int64])
@@ -254,6 +256,13 @@ class ObjectScene:
     def upload_params(self, planar):
         a, n = self._planar(planar)
         _check(_lib.cpx_grid_upload_params(self._h, a, n), "cpx_grid_upload_params")
+
+    def upload_params_device(self, planar_dev):
+        """planar_dev: CUDA float32 tensor [n_arrays, n_active] (or [n_arrays*n_active])."""
+        n = self.actual_grid_nums
+        if planar_dev.numel() != self.n_arrays * n or not planar_dev.is_contiguous():
+            raise ValueError("expected a contiguous CUDA tensor of n_arrays x n_active floats")
+        _check(_lib.cpx_grid_upload_params_device(self._h, _ptr(planar_dev), n), "cpx_grid_upload_params_device")
 
     def download_params(self):
         n = self.actual_grid_nums

@@ -284,6 +284,18 @@ cpx_status cpx_grid_upload_params(cpx_grid* g, const float* planar, int64_t n)
     return planar_to_records(g->params[g->cur], planar, n, g->n_arrays, g->rec, g->density);
 }
 
+cpx_status cpx_grid_upload_params_device(cpx_grid* g, const float* planar_dev, int64_t n)
+{
+    if (check_grid(g) || !planar_dev) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
+    for (int a = 0; a < g->n_arrays; a++) {
+        k_set_column<<<blocks_for(n), 256>>>(g->params[g->cur], planar_dev + (int64_t)a * n, n, g->rec, a,
+                                              a == 0 ? g->density : nullptr);
+        count_launch();
+    }
+    return cuda_status(cudaDeviceSynchronize(), "device upload");
+}
+
 cpx_status cpx_grid_download_params(const cpx_grid* g, float* planar, int64_t n)
 {
     if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;

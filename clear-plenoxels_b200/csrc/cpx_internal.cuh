@@ -189,6 +189,10 @@ inline RaysView rays_view(cpx_rays* r)
 cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                         int mode, double* losses, double mask_coef, float huber,
                         cudaStream_t s);
+cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                             int mode, double* losses, double mask_coef, float huber,
+                             const MarchScratch& s, cudaStream_t st);
+int march_samples_per_ray(const cpx_grid* g);
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
                       double sh_lr, int timestep, cudaStream_t s);
 cpx_status tv_launch(cpx_grid* g, double lam_d, double lam_sh, int type, int nbrs,

@@ -53,25 +53,29 @@ __device__ __forceinline__ unsigned corner_vertex(const GridView& g, unsigned b0
     return idx;
 }
 
-// ---------------------------------------------------------------------------
-// Stage 1: sample placement (exact).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int32_t* sidx,
-                                               int start, int len, int64_t n_rays,
-                                               SampleRec* samples, int maxs, int* counts,
-                                               double* acc_out, int* err)
+// L1 prefetch of the four 32-byte density sectors that hold a cell's 8 corners (dense grids).
+__device__ __forceinline__ void prefetch_cell(const GridView& g, unsigned b0, unsigned b1, unsigned b2)
 {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= len) return;
-    const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
-    if (ri < 0 || ri >= n_rays) {
-        atomicOr(err, 2);
-        counts[b] = -2;  // invalid ray index: nothing is read or written for it
-        return;
+#pragma unroll
+    for (int q = 0; q < 8; q += 2) {  // corners q and q+2 differ only in x: same sector
+        const float* a = g.density + corner_vertex(g, b0, b1, b2, q);
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(a));
     }
-    // renderRaysGPU zeroes the outputs first (RenderUtils.cu:1927-1941)
-    r.acc_den[ri] = 0.f;
-    r.acc_w[ri] = 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// Sample placement (exact): one thread per ray.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
+                                          SampleRec* samples, int maxs, int* counts,
+                                          double* acc_out, int* err, bool write_fwd)
+{
+    // renderRaysGPU zeroes the outputs first (RenderUtils.cu:1927-1941); the backward alone
+    // leaves the forward's outputs as they are
+    if (write_fwd) {
+        r.acc_den[ri] = 0.f;
+        r.acc_w[ri] = 0.f;
+    }
     const float near_t = r.near_t[ri];
     const float far_t = r.far_t[ri];
     if (near_t > far_t) {  // RenderUtils.cu:1943-1946: no samples, no background
@@ -82,7 +86,6 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
     const float ox = r.ox[ri], oy = r.oy[ri], oz = r.oz[ri];
     const float dx = r.dx[ri], dy = r.dy[ri], dz = r.dz[ri];
     const float step = g.step;
-    // Provable bound on loop trips: every step is >= step - w and the weights sum to <= 1.
     // maxs bounds every ray inside the grid box; longer (or non-finite) rays stop there with
     // the error flag set instead of marching on.
     const double bound = floor(((double)far_t - (double)near_t + 2.0) / (double)step) + 4.0;
@@ -95,6 +98,9 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
     double accD = 0.;
     float accDen = 0.f;
     int intT = 0, n = 0, it = 0;
+    // densities of the last cell visited (consecutive samples mostly share a cell)
+    unsigned cb0 = 0xffffffffu, cb1 = 0, cb2 = 0;
+    float cd[8];
     while (t < far_t) {
         if (++it > it_cap || n >= maxs) {
             atomicOr(err, 1);
@@ -118,6 +124,23 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
             ++intT;
             continue;
         }
+        if (b0 != cb0 || b1 != cb1 || b2 != cb2) {
+#pragma unroll
+            for (int q = 0; q < 8; q++) cd[q] = g.density[corner_vertex(g, b0, b1, b2, q)];
+            cb0 = b0;
+            cb1 = b1;
+            cb2 = b2;
+            // the march waits on every new cell's densities; fetch the cells one and two
+            // voxels further along the ray into L1 now, while this sample is evaluated
+            if (!g.sparse) {
+#pragma unroll
+                for (int k = 1; k <= 2; k++) {
+                    const double ta = t + (double)k;
+                    prefetch_cell(g, (unsigned)(ox + ta * dx), (unsigned)(oy + ta * dy),
+                                  (unsigned)(oz + ta * dz));
+                }
+            }
+        }
         const double x = bc0 - b0;
         const double y = bc1 - b1;
         const double z = bc2 - b2;
@@ -125,21 +148,21 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
         float tri0 = 0.f;
         double c;
         c = (1. - x) * (1. - y) * (1. - z);
-        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 0)];
+        tri0 += c * cd[0];
         c = (1. - x) * y * (1. - z);
-        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 1)];
+        tri0 += c * cd[1];
         c = x * (1. - y) * (1. - z);
-        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 2)];
+        tri0 += c * cd[2];
         c = x * y * (1. - z);
-        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 3)];
+        tri0 += c * cd[3];
         c = (1. - x) * (1. - y) * z;
-        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 4)];
+        tri0 += c * cd[4];
         c = (1. - x) * y * z;
-        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 5)];
+        tri0 += c * cd[5];
         c = x * (1. - y) * z;
-        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 6)];
+        tri0 += c * cd[6];
         c = x * y * z;
-        tri0 += c * g.density[corner_vertex(g, b0, b1, b2, 7)];
+        tri0 += c * cd[7];
         // density_activation (RenderUtils.cu:491) and the weight (RenderUtils.cu:1693-1704)
         const float sigma = logf(1.f + expf(tri0 - 13.f));
         const double w = Ti * (1. - expf(-sigma * step));
@@ -164,8 +187,10 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
         ++intT;
         ++n;
     }
-    r.acc_den[ri] = accDen;
-    r.acc_w[ri] = (float)acc;
+    if (write_fwd) {
+        r.acc_den[ri] = accDen;
+        r.acc_w[ri] = (float)acc;
+    }
     acc_out[b] = acc;
     counts[b] = n;
 }
@@ -270,23 +295,82 @@ __device__ __forceinline__ void gather_sh(const GridView& g, const Corners& c, f
     }
 }
 
-template <int NSH, int MODE>
-__global__ void __launch_bounds__(128) k_shade(GridView g, RaysView r, const int32_t* sidx,
-                                                int start, int len, const SampleRec* samples,
-                                                float4* colours, int maxs, const int* counts,
-                                                const double* acc_in, double* losses,
-                                                double mask_coef, float huber)
+// Per-warp table that merges the corner contributions of one 32-sample chunk: key =
+// vertex index, value = (density grad, R, G, B colour-grad sums before the SH basis).
+constexpr int kHashSlots = 256;
+constexpr uint32_t kEmpty = 0xffffffffu;
+
+struct WarpTable {
+    uint32_t* keys;  // [kHashSlots]
+    float4* vals;    // [kHashSlots]
+};
+
+__device__ __forceinline__ void table_add(const WarpTable& t, uint32_t key, float a, float b0,
+                                          float b1, float b2)
+{
+    uint32_t h = (key * 0x9E3779B1u) >> 24;  // 8 bits
+    for (int probe = 0; probe < kHashSlots; probe++) {
+        const uint32_t old = atomicCAS(&t.keys[h], kEmpty, key);
+        if (old == kEmpty || old == key) {
+            atomicAdd(&t.vals[h].x, a);
+            atomicAdd(&t.vals[h].y, b0);
+            atomicAdd(&t.vals[h].z, b1);
+            atomicAdd(&t.vals[h].w, b2);
+            return;
+        }
+        h = (h + 1) & (kHashSlots - 1);
+    }
+}
+
+// Flush the table: one vertex record of gradients per distinct key, 16-byte vector atomics.
+template <int NSH>
+__device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& g, const float* shs,
+                                            int lane)
 {
     using RS = RecShape<NSH>;
-    const int lane = threadIdx.x & 31;
-    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
-    if (b >= len) return;  // warp-uniform
-    const int cnt = counts[b];  // -1: ray misses the box, -2: invalid ray index
-    if (cnt == -2) {
-        if ((MODE & kBackward) && lane == 0) losses[b] = 0.;
-        return;
+    __syncwarp();
+    for (int s = lane; s < kHashSlots; s += 32) {
+        const uint32_t key = t.keys[s];
+        if (key == kEmpty) continue;
+        const float4 v = t.vals[s];
+        const float bch[3] = {v.y, v.z, v.w};
+        float4* dst = reinterpret_cast<float4*>(g.grad + (size_t)key * RS::REC);
+#pragma unroll
+        for (int q = 0; q < RS::NV4; q++) {
+            float e4[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int e = 4 * q + k;
+                float val = 0.f;
+                if (e == 0) {
+                    val = v.x;
+                } else if (e < RS::NA) {
+                    const int ch = (e - 1) / NSH;
+                    const int kk = (e - 1) % NSH;
+                    bool on = true;
+                    if (g.hierarchy) on = kk >= g.band * g.band && kk < g.n_sh_fwd;
+                    val = on ? bch[ch] * shs[kk] : 0.f;
+                }
+                e4[k] = val;
+            }
+            atomicAdd(dst + q, make_float4(e4[0], e4[1], e4[2], e4[3]));
+        }
+        t.keys[s] = kEmpty;
+        t.vals[s] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
+    __syncwarp();
+}
+
+// Shade one ray with a whole warp: forward colour (lane per sample, warp reduction), then
+// the backward of renderRays_withGradients_RGBGPU (RenderUtils.cu:2145-2256) with warp prefix
+// scans for the running weight/colour sums and the merged gradient scatter.
+template <int NSH, int MODE>
+__device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
+                                          int cnt, const SampleRec* samples, float4* colours,
+                                          int maxs, const double* acc_in, double* losses,
+                                          double mask_coef, float huber, const WarpTable& tab,
+                                          int lane)
+{
     const bool miss = cnt < 0;
     const int n = miss ? 0 : cnt;
     float shs[NSH];
@@ -345,7 +429,7 @@ __global__ void __launch_bounds__(128) k_shade(GridView g, RaysView r, const int
     }
     if (!(MODE & kBackward)) return;
 
-    // ---- backward (renderRays_withGradients_RGBGPU, RenderUtils.cu:2145-2256) ----
+    // ---- backward ----
     if (miss) {
         if (lane == 0) losses[b] = 0.;
         return;
@@ -355,7 +439,7 @@ __global__ void __launch_bounds__(128) k_shade(GridView g, RaysView r, const int
         pred[1] - r.g[ri] / 255.,
         pred[2] - r.b[ri] / 255.,
     };
-    double loss = (fabs(res[0]) + fabs(res[1]) + fabs(res[2])) * 255. / 3.;
+    const double loss = (fabs(res[0]) + fabs(res[1]) + fabs(res[2])) * 255. / 3.;
     if (isnan(loss)) {
         if (lane == 0) losses[b] = 255.;
         return;
@@ -390,10 +474,10 @@ __global__ void __launch_bounds__(128) k_shade(GridView g, RaysView r, const int
             s.w = 0.f;
         }
         const double w = valid ? (double)s.w : 0.;
-        double aw = warp_inclusive_scan(w, lane);
-        double a0 = warp_inclusive_scan(w * col.x, lane);
-        double a1 = warp_inclusive_scan(w * col.y, lane);
-        double a2 = warp_inclusive_scan(w * col.z, lane);
+        const double aw = warp_inclusive_scan(w, lane);
+        const double a0 = warp_inclusive_scan(w * col.x, lane);
+        const double a1 = warp_inclusive_scan(w * col.y, lane);
+        const double a2 = warp_inclusive_scan(w * col.z, lane);
         const double acc_i = carry_w + aw;
         const double acc_rgb0 = carry_c0 + a0;
         const double acc_rgb1 = carry_c1 + a1;
@@ -402,51 +486,84 @@ __global__ void __launch_bounds__(128) k_shade(GridView g, RaysView r, const int
         carry_c0 += __shfl_sync(0xffffffffu, a0, 31);
         carry_c1 += __shfl_sync(0xffffffffu, a1, 31);
         carry_c2 += __shfl_sync(0xffffffffu, a2, 31);
-        if (!valid) continue;
-
-        float grad[4];
-        grad[1] = 0.6667f * w * res[0] * colour_deriv_from_act(col.x);
-        grad[2] = 0.6667f * w * res[1] * colour_deriv_from_act(col.y);
-        grad[3] = 0.6667f * w * res[2] * colour_deriv_from_act(col.z);
-        const double Ti = (double)s.tn;
-        grad[0] = res[0] * (Ti * col.x - (pred[0] - acc_rgb0));
-        grad[0] += res[1] * (Ti * col.y - (pred[1] - acc_rgb1));
-        grad[0] += res[2] * (Ti * col.z - (pred[2] - acc_rgb2));
-        const float dd = 1.f / (1.f + expf(13.f - s.raw));  // density_derivation (RenderUtils.cu:497)
-        grad[0] *= 0.6667 * step * dd;
-        grad[0] += step * dd * (accw_f - acc_i - Ti) * mask_loss;
-
-        // scatter: corner q receives grad[0]*w_q and grad[1+ch]*w_q*basis[k]
-        Corners cr;
-        sample_corners(g, s, cr);
+        if (valid) {
+            float grad[4];
+            grad[1] = 0.6667f * w * res[0] * colour_deriv_from_act(col.x);
+            grad[2] = 0.6667f * w * res[1] * colour_deriv_from_act(col.y);
+            grad[3] = 0.6667f * w * res[2] * colour_deriv_from_act(col.z);
+            const double Ti = (double)s.tn;
+            grad[0] = res[0] * (Ti * col.x - (pred[0] - acc_rgb0));
+            grad[0] += res[1] * (Ti * col.y - (pred[1] - acc_rgb1));
+            grad[0] += res[2] * (Ti * col.z - (pred[2] - acc_rgb2));
+            const float dd = 1.f / (1.f + expf(13.f - s.raw));  // density_derivation (RenderUtils.cu:497)
+            grad[0] *= 0.6667 * step * dd;
+            grad[0] += step * dd * (accw_f - acc_i - Ti) * mask_loss;
+            // corner q receives grad[0]*w_q and grad[1+ch]*w_q*basis[k]: merge per vertex first
+            Corners cr;
+            sample_corners(g, s, cr);
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const float wq = cr.w[q];
-            const float a = grad[0] * wq;
-            const float bch[3] = {grad[1] * wq, grad[2] * wq, grad[3] * wq};
-            float4* dst = reinterpret_cast<float4*>(g.grad + (size_t)cr.idx[q] * RS::REC);
-#pragma unroll
-            for (int v = 0; v < RS::NV4; v++) {
-                float e4[4];
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int e = 4 * v + k;
-                    float val = 0.f;
-                    if (e == 0) {
-                        val = a;
-                    } else if (e < RS::NA) {
-                        const int ch = (e - 1) / NSH;
-                        const int kk = (e - 1) % NSH;
-                        bool on = true;
-                        if (g.hierarchy) on = kk >= g.band * g.band && kk < g.n_sh_fwd;
-                        val = on ? bch[ch] * shs[kk] : 0.f;
-                    }
-                    e4[k] = val;
-                }
-                atomicAdd(dst + v, make_float4(e4[0], e4[1], e4[2], e4[3]));
+            for (int q = 0; q < 8; q++) {
+                const float wq = cr.w[q];
+                table_add(tab, cr.idx[q], grad[0] * wq, grad[1] * wq, grad[2] * wq, grad[3] * wq);
             }
         }
+        table_flush<NSH>(tab, g, shs, lane);
     }
+}
+
+// ---------------------------------------------------------------------------
+// The two stages as kernels.  Placement is latency-bound per ray and needs only one thread
+// per ray, all resident in one wave; shading is throughput-bound and takes a warp per ray.
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int32_t* sidx, int start,
+                                               int len, int64_t n_rays, SampleRec* samples, int maxs,
+                                               int* counts, double* acc, int* err)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= len) return;
+    const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
+    if (ri < 0 || ri >= n_rays) {
+        atomicOr(err, 2);
+        counts[b] = -2;  // invalid ray index: nothing is read or written for it
+        return;
+    }
+    place_ray(g, r, b, ri, samples, maxs, counts, acc, err, (MODE & kForward) != 0);
+}
+
+constexpr int kShadeWarps = 4;
+
+template <int NSH, int MODE>
+__global__ void __launch_bounds__(kShadeWarps * 32) k_shade(GridView g, RaysView r,
+                                                             const int32_t* sidx, int start,
+                                                             int len, const SampleRec* samples,
+                                                             float4* colours, int maxs,
+                                                             const int* counts, const double* acc,
+                                                             double* losses, double mask_coef,
+                                                             float huber)
+{
+    __shared__ uint32_t h_keys[kShadeWarps][kHashSlots];
+    __shared__ float4 h_vals[kShadeWarps][kHashSlots];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    if (MODE & kBackward) {
+        for (int s = lane; s < kHashSlots; s += 32) {
+            h_keys[warp][s] = kEmpty;
+            h_vals[warp][s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncwarp();
+    }
+    const int b = blockIdx.x * kShadeWarps + warp;
+    if (b >= len) return;  // warp-uniform
+    const int cnt = counts[b];
+    if (cnt == -2) {
+        if ((MODE & kBackward) && lane == 0) losses[b] = 0.;
+        return;
+    }
+    const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
+    const WarpTable tab{h_keys[warp], h_vals[warp]};
+    shade_ray<NSH, MODE>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber, tab,
+                         lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -524,28 +641,33 @@ static cpx_status ensure_scratch(cpx_grid* g, int len)
 }
 
 template <int NSH>
-static void launch_shade(int mode, dim3 grid, dim3 block, cudaStream_t st, GridView gv,
-                         RaysView rv, const int32_t* sidx, int start, int len,
+static void launch_march(int mode, cudaStream_t st, const GridView& gv, const RaysView& rv,
+                         const int32_t* sidx, int start, int len, int64_t n_rays,
                          const MarchScratch& s, double* losses, double mask_coef, float huber)
 {
-    if (mode == kForward)
-        k_shade<NSH, kForward><<<grid, block, 0, st>>>(gv, rv, sidx, start, len, s.samples,
-                                                       s.colours, s.maxs, s.counts, s.acc,
-                                                       losses, mask_coef, huber);
-    else if (mode == kBackward)
-        k_shade<NSH, kBackward><<<grid, block, 0, st>>>(gv, rv, sidx, start, len, s.samples,
-                                                        s.colours, s.maxs, s.counts, s.acc,
-                                                        losses, mask_coef, huber);
-    else
-        k_shade<NSH, kForwardBackward><<<grid, block, 0, st>>>(gv, rv, sidx, start, len,
-                                                               s.samples, s.colours, s.maxs,
-                                                               s.counts, s.acc, losses,
-                                                               mask_coef, huber);
+    const dim3 pgrid((unsigned)((len + 31) / 32));
+    const dim3 sgrid((unsigned)((len + kShadeWarps - 1) / kShadeWarps));
+    const dim3 sblock(kShadeWarps * 32);
+#define CPX_SHADE_ARGS gv, rv, sidx, start, len, s.samples, s.colours, s.maxs, s.counts, s.acc, losses, \
+                       mask_coef, huber
+    if (mode == kForward) {
+        k_place<kForward><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
+                                                s.counts, s.acc, s.err);
+        k_shade<NSH, kForward><<<sgrid, sblock, 0, st>>>(CPX_SHADE_ARGS);
+    } else if (mode == kBackward) {
+        k_place<kBackward><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
+                                                 s.counts, s.acc, s.err);
+        k_shade<NSH, kBackward><<<sgrid, sblock, 0, st>>>(CPX_SHADE_ARGS);
+    } else {
+        k_place<kForwardBackward><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples,
+                                                        s.maxs, s.counts, s.acc, s.err);
+        k_shade<NSH, kForwardBackward><<<sgrid, sblock, 0, st>>>(CPX_SHADE_ARGS);
+    }
+#undef CPX_SHADE_ARGS
 }
 
-cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
-                        int mode, double* losses, double mask_coef, float huber,
-                        cudaStream_t st)
+static cpx_status march_check_args(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start,
+                                   int len, int mode, double* losses)
 {
     if (len < 0 || start < 0) {
         set_error("negative start/len");
@@ -563,28 +685,42 @@ cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start
         set_error("sparse grid without occupancy");
         return CPX_ERR_NOT_READY;
     }
-    g->last_len = len;
-    if (len == 0) return CPX_OK;
-    cpx_status rc = ensure_scratch(g, len);
-    if (rc != CPX_OK) return rc;
+    return CPX_OK;
+}
+
+int march_samples_per_ray(const cpx_grid* g) { return max_samples_per_ray(g); }
+
+cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                             int mode, double* losses, double mask_coef, float huber,
+                             const MarchScratch& s, cudaStream_t st)
+{
+    cpx_status rc = march_check_args(g, r, sidx, start, len, mode, losses);
+    if (rc != CPX_OK || len == 0) return rc;
     const GridView gv = grid_view(g);
     const RaysView rv = rays_view(r);
-    const MarchScratch& s = g->scratch;
-    k_place<<<(len + 31) / 32, 32, 0, st>>>(gv, rv, sidx, start, len, r->n, s.samples, s.maxs,
-                                            s.counts, s.acc, s.err);
-    count_launch();
-    const dim3 block(128);
-    const dim3 grid((unsigned)(((int64_t)len * 32 + 127) / 128));
     switch (g->sh_dim) {
-    case 1: launch_shade<1>(mode, grid, block, st, gv, rv, sidx, start, len, s, losses, mask_coef, huber); break;
-    case 4: launch_shade<4>(mode, grid, block, st, gv, rv, sidx, start, len, s, losses, mask_coef, huber); break;
-    case 9: launch_shade<9>(mode, grid, block, st, gv, rv, sidx, start, len, s, losses, mask_coef, huber); break;
+    case 1: launch_march<1>(mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber); break;
+    case 4: launch_march<4>(mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber); break;
+    case 9: launch_march<9>(mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber); break;
     default:
         set_error("sh_dim %d unsupported", g->sh_dim);
         return CPX_ERR_UNSUPPORTED;
     }
-    count_launch();
+    count_launch(2);
     return cuda_status(cudaGetLastError(), "march");
+}
+
+cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                        int mode, double* losses, double mask_coef, float huber,
+                        cudaStream_t st)
+{
+    cpx_status rc = march_check_args(g, r, sidx, start, len, mode, losses);
+    if (rc != CPX_OK) return rc;
+    g->last_len = len;
+    if (len == 0) return CPX_OK;
+    rc = ensure_scratch(g, len);
+    if (rc != CPX_OK) return rc;
+    return march_launch_with(g, r, sidx, start, len, mode, losses, mask_coef, huber, g->scratch, st);
 }
 
 }  // namespace cpx

@@ -19,10 +19,7 @@ namespace cpx {
 
 struct SweepArgs {
     int W, H, D;
-    int S;  // float4 slots per record
-    int n_arrays, sh_dim, band, hierarchy;
-    int64_t n_act;
-    int sparse;
+    uint32_t n_act;
     const float4* __restrict__ p_in;
     float4* p_out;
     float4* grad;
@@ -32,30 +29,13 @@ struct SweepArgs {
     const float* __restrict__ adaptive_lr;
     const uint32_t* __restrict__ index_offsets;
     const uint32_t* __restrict__ compact_to_dense;
+    const uint8_t* __restrict__ in_cage;  // dense in-cage flags (sparse TV gate, see k_sweep)
+    uint32_t tv_mask;    // bit e: parameter e of a record gets the TV term (RenderUtils.cu:2743-2746)
+    uint32_t adam_mask;  // bit e: parameter e is updated by Adam (Optimizer.cu:380-413)
     float lam_d, lam_sh;
     float lr, sh_lr;
     int timestep;
 };
-
-// Which parameter of a record the Adam step updates (Optimizer.cu:380-413).
-__device__ __forceinline__ bool adam_applies(const SweepArgs& a, int e)
-{
-    if (e == 0) return true;
-    if (e >= a.n_arrays) return false;
-    if (!a.hierarchy) return true;
-    const int k = (e - 1) % a.sh_dim;
-    return k >= a.band * a.band && k < (a.band + 1) * (a.band + 1);
-}
-
-// Which parameter the TV term touches (RenderUtils.cu:2743-2746).
-__device__ __forceinline__ bool tv_applies(const SweepArgs& a, int e)
-{
-    if (e == 0) return true;
-    if (e >= a.n_arrays) return false;
-    const int k = (e - 1) % a.sh_dim;
-    const int lo = a.hierarchy ? a.band * a.band : 0;
-    return k >= lo && k < (a.band + 1) * (a.band + 1);
-}
 
 __device__ __forceinline__ float f4get(const float4& v, int c)
 {
@@ -80,161 +60,217 @@ __device__ __forceinline__ float tv6(float self, const float* nb, float lam)
         sum += d * d;
         disp = (j == 0) ? d : disp + d;
     }
-    sum = sqrtf(sum) / 6.f;
-    return lam / (sum + 1.e-6f) * disp;
+    const float sd = sqrtf(sum) / 6.f;
+    return __fdividef(lam * disp, sd + 1.e-6f);
 }
 
-template <bool TV, bool SPARSE>
-__global__ void __launch_bounds__(256) k_sweep(SweepArgs a)
+// One 16-byte slot: optional TV term from six neighbour slots, then Adam; writes the slot.
+template <bool TV>
+__device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint32_t v, int j,
+                                           bool tv_on, const uint32_t* nb_slot, const bool* nb_self,
+                                           float inv_bc1, float inv_bc2, float lr_density)
 {
-    __shared__ float s_bc[2];
-    if (threadIdx.x == 0) {
-        // bias corrections exactly as the reference forms them (powf of float beta)
-        s_bc[0] = 1.f / (float)(1. - powf(0.9f, a.timestep));
-        s_bc[1] = 1.f / (float)(1. - powf(0.999f, a.timestep));
-    }
-    __syncthreads();
-    const float inv_bc1 = s_bc[0], inv_bc2 = s_bc[1];
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
-    const int S = a.S;
-    const int64_t WH = (int64_t)a.W * a.H;
-
-    // Dense: one block per (y,z) row; sparse: blocks tile the compact slots.
-    int64_t slot_begin, slot_end;
-    int y = 0, z = 0;
-    if (!SPARSE) {
-        const int row = blockIdx.x;
-        y = row % a.H;
-        z = row / a.H;
-        slot_begin = ((int64_t)z * WH + (int64_t)y * a.W) * S;
-        slot_end = slot_begin + (int64_t)a.W * S;
-    } else {
-        const int64_t per_block = (int64_t)blockDim.x * 8;
-        slot_begin = (int64_t)blockIdx.x * per_block;
-        slot_end = min(slot_begin + per_block, a.n_act * S);
-    }
-    const bool row_interior = !SPARSE && y >= 1 && y <= a.H - 2 && z >= 1 && z <= a.D - 2;
-
-    for (int64_t sl = slot_begin + threadIdx.x; sl < slot_end; sl += blockDim.x) {
-        const int64_t v = sl / S;
-        const int j = (int)(sl - v * S);
-        float4 p = a.p_in[sl];
-        float4 g = a.grad[sl];
-        float4 m = a.m[sl];
-        float4 vv = a.v[sl];
-        if (TV) {
-            bool interior;
-            int64_t nb_slot[6];
-            bool nb_self[6] = {false, false, false, false, false, false};
-            if (!SPARSE) {
-                const int x = (int)(v - ((int64_t)z * WH + (int64_t)y * a.W));
-                interior = row_interior && x >= 1 && x <= a.W - 2;
-                const int64_t off[6] = {-WH, -(int64_t)a.W, -1, 1, (int64_t)a.W, WH};
+    const float4 p = a.p_in[sl];
+    float4 g = a.grad[sl];
+    float4 m = a.m[sl];
+    float4 vv = a.v[sl];
+    if (TV && tv_on) {
+        float4 nbv[6];
 #pragma unroll
-                for (int k = 0; k < 6; k++) nb_slot[k] = (v + off[k]) * S + j;
-            } else {
-                const int64_t dv = a.compact_to_dense[v];
-                const int x = (int)(dv % a.W);
-                const int yy = (int)((dv / a.W) % a.H);
-                const int zz = (int)(dv / WH);
-                interior = x >= 1 && x <= a.W - 2 && yy >= 1 && yy <= a.H - 2 && zz >= 1 &&
-                           zz <= a.D - 2;
-                if (interior) {
-                    const int64_t off[6] = {-WH, -(int64_t)a.W, -1, 1, (int64_t)a.W, WH};
-#pragma unroll
-                    for (int k = 0; k < 6; k++) {
-                        const uint32_t ci = a.index_offsets[dv + off[k]];
-                        nb_self[k] = ci == 0;  // compact index 0 reads as the vertex itself
-                        nb_slot[k] = (int64_t)ci * S + j;
-                    }
-                }
-            }
-            if (interior) {
-                float4 nbv[6];
-#pragma unroll
-                for (int k = 0; k < 6; k++) nbv[k] = nb_self[k] ? p : a.p_in[nb_slot[k]];
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const int e = 4 * j + c;
-                    if (!tv_applies(a, e)) continue;
-                    float nb[6];
-#pragma unroll
-                    for (int k = 0; k < 6; k++) nb[k] = f4get(nbv[k], c);
-                    const float lam = e == 0 ? a.lam_d : a.lam_sh;
-                    f4set(g, c, f4get(g, c) + tv6(f4get(p, c), nb, lam));
-                }
-            }
-        }
-        // Adam (Optimizer.cu:374-413)
-        float4 pn = p;
+        for (int k = 0; k < 6; k++) nbv[k] = nb_self[k] ? p : a.p_in[nb_slot[k]];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const int e = 4 * j + c;
-            if (!adam_applies(a, e)) continue;
-            const float gc = f4get(g, c);
-            const float mc = fmaf(1.f - beta1, gc, beta1 * f4get(m, c));
-            const float vc = fmaf((1.f - beta2) * gc, gc, beta2 * f4get(vv, c));
-            f4set(m, c, mc);
-            f4set(vv, c, vc);
-            const float cm = mc * inv_bc1;
-            const float cv = vc * inv_bc2;
-            float lr = a.sh_lr;
-            if (e == 0) lr = (!SPARSE && a.adaptive_lr) ? a.lr * a.adaptive_lr[v] : a.lr;
-            float np = f4get(p, c) - lr * cm / (sqrtf(cv) + eps);
-            if (e == 0) np = np < 0.f ? 0.f : np;  // density clamp (Optimizer.cu:384)
-            f4set(pn, c, np);
-            f4set(g, c, 0.f);
+            if (!((a.tv_mask >> e) & 1u)) continue;
+            float nb[6];
+#pragma unroll
+            for (int k = 0; k < 6; k++) nb[k] = f4get(nbv[k], c);
+            f4set(g, c, f4get(g, c) + tv6(f4get(p, c), nb, e == 0 ? a.lam_d : a.lam_sh));
         }
-        a.p_out[sl] = pn;
-        a.m[sl] = m;
-        a.v[sl] = vv;
-        a.grad[sl] = g;
-        if (j == 0) a.density_out[v] = pn.x;
     }
+    float4 pn = p;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int e = 4 * j + c;
+        if (!((a.adam_mask >> e) & 1u)) continue;
+        const float gc = f4get(g, c);
+        const float mc = fmaf(1.f - beta1, gc, beta1 * f4get(m, c));
+        const float vc = fmaf((1.f - beta2) * gc, gc, beta2 * f4get(vv, c));
+        f4set(m, c, mc);
+        f4set(vv, c, vc);
+        const float lr = e == 0 ? lr_density : a.sh_lr;
+        float np = f4get(p, c) - __fdividef(lr * (mc * inv_bc1), sqrtf(vc * inv_bc2) + eps);
+        if (e == 0) np = np < 0.f ? 0.f : np;  // density clamp (Optimizer.cu:384)
+        f4set(pn, c, np);
+        f4set(g, c, 0.f);
+    }
+    a.p_out[sl] = pn;
+    a.m[sl] = m;
+    a.v[sl] = vv;
+    a.grad[sl] = g;
+    if (j == 0) a.density_out[v] = pn.x;
+}
+
+__device__ __forceinline__ void bias_corrections(int t, float* s_bc)
+{
+    if (threadIdx.x == 0) {
+        // bias corrections as the reference forms them (powf of the float betas)
+        s_bc[0] = 1.f / (float)(1. - powf(0.9f, t));
+        s_bc[1] = 1.f / (float)(1. - powf(0.999f, t));
+    }
+    __syncthreads();
+}
+
+// Dense grid: one block per (y, z) row of W vertices, S slots each.
+template <int S, bool TV>
+__global__ void __launch_bounds__(256) k_sweep_dense(SweepArgs a)
+{
+    __shared__ float s_bc[2];
+    bias_corrections(a.timestep, s_bc);
+    const int row = blockIdx.x;
+    const int y = row % a.H;
+    const int z = row / a.H;
+    const uint32_t WH = (uint32_t)a.W * a.H;
+    const uint32_t v0 = (uint32_t)z * WH + (uint32_t)y * a.W;
+    const bool row_interior = y >= 1 && y <= a.H - 2 && z >= 1 && z <= a.D - 2;
+    const uint32_t n_slots = (uint32_t)a.W * S;
+    for (uint32_t li = threadIdx.x; li < n_slots; li += blockDim.x) {
+        const uint32_t x = li / S;
+        const int j = (int)(li - x * S);
+        const uint32_t v = v0 + x;
+        const uint32_t sl = v * S + j;
+        const bool tv_on = row_interior && x >= 1 && x + 2 <= (uint32_t)a.W;
+        uint32_t nb_slot[6];
+        const bool nb_self[6] = {false, false, false, false, false, false};
+        nb_slot[0] = sl - WH * S;
+        nb_slot[1] = sl - (uint32_t)a.W * S;
+        nb_slot[2] = sl - S;
+        nb_slot[3] = sl + S;
+        nb_slot[4] = sl + (uint32_t)a.W * S;
+        nb_slot[5] = sl + WH * S;
+        const float lr_d = a.adaptive_lr ? a.lr * a.adaptive_lr[v] : a.lr;
+        sweep_slot<TV>(a, sl, v, j, tv_on, nb_slot, nb_self, s_bc[0], s_bc[1], lr_d);
+    }
+}
+
+// Sparse grid: blocks tile the compact slots; positions from the compact->dense table.
+template <int S, bool TV>
+__global__ void __launch_bounds__(256) k_sweep_sparse(SweepArgs a)
+{
+    __shared__ float s_bc[2];
+    bias_corrections(a.timestep, s_bc);
+    const uint32_t WH = (uint32_t)a.W * a.H;
+    const uint32_t total = a.n_act * S;
+    const uint32_t begin = blockIdx.x * blockDim.x * 8u;
+    const uint32_t end = min(begin + blockDim.x * 8u, total);
+    for (uint32_t sl = begin + threadIdx.x; sl < end; sl += blockDim.x) {
+        const uint32_t v = sl / S;
+        const int j = (int)(sl - v * S);
+        bool tv_on = false;
+        uint32_t nb_slot[6] = {0, 0, 0, 0, 0, 0};
+        bool nb_self[6] = {false, false, false, false, false, false};
+        if (TV) {
+            const uint32_t dv = a.compact_to_dense[v];
+            const uint32_t x = dv % a.W;
+            const uint32_t yy = (dv / a.W) % a.H;
+            const uint32_t zz = dv / WH;
+            // The reference gates sparse TV with inCageInfo[indexOffsets[v]] -- the dense flag
+            // array read at the compact index (RenderUtils.cu:2669) -- so vertex c gets its TV
+            // term only when dense vertex #c is in cage.
+            tv_on = x >= 1 && x + 2 <= (uint32_t)a.W && yy >= 1 && yy + 2 <= (uint32_t)a.H && zz >= 1 &&
+                    zz + 2 <= (uint32_t)a.D && a.in_cage[v] != 0;
+            if (tv_on) {
+                const uint32_t nbd[6] = {dv - WH, dv - a.W, dv - 1, dv + 1, dv + a.W, dv + WH};
+#pragma unroll
+                for (int k = 0; k < 6; k++) {
+                    const uint32_t ci = a.index_offsets[nbd[k]];
+                    nb_self[k] = ci == 0;  // compact index 0 reads as the vertex itself
+                    nb_slot[k] = ci * S + j;
+                }
+            }
+        }
+        sweep_slot<TV>(a, sl, v, j, tv_on, nb_slot, nb_self, s_bc[0], s_bc[1], a.lr);
+    }
+}
+
+template <int S>
+static void launch_sweep(const cpx_grid* g, const SweepArgs& a, bool tv, cudaStream_t st)
+{
+    if (!g->sparse) {
+        const unsigned rows = (unsigned)((int64_t)g->H * g->D);
+        if (tv)
+            k_sweep_dense<S, true><<<rows, 256, 0, st>>>(a);
+        else
+            k_sweep_dense<S, false><<<rows, 256, 0, st>>>(a);
+    } else {
+        const unsigned blocks = (unsigned)(((int64_t)g->n_act * S + 2047) / 2048);
+        if (tv)
+            k_sweep_sparse<S, true><<<blocks, 256, 0, st>>>(a);
+        else
+            k_sweep_sparse<S, false><<<blocks, 256, 0, st>>>(a);
+    }
+}
+
+// Element masks of a record (element e: 0 density, 1 + c*sh_dim + k SH, >= n_arrays padding).
+static void element_masks(const cpx_grid* g, uint32_t* tv_mask, uint32_t* adam_mask)
+{
+    uint32_t tvm = 0, am = 0;
+    const int lo_tv = g->hierarchy ? g->band * g->band : 0;
+    const int hi = (g->band + 1) * (g->band + 1);
+    for (int e = 0; e < g->rec; e++) {
+        bool t = false, ad = false;
+        if (e == 0) {
+            t = ad = true;
+        } else if (e < g->n_arrays) {
+            const int k = (e - 1) % g->sh_dim;
+            t = k >= lo_tv && k < hi;
+            ad = !g->hierarchy || (k >= g->band * g->band && k < hi);
+        }
+        if (t) tvm |= 1u << e;
+        if (ad) am |= 1u << e;
+    }
+    *tv_mask = tvm;
+    *adam_mask = am;
 }
 
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
                       double sh_lr, int timestep, cudaStream_t st)
 {
     if (g->n_act == 0) return CPX_OK;
+    const int S = g->rec / 4;
+    if (g->n_act * S >= ((int64_t)1 << 32)) {
+        set_error("grid too large for 32-bit slot indices");
+        return CPX_ERR_UNSUPPORTED;
+    }
     SweepArgs a;
     a.W = g->W;
     a.H = g->H;
     a.D = g->D;
-    a.S = g->rec / 4;
-    a.n_arrays = g->n_arrays;
-    a.sh_dim = g->sh_dim;
-    a.band = g->band;
-    a.hierarchy = g->hierarchy;
-    a.n_act = g->n_act;
-    a.sparse = g->sparse;
+    a.n_act = (uint32_t)g->n_act;
     a.p_in = reinterpret_cast<const float4*>(g->params[g->cur]);
     a.p_out = reinterpret_cast<float4*>(g->params[g->cur ^ 1]);
     a.grad = reinterpret_cast<float4*>(g->grad);
     a.m = reinterpret_cast<float4*>(g->m);
     a.v = reinterpret_cast<float4*>(g->v);
     a.density_out = g->density;
-    a.adaptive_lr = g->adaptive_lr;
+    a.adaptive_lr = g->sparse ? nullptr : g->adaptive_lr;
     a.index_offsets = g->index_offsets;
     a.compact_to_dense = g->compact_to_dense;
+    a.in_cage = g->in_cage;
+    element_masks(g, &a.tv_mask, &a.adam_mask);
     a.lam_d = (float)lam_d;
     a.lam_sh = (float)lam_sh;
     a.lr = (float)lr;
     a.sh_lr = (float)sh_lr;
     a.timestep = timestep;
-    if (!g->sparse) {
-        const unsigned rows = (unsigned)((int64_t)g->H * g->D);
-        if (fused_tv)
-            k_sweep<true, false><<<rows, 256, 0, st>>>(a);
-        else
-            k_sweep<false, false><<<rows, 256, 0, st>>>(a);
-    } else {
-        const int64_t slots = g->n_act * a.S;
-        const unsigned blocks = (unsigned)((slots + 256 * 8 - 1) / (256 * 8));
-        if (fused_tv)
-            k_sweep<true, true><<<blocks, 256, 0, st>>>(a);
-        else
-            k_sweep<false, true><<<blocks, 256, 0, st>>>(a);
+    switch (S) {
+    case 1: launch_sweep<1>(g, a, fused_tv, st); break;
+    case 4: launch_sweep<4>(g, a, fused_tv, st); break;
+    case 7: launch_sweep<7>(g, a, fused_tv, st); break;
+    default:
+        set_error("record of %d slots unsupported", S);
+        return CPX_ERR_UNSUPPORTED;
     }
     count_launch();
     g->cur ^= 1;
@@ -287,8 +323,12 @@ __global__ void k_tv_type0(TvArgs a, int nbrs)
             for (int dx = -1; dx < 2; dx++)
                 ix[(dz + 1) * 9 + (dy + 1) * 3 + dx + 1] = nb_index(a, x + dx, y + dy, z + dz);
     if (a.sparse) {
+        // the reference's gate inCageInfo[indexOffsets[v]] (RenderUtils.cu:2669, 2608, 2770):
+        // the dense flag array read at the compact index.  Non-caged vertices (compact index 0)
+        // are skipped outright: when dense vertex 0 is in cage the reference would add racy
+        // terms to compact vertex 0 from every such position, which is not reproduced.
         const uint32_t dv = (uint32_t)(z * a.W * a.H + y * a.W + x);
-        if (!a.in_cage[dv]) return;
+        if (!a.in_cage[dv] || !a.in_cage[ix[13]]) return;
     }
     const int startSH = a.hierarchy ? a.band * a.band : 0;
     const int endSH = (a.band + 1) * (a.band + 1);

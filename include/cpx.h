@@ -93,6 +93,8 @@ cpx_status cpx_grid_info(const cpx_grid* g, int64_t* n_active, int* n_arrays, in
 /* Planar [n_arrays][n_active] host copies of parameters, gradients and moments. */
 cpx_status cpx_grid_upload_params(cpx_grid* g, const float* planar, int64_t n_active);
 cpx_status cpx_grid_download_params(const cpx_grid* g, float* planar, int64_t n_active);
+/* Same as cpx_grid_upload_params from a planar block already in device memory. */
+cpx_status cpx_grid_upload_params_device(cpx_grid* g, const float* planar_dev, int64_t n_active);
 cpx_status cpx_grid_upload_grads(cpx_grid* g, const float* planar, int64_t n_active);
 cpx_status cpx_grid_download_grads(const cpx_grid* g, float* planar, int64_t n_active);
 cpx_status cpx_grid_upload_moments(cpx_grid* g, const float* m, const float* v, int64_t n_active);

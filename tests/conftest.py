@@ -12,7 +12,7 @@ import sys
 import pytest
 
 REPO = pathlib.Path(__file__).resolve().parents[1]
-for sub in ("clear-plenoxels_b200", "oracle", "tests/golden"):
+for sub in ("", "clear-plenoxels_b200", "oracle", "tests/golden"):
     p = str(REPO / sub)
     if p not in sys.path:
         sys.path.insert(0, p)
