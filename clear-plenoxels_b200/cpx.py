@@ -53,7 +53,7 @@ EXPORTED = [
     "cpx_rays_upload", "cpx_rays_upload_packed", "cpx_rays_download", "cpx_rays_init_camera",
     "cpx_render_forward", "cpx_render_backward", "cpx_render_forward_backward", "cpx_tv_grad",
     "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_grid_check",
-    "cpx_last_sample_counts", "cpx_kernel_launches",
+    "cpx_last_sample_counts", "cpx_kernel_launches", "cpx_render_forward_backward_noalloc",
 ]
 
 

@@ -162,6 +162,21 @@ cpx_status cpx_render_backward(cpx_grid* g, cpx_rays* r, double* losses_dev,
 cpx_status cpx_render_forward_backward(cpx_grid* g, cpx_rays* r, double* losses_dev,
                                        const int32_t* sample_index_dev, int start, int len,
                                        double mask_coef, float huber_delta, cpx_stream stream);
+/* The same forward+backward as cpx_render_forward_backward without allocating device
+ * memory.  No counterpart in the reference: it is for callers that cannot allocate while
+ * they run -- a host whose own pool allocator owns the device memory, or a loop that may
+ * not allocate once it has started.  Its sample scratch is one fixed array (about 48 MiB)
+ * that the library holds on every device that loads it until the process exits; a batch
+ * may use at most 16384 rays and 1048576 sample slots (rays times the grid's per-ray sample
+ * bound), larger batches return CPX_ERR_INVALID_ARGUMENT.  The first call on a device looks
+ * up the array's device address; make that first call before any stream capture.  Every
+ * call on a device shares the array and overwrites it, so calls that overlap on the GPU
+ * race.  The call returns once the batch has run, with the status of its device-side
+ * checks; cpx_last_sample_counts does not see its counts. */
+cpx_status cpx_render_forward_backward_noalloc(cpx_grid* g, cpx_rays* r, double* losses_dev,
+                                               const int32_t* sample_index_dev, int start,
+                                               int len, double mask_coef, float huber_delta,
+                                               cpx_stream stream);
 /* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,
  * type 2 both. */
 cpx_status cpx_tv_grad(cpx_grid* g, double lam_density, double lam_sh, int type,
