@@ -41,26 +41,46 @@ __device__ __forceinline__ bool cell_occupied(const GridView& g, unsigned b0, un
     return (g.occ_bits[ci >> 5] >> (ci & 31)) & 1u;
 }
 
-__device__ __forceinline__ unsigned corner_vertex(const GridView& g, unsigned b0, unsigned b1,
-                                                  unsigned b2, int q)
+__device__ __forceinline__ int clamp_axis(unsigned b, int n)
 {
-    const int ox = (q >> 1) & 1;  // corner order 000,010,100,110,001,011,101,111 (x,y,z)
-    const int oy = q & 1;
-    const int oz = (q >> 2) & 1;
-    unsigned idx = (unsigned)scene_index((int)(b0 + ox), (int)(b1 + oy), (int)(b2 + oz), g.W,
-                                         g.H, g.D);
-    if (g.sparse) idx = g.index_offsets[idx];
-    return idx;
+    const int v = (int)b;  // getSceneIndex takes int coordinates (RenderUtils.cu:3-13)
+    return v < 0 ? 0 : (v > n - 1 ? n - 1 : v);
 }
 
-// L1 prefetch of the four 32-byte density sectors that hold a cell's 8 corners (dense grids).
+// The 8 corner vertices of cell (b0,b1,b2) in the reference's order 000,010,100,110,001,011,
+// 101,111 (x,y,z), each coordinate clamped to the grid as getSceneIndex does; sparse grids
+// map them through index_offsets (RenderUtils.cu:855-990).
+__device__ __forceinline__ void cell_corners(const GridView& g, unsigned b0, unsigned b1, unsigned b2,
+                                             unsigned* idx)
+{
+    const int x0 = clamp_axis(b0, g.W), x1 = clamp_axis(b0 + 1u, g.W);
+    const int y0 = clamp_axis(b1, g.H), y1 = clamp_axis(b1 + 1u, g.H);
+    const int z0 = clamp_axis(b2, g.D), z1 = clamp_axis(b2 + 1u, g.D);
+    const int WH = g.W * g.H;
+    const int r00 = z0 * WH + y0 * g.W, r01 = z0 * WH + y1 * g.W;
+    const int r10 = z1 * WH + y0 * g.W, r11 = z1 * WH + y1 * g.W;
+    idx[0] = (unsigned)(r00 + x0);
+    idx[1] = (unsigned)(r01 + x0);
+    idx[2] = (unsigned)(r00 + x1);
+    idx[3] = (unsigned)(r01 + x1);
+    idx[4] = (unsigned)(r10 + x0);
+    idx[5] = (unsigned)(r11 + x0);
+    idx[6] = (unsigned)(r10 + x1);
+    idx[7] = (unsigned)(r11 + x1);
+    if (g.sparse) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) idx[q] = g.index_offsets[idx[q]];
+    }
+}
+
+// L1 prefetch of the four 32-byte density sectors that hold a cell's 8 corners (dense grids:
+// corners q and q+2 differ only in x and share a sector).
 __device__ __forceinline__ void prefetch_cell(const GridView& g, unsigned b0, unsigned b1, unsigned b2)
 {
+    unsigned idx[8];
+    cell_corners(g, b0, b1, b2, idx);
 #pragma unroll
-    for (int q = 0; q < 8; q += 2) {  // corners q and q+2 differ only in x: same sector
-        const float* a = g.density + corner_vertex(g, b0, b1, b2, q);
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(a));
-    }
+    for (int q = 0; q < 8; q += 2) asm volatile("prefetch.global.L1 [%0];" ::"l"(g.density + idx[q]));
 }
 
 // ---------------------------------------------------------------------------
@@ -125,8 +145,10 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
             continue;
         }
         if (b0 != cb0 || b1 != cb1 || b2 != cb2) {
+            unsigned idx[8];
+            cell_corners(g, b0, b1, b2, idx);
 #pragma unroll
-            for (int q = 0; q < 8; q++) cd[q] = g.density[corner_vertex(g, b0, b1, b2, q)];
+            for (int q = 0; q < 8; q++) cd[q] = g.density[idx[q]];
             cb0 = b0;
             cb1 = b1;
             cb2 = b2;
@@ -260,8 +282,7 @@ __device__ __forceinline__ void sample_corners(const GridView& g, const SampleRe
     c.w[5] = x0 * y * z;
     c.w[6] = x * y0 * z;
     c.w[7] = x * y * z;
-#pragma unroll
-    for (int q = 0; q < 8; q++) c.idx[q] = corner_vertex(g, s.bx, s.by, s.bz, q);
+    cell_corners(g, s.bx, s.by, s.bz, c.idx);
 }
 
 template <int NSH>
@@ -271,17 +292,60 @@ struct RecShape {
     static constexpr int NV4 = REC / 4;
 };
 
-// Trilinear SH (raw, before the basis product) of one sample.
+// Per-warp table of the distinct corner vertices of one 32-sample chunk (about 100 of the
+// 256 corner references): key = vertex index.  In the forward the values hold each vertex's
+// view-dependent raw colour sum_k SH_ck * basis_k (the basis is constant along a ray, so a
+// sample's raw colour is the trilinear blend of its corners' raw colours); in the backward
+// they accumulate (density grad, R, G, B colour grads) before the scatter.  Values are four
+// separate arrays so neighbouring slots sit in different banks.
+constexpr int kHashSlots = 256;
+constexpr uint32_t kEmpty = 0xffffffffu;
+
+struct WarpTable {
+    uint32_t* keys;  // [kHashSlots]
+    float* va;       // [kHashSlots] x4
+    float* vb0;
+    float* vb1;
+    float* vb2;
+};
+
+__device__ __forceinline__ int table_slot(const WarpTable& t, uint32_t key)
+{
+    uint32_t h = (key * 0x9E3779B1u) >> 24;  // 8 bits
+    for (int probe = 0; probe < kHashSlots; probe++) {
+        const uint32_t old = atomicCAS(&t.keys[h], kEmpty, key);
+        if (old == kEmpty || old == key) return (int)h;
+        h = (h + 1) & (kHashSlots - 1);
+    }
+    return -1;  // unreachable: a chunk references at most 256 vertices
+}
+
+__device__ __forceinline__ void table_clear(const WarpTable& t, int lane)
+{
+    __syncwarp();
+    for (int s = lane; s < kHashSlots; s += 32) {
+        if (t.keys[s] == kEmpty) continue;
+        t.keys[s] = kEmpty;
+        t.va[s] = 0.f;
+        t.vb0[s] = 0.f;
+        t.vb1[s] = 0.f;
+        t.vb2[s] = 0.f;
+    }
+    __syncwarp();
+}
+
+// Raw view-dependent colour of every vertex in the table (forward).
 template <int NSH>
-__device__ __forceinline__ void gather_sh(const GridView& g, const Corners& c, float* sh)
+__device__ __forceinline__ void table_colours(const WarpTable& t, const GridView& g, const float* shs,
+                                              int lane)
 {
     using RS = RecShape<NSH>;
-#pragma unroll
-    for (int e = 0; e < 3 * NSH; e++) sh[e] = 0.f;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        const float4* rec = reinterpret_cast<const float4*>(g.params + (size_t)c.idx[q] * RS::REC);
-        const float wq = c.w[q];
+    __syncwarp();
+    for (int s = lane; s < kHashSlots; s += 32) {
+        const uint32_t key = t.keys[s];
+        if (key == kEmpty) continue;
+        const float4* rec = reinterpret_cast<const float4*>(g.params + (size_t)key * RS::REC);
+        float col[3] = {0.f, 0.f, 0.f};
 #pragma unroll
         for (int v = 0; v < RS::NV4; v++) {
             const float4 p = __ldg(rec + v);
@@ -289,37 +353,18 @@ __device__ __forceinline__ void gather_sh(const GridView& g, const Corners& c, f
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const int e = 4 * v + k;
-                if (e >= 1 && e < RS::NA) sh[e - 1] = fmaf(wq, pv[k], sh[e - 1]);
+                if (e >= 1 && e < RS::NA) {
+                    const int ch = (e - 1) / NSH;
+                    const int kk = (e - 1) % NSH;
+                    if (kk < g.n_sh_fwd) col[ch] = fmaf(pv[k], shs[kk], col[ch]);
+                }
             }
         }
+        t.vb0[s] = col[0];
+        t.vb1[s] = col[1];
+        t.vb2[s] = col[2];
     }
-}
-
-// Per-warp table that merges the corner contributions of one 32-sample chunk: key =
-// vertex index, value = (density grad, R, G, B colour-grad sums before the SH basis).
-constexpr int kHashSlots = 256;
-constexpr uint32_t kEmpty = 0xffffffffu;
-
-struct WarpTable {
-    uint32_t* keys;  // [kHashSlots]
-    float4* vals;    // [kHashSlots]
-};
-
-__device__ __forceinline__ void table_add(const WarpTable& t, uint32_t key, float a, float b0,
-                                          float b1, float b2)
-{
-    uint32_t h = (key * 0x9E3779B1u) >> 24;  // 8 bits
-    for (int probe = 0; probe < kHashSlots; probe++) {
-        const uint32_t old = atomicCAS(&t.keys[h], kEmpty, key);
-        if (old == kEmpty || old == key) {
-            atomicAdd(&t.vals[h].x, a);
-            atomicAdd(&t.vals[h].y, b0);
-            atomicAdd(&t.vals[h].z, b1);
-            atomicAdd(&t.vals[h].w, b2);
-            return;
-        }
-        h = (h + 1) & (kHashSlots - 1);
-    }
+    __syncwarp();
 }
 
 // Flush the table: one vertex record of gradients per distinct key, 16-byte vector atomics.
@@ -332,8 +377,8 @@ __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& 
     for (int s = lane; s < kHashSlots; s += 32) {
         const uint32_t key = t.keys[s];
         if (key == kEmpty) continue;
-        const float4 v = t.vals[s];
-        const float bch[3] = {v.y, v.z, v.w};
+        const float va = t.va[s];
+        const float bch[3] = {t.vb0[s], t.vb1[s], t.vb2[s]};
         float4* dst = reinterpret_cast<float4*>(g.grad + (size_t)key * RS::REC);
 #pragma unroll
         for (int q = 0; q < RS::NV4; q++) {
@@ -343,7 +388,7 @@ __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& 
                 const int e = 4 * q + k;
                 float val = 0.f;
                 if (e == 0) {
-                    val = v.x;
+                    val = va;
                 } else if (e < RS::NA) {
                     const int ch = (e - 1) / NSH;
                     const int kk = (e - 1) % NSH;
@@ -356,7 +401,10 @@ __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& 
             atomicAdd(dst + q, make_float4(e4[0], e4[1], e4[2], e4[3]));
         }
         t.keys[s] = kEmpty;
-        t.vals[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        t.va[s] = 0.f;
+        t.vb0[s] = 0.f;
+        t.vb1[s] = 0.f;
+        t.vb2[s] = 0.f;
     }
     __syncwarp();
 }
@@ -382,27 +430,33 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
     double s0 = 0., s1 = 0., s2 = 0.;
     for (int base = 0; base < n; base += 32) {
         const int i = base + lane;
-        if (i < n) {
-            const SampleRec s = S[i];
-            Corners cr;
+        const bool valid = i < n;
+        SampleRec s;
+        Corners cr;
+        int slot[8];
+        if (valid) {
+            s = S[i];
             sample_corners(g, s, cr);
-            float sh[3 * NSH];
-            gather_sh<NSH>(g, cr, sh);
-            float col[3];
 #pragma unroll
-            for (int ch = 0; ch < 3; ch++) {
-                float a = 0.f;
+            for (int q = 0; q < 8; q++) slot[q] = table_slot(tab, cr.idx[q]);
+        }
+        table_colours<NSH>(tab, g, shs, lane);
+        if (valid) {
+            float raw[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                for (int k = 0; k < NSH; k++)
-                    if (k < g.n_sh_fwd) a = fmaf(sh[ch * NSH + k], shs[k], a);
-                col[ch] = colour_act(a);
+            for (int q = 0; q < 8; q++) {
+                raw[0] = fmaf(cr.w[q], tab.vb0[slot[q]], raw[0]);
+                raw[1] = fmaf(cr.w[q], tab.vb1[slot[q]], raw[1]);
+                raw[2] = fmaf(cr.w[q], tab.vb2[slot[q]], raw[2]);
             }
+            const float col[3] = {colour_act(raw[0]), colour_act(raw[1]), colour_act(raw[2])};
             C[i] = make_float4(col[0], col[1], col[2], 0.f);
             const double w = (double)s.w;
             s0 += w * col[0];
             s1 += w * col[1];
             s2 += w * col[2];
         }
+        table_clear(tab, lane);
     }
     s0 = warp_sum(s0);
     s1 = warp_sum(s1);
@@ -504,7 +558,11 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
 #pragma unroll
             for (int q = 0; q < 8; q++) {
                 const float wq = cr.w[q];
-                table_add(tab, cr.idx[q], grad[0] * wq, grad[1] * wq, grad[2] * wq, grad[3] * wq);
+                const int sl = table_slot(tab, cr.idx[q]);
+                atomicAdd(&tab.va[sl], grad[0] * wq);
+                atomicAdd(&tab.vb0[sl], grad[1] * wq);
+                atomicAdd(&tab.vb1[sl], grad[2] * wq);
+                atomicAdd(&tab.vb2[sl], grad[3] * wq);
             }
         }
         table_flush<NSH>(tab, g, shs, lane);
@@ -534,7 +592,7 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
 constexpr int kShadeWarps = 4;
 
 template <int NSH, int MODE>
-__global__ void __launch_bounds__(kShadeWarps * 32) k_shade(GridView g, RaysView r,
+__global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysView r,
                                                              const int32_t* sidx, int start,
                                                              int len, const SampleRec* samples,
                                                              float4* colours, int maxs,
@@ -543,16 +601,14 @@ __global__ void __launch_bounds__(kShadeWarps * 32) k_shade(GridView g, RaysView
                                                              float huber)
 {
     __shared__ uint32_t h_keys[kShadeWarps][kHashSlots];
-    __shared__ float4 h_vals[kShadeWarps][kHashSlots];
+    __shared__ float h_vals[kShadeWarps][4][kHashSlots];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    if (MODE & kBackward) {
-        for (int s = lane; s < kHashSlots; s += 32) {
-            h_keys[warp][s] = kEmpty;
-            h_vals[warp][s] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        __syncwarp();
+    for (int s = lane; s < kHashSlots; s += 32) {
+        h_keys[warp][s] = kEmpty;
+        h_vals[warp][0][s] = h_vals[warp][1][s] = h_vals[warp][2][s] = h_vals[warp][3][s] = 0.f;
     }
+    __syncwarp();
     const int b = blockIdx.x * kShadeWarps + warp;
     if (b >= len) return;  // warp-uniform
     const int cnt = counts[b];
@@ -561,7 +617,7 @@ __global__ void __launch_bounds__(kShadeWarps * 32) k_shade(GridView g, RaysView
         return;
     }
     const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
-    const WarpTable tab{h_keys[warp], h_vals[warp]};
+    const WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
     shade_ray<NSH, MODE>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber, tab,
                          lane);
 }
