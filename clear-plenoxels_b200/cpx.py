@@ -54,6 +54,7 @@ EXPORTED = [
     "cpx_render_forward", "cpx_render_backward", "cpx_render_forward_backward", "cpx_tv_grad",
     "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_grid_check",
     "cpx_last_sample_counts", "cpx_kernel_launches", "cpx_render_forward_backward_noalloc",
+    "cpx_render_image", "cpx_image_mse",
 ]
 
 
@@ -148,6 +149,8 @@ _sig("cpx_tv_adam_step", [_vp, C.c_double, C.c_double, C.c_double, C.c_double, C
 _sig("cpx_train_step", [_vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), _vp,
                         C.POINTER(C.c_double), _vp])
 _sig("cpx_last_sample_counts", [_vp, _i32p, C.c_int])
+_sig("cpx_render_image", [_vp, C.POINTER(Camera), C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp])
+_sig("cpx_image_mse", [_vp, _vp, C.c_int64, C.POINTER(C.c_double), _vp])
 
 
 def _check(rc: int, where: str):
@@ -461,6 +464,25 @@ class RenderUtils:
                "renderRays_forwardBackward")
 
     @staticmethod
+    def renderImage(scene: ObjectScene, camera: Camera, width: int, height: int, whiteBG: bool = True,
+                    outputs=("rgb", "rgb8", "depth", "mask"), stream=None) -> dict:
+        """Held-out view render (RenderUtils::renderImage, RenderUtils.cu:1802).  Returns CUDA
+        tensors: rgb float32 [3, h*w], rgb8 uint8 [3, h*w], depth float32 [h*w], mask uint8
+        [h*w] (those named in `outputs`).  Pixel p is at row p // width and column
+        p % height, as the reference indexes it."""
+        import torch
+
+        n = int(width) * int(height)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        shapes = {"rgb": ((3, n), torch.float32), "rgb8": ((3, n), torch.uint8),
+                  "depth": ((n,), torch.float32), "mask": ((n,), torch.uint8)}
+        out = {k: torch.empty(shapes[k][0], dtype=shapes[k][1], device=dev) for k in outputs}
+        _check(_lib.cpx_render_image(scene.handle, C.byref(camera), int(width), int(height), int(bool(whiteBG)),
+                                     _ptr(out.get("rgb")), _ptr(out.get("rgb8")), _ptr(out.get("depth")),
+                                     _ptr(out.get("mask")), _stream(stream)), "renderImage")
+        return out
+
+    @staticmethod
     def addVarianceLoss(scene: ObjectScene, varianceCoefficient: float = 0.001,
                         shCoefficient: float = 0.001, varianceType: int = 0,
                         neighboorNums: int = 6, stream=None):
@@ -514,6 +536,21 @@ def train_step(scene: ObjectScene, rays: Rays, losses, *, start: int = 0, length
 def lr_decay(lr: float, batch_count: int, epoch: int) -> float:
     """Per-batch learning-rate decay of the reference (Render.cu:499-500)."""
     return lr / (2.0 ** (1.0 / batch_count / (epoch + 1.0)))
+
+
+def image_mse(a, b, stream=None) -> float:
+    """Mean squared difference of two float32 CUDA tensors of equal size (double sums)."""
+    if (a.numel() != b.numel() or str(a.dtype) != "torch.float32" or str(b.dtype) != "torch.float32"
+            or not a.is_contiguous() or not b.is_contiguous()):
+        raise ValueError("image_mse wants two contiguous tensors of the same size and dtype")
+    out = C.c_double(0.0)
+    _check(_lib.cpx_image_mse(_ptr(a), _ptr(b), int(a.numel()), C.byref(out), _stream(stream)), "image_mse")
+    return out.value
+
+
+def image_psnr(a, b, stream=None) -> float:
+    """PSNR of two images in [0, 1]: 10 log10(1 / mse)."""
+    return float(10.0 * np.log10(1.0 / image_mse(a, b, stream)))
 
 
 def psnr_from_mse(mse: float) -> float:

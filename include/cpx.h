@@ -177,6 +177,22 @@ cpx_status cpx_render_forward_backward_noalloc(cpx_grid* g, cpx_rays* r, double*
                                                const int32_t* sample_index_dev, int start,
                                                int len, double mask_coef, float huber_delta,
                                                cpx_stream stream);
+/* Held-out view render (RenderUtils::renderImage, SVRF/RenderUtils.cu:1801; the RGB branch of
+ * renderImageGPU, RenderUtils.cu:1720).  One ray per pixel of a width x height image through
+ * `cam`, in double as the reference sets it up (getBound), pixel p at row p / width and
+ * column p % height as the reference indexes it.  Outputs are device buffers, any may be
+ * NULL: rgb_dev float [3][w*h] (Image.red/green/blueFloatDevice, white background added
+ * when white_bg), rgb8_dev u8 [3][w*h] (red/green/blueDevice, composited on white),
+ * depth_dev float [w*h] (disparityDevice, the expected t), mask_dev u8 [w*h] (opacity x 255).
+ * Does not synchronise. */
+cpx_status cpx_render_image(cpx_grid* g, const cpx_camera* cam, int width, int height,
+                            int white_bg, float* rgb_dev, uint8_t* rgb8_dev, float* depth_dev,
+                            uint8_t* mask_dev, cpx_stream stream);
+/* No reference counterpart (the reference's Render::travelScene, SVRF/Render.cu:947, only
+ * saves its renders): mean of squared differences of two device float arrays of n elements,
+ * summed in double on the device, for held-out PSNR; synchronises. */
+cpx_status cpx_image_mse(const float* a_dev, const float* b_dev, int64_t n, double* mse_out,
+                         cpx_stream stream);
 /* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,
  * type 2 both. */
 cpx_status cpx_tv_grad(cpx_grid* g, double lam_density, double lam_sh, int type,

@@ -816,6 +816,100 @@ void orc_compact(const float* dense, int n_arrays, int64_t n_dense, const uint8_
     }
 }
 
+/* ------------------------------------------------------ R13 image render */
+
+/* getBound of the image path, all in double (RenderUtils.cu:34-97). */
+static void image_ray(const double* alpha, const double* principle, const double* c2w,
+                      const double* centre, const int* bbox, int row, int col, double info[5])
+{
+    const double xin[4] = {((double)col + 0.5 - principle[0]) / alpha[0],
+                           ((double)row + 0.5 - principle[1]) / alpha[1], 1.0, 1.0};
+    double sp[4];
+    for (int r = 0; r < 4; r++) {
+        sp[r] = 0.;
+        for (int c = 0; c < 4; c++) sp[r] = fma(c2w[r * 4 + c], xin[c], sp[r]);
+        sp[r] -= centre[r];
+    }
+    double sum = fma(sp[2], sp[2], fma(sp[0], sp[0], sp[1] * sp[1]));
+    sum = sqrt(sum);
+    sp[0] /= sum;
+    sp[1] /= sum;
+    sp[2] /= sum;
+    double t[6] = {
+        ((double)bbox[1] - centre[0]) / sp[0], ((double)bbox[0] - centre[0]) / sp[0],
+        ((double)bbox[3] - centre[1]) / sp[1], ((double)bbox[2] - centre[1]) / sp[1],
+        ((double)bbox[5] - centre[2]) / sp[2], ((double)bbox[4] - centre[2]) / sp[2],
+    };
+    double t_min = minf_d(t[0], t[1]);
+    double t_max = maxf_d(t[0], t[1]);
+    t_min = maxf_d(t_min, minf_d(t[2], t[3]));
+    t_max = minf_d(t_max, maxf_d(t[2], t[3]));
+    t_min = maxf_d(t_min, minf_d(t[4], t[5]));
+    t_max = minf_d(t_max, maxf_d(t[4], t[5]));
+    info[0] = t_min;
+    info[1] = t_max;
+    info[2] = sp[0];
+    info[3] = sp[1];
+    info[4] = sp[2];
+}
+
+void orc_render_image(const orc_scene* s, const double* alpha, const double* principle,
+                      const double* c2w, const double* centre, const int* bbox, int width,
+                      int height, int white_bg, float* rgb, uint8_t* rgb8, float* depth,
+                      uint8_t* mask)
+{
+    const int64_t npix = (int64_t)width * height;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(orc_get_threads())
+    for (int64_t p = 0; p < npix; p++) {
+        const int row = (int)(p / width);
+        const int col = (int)(p % height); /* the reference's column uses % height (RenderUtils.cu:1727) */
+        float acc_rgb[3] = {0.f, 0.f, 0.f};
+        float disp = 0.f;
+        uint8_t px8[3] = {0, 0, 0};
+        uint8_t m = 0;
+        double info[5];
+        image_ray(alpha, principle, c2w, centre, bbox, row, col, info);
+        if (info[0] > info[1]) {
+            px8[0] = px8[1] = px8[2] = 255;
+            if (white_bg) acc_rgb[0] = acc_rgb[1] = acc_rgb[2] = 1.f;
+        } else {
+            const float dir[3] = {(float)info[2], (float)info[3], (float)info[4]};
+            float shs[25];
+            orc_sh_basis(dir, shs);
+            double t = info[0], acc = 0., accd = 0.;
+            float tri[4];
+            while (t < info[1]) {
+                double bc[3];
+                for (int a = 0; a < 3; a++) bc[a] = fma(t, info[2 + a], centre[a]);
+                if (!trilerp_rgb(s, bc, shs, tri)) {
+                    t += (double)s->step;
+                    continue;
+                }
+                const float sigma = orc_density_activation(tri[0]);
+                const float c0 = orc_sigmoid(tri[1]), c1 = orc_sigmoid(tri[2]), c2 = orc_sigmoid(tri[3]);
+                const double Ti = exp(-accd);
+                const double w = Ti * (1. - (double)expf(-sigma * s->step));
+                acc += w;
+                disp = (float)fma(w, t, (double)disp);
+                acc_rgb[0] = (float)fma(w, (double)c0, (double)acc_rgb[0]);
+                acc_rgb[1] = (float)fma(w, (double)c1, (double)acc_rgb[1]);
+                acc_rgb[2] = (float)fma(w, (double)c2, (double)acc_rgb[2]);
+                accd = accd_add(accd, sigma, s->step);
+                t += fabs((double)s->step - w);
+            }
+            /* (int)((c + 1. - acc) * 255 + 0.5) with the multiply-add fused (RenderUtils.cu:1565) */
+            for (int c = 0; c < 3; c++) px8[c] = (uint8_t)(int)fma(((double)acc_rgb[c] + 1.) - acc, 255., 0.5);
+            if (white_bg)
+                for (int c = 0; c < 3; c++) acc_rgb[c] = (float)((double)acc_rgb[c] + (1. - acc));
+            m = (uint8_t)(acc * 255);
+        }
+        if (rgb) for (int c = 0; c < 3; c++) rgb[(int64_t)c * npix + p] = acc_rgb[c];
+        if (rgb8) for (int c = 0; c < 3; c++) rgb8[(int64_t)c * npix + p] = px8[c];
+        if (depth) depth[p] = disp;
+        if (mask) mask[p] = m;
+    }
+}
+
 /* ------------------------------------------------------ R11 */
 
 double orc_mse(const double* losses, int n)

@@ -121,6 +121,15 @@ uint32_t orc_occupancy(const float* density, int W, int H, int D, float threshol
 void orc_compact(const float* dense, int n_arrays, int64_t n_dense, const uint8_t* in_cage,
                  float* compact, int64_t n_compact);
 
+/* R13: render one view (renderImageGPU + volumeRender_RGB, RenderUtils.cu:1720-1810,
+ * 1443-1580, getBound in double at RenderUtils.cu:34-97).  Outputs (any may be NULL):
+ * rgb float planes [3][w*h] (background added when white_bg), rgb8 planes [3][w*h],
+ * depth (sum of w*t) [w*h], mask (acc*255) [w*h]. */
+void orc_render_image(const orc_scene* s, const double* alpha, const double* principle,
+                      const double* c2w, const double* centre, const int* bbox, int width,
+                      int height, int white_bg, float* rgb, uint8_t* rgb8, float* depth,
+                      uint8_t* mask);
+
 /* R11: batch MSE of the per-ray losses (Utils.cu:311-320). */
 double orc_mse(const double* losses, int n);
 

@@ -70,6 +70,7 @@ _fn("orc_occupancy", [_vp, C.c_int, C.c_int, C.c_int, C.c_float, _vp, _vp, _vp, 
 _fn("orc_compact", [_vp, C.c_int, C.c_int64, _vp, _vp, C.c_int64])
 _fn("orc_mse", [_vp, C.c_int], C.c_double)
 _fn("orc_composite_kat", [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp])
+_fn("orc_render_image", [C.POINTER(_Scene)] + [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
 
 
 def set_contract_mode(mode: int):
@@ -166,6 +167,23 @@ def rays_from_camera(cam, bbox, img_w, red, green, blue, mask, white_bg, pix, ou
     _lib.orc_rays_from_camera(_p(alpha), _p(principle), _p(c2w), _p(centre), _p(bb), int(img_w), _p(red),
                               _p(green), _p(blue), _p(mask), 1 if white_bg else 0, _p(pix), pix.size,
                               C.byref(out.c), int(out_start))
+
+
+def render_image(scene: Scene, cam, bbox, width, height, white_bg=True):
+    """Held-out view (RenderUtils::renderImage, RenderUtils.cu:1720-1810) -> dict of
+    rgb float32 [3, w*h], rgb8 uint8 [3, w*h], depth float32 [w*h], mask uint8 [w*h]."""
+    alpha = np.ascontiguousarray(cam["alpha"], np.float64)
+    principle = np.ascontiguousarray(cam["principle"], np.float64)
+    c2w = np.ascontiguousarray(cam["c2w"], np.float64).reshape(16)
+    centre = np.ascontiguousarray(cam["centre"], np.float64).reshape(4)
+    bb = np.ascontiguousarray(bbox, np.int32)
+    n = int(width) * int(height)
+    out = {"rgb": np.zeros((3, n), np.float32), "rgb8": np.zeros((3, n), np.uint8),
+           "depth": np.zeros(n, np.float32), "mask": np.zeros(n, np.uint8)}
+    _lib.orc_render_image(C.byref(scene.c), _p(alpha), _p(principle), _p(c2w), _p(centre), _p(bb), int(width),
+                          int(height), 1 if white_bg else 0, _p(out["rgb"]), _p(out["rgb8"]), _p(out["depth"]),
+                          _p(out["mask"]))
+    return out
 
 
 def render_forward(scene: Scene, rays: RaySet, sample_index=None, start=0, length=None):

@@ -311,6 +311,61 @@ int ref_rays_init(void* h, int ncam, const double* alpha, const double* principl
 
 int ref_rays_count(void* h) { return ((RefCtx*)h)->rays.totalRays; }
 
+// RenderUtils::renderImage (RenderUtils.cu:1802) of one camera into host buffers:
+// rgb float [3][w*h], rgb8 u8 [3][w*h], depth float [w*h], mask u8 [w*h].
+int ref_render_image(void* h, const double* alpha, const double* principle, const double* c2w,
+                     const double* centre, int width, int height, int white_bg, float* rgb,
+                     uint8_t* rgb8, float* depth, uint8_t* mask)
+{
+    RefCtx* c = (RefCtx*)h;
+    const size_t n = (size_t)width * height;
+    Camera cam;
+    cudaMalloc((void**)&cam.alphaDevice, sizeof(double) * 2);
+    cudaMemcpy(cam.alphaDevice, alpha, sizeof(double) * 2, cudaMemcpyHostToDevice);
+    cudaMalloc((void**)&cam.principleDevice, sizeof(double) * 2);
+    cudaMemcpy(cam.principleDevice, principle, sizeof(double) * 2, cudaMemcpyHostToDevice);
+    cudaMalloc((void**)&cam.c2wExternalMatDevice, sizeof(double) * 16);
+    cudaMemcpy(cam.c2wExternalMatDevice, c2w, sizeof(double) * 16, cudaMemcpyHostToDevice);
+    cudaMalloc((void**)&cam.cameraCenterDevice, sizeof(double) * 4);
+    cudaMemcpy(cam.cameraCenterDevice, centre, sizeof(double) * 4, cudaMemcpyHostToDevice);
+    Image im;
+    im.width = width;
+    im.height = height;
+    im.grayImage = false;
+    im.whiteBG = white_bg != 0;
+    float* fl[4];
+    uint8_t* by[4];
+    for (int p = 0; p < 4; p++) {
+        cudaMalloc((void**)&fl[p], sizeof(float) * n);
+        cudaMalloc((void**)&by[p], n);
+    }
+    im.redFloatDevice = fl[0];
+    im.greenFloatDevice = fl[1];
+    im.blueFloatDevice = fl[2];
+    im.disparityDevice = fl[3];
+    im.redDevice = by[0];
+    im.greenDevice = by[1];
+    im.blueDevice = by[2];
+    im.maskDevice = by[3];
+    RenderUtils::renderImage(im, cam, c->scene);
+    int rc = fail(cudaDeviceSynchronize());
+    for (int p = 0; p < 3; p++) {
+        if (!rc) rc = fail(cudaMemcpy(rgb + p * n, fl[p], sizeof(float) * n, cudaMemcpyDeviceToHost));
+        if (!rc) rc = fail(cudaMemcpy(rgb8 + p * n, by[p], n, cudaMemcpyDeviceToHost));
+    }
+    if (!rc) rc = fail(cudaMemcpy(depth, fl[3], sizeof(float) * n, cudaMemcpyDeviceToHost));
+    if (!rc) rc = fail(cudaMemcpy(mask, by[3], n, cudaMemcpyDeviceToHost));
+    for (int p = 0; p < 4; p++) {
+        cudaFree(fl[p]);
+        cudaFree(by[p]);
+    }
+    cudaFree(cam.alphaDevice);
+    cudaFree(cam.principleDevice);
+    cudaFree(cam.c2wExternalMatDevice);
+    cudaFree(cam.cameraCenterDevice);
+    return rc;
+}
+
 // Download the ray table: 8 float inputs, 4 byte inputs, 5 float outputs.
 int ref_rays_download(void* h, float* ox, float* oy, float* oz, float* dx, float* dy, float* dz,
                       float* near_t, float* far_t, uint8_t* mask, uint8_t* r, uint8_t* g,

@@ -52,6 +52,7 @@ def _setup(L):
     s("ref_rays_create", [_vp, C.c_int, C.c_int] + [_vp] * 12)
     s("ref_rays_init", [_vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int])
     s("ref_rays_count", [_vp])
+    s("ref_render_image", [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
     s("ref_rays_download", [_vp] + [_vp] * 17)
     s("ref_render_forward", [_vp, C.c_int, C.c_int])
     s("ref_render_backward", [_vp, C.c_int, C.c_int, C.c_double, C.c_float, _vp])
@@ -143,6 +144,20 @@ class RefScene:
                  "acc_density", "acc_weights", "acc_r", "acc_g", "acc_b")
         out = {k: np.zeros(n, np.uint8 if k in ("mask", "r", "g", "b") else np.float32) for k in names}
         _ck(lib().ref_rays_download(self.h, *[_p(out[k]) for k in names]), "rays_download")
+        return out
+
+    def render_image(self, cam, width, height, white_bg=True):
+        """RenderUtils::renderImage of one camera -> rgb [3, w*h], rgb8 [3, w*h], depth, mask."""
+        alpha = np.ascontiguousarray(cam["alpha"], np.float64)
+        principle = np.ascontiguousarray(cam["principle"], np.float64)
+        c2w = np.ascontiguousarray(cam["c2w"], np.float64).reshape(16)
+        centre = np.ascontiguousarray(cam["centre"], np.float64).reshape(4)
+        n = int(width) * int(height)
+        out = {"rgb": np.zeros((3, n), np.float32), "rgb8": np.zeros((3, n), np.uint8),
+               "depth": np.zeros(n, np.float32), "mask": np.zeros(n, np.uint8)}
+        _ck(lib().ref_render_image(self.h, _p(alpha), _p(principle), _p(c2w), _p(centre), int(width), int(height),
+                                   1 if white_bg else 0, _p(out["rgb"]), _p(out["rgb8"]), _p(out["depth"]),
+                                   _p(out["mask"])), "render_image")
         return out
 
     def render_forward(self, start, length):
