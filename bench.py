@@ -226,7 +226,7 @@ def run_ours(args, wl, world, rank, local):
     torch.cuda.empty_cache()
 
     # ---- training grid and the ray pool in its voxel space
-    scene = cpx.ObjectScene(n, n, n, SH_DIM)
+    scene = cpx.ObjectScene(n, n, n, SH_DIM, precision=args.precision, sr_seed=wl["seed"] + 1)
     init = torch.zeros((1 + 3 * SH_DIM, n ** 3), dtype=torch.float32, device=dev)
     init[0] = wl["init_density"]
     scene.upload_params_device(init)
@@ -280,6 +280,16 @@ def run_ours(args, wl, world, rank, local):
     clk = clocks.stop()
     dist_barrier(world)
     scene.check()
+    # vertices whose gradient records a sweep reads: counted on untimed batches of the pool
+    tcounts = []
+    for k in range(min(4, wl["pool_batches"])):
+        b = (W + K + k) % wl["pool_batches"]
+        cpx.RenderUtils.renderRays_forwardBackward(scene, pool, losses, None, b * R, R, STEP["mask_coef"],
+                                                   STEP["huber"], stream=stream)
+        tcounts.append(scene.touched_count())
+        cpx.Optimizer.varianceAndUpdate(scene, STEP["lam_density"], STEP["lam_sh"], lr[0], lr[1], W + K + k + 1,
+                                        stream=stream)
+    touched = float(np.mean(tcounts))
     ms_local = t0.elapsed_time(t1)
     ms = dist_max(ms_local, world, True)
     march_ms = float(np.mean([evs[k][0].elapsed_time(evs[k][1]) for k in range(K)]))
@@ -298,7 +308,7 @@ def run_ours(args, wl, world, rank, local):
         batch_rays.upload_packed(host_pool[b * R:(b + 1) * R], stream=stream)
         mses.append(cpx.train_step(scene, batch_rays, losses, start=0, length=R, mask_coef=STEP["mask_coef"],
                                    huber_delta=STEP["huber"], lam_density=STEP["lam_density"],
-                                   lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1], timestep=W + K + k + 1,
+                                   lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1], timestep=W + K + 4 + k + 1,
                                    want_mse=True, stream=stream))
     e1.record(stream)
     torch.cuda.synchronize()
@@ -309,25 +319,37 @@ def run_ours(args, wl, world, rank, local):
     # ---- roofline of the fused TV+Adam sweep
     N = n ** 3
     rec = 28 * 4
-    alg_bytes = N * (8 * rec + 4 + 4)  # params r+w, grad r+zero-w, m r+w, v r+w, density mirror w, LR mult r
+    # gradient records are read and zeroed only for the vertices the batch touched
+    if args.precision == "fp32":
+        # params r+w, m r+w, v r+w, density mirror w, LR mult r; grad r + zero-w where touched
+        alg_bytes = N * (6 * rec + 4 + 4) + touched * 2 * rec
+        sweep_kernel = "k_sweep<TV,dense> (fused TV type0/6 + Adam)"
+    else:
+        # density r+w, 16-bit SH r+w, 16-bit m r+w, 16-bit v r+w, LR mult r; FP32 grad r +
+        # zero-w where touched
+        lrec = 28 * 2
+        alg_bytes = N * (8 + 6 * lrec + 4) + touched * 2 * rec
+        sweep_kernel = "k_sweep_lowp_dense<TV> (fused TV type0/6 + Adam, 16-bit storage, stochastic rounding)"
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
-    tpv = profiled_traffic_per_vertex()
-    roofline = {"bound": "hbm", "kernel": "k_sweep<TV,dense> (fused TV type0/6 + Adam)", "achieved": round(achieved, 1),
+    tpv = profiled_traffic_per_vertex() if args.precision == "fp32" else None
+    roofline = {"bound": "hbm", "kernel": sweep_kernel, "achieved": round(achieved, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "alg_bytes_per_launch": int(alg_bytes), "traffic": None if tpv is None else int(tpv * N),
+                "alg_bytes_per_launch": int(alg_bytes), "touched_vertices_per_launch": int(touched),
+                "traffic": None if tpv is None else int(tpv * N),
                 "launch_ms": round(sweep_ms, 4)}
 
     result = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": "f32" if args.precision == "fp32" else "f32 arithmetic, %s SH + bf16 moments" % args.precision,
         "data": "synthetic: seeded 64-blob 512^3 hidden grid rendered by the plain forward; no dataset",
         "config": {
             "workload": "plain FP32 training at scale: %d^3 grid SH band 2 (density 0.1, SH 0 init), %d-ray "
                         "batches from %d %dx%d views of a hidden %d^3 64-blob grid, TV type 0/6 + Adam every batch"
                         % (n, R, wl["cams"], wl["img"], wl["img"], wl["gt_n"]),
             "grid": n, "sh_dim": SH_DIM, "batch_rays": R, "pool_rays": P, "step_constants": STEP,
+            "precision": args.precision,
             "l2": "inputs larger than L2: the sweep streams %.1f GB of grid state per step" % (alg_bytes / 1e9),
             "parallelism": "replicas" if world > 1 else "single GPU",
         },
@@ -448,7 +470,7 @@ def run_reference(args, wl):
     return {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
         "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "impl": "reference",
+        "dtype": "f32" if args.precision == "fp32" else "f32 arithmetic, %s SH + bf16 moments" % args.precision, "impl": "reference",
         "data": "synthetic: seeded 64-blob 512^3 hidden grid rendered by the reference's forward; no dataset",
         "config": {"workload": "same as --impl ours", "grid": n, "batch_rays": R, "step_constants": STEP,
                    "entry_points": "RenderUtils::renderRays, renderRays_withGradients_RGB, losses D2H + "
@@ -472,6 +494,8 @@ def main():
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="plain256")
     ap.add_argument("--cpu-rays", type=int, default=512, help="rays in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=("fp32", "bf16", "fp16"), default="fp32",
+                    help="storage form of the training grid (fp32: the reference's)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

@@ -54,7 +54,7 @@ EXPORTED = [
     "cpx_render_forward", "cpx_render_backward", "cpx_render_forward_backward", "cpx_tv_grad",
     "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_grid_check",
     "cpx_last_sample_counts", "cpx_kernel_launches", "cpx_render_forward_backward_noalloc",
-    "cpx_render_image", "cpx_image_mse",
+    "cpx_render_image", "cpx_image_mse", "cpx_grid_touched_count",
 ]
 
 
@@ -70,8 +70,12 @@ class GridDesc(C.Structure):
     _fields_ = [
         ("width", C.c_int), ("height", C.c_int), ("depth", C.c_int),
         ("sh_dim", C.c_int), ("optimizing_band", C.c_int), ("hierarchy_strategy", C.c_int),
-        ("step_size", C.c_float), ("bbox", C.c_int * 6),
+        ("step_size", C.c_float), ("bbox", C.c_int * 6), ("precision", C.c_int), ("sr_seed", C.c_uint32),
     ]
+
+
+# storage forms (cpx_precision)
+PRECISIONS = {"fp32": 0, "bf16": 1, "fp16": 2}
 
 
 class Camera(C.Structure):
@@ -151,6 +155,7 @@ _sig("cpx_train_step", [_vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), _v
 _sig("cpx_last_sample_counts", [_vp, _i32p, C.c_int])
 _sig("cpx_render_image", [_vp, C.POINTER(Camera), C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _sig("cpx_image_mse", [_vp, _vp, C.c_int64, C.POINTER(C.c_double), _vp])
+_sig("cpx_grid_touched_count", [_vp, C.POINTER(C.c_int64)])
 
 
 def _check(rc: int, where: str):
@@ -191,7 +196,9 @@ class ObjectScene:
     """Grid + optimizer state (objectScene, SceneUtils.cuh:4-98, and optimizer, Optimizer.cuh)."""
 
     def __init__(self, width, height, depth, sh_dim=9, optimizing_band=None, step_size=0.5,
-                 hierarchy_strategy=False, bbox=None):
+                 hierarchy_strategy=False, bbox=None, precision="fp32", sr_seed=0):
+        """precision: "fp32" (the reference's form) or the mixed forms "bf16" / "fp16"
+        (16-bit SH and moments, FP32 density, gradients and march, stochastic rounding)."""
         if optimizing_band is None:
             optimizing_band = int(round(sh_dim ** 0.5)) - 1
         if bbox is None:  # initSelf: bbox spans the grid (SceneUtils.cu:107-112)
@@ -203,6 +210,11 @@ class ObjectScene:
         d.hierarchy_strategy = 1 if hierarchy_strategy else 0
         d.step_size = float(step_size)
         d.bbox[:] = [int(b) for b in bbox]
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        d.precision = PRECISIONS[precision]
+        d.sr_seed = int(sr_seed) & 0xFFFFFFFF
+        self.precision = precision
         self.desc = d
         self.width, self.height, self.depth = d.width, d.height, d.depth
         self.sh_dim = d.sh_dim
@@ -321,6 +333,12 @@ class ObjectScene:
         _check(_lib.cpx_occupancy_build(self._h, float(threshold), occ.ctypes.data, cage.ctypes.data,
                                         idx.ctypes.data, C.byref(cnt)), "cpx_occupancy_build")
         return occ, cage, idx, int(cnt.value)
+
+    def touched_count(self) -> int:
+        """Vertices whose gradient records the next optimizer sweep will read."""
+        t = C.c_int64()
+        _check(_lib.cpx_grid_touched_count(self._h, C.byref(t)), "cpx_grid_touched_count")
+        return int(t.value)
 
     def make_sparse(self):
         _check(_lib.cpx_grid_make_sparse(self._h), "cpx_grid_make_sparse")

@@ -51,6 +51,35 @@ __global__ void k_get_column(float* col, const float* aos, int64_t n, int rec, i
     col[i] = aos[i * rec + e];
 }
 
+// Column e of 16-bit records <-> a packed float array (round to nearest on the way in).
+template <int PREC>
+__global__ void k_set_column16(uint16_t* recs, const float* col, int64_t n, int slots, int e)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    recs[i * slots + e] = f_to_sh_rn<PREC>(col[i]);
+}
+
+template <int PREC>
+__global__ void k_get_column16(float* col, const uint16_t* recs, int64_t n, int slots, int e)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    col[i] = sh_to_f<PREC>(recs[i * slots + e]);
+}
+
+// Number of set bits of a word array (block reduction, one atomic per block).
+__global__ void k_popcount(const uint32_t* __restrict__ w, int64_t n, unsigned long long* out)
+{
+    __shared__ unsigned int part;
+    if (threadIdx.x == 0) part = 0;
+    __syncthreads();
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(&part, (unsigned)__popc(w[i]));
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(out, (unsigned long long)part);
+}
+
 __global__ void k_fill(float* p, int64_t n, float v)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -82,19 +111,60 @@ __global__ void k_unpack_rays(const uint32_t* __restrict__ src, int64_t count, i
 
 static unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
-// Host planar [n_arrays][n] <-> device records, one array at a time through a staging column.
-static cpx_status planar_to_records(float* aos, const float* planar, int64_t n, int n_arrays,
-                                    int rec, float* density_out)
+// Which per-vertex state a planar column belongs to.
+enum Field { kParams = 0, kGrads = 1, kMoment1 = 2, kMoment2 = 3 };
+
+// Device column a (n floats) -> the grid's storage of `f`.
+static void set_column(cpx_grid* g, Field f, const float* col, int64_t n, int a)
+{
+    const unsigned nb = blocks_for(n);
+    if (f == kGrads) {
+        k_set_column<<<nb, 256>>>(g->grad, col, n, g->rec, a, nullptr);
+    } else if (g->prec == kPrecFP32) {
+        float* dst = f == kParams ? g->params[g->cur] : (f == kMoment1 ? g->m : g->v);
+        k_set_column<<<nb, 256>>>(dst, col, n, g->rec, a, (f == kParams && a == 0) ? g->density : nullptr);
+    } else if (f == kParams && a == 0) {
+        k_set_column<<<nb, 256>>>(g->dens[g->cur], col, n, 1, 0, nullptr);
+    } else if (f == kParams && g->prec == kPrecFP16) {
+        k_set_column16<kPrecFP16><<<nb, 256>>>(g->sh16[g->cur], col, n, g->slots, a);
+    } else {
+        uint16_t* dst = f == kParams ? g->sh16[g->cur] : (f == kMoment1 ? g->m16 : g->v16);
+        k_set_column16<kPrecBF16><<<nb, 256>>>(dst, col, n, g->slots, a);
+    }
+    count_launch();
+}
+
+// The grid's storage of `f`, column a -> device column (n floats).
+static void get_column(const cpx_grid* g, Field f, float* col, int64_t n, int a)
+{
+    const unsigned nb = blocks_for(n);
+    if (f == kGrads) {
+        k_get_column<<<nb, 256>>>(col, g->grad, n, g->rec, a);
+    } else if (g->prec == kPrecFP32) {
+        const float* src = f == kParams ? g->params[g->cur] : (f == kMoment1 ? g->m : g->v);
+        k_get_column<<<nb, 256>>>(col, src, n, g->rec, a);
+    } else if (f == kParams && a == 0) {
+        k_get_column<<<nb, 256>>>(col, g->dens[g->cur], n, 1, 0);
+    } else if (f == kParams && g->prec == kPrecFP16) {
+        k_get_column16<kPrecFP16><<<nb, 256>>>(col, g->sh16[g->cur], n, g->slots, a);
+    } else {
+        const uint16_t* src = f == kParams ? g->sh16[g->cur] : (f == kMoment1 ? g->m16 : g->v16);
+        k_get_column16<kPrecBF16><<<nb, 256>>>(col, src, n, g->slots, a);
+    }
+    count_launch();
+}
+
+// Host planar [n_arrays][n] <-> device storage, one array at a time through a staging column.
+static cpx_status planar_to_records(cpx_grid* g, Field f, const float* planar, int64_t n)
 {
     if (n == 0) return CPX_OK;
     float* col = nullptr;
     cudaError_t e = cudaMalloc((void**)&col, n * sizeof(float));
     if (e != cudaSuccess) return cuda_status(e, "upload staging");
-    for (int a = 0; a < n_arrays && e == cudaSuccess; a++) {
+    for (int a = 0; a < g->n_arrays && e == cudaSuccess; a++) {
         e = cudaMemcpy(col, planar + (int64_t)a * n, n * sizeof(float), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) break;
-        k_set_column<<<blocks_for(n), 256>>>(aos, col, n, rec, a, a == 0 ? density_out : nullptr);
-        count_launch();
+        set_column(g, f, col, n, a);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -102,16 +172,14 @@ static cpx_status planar_to_records(float* aos, const float* planar, int64_t n, 
     return cuda_status(e, "upload");
 }
 
-static cpx_status records_to_planar(float* planar, const float* aos, int64_t n, int n_arrays,
-                                    int rec)
+static cpx_status records_to_planar(const cpx_grid* g, Field f, float* planar, int64_t n)
 {
     if (n == 0) return CPX_OK;
     float* col = nullptr;
     cudaError_t e = cudaMalloc((void**)&col, n * sizeof(float));
     if (e != cudaSuccess) return cuda_status(e, "download staging");
-    for (int a = 0; a < n_arrays && e == cudaSuccess; a++) {
-        k_get_column<<<blocks_for(n), 256>>>(col, aos, n, rec, a);
-        count_launch();
+    for (int a = 0; a < g->n_arrays && e == cudaSuccess; a++) {
+        get_column(g, f, col, n, a);
         e = cudaMemcpy(planar + (int64_t)a * n, col, n * sizeof(float), cudaMemcpyDeviceToHost);
     }
     cudaFree(col);
@@ -137,14 +205,24 @@ static cpx_status check_n(const cpx_grid* g, int64_t n)
     return CPX_OK;
 }
 
+// Frees the per-vertex state (parameters, gradients, moments, density) and clears the pointers.
+void free_state(cpx_grid* g)
+{
+    if (g->prec == kPrecFP32) cudaFree(g->density);  // the mixed forms alias dens[cur]
+    g->density = nullptr;
+    void** bufs[13] = {(void**)&g->params[0], (void**)&g->params[1], (void**)&g->grad, (void**)&g->m,
+                       (void**)&g->v, (void**)&g->sh16[0], (void**)&g->sh16[1], (void**)&g->m16,
+                       (void**)&g->v16, (void**)&g->dens[0], (void**)&g->dens[1],
+                       (void**)&g->touched[0], (void**)&g->touched[1]};
+    for (auto b : bufs) {
+        cudaFree(*b);
+        *b = nullptr;
+    }
+}
+
 static void free_grid(cpx_grid* g)
 {
-    cudaFree(g->params[0]);
-    cudaFree(g->params[1]);
-    cudaFree(g->grad);
-    cudaFree(g->m);
-    cudaFree(g->v);
-    cudaFree(g->density);
+    free_state(g);
     cudaFree(g->adaptive_lr);
     cudaFree(g->occ_bytes);
     cudaFree(g->occ_bits);
@@ -158,6 +236,41 @@ static void free_grid(cpx_grid* g)
     cudaFree(g->scratch.acc);
     cudaFree(g->scratch.err);
     cudaFree(g->scratch.mse);
+}
+
+// Zeroed per-vertex state of `n` active vertices in the grid's storage form.
+cudaError_t alloc_state(cpx_grid* g, int64_t n)
+{
+    const int64_t nn = n > 0 ? n : 1;
+    const size_t rb = (size_t)nn * g->rec * sizeof(float);
+    cudaError_t e = cudaSuccess;
+    auto get = [&](void** p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+    };
+    get((void**)&g->grad, rb);
+    const size_t tb = (size_t)((nn + 31) / 32) * sizeof(uint32_t);
+    get((void**)&g->touched[0], tb);
+    get((void**)&g->touched[1], tb);
+    g->tcur = 0;
+    g->all_touched = 0;
+    if (g->prec == kPrecFP32) {
+        get((void**)&g->params[0], rb);
+        get((void**)&g->params[1], rb);
+        get((void**)&g->m, rb);
+        get((void**)&g->v, rb);
+        get((void**)&g->density, (size_t)nn * sizeof(float));
+    } else {
+        const size_t hb = (size_t)nn * g->slots * sizeof(uint16_t);
+        get((void**)&g->sh16[0], hb);
+        get((void**)&g->sh16[1], hb);
+        get((void**)&g->m16, hb);
+        get((void**)&g->v16, hb);
+        get((void**)&g->dens[0], (size_t)nn * sizeof(float));
+        get((void**)&g->dens[1], (size_t)nn * sizeof(float));
+        g->density = g->dens[g->cur];
+    }
+    return e;
 }
 
 }  // namespace cpx
@@ -217,6 +330,11 @@ cpx_status cpx_grid_create(const cpx_grid_desc* d, cpx_grid** out)
         set_error("step_size must be positive and finite");
         return CPX_ERR_INVALID_ARGUMENT;
     }
+    if (d->precision != CPX_PRECISION_FP32 && d->precision != CPX_PRECISION_BF16 &&
+        d->precision != CPX_PRECISION_FP16) {
+        set_error("unknown precision %d", d->precision);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
     cpx_grid* g = new (std::nothrow) cpx_grid();
     if (!g) return CPX_ERR_OUT_OF_MEMORY;
     g->W = d->width;
@@ -232,15 +350,10 @@ cpx_status cpx_grid_create(const cpx_grid_desc* d, cpx_grid** out)
     for (int i = 0; i < 6; i++) g->bbox[i] = d->bbox[i];
     g->n_dense = n;
     g->n_act = n;
-    const size_t rb = (size_t)n * g->rec * sizeof(float);
-    cudaError_t e = cudaSuccess;
-    float** bufs[5] = {&g->params[0], &g->params[1], &g->grad, &g->m, &g->v};
-    for (auto b : bufs) {
-        if (e == cudaSuccess) e = cudaMalloc((void**)b, rb);
-        if (e == cudaSuccess) e = cudaMemset(*b, 0, rb);
-    }
-    if (e == cudaSuccess) e = cudaMalloc((void**)&g->density, n * sizeof(float));
-    if (e == cudaSuccess) e = cudaMemset(g->density, 0, n * sizeof(float));
+    g->prec = d->precision;
+    g->sr_seed = d->sr_seed;
+    g->slots = lowp_slots(g->n_arrays);
+    cudaError_t e = alloc_state(g, n);
     if (e == cudaSuccess) e = cudaMalloc((void**)&g->adaptive_lr, n * sizeof(float));
     if (e == cudaSuccess) {
         k_fill<<<blocks_for(n), 256>>>(g->adaptive_lr, n, 1.f);
@@ -281,18 +394,14 @@ cpx_status cpx_grid_upload_params(cpx_grid* g, const float* planar, int64_t n)
 {
     if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
-    return planar_to_records(g->params[g->cur], planar, n, g->n_arrays, g->rec, g->density);
+    return planar_to_records(g, kParams, planar, n);
 }
 
 cpx_status cpx_grid_upload_params_device(cpx_grid* g, const float* planar_dev, int64_t n)
 {
     if (check_grid(g) || !planar_dev) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
-    for (int a = 0; a < g->n_arrays; a++) {
-        k_set_column<<<blocks_for(n), 256>>>(g->params[g->cur], planar_dev + (int64_t)a * n, n, g->rec, a,
-                                              a == 0 ? g->density : nullptr);
-        count_launch();
-    }
+    for (int a = 0; a < g->n_arrays; a++) set_column(g, kParams, planar_dev + (int64_t)a * n, n, a);
     return cuda_status(cudaDeviceSynchronize(), "device upload");
 }
 
@@ -301,14 +410,15 @@ cpx_status cpx_grid_download_params(const cpx_grid* g, float* planar, int64_t n)
     if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
     cudaDeviceSynchronize();
-    return records_to_planar(planar, g->params[g->cur], n, g->n_arrays, g->rec);
+    return records_to_planar(g, kParams, planar, n);
 }
 
 cpx_status cpx_grid_upload_grads(cpx_grid* g, const float* planar, int64_t n)
 {
     if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
-    return planar_to_records(g->grad, planar, n, g->n_arrays, g->rec, nullptr);
+    g->all_touched = 1;  // gradients may be non-zero anywhere
+    return planar_to_records(g, kGrads, planar, n);
 }
 
 cpx_status cpx_grid_download_grads(const cpx_grid* g, float* planar, int64_t n)
@@ -316,16 +426,16 @@ cpx_status cpx_grid_download_grads(const cpx_grid* g, float* planar, int64_t n)
     if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
     cudaDeviceSynchronize();
-    return records_to_planar(planar, g->grad, n, g->n_arrays, g->rec);
+    return records_to_planar(g, kGrads, planar, n);
 }
 
 cpx_status cpx_grid_upload_moments(cpx_grid* g, const float* m, const float* v, int64_t n)
 {
     if (check_grid(g) || !m || !v) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
-    cpx_status s = planar_to_records(g->m, m, n, g->n_arrays, g->rec, nullptr);
+    cpx_status s = planar_to_records(g, kMoment1, m, n);
     if (s != CPX_OK) return s;
-    return planar_to_records(g->v, v, n, g->n_arrays, g->rec, nullptr);
+    return planar_to_records(g, kMoment2, v, n);
 }
 
 cpx_status cpx_grid_download_moments(const cpx_grid* g, float* m, float* v, int64_t n)
@@ -333,9 +443,9 @@ cpx_status cpx_grid_download_moments(const cpx_grid* g, float* m, float* v, int6
     if (check_grid(g) || !m || !v) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
     cudaDeviceSynchronize();
-    cpx_status s = records_to_planar(m, g->m, n, g->n_arrays, g->rec);
+    cpx_status s = records_to_planar(g, kMoment1, m, n);
     if (s != CPX_OK) return s;
-    return records_to_planar(v, g->v, n, g->n_arrays, g->rec);
+    return records_to_planar(g, kMoment2, v, n);
 }
 
 cpx_status cpx_grid_set_adaptive_lr(cpx_grid* g, const float* lr_mult, int64_t n_dense)
@@ -627,10 +737,14 @@ cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int sta
 {
     if (check_grid(g) || !r || !a) return CPX_ERR_INVALID_ARGUMENT;
     cudaStream_t st = (cudaStream_t)stream;
+    const bool fuse = a->do_tv && a->tv_type == 0 && a->tv_neighbours == 6;
+    if (a->do_tv && !fuse && g->prec != kPrecFP32) {
+        set_error("the mixed forms run TV type 0 / 6 neighbours fused into the optimizer sweep only");
+        return CPX_ERR_UNSUPPORTED;
+    }
     cpx_status s = march_launch(g, r, sidx, start, len, kForwardBackward, losses, a->mask_coef,
                                 a->huber_delta, st);
     if (s != CPX_OK) return s;
-    const bool fuse = a->do_tv && a->tv_type == 0 && a->tv_neighbours == 6;
     if (a->do_tv && !fuse) {
         s = tv_launch(g, a->lam_density, a->lam_sh, a->tv_type, a->tv_neighbours, st);
         if (s != CPX_OK) return s;
@@ -650,6 +764,27 @@ cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int sta
         if (e != cudaSuccess) return cuda_status(e, "mse");
     }
     return CPX_OK;
+}
+
+cpx_status cpx_grid_touched_count(cpx_grid* g, int64_t* count)
+{
+    if (check_grid(g) || !count) return CPX_ERR_INVALID_ARGUMENT;
+    if (g->all_touched) {
+        *count = g->n_act;
+        return CPX_OK;
+    }
+    unsigned long long* d = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_status(e, "touched count");
+    cudaMemset(d, 0, sizeof(unsigned long long));
+    const int64_t words = (g->n_act + 31) / 32;
+    k_popcount<<<blocks_for(words), 256>>>(g->touched[g->tcur], words, d);
+    count_launch();
+    unsigned long long v = 0;
+    e = cudaMemcpy(&v, d, sizeof(v), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    *count = (int64_t)v;
+    return cuda_status(e, "touched count");
 }
 
 cpx_status cpx_grid_check(cpx_grid* g)

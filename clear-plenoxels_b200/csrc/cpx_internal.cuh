@@ -18,6 +18,7 @@
 #include <cstdio>
 
 #include "../../include/cpx.h"
+#include "lowp.cuh"
 
 namespace cpx {
 
@@ -41,7 +42,11 @@ struct GridView {
     float step;
     int sparse;
     int64_t n_act;
-    const float* __restrict__ params;   // [n_act][rec]
+    // FP32 form: parameter records [n_act][rec].  Mixed forms: the 16-bit SH records
+    // [n_act][slots], read through sh16_records() by kernels instantiated for those forms
+    // (the storage form is a template parameter of every kernel, so the view stays as small
+    // as the FP32 kernels need).
+    const float* __restrict__ params;
     const float* __restrict__ density;  // [n_act]
     float* grad;                        // [n_act][rec]
     const uint32_t* __restrict__ occ_bits;       // [(C + 31) / 32]
@@ -95,12 +100,27 @@ struct cpx_grid {
     int bbox[6];
     int64_t n_dense, n_act;
     int sparse = 0;
-    float* params[2] = {nullptr, nullptr};
+    int prec = 0;          // cpx_precision
+    uint32_t sr_seed = 0;
+    int slots = 0;         // 16-bit slots per record of the mixed forms
+    float* params[2] = {nullptr, nullptr};  // FP32 form: parameter records, ping-pong
     int cur = 0;
     float* grad = nullptr;
-    float* m = nullptr;
+    float* m = nullptr;    // FP32 form: Adam moment records
     float* v = nullptr;
-    float* density = nullptr;
+    float* density = nullptr;  // FP32 form: density mirror; mixed forms: dens[cur]
+    uint16_t* sh16[2] = {nullptr, nullptr};  // mixed forms: SH records, ping-pong
+    uint16_t* m16 = nullptr;                  // mixed forms: bfloat16 moment records
+    uint16_t* v16 = nullptr;
+    float* dens[2] = {nullptr, nullptr};      // mixed forms: FP32 density, ping-pong
+    // Touched-vertex bitmaps (1 bit per active vertex): the backward marks every vertex it
+    // scatters gradients into, so the optimizer sweep reads and clears gradient records only
+    // where they can be non-zero.  Two maps alternate: a sweep reads map `tcur` and clears the
+    // other one for the next batch.  all_touched: gradients were written by another route
+    // (upload, standalone TV), so the next sweep reads every record.
+    uint32_t* touched[2] = {nullptr, nullptr};
+    int tcur = 0;
+    int all_touched = 0;
     float* adaptive_lr = nullptr;  // [n_dense]
     // occupancy (built by cpx_occupancy_build)
     int have_occupancy = 0;
@@ -134,6 +154,17 @@ void set_error(const char* fmt, ...);
 cpx_status cuda_status(cudaError_t e, const char* where);
 void count_launch(int n = 1);
 
+// Touched-map bit of vertex v (a null map means every vertex).
+__device__ __forceinline__ bool touched_bit(const uint32_t* __restrict__ map, uint32_t v)
+{
+    return map == nullptr || ((__ldg(map + (v >> 5)) >> (v & 31u)) & 1u);
+}
+
+__device__ __forceinline__ const uint16_t* sh16_records(const GridView& g)
+{
+    return reinterpret_cast<const uint16_t*>(g.params);
+}
+
 inline GridView grid_view(cpx_grid* g)
 {
     GridView v;
@@ -149,7 +180,7 @@ inline GridView grid_view(cpx_grid* g)
     v.step = g->step;
     v.sparse = g->sparse;
     v.n_act = g->n_act;
-    v.params = g->params[g->cur];
+    v.params = g->prec == kPrecFP32 ? g->params[g->cur] : reinterpret_cast<const float*>(g->sh16[g->cur]);
     v.density = g->density;
     v.grad = g->grad;
     v.occ_bits = g->occ_bits;
@@ -185,6 +216,10 @@ inline RaysView rays_view(cpx_rays* r)
     return v;
 }
 
+// Per-vertex state of the grid's storage form (api.cu).
+cudaError_t alloc_state(cpx_grid* g, int64_t n);
+void free_state(cpx_grid* g);
+
 // Launch helpers implemented in the kernel files.
 cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                         int mode, double* losses, double mask_coef, float huber,
@@ -195,6 +230,8 @@ cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int 
 int march_samples_per_ray(const cpx_grid* g);
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
                       double sh_lr, int timestep, cudaStream_t s);
+cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
+                           int timestep, uint32_t tv_mask, uint32_t adam_mask, cudaStream_t st);
 cpx_status tv_launch(cpx_grid* g, double lam_d, double lam_sh, int type, int nbrs,
                      cudaStream_t s);
 cpx_status occupancy_launch(cpx_grid* g, float threshold);

@@ -1,0 +1,120 @@
+// lowp.cuh -- 16-bit storage of the mixed-precision grid form.
+//
+// The mixed form keeps density (and the march: positions, transmittance, weights,
+// colour accumulation and gradients) in FP32 and stores the SH coefficients and both
+// Adam moments as 16-bit values:
+//   * BF16: SH and moments in bfloat16;
+//   * FP16: SH in half, moments in bfloat16 (a second moment g^2 of 1e-10 is far below
+//     half's smallest subnormal, 6e-8; bfloat16 has FP32's exponent range).
+// Records of `slots` 16-bit values per vertex (slots = n_arrays rounded up to 4, the FP32
+// record's length, so a record is a whole number of 8-byte quads: 56 B at SH band 2 and
+// quad j lines up with float4 j of the FP32 gradient record); slot e holds parameter e of
+// the reference's order (0 = density, 1..3*sh_dim = R, G, B coefficients), so SH records
+// leave slot 0 unused and moment records use it for the density's moments.
+//
+// Optimizer write-back rounds stochastically: a value lands on either neighbouring
+// 16-bit number with probability proportional to closeness, so small Adam steps are not
+// lost to round-to-nearest.  The random bits come from a counter-based hash of (seed,
+// timestep, vertex, record quad, element): MurmurHash3's 32-bit finaliser (Appleby, public
+// domain) applied in a chain, then a multiply-xorshift draw per element whose low 16 bits
+// round the parameter and whose high 16 bits round both moments.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+
+namespace cpx {
+
+constexpr int kPrecFP32 = 0;
+constexpr int kPrecBF16 = 1;
+constexpr int kPrecFP16 = 2;
+
+inline int lowp_slots(int n_arrays) { return (n_arrays + 3) & ~3; }
+
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// bfloat16 bits -> float
+__device__ __forceinline__ float bf16_to_f(uint16_t b) { return __uint_as_float((uint32_t)b << 16); }
+__device__ __forceinline__ float h16_to_f(uint16_t b) { return __half2float(__ushort_as_half(b)); }
+
+template <int PREC>
+__device__ __forceinline__ float sh_to_f(uint16_t b)
+{
+    return PREC == kPrecFP16 ? h16_to_f(b) : bf16_to_f(b);
+}
+
+__device__ __forceinline__ uint16_t f_to_bf16_rn(float x)
+{
+    return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+__device__ __forceinline__ uint16_t f_to_h16_rn(float x) { return __half_as_ushort(__float2half_rn(x)); }
+
+template <int PREC>
+__device__ __forceinline__ uint16_t f_to_sh_rn(float x)
+{
+    return PREC == kPrecFP16 ? f_to_h16_rn(x) : f_to_bf16_rn(x);
+}
+
+// Stochastic rounding (both forms take 16 random bits in the low half of rnd).
+// To bfloat16: add the random bits below the kept mantissa and truncate (the magnitude
+// rounds up with probability equal to the dropped fraction).
+__device__ __forceinline__ uint16_t f_to_bf16_sr(float x, uint32_t rnd)
+{
+    const uint32_t b = __float_as_uint(x);
+    if ((b & 0x7f800000u) == 0x7f800000u) return f_to_bf16_rn(x);  // inf / NaN
+    return (uint16_t)((b + (rnd & 0xffffu)) >> 16);
+}
+
+// Stochastic rounding to half: between the value rounded toward zero and the next half
+// away from zero, pick the upper one with probability (|x| - |lo|) / (|hi| - |lo|)
+// (compared as u * (|hi| - |lo|) < |x| - |lo|, no division).
+__device__ __forceinline__ uint16_t f_to_h16_sr(float x, uint32_t rnd)
+{
+    const __half lo = __float2half_rz(x);
+    const float lf = __half2float(lo);
+    if (lf == x || !isfinite(x)) return f_to_h16_rn(x);
+    const uint16_t lb = __half_as_ushort(lo);
+    const uint16_t hb = (uint16_t)(lb + 1u);  // same sign, one unit further from zero
+    const float hf = __half2float(__ushort_as_half(hb));
+    const float u = (float)(rnd & 0xffffu) * (1.f / 65536.f);
+    return u * (fabsf(hf) - fabsf(lf)) < fabsf(x) - fabsf(lf) ? hb : lb;
+}
+
+// Cheap 32-bit mixer for words drawn from one hashed counter (multiply, xorshift).
+__device__ __forceinline__ uint32_t draw32(uint32_t h, uint32_t k)
+{
+    uint32_t w = (h ^ (h >> 15)) * k;
+    return w ^ (w >> 13);
+}
+
+template <int PREC>
+__device__ __forceinline__ uint16_t f_to_sh_sr(float x, uint32_t rnd)
+{
+    return PREC == kPrecFP16 ? f_to_h16_sr(x, rnd) : f_to_bf16_sr(x, rnd);
+}
+
+// 4 packed 16-bit values (one quad) <-> floats
+template <int PREC>
+__device__ __forceinline__ void unpack4(const uint2& q, float* f)
+{
+    f[0] = sh_to_f<PREC>((uint16_t)(q.x & 0xffffu));
+    f[1] = sh_to_f<PREC>((uint16_t)(q.x >> 16));
+    f[2] = sh_to_f<PREC>((uint16_t)(q.y & 0xffffu));
+    f[3] = sh_to_f<PREC>((uint16_t)(q.y >> 16));
+}
+
+__device__ __forceinline__ uint2 pack4(const uint16_t* h)
+{
+    return make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
+}
+
+}  // namespace cpx

@@ -23,6 +23,8 @@
 // Reference citations: file:line in SparseVolumeRadianceField/.
 #include "cpx_internal.cuh"
 
+#include <type_traits>
+
 namespace cpx {
 
 // getSceneIndex (RenderUtils.cu:3-13).
@@ -83,9 +85,16 @@ __device__ __forceinline__ void prefetch_cell(const GridView& g, unsigned b0, un
     for (int q = 0; q < 8; q += 2) asm volatile("prefetch.global.L1 [%0];" ::"l"(g.density + idx[q]));
 }
 
+// exp in the march's precision
+__device__ __forceinline__ double real_exp(double x) { return exp(x); }
+__device__ __forceinline__ float real_exp(float x) { return expf(x); }
+
 // ---------------------------------------------------------------------------
-// Sample placement (exact): one thread per ray.
+// Sample placement: one thread per ray.  With Real = double this is the reference's
+// recurrence operation for operation (the FP32 form); the mixed forms march in FP32
+// (Real = float): the same recurrence with t, transmittance and weights in float.
 // ---------------------------------------------------------------------------
+template <typename Real>
 __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
                                           SampleRec* samples, int maxs, int* counts,
                                           double* acc_out, int* err, bool write_fwd)
@@ -112,10 +121,10 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
     const int it_cap = bound < (double)(maxs + 16) ? (int)bound : maxs + 16;
 
     SampleRec* out = samples + (size_t)b * maxs;
-    double t = near_t;
-    double Ti = 1.0;
-    double acc = 0.;
-    double accD = 0.;
+    Real t = near_t;
+    Real Ti = 1;
+    Real acc = 0;
+    Real accD = 0;
     float accDen = 0.f;
     int intT = 0, n = 0, it = 0;
     // densities of the last cell visited (consecutive samples mostly share a cell)
@@ -126,16 +135,16 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
             atomicOr(err, 1);
             break;
         }
-        double ofx = 0., ofy = 0., ofz = 0.;
+        Real ofx = 0, ofy = 0, ofz = 0;
         if (intT < g.n_off) {
-            ofx = g.off_x[intT];
-            ofy = g.off_y[intT];
-            ofz = g.off_z[intT];
+            ofx = (Real)g.off_x[intT];
+            ofy = (Real)g.off_y[intT];
+            ofz = (Real)g.off_z[intT];
         }
         // RenderUtils.cu:1676-1678
-        const double bc0 = ox + t * dx + ofx;
-        const double bc1 = oy + t * dy + ofy;
-        const double bc2 = oz + t * dz + ofz;
+        const Real bc0 = ox + t * dx + ofx;
+        const Real bc1 = oy + t * dy + ofy;
+        const Real bc2 = oz + t * dz + ofz;
         const unsigned b0 = (unsigned int)bc0;
         const unsigned b1 = (unsigned int)bc1;
         const unsigned b2 = (unsigned int)bc2;
@@ -157,41 +166,42 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
             if (!g.sparse) {
 #pragma unroll
                 for (int k = 1; k <= 2; k++) {
-                    const double ta = t + (double)k;
+                    const Real ta = t + (Real)k;
                     prefetch_cell(g, (unsigned)(ox + ta * dx), (unsigned)(oy + ta * dy),
                                   (unsigned)(oz + ta * dz));
                 }
             }
         }
-        const double x = bc0 - b0;
-        const double y = bc1 - b1;
-        const double z = bc2 - b2;
+        const Real x = bc0 - b0;
+        const Real y = bc1 - b1;
+        const Real z = bc2 - b2;
+        const Real one = 1;
         // trilerpRGB density term (RenderUtils.cu:855-990), corners in the reference's order
         float tri0 = 0.f;
-        double c;
-        c = (1. - x) * (1. - y) * (1. - z);
+        Real c;
+        c = (one - x) * (one - y) * (one - z);
         tri0 += c * cd[0];
-        c = (1. - x) * y * (1. - z);
+        c = (one - x) * y * (one - z);
         tri0 += c * cd[1];
-        c = x * (1. - y) * (1. - z);
+        c = x * (one - y) * (one - z);
         tri0 += c * cd[2];
-        c = x * y * (1. - z);
+        c = x * y * (one - z);
         tri0 += c * cd[3];
-        c = (1. - x) * (1. - y) * z;
+        c = (one - x) * (one - y) * z;
         tri0 += c * cd[4];
-        c = (1. - x) * y * z;
+        c = (one - x) * y * z;
         tri0 += c * cd[5];
-        c = x * (1. - y) * z;
+        c = x * (one - y) * z;
         tri0 += c * cd[6];
         c = x * y * z;
         tri0 += c * cd[7];
         // density_activation (RenderUtils.cu:491) and the weight (RenderUtils.cu:1693-1704)
         const float sigma = logf(1.f + expf(tri0 - 13.f));
-        const double w = Ti * (1. - expf(-sigma * step));
+        const Real w = Ti * (one - expf(-sigma * step));
         acc += w;
         accDen += sigma;
         accD += sigma * step;
-        const double Tn = exp(-accD);
+        const Real Tn = real_exp(-accD);
         SampleRec rec;
         rec.bx = (uint16_t)(b0 < 65535u ? b0 : 65535u);
         rec.by = (uint16_t)(b1 < 65535u ? b1 : 65535u);
@@ -205,7 +215,7 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
         rec.tn = (float)Tn;
         out[n] = rec;
         Ti = Tn;
-        t += fabs(step - w);
+        t += fabs(step - w);  // fabs(float) is the float overload
         ++intT;
         ++n;
     }
@@ -213,7 +223,7 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
         r.acc_den[ri] = accDen;
         r.acc_w[ri] = (float)acc;
     }
-    acc_out[b] = acc;
+    acc_out[b] = (double)acc;
     counts[b] = n;
 }
 
@@ -334,8 +344,9 @@ __device__ __forceinline__ void table_clear(const WarpTable& t, int lane)
     __syncwarp();
 }
 
-// Raw view-dependent colour of every vertex in the table (forward).
-template <int NSH>
+// Raw view-dependent colour of every vertex in the table (forward).  PREC selects the SH
+// storage: FP32 parameter records, or 16-bit SH records of the mixed forms.
+template <int NSH, int PREC>
 __device__ __forceinline__ void table_colours(const WarpTable& t, const GridView& g, const float* shs,
                                               int lane)
 {
@@ -344,19 +355,38 @@ __device__ __forceinline__ void table_colours(const WarpTable& t, const GridView
     for (int s = lane; s < kHashSlots; s += 32) {
         const uint32_t key = t.keys[s];
         if (key == kEmpty) continue;
-        const float4* rec = reinterpret_cast<const float4*>(g.params + (size_t)key * RS::REC);
         float col[3] = {0.f, 0.f, 0.f};
+        if (PREC == kPrecFP32) {
+            const float4* rec = reinterpret_cast<const float4*>(g.params + (size_t)key * RS::REC);
 #pragma unroll
-        for (int v = 0; v < RS::NV4; v++) {
-            const float4 p = __ldg(rec + v);
-            const float pv[4] = {p.x, p.y, p.z, p.w};
+            for (int v = 0; v < RS::NV4; v++) {
+                const float4 p = __ldg(rec + v);
+                const float pv[4] = {p.x, p.y, p.z, p.w};
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int e = 4 * v + k;
-                if (e >= 1 && e < RS::NA) {
-                    const int ch = (e - 1) / NSH;
-                    const int kk = (e - 1) % NSH;
-                    if (kk < g.n_sh_fwd) col[ch] = fmaf(pv[k], shs[kk], col[ch]);
+                for (int k = 0; k < 4; k++) {
+                    const int e = 4 * v + k;
+                    if (e >= 1 && e < RS::NA) {
+                        const int ch = (e - 1) / NSH;
+                        const int kk = (e - 1) % NSH;
+                        if (kk < g.n_sh_fwd) col[ch] = fmaf(pv[k], shs[kk], col[ch]);
+                    }
+                }
+            }
+        } else {
+            // 16-bit record of REC slots: NV4 quads of 8 bytes
+            const uint2* rec = reinterpret_cast<const uint2*>(sh16_records(g) + (size_t)key * RS::REC);
+#pragma unroll
+            for (int v = 0; v < RS::NV4; v++) {
+                float pv[4];
+                unpack4<PREC>(__ldg(rec + v), pv);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int e = 4 * v + k;
+                    if (e >= 1 && e < RS::NA) {
+                        const int ch = (e - 1) / NSH;
+                        const int kk = (e - 1) % NSH;
+                        if (kk < g.n_sh_fwd) col[ch] = fmaf(pv[k], shs[kk], col[ch]);
+                    }
                 }
             }
         }
@@ -370,7 +400,7 @@ __device__ __forceinline__ void table_colours(const WarpTable& t, const GridView
 // Flush the table: one vertex record of gradients per distinct key, 16-byte vector atomics.
 template <int NSH>
 __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& g, const float* shs,
-                                            int lane)
+                                            uint32_t* touched, int lane)
 {
     using RS = RecShape<NSH>;
     __syncwarp();
@@ -400,6 +430,7 @@ __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& 
             }
             atomicAdd(dst + q, make_float4(e4[0], e4[1], e4[2], e4[3]));
         }
+        atomicOr(touched + (key >> 5), 1u << (key & 31u));
         t.keys[s] = kEmpty;
         t.va[s] = 0.f;
         t.vb0[s] = 0.f;
@@ -412,12 +443,12 @@ __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& 
 // Shade one ray with a whole warp: forward colour (lane per sample, warp reduction), then
 // the backward of renderRays_withGradients_RGBGPU (RenderUtils.cu:2145-2256) with warp prefix
 // scans for the running weight/colour sums and the merged gradient scatter.
-template <int NSH, int MODE>
+template <int NSH, int MODE, int PREC>
 __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
                                           int cnt, const SampleRec* samples, float4* colours,
                                           int maxs, const double* acc_in, double* losses,
                                           double mask_coef, float huber, const WarpTable& tab,
-                                          int lane)
+                                          uint32_t* touched, int lane)
 {
     const bool miss = cnt < 0;
     const int n = miss ? 0 : cnt;
@@ -440,7 +471,7 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
 #pragma unroll
             for (int q = 0; q < 8; q++) slot[q] = table_slot(tab, cr.idx[q]);
         }
-        table_colours<NSH>(tab, g, shs, lane);
+        table_colours<NSH, PREC>(tab, g, shs, lane);
         if (valid) {
             float raw[3] = {0.f, 0.f, 0.f};
 #pragma unroll
@@ -565,7 +596,7 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
                 atomicAdd(&tab.vb2[sl], grad[3] * wq);
             }
         }
-        table_flush<NSH>(tab, g, shs, lane);
+        table_flush<NSH>(tab, g, shs, touched, lane);
     }
 }
 
@@ -573,7 +604,7 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
 // The two stages as kernels.  Placement is latency-bound per ray and needs only one thread
 // per ray, all resident in one wave; shading is throughput-bound and takes a warp per ray.
 // ---------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, typename Real>
 __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int32_t* sidx, int start,
                                                int len, int64_t n_rays, SampleRec* samples, int maxs,
                                                int* counts, double* acc, int* err)
@@ -586,19 +617,19 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
         counts[b] = -2;  // invalid ray index: nothing is read or written for it
         return;
     }
-    place_ray(g, r, b, ri, samples, maxs, counts, acc, err, (MODE & kForward) != 0);
+    place_ray<Real>(g, r, b, ri, samples, maxs, counts, acc, err, (MODE & kForward) != 0);
 }
 
 constexpr int kShadeWarps = 4;
 
-template <int NSH, int MODE>
+template <int NSH, int MODE, int PREC>
 __global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysView r,
                                                              const int32_t* sidx, int start,
                                                              int len, const SampleRec* samples,
                                                              float4* colours, int maxs,
                                                              const int* counts, const double* acc,
                                                              double* losses, double mask_coef,
-                                                             float huber)
+                                                             float huber, uint32_t* touched)
 {
     __shared__ uint32_t h_keys[kShadeWarps][kHashSlots];
     __shared__ float h_vals[kShadeWarps][4][kHashSlots];
@@ -618,8 +649,8 @@ __global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysV
     }
     const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
     const WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
-    shade_ray<NSH, MODE>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber, tab,
-                         lane);
+    shade_ray<NSH, MODE, PREC>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber,
+                               tab, touched, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -696,30 +727,52 @@ static cpx_status ensure_scratch(cpx_grid* g, int len)
     return CPX_OK;
 }
 
-template <int NSH>
-static void launch_march(int mode, cudaStream_t st, const GridView& gv, const RaysView& rv,
-                         const int32_t* sidx, int start, int len, int64_t n_rays,
-                         const MarchScratch& s, double* losses, double mask_coef, float huber)
+template <int MODE, int NSH, int PREC>
+static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv, const int32_t* sidx,
+                        int start, int len, int64_t n_rays, const MarchScratch& s, double* losses,
+                        double mask_coef, float huber, uint32_t* touched)
 {
+    using Real = typename std::conditional<PREC == kPrecFP32, double, float>::type;
     const dim3 pgrid((unsigned)((len + 31) / 32));
     const dim3 sgrid((unsigned)((len + kShadeWarps - 1) / kShadeWarps));
     const dim3 sblock(kShadeWarps * 32);
-#define CPX_SHADE_ARGS gv, rv, sidx, start, len, s.samples, s.colours, s.maxs, s.counts, s.acc, losses, \
-                       mask_coef, huber
-    if (mode == kForward) {
-        k_place<kForward><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
-                                                s.counts, s.acc, s.err);
-        k_shade<NSH, kForward><<<sgrid, sblock, 0, st>>>(CPX_SHADE_ARGS);
-    } else if (mode == kBackward) {
-        k_place<kBackward><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
-                                                 s.counts, s.acc, s.err);
-        k_shade<NSH, kBackward><<<sgrid, sblock, 0, st>>>(CPX_SHADE_ARGS);
-    } else {
-        k_place<kForwardBackward><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples,
-                                                        s.maxs, s.counts, s.acc, s.err);
-        k_shade<NSH, kForwardBackward><<<sgrid, sblock, 0, st>>>(CPX_SHADE_ARGS);
+    k_place<MODE, Real><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs, s.counts,
+                                              s.acc, s.err);
+    k_shade<NSH, MODE, PREC><<<sgrid, sblock, 0, st>>>(gv, rv, sidx, start, len, s.samples, s.colours, s.maxs,
+                                                       s.counts, s.acc, losses, mask_coef, huber, touched);
+}
+
+template <int NSH, int PREC>
+static void launch_march(int mode, cudaStream_t st, const GridView& gv, const RaysView& rv,
+                         const int32_t* sidx, int start, int len, int64_t n_rays,
+                         const MarchScratch& s, double* losses, double mask_coef, float huber,
+                         uint32_t* touched)
+{
+    if (mode == kForward)
+        launch_mode<kForward, NSH, PREC>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber,
+                                         touched);
+    else if (mode == kBackward)
+        launch_mode<kBackward, NSH, PREC>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber,
+                                          touched);
+    else
+        launch_mode<kForwardBackward, NSH, PREC>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef,
+                                                 huber, touched);
+}
+
+template <int PREC>
+static cpx_status launch_prec(int sh_dim, int mode, cudaStream_t st, const GridView& gv, const RaysView& rv,
+                              const int32_t* sidx, int start, int len, int64_t n_rays, const MarchScratch& s,
+                              double* losses, double mask_coef, float huber, uint32_t* touched)
+{
+    switch (sh_dim) {
+    case 1: launch_march<1, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched); break;
+    case 4: launch_march<4, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched); break;
+    case 9: launch_march<9, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched); break;
+    default:
+        set_error("sh_dim %d unsupported", sh_dim);
+        return CPX_ERR_UNSUPPORTED;
     }
-#undef CPX_SHADE_ARGS
+    return CPX_OK;
 }
 
 static cpx_status march_check_args(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start,
@@ -754,14 +807,17 @@ cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int 
     if (rc != CPX_OK || len == 0) return rc;
     const GridView gv = grid_view(g);
     const RaysView rv = rays_view(r);
-    switch (g->sh_dim) {
-    case 1: launch_march<1>(mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber); break;
-    case 4: launch_march<4>(mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber); break;
-    case 9: launch_march<9>(mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber); break;
-    default:
-        set_error("sh_dim %d unsupported", g->sh_dim);
-        return CPX_ERR_UNSUPPORTED;
-    }
+    uint32_t* touched = g->touched[g->tcur];
+    if (g->prec == kPrecFP32)
+        rc = launch_prec<kPrecFP32>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
+                                    touched);
+    else if (g->prec == kPrecBF16)
+        rc = launch_prec<kPrecBF16>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
+                                    touched);
+    else
+        rc = launch_prec<kPrecFP16>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
+                                    touched);
+    if (rc != CPX_OK) return rc;
     count_launch(2);
     return cuda_status(cudaGetLastError(), "march");
 }

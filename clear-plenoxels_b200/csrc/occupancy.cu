@@ -218,6 +218,19 @@ __global__ void k_compact(const float4* __restrict__ src, float4* dst, float* de
     c2d[c] = (uint32_t)v;
 }
 
+// The same for the mixed forms: FP32 density and 16-bit SH records (S = 8-byte quads).
+__global__ void k_compact16(const float* __restrict__ dens_in, const uint2* __restrict__ src, float* dens_out,
+                            uint2* dst, const uint8_t* __restrict__ in_cage,
+                            const uint32_t* __restrict__ index_offsets, uint32_t* c2d, int64_t N, int S)
+{
+    const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (v >= N || !in_cage[v]) return;
+    const uint32_t c = index_offsets[v];
+    for (int j = 0; j < S; j++) dst[(int64_t)c * S + j] = src[v * S + j];
+    dens_out[c] = dens_in[v];
+    c2d[c] = (uint32_t)v;
+}
+
 cpx_status make_sparse_launch(cpx_grid* g)
 {
     if (!g->have_occupancy) {
@@ -229,48 +242,58 @@ cpx_status make_sparse_launch(cpx_grid* g)
         return CPX_ERR_INVALID_ARGUMENT;
     }
     const int64_t n = g->in_cage_count;
-    const int64_t nalloc = n > 0 ? n : 1;
-    const size_t rec_bytes = (size_t)g->rec * sizeof(float);
-    float *p0 = nullptr, *p1 = nullptr, *gr = nullptr, *m = nullptr, *v = nullptr, *dens = nullptr;
+    // the compact state is built in a holder of the same form, then replaces the dense one
+    cpx_grid t;
+    t.prec = g->prec;
+    t.rec = g->rec;
+    t.slots = g->slots;
+    t.cur = 0;
     uint32_t* c2d = nullptr;
-    if (cudaMalloc((void**)&p0, nalloc * rec_bytes) != cudaSuccess ||
-        cudaMalloc((void**)&p1, nalloc * rec_bytes) != cudaSuccess ||
-        cudaMalloc((void**)&gr, nalloc * rec_bytes) != cudaSuccess ||
-        cudaMalloc((void**)&m, nalloc * rec_bytes) != cudaSuccess ||
-        cudaMalloc((void**)&v, nalloc * rec_bytes) != cudaSuccess ||
-        cudaMalloc((void**)&dens, nalloc * sizeof(float)) != cudaSuccess ||
-        cudaMalloc((void**)&c2d, nalloc * sizeof(uint32_t)) != cudaSuccess) {
+    cudaError_t e = alloc_state(&t, n);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&c2d, (n > 0 ? n : 1) * sizeof(uint32_t));
+    if (e != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(p0); cudaFree(p1); cudaFree(gr); cudaFree(m); cudaFree(v); cudaFree(dens); cudaFree(c2d);
+        free_state(&t);
+        cudaFree(c2d);
         set_error("sparse buffers for %lld vertices could not be allocated", (long long)n);
         return CPX_ERR_OUT_OF_MEMORY;
     }
-    cudaMemset(p0, 0, nalloc * rec_bytes);
-    cudaMemset(p1, 0, nalloc * rec_bytes);
-    cudaMemset(gr, 0, nalloc * rec_bytes);
-    cudaMemset(m, 0, nalloc * rec_bytes);
-    cudaMemset(v, 0, nalloc * rec_bytes);
-    const int S = g->rec / 4;
-    k_compact<<<(unsigned)((g->n_dense + 255) / 256), 256>>>(
-        reinterpret_cast<const float4*>(g->params[g->cur]), reinterpret_cast<float4*>(p0), dens,
-        g->in_cage, g->index_offsets, c2d, g->n_dense, S);
+    const unsigned blocks = (unsigned)((g->n_dense + 255) / 256);
+    if (g->prec == kPrecFP32) {
+        k_compact<<<blocks, 256>>>(reinterpret_cast<const float4*>(g->params[g->cur]),
+                                   reinterpret_cast<float4*>(t.params[0]), t.density, g->in_cage,
+                                   g->index_offsets, c2d, g->n_dense, g->rec / 4);
+    } else {
+        k_compact16<<<blocks, 256>>>(g->dens[g->cur], reinterpret_cast<const uint2*>(g->sh16[g->cur]),
+                                     t.dens[0], reinterpret_cast<uint2*>(t.sh16[0]), g->in_cage,
+                                     g->index_offsets, c2d, g->n_dense, g->slots / 4);
+    }
     count_launch();
-    cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) return cuda_status(e, "compaction");
-    cudaFree(g->params[0]);
-    cudaFree(g->params[1]);
-    cudaFree(g->grad);
-    cudaFree(g->m);
-    cudaFree(g->v);
-    cudaFree(g->density);
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        free_state(&t);
+        cudaFree(c2d);
+        return cuda_status(e, "compaction");
+    }
+    free_state(g);
     cudaFree(g->compact_to_dense);
-    g->params[0] = p0;
-    g->params[1] = p1;
+    g->params[0] = t.params[0];
+    g->params[1] = t.params[1];
+    g->grad = t.grad;
+    g->m = t.m;
+    g->v = t.v;
+    g->sh16[0] = t.sh16[0];
+    g->sh16[1] = t.sh16[1];
+    g->m16 = t.m16;
+    g->v16 = t.v16;
+    g->dens[0] = t.dens[0];
+    g->dens[1] = t.dens[1];
+    g->touched[0] = t.touched[0];
+    g->touched[1] = t.touched[1];
+    g->tcur = 0;
+    g->all_touched = 0;
     g->cur = 0;
-    g->grad = gr;
-    g->m = m;
-    g->v = v;
-    g->density = dens;
+    g->density = g->prec == kPrecFP32 ? t.density : g->dens[0];
     g->compact_to_dense = c2d;
     g->n_act = n;
     g->sparse = 1;

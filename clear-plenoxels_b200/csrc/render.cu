@@ -30,7 +30,7 @@ __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : 
 
 __device__ __forceinline__ int clampi(int v, int n) { return v < 0 ? 0 : (v > n - 1 ? n - 1 : v); }
 
-template <int NSH>
+template <int NSH, int PREC>
 __global__ void __launch_bounds__(128) k_render_image(GridView g, ImageArgs a)
 {
     constexpr int NA = 1 + 3 * NSH;
@@ -144,14 +144,28 @@ __global__ void __launch_bounds__(128) k_render_image(GridView g, ImageArgs a)
                 case 6: contributes = x * (1. - y) * z; break;
                 default: contributes = x * y * z; break;
                 }
-                const float* rec = g.params + (size_t)idx * REC;
-                tri0 += contributes * rec[0];
+                if (PREC == kPrecFP32) {
+                    const float* rec = g.params + (size_t)idx * REC;
+                    tri0 += contributes * rec[0];
 #pragma unroll
-                for (int i = 0; i < NSH; i++) {
-                    if (i < g.n_sh_fwd) {
-                        sh_tri[i] += contributes * rec[1 + i];
-                        sh_tri[NSH + i] += contributes * rec[1 + NSH + i];
-                        sh_tri[2 * NSH + i] += contributes * rec[1 + 2 * NSH + i];
+                    for (int i = 0; i < NSH; i++) {
+                        if (i < g.n_sh_fwd) {
+                            sh_tri[i] += contributes * rec[1 + i];
+                            sh_tri[NSH + i] += contributes * rec[1 + NSH + i];
+                            sh_tri[2 * NSH + i] += contributes * rec[1 + 2 * NSH + i];
+                        }
+                    }
+                } else {
+                    // mixed forms: FP32 density, 16-bit SH record (slot e = parameter e)
+                    const uint16_t* rec = sh16_records(g) + (size_t)idx * REC;
+                    tri0 += contributes * g.density[idx];
+#pragma unroll
+                    for (int i = 0; i < NSH; i++) {
+                        if (i < g.n_sh_fwd) {
+                            sh_tri[i] += contributes * sh_to_f<PREC>(rec[1 + i]);
+                            sh_tri[NSH + i] += contributes * sh_to_f<PREC>(rec[1 + NSH + i]);
+                            sh_tri[2 * NSH + i] += contributes * sh_to_f<PREC>(rec[1 + 2 * NSH + i]);
+                        }
                     }
                 }
             }
@@ -246,14 +260,24 @@ extern "C" cpx_status cpx_render_image(cpx_grid* g, const cpx_camera* cam, int w
     const int64_t npix = (int64_t)width * height;
     const unsigned blocks = (unsigned)((npix + 127) / 128);
     cudaStream_t st = (cudaStream_t)stream;
-    switch (g->sh_dim) {
-    case 1: k_render_image<1><<<blocks, 128, 0, st>>>(gv, a); break;
-    case 4: k_render_image<4><<<blocks, 128, 0, st>>>(gv, a); break;
-    case 9: k_render_image<9><<<blocks, 128, 0, st>>>(gv, a); break;
-    default:
+    if (g->sh_dim != 1 && g->sh_dim != 4 && g->sh_dim != 9) {
         set_error("sh_dim %d unsupported", g->sh_dim);
         return CPX_ERR_UNSUPPORTED;
     }
+#define CPX_IMAGE(PREC)                                                                \
+    switch (g->sh_dim) {                                                               \
+    case 1: k_render_image<1, PREC><<<blocks, 128, 0, st>>>(gv, a); break;             \
+    case 4: k_render_image<4, PREC><<<blocks, 128, 0, st>>>(gv, a); break;             \
+    default: k_render_image<9, PREC><<<blocks, 128, 0, st>>>(gv, a); break;            \
+    }
+    if (g->prec == kPrecFP32) {
+        CPX_IMAGE(kPrecFP32)
+    } else if (g->prec == kPrecBF16) {
+        CPX_IMAGE(kPrecBF16)
+    } else {
+        CPX_IMAGE(kPrecFP16)
+    }
+#undef CPX_IMAGE
     count_launch();
     return cuda_status(cudaGetLastError(), "render image");
 }

@@ -30,6 +30,8 @@ struct SweepArgs {
     const uint32_t* __restrict__ index_offsets;
     const uint32_t* __restrict__ compact_to_dense;
     const uint8_t* __restrict__ in_cage;  // dense in-cage flags (sparse TV gate, see k_sweep)
+    const uint32_t* __restrict__ touched;  // vertices whose gradients may be non-zero; null = all
+    uint32_t* clear;                       // the other touched map, cleared for the next batch
     uint32_t tv_mask;    // bit e: parameter e of a record gets the TV term (RenderUtils.cu:2743-2746)
     uint32_t adam_mask;  // bit e: parameter e is updated by Adam (Optimizer.cu:380-413)
     float lam_d, lam_sh;
@@ -65,6 +67,7 @@ __device__ __forceinline__ float tv6(float self, const float* nb, float lam)
 }
 
 // One 16-byte slot: optional TV term from six neighbour slots, then Adam; writes the slot.
+// touched_bit is shared with the mixed-form sweep (cpx_internal.cuh).
 template <bool TV>
 __device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint32_t v, int j,
                                            bool tv_on, const uint32_t* nb_slot, const bool* nb_self,
@@ -72,7 +75,10 @@ __device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint
 {
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
     const float4 p = a.p_in[sl];
-    float4 g = a.grad[sl];
+    // untouched vertices have zero gradients: their records are neither read nor written
+    const bool tch = touched_bit(a.touched, v);
+    if (a.clear && j == 0 && (v & 31u) == 0) a.clear[v >> 5] = 0u;
+    float4 g = tch ? a.grad[sl] : make_float4(0.f, 0.f, 0.f, 0.f);
     float4 m = a.m[sl];
     float4 vv = a.v[sl];
     if (TV && tv_on) {
@@ -108,7 +114,7 @@ __device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint
     a.p_out[sl] = pn;
     a.m[sl] = m;
     a.v[sl] = vv;
-    a.grad[sl] = g;
+    if (tch) a.grad[sl] = g;
     if (j == 0) a.density_out[v] = pn.x;
 }
 
@@ -238,6 +244,11 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
                       double sh_lr, int timestep, cudaStream_t st)
 {
     if (g->n_act == 0) return CPX_OK;
+    if (g->prec != kPrecFP32) {
+        uint32_t tvm, am;
+        element_masks(g, &tvm, &am);
+        return sweep_adam_lowp(g, fused_tv, lam_d, lam_sh, lr, sh_lr, timestep, tvm, am, st);
+    }
     const int S = g->rec / 4;
     if (g->n_act * S >= ((int64_t)1 << 32)) {
         set_error("grid too large for 32-bit slot indices");
@@ -258,6 +269,8 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
     a.index_offsets = g->index_offsets;
     a.compact_to_dense = g->compact_to_dense;
     a.in_cage = g->in_cage;
+    a.touched = g->all_touched ? nullptr : g->touched[g->tcur];
+    a.clear = g->touched[g->tcur ^ 1];
     element_masks(g, &a.tv_mask, &a.adam_mask);
     a.lam_d = (float)lam_d;
     a.lam_sh = (float)lam_sh;
@@ -274,6 +287,8 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
     }
     count_launch();
     g->cur ^= 1;
+    g->tcur ^= 1;
+    g->all_touched = 0;
     return cuda_status(cudaGetLastError(), "adam sweep");
 }
 
@@ -422,6 +437,11 @@ cpx_status tv_launch(cpx_grid* g, double lam_d, double lam_sh, int type, int nbr
         set_error("sparse grid without occupancy");
         return CPX_ERR_NOT_READY;
     }
+    if (g->prec != kPrecFP32) {
+        set_error("the mixed forms run TV type 0 / 6 neighbours fused into the optimizer sweep only");
+        return CPX_ERR_UNSUPPORTED;
+    }
+    g->all_touched = 1;  // TV writes gradients of vertices no ray touched
     TvArgs a;
     a.W = g->W;
     a.H = g->H;

@@ -64,7 +64,22 @@ typedef struct cpx_grid_desc {
     int hierarchy_strategy;   /* Optimizer::hierarchyStrategy (band-restricted grads/updates) */
     float step_size;          /* ObjectScene::stepSize, > 0 */
     int bbox[6];              /* ray AABB in voxel space: wmin,wmax,hmin,hmax,dmin,dmax */
+    int precision;            /* cpx_precision: storage and march form (no reference
+                                 counterpart beyond CPX_PRECISION_FP32, its own form) */
+    uint32_t sr_seed;         /* seed of the stochastic rounding of the 16-bit forms */
 } cpx_grid_desc;
+
+/* Storage forms.  FP32 is the reference's (every parameter and moment in float, the march
+ * in the reference's FP64/FP32 mix, bit-compatible with it).  The mixed forms store the SH
+ * coefficients in bfloat16 (BF16) or half (FP16) and both Adam moments in bfloat16, keep
+ * density, gradients and all accumulation in FP32, march in FP32, and write the optimizer
+ * results back with stochastic rounding.  They support TV type 0 with 6 neighbours, fused
+ * into the optimizer sweep (cpx_tv_adam_step / cpx_train_step), or no TV. */
+typedef enum cpx_precision {
+    CPX_PRECISION_FP32 = 0,
+    CPX_PRECISION_BF16 = 1,
+    CPX_PRECISION_FP16 = 2
+} cpx_precision;
 
 /* Pinhole camera as the reference's getBound reads it (SVRF/CameraUtils.cuh:16-26):
  * focal lengths, principal point, camera-to-world 4x4 (row-major) and centre. */
@@ -230,6 +245,11 @@ cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sample_index_
  * earlier asynchronous calls: CPX_ERR_ITERATION_CAP when a ray's march exceeded its
  * sample bound, CPX_ERR_INVALID_ARGUMENT when a sample index was out of range. */
 cpx_status cpx_grid_check(cpx_grid* g);
+/* No reference counterpart (a diagnostic): the number of vertices marked in the touched map
+ * the next optimizer sweep will read.  The backward marks every vertex it scatters gradients
+ * into and a sweep reads and clears gradient records only there; after
+ * cpx_grid_upload_grads or a standalone cpx_tv_grad every vertex counts.  Synchronous. */
+cpx_status cpx_grid_touched_count(cpx_grid* g, int64_t* count);
 
 /* Per-ray sample counts of the last forward/backward batch (device int32[len], or a
  * host copy) -- the march's sample sequence, for bit-exact checks. */

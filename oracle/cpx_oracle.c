@@ -954,3 +954,225 @@ void orc_composite_kat(const double* opacity, const double* colour, int n, const
         }
     }
 }
+
+/* ------------------------------------------------------ FP64 oracle */
+
+static void sh_basis64(const double d[3], double shs[9])
+{
+    shs[0] = 1.;
+    shs[1] = d[1];
+    shs[2] = d[2];
+    shs[3] = d[0];
+    shs[4] = d[0] * d[1];
+    shs[5] = d[1] * d[2];
+    shs[6] = 3. * d[2] * d[2] - 1.;
+    shs[7] = d[0] * d[2];
+    shs[8] = d[0] * d[0] - d[1] * d[1];
+}
+
+static inline double softplus64(double x) { return log(1. + exp(x - 13.)); }
+static inline double softplus64_d(double x) { return 1. / (1. + exp(13. - x)); }
+static inline double sigmoid64(double x) { return 1. / (1. + exp(-0.1 * x)); }
+
+/* Raw density and raw colours at bc, all in double; 0 when the sparse occupancy skips. */
+static int trilerp64(const orc_scene* s, const double bc[3], const double* shs, double tri[4],
+                     double* wq, int64_t* iq)
+{
+    uint32_t bi[3] = {sat_u32(bc[0]), sat_u32(bc[1]), sat_u32(bc[2])};
+    if (!occupied(s, bi)) return 0;
+    const double x = bc[0] - (double)bi[0];
+    const double y = bc[1] - (double)bi[1];
+    const double z = bc[2] - (double)bi[2];
+    const int nsh = n_active_sh(s);
+    const int64_t n = s->n_act;
+    tri[0] = tri[1] = tri[2] = tri[3] = 0.;
+    for (int q = 0; q < 8; q++) {
+        const int64_t idx = corner_index(s, bi, q);
+        const double c = corner_weight(q, x, y, z);
+        wq[q] = c;
+        iq[q] = idx;
+        tri[0] += c * (double)s->params[idx];
+        for (int ch = 0; ch < 3; ch++)
+            for (int i = 0; i < nsh; i++)
+                tri[1 + ch] += c * (double)s->params[(int64_t)(1 + ch * s->sh_dim + i) * n + idx] * shs[i];
+    }
+    return 1;
+}
+
+static void ray64(const orc_scene* s, const orc_rays* r, int tid, int ri, double mask_coef,
+                  double huber, double* pred, double* accw_out, double* losses, double* grad)
+{
+    pred[3 * tid] = pred[3 * tid + 1] = pred[3 * tid + 2] = 0.;
+    accw_out[tid] = 0.;
+    losses[tid] = 0.;
+    if (r->near_t[ri] > r->far_t[ri]) return;
+    const double o[3] = {r->ox[ri], r->oy[ri], r->oz[ri]};
+    const double d[3] = {r->dx[ri], r->dy[ri], r->dz[ri]};
+    double shs[9];
+    sh_basis64(d, shs);
+    const double step = s->step;
+    const double far_t = r->far_t[ri];
+    /* forward */
+    double t = r->near_t[ri], accd = 0., acc = 0., rgb[3] = {0., 0., 0.};
+    double tri[4], wq[8];
+    int64_t iq[8];
+    while (t < far_t) {
+        double bc[3];
+        for (int a = 0; a < 3; a++) bc[a] = o[a] + t * d[a];
+        if (!trilerp64(s, bc, shs, tri, wq, iq)) {
+            t += step;
+            continue;
+        }
+        const double sigma = softplus64(tri[0]);
+        const double w = exp(-accd) * (1. - exp(-sigma * step));
+        acc += w;
+        for (int c = 0; c < 3; c++) rgb[c] += w * sigmoid64(tri[1 + c]);
+        accd += sigma * step;
+        t += fabs(step - w);
+    }
+    const double bg = r->white_bg ? 1. - acc : 0.;
+    for (int c = 0; c < 3; c++) pred[3 * tid + c] = rgb[c] + bg;
+    accw_out[tid] = acc;
+    /* backward (renderRays_withGradients_RGBGPU, RenderUtils.cu:2051-2256, in double) */
+    const double gt[3] = {r->r[ri] / 255., r->g[ri] / 255., r->b[ri] / 255.};
+    double res[3];
+    for (int c = 0; c < 3; c++) res[c] = pred[3 * tid + c] - gt[c];
+    losses[tid] = (fabs(res[0]) + fabs(res[1]) + fabs(res[2])) * 255. / 3.;
+    if (isnan(losses[tid])) {
+        losses[tid] = 255.;
+        return;
+    }
+    for (int c = 0; c < 3; c++) {
+        if (res[c] > huber)
+            res[c] = huber - 0.5 * huber * huber;
+        else if (res[c] < -huber)
+            res[c] = 0.5 * huber * huber - huber;
+    }
+    double mask_loss = 0.;
+    if (r->mask[ri] && acc < 1.) mask_loss = (r->mask[ri] / 255. - acc) * mask_coef;
+    double wpre = acc < 1e-6 ? 1e-6 : acc;
+    wpre = wpre > 1 - 1e-6 ? 1 - 1e-6 : wpre;
+    mask_loss += (log(wpre) - log(1. - wpre)) * 1e-3;
+    const int64_t n = s->n_act;
+    const int nsh = n_active_sh(s);
+    t = r->near_t[ri];
+    accd = 0.;
+    double accw = 0., acc_rgb[3] = {0., 0., 0.};
+    while (t < far_t) {
+        double bc[3];
+        for (int a = 0; a < 3; a++) bc[a] = o[a] + t * d[a];
+        if (!trilerp64(s, bc, shs, tri, wq, iq)) {
+            t += step;
+            continue;
+        }
+        const double sigma = softplus64(tri[0]);
+        const double w = exp(-accd) * (1. - exp(-sigma * step));
+        accw += w;
+        double col[3], g[4];
+        for (int c = 0; c < 3; c++) {
+            col[c] = sigmoid64(tri[1 + c]);
+            acc_rgb[c] += w * col[c];
+            g[1 + c] = 0.6667 * w * res[c] * 0.1 * col[c] * (1. - col[c]);
+        }
+        accd += sigma * step;
+        const double Tn = exp(-accd);
+        g[0] = 0.;
+        for (int c = 0; c < 3; c++) g[0] += res[c] * (Tn * col[c] - (pred[3 * tid + c] - acc_rgb[c]));
+        const double dd = softplus64_d(tri[0]);
+        g[0] *= 0.6667 * step * dd;
+        g[0] += step * dd * (acc - accw - Tn) * mask_loss;
+        for (int q = 0; q < 8; q++) {
+            const int64_t idx = iq[q];
+            grad_add(&grad[idx], g[0] * wq[q]);
+            for (int ch = 0; ch < 3; ch++) {
+                int k0 = 0, k1 = s->sh_dim;
+                if (s->hierarchy) {
+                    k0 = s->band * s->band;
+                    k1 = nsh;
+                }
+                for (int k = k0; k < k1; k++)
+                    grad_add(&grad[(int64_t)(1 + ch * s->sh_dim + k) * n + idx], g[1 + ch] * wq[q] * (k < 9 ? shs[k] : 0.));
+            }
+        }
+        t += fabs(step - w);
+    }
+}
+
+void orc64_forward_backward(const orc_scene* s, const orc_rays* r, int start, int len,
+                            double mask_coef, double huber, double* pred, double* accw,
+                            double* losses, double* grad)
+{
+#pragma omp parallel for schedule(dynamic, 16) num_threads(orc_get_threads())
+    for (int tid = 0; tid < len; tid++)
+        ray64(s, r, tid, tid + start, mask_coef, huber, pred, accw, losses, grad);
+}
+
+void orc64_tv6(const orc_scene* s, const double* params, double* grad, double lam_d, double lam_sh)
+{
+    const int64_t n = s->n_act;
+    const int W = s->W, H = s->H, D = s->D;
+    const int nsh = n_active_sh(s);
+    const int lo = s->hierarchy ? s->band * s->band : 0;
+#pragma omp parallel for schedule(static) num_threads(orc_get_threads())
+    for (int64_t dv = 0; dv < (int64_t)W * H * D; dv++) {
+        const int x = (int)(dv % W), y = (int)((dv / W) % H), z = (int)(dv / ((int64_t)W * H));
+        if (x < 1 || x > W - 2 || y < 1 || y > H - 2 || z < 1 || z > D - 2) continue;
+        int64_t self = dv;
+        int64_t nb[6] = {dv - (int64_t)W * H, dv - W, dv - 1, dv + 1, dv + W, dv + (int64_t)W * H};
+        if (s->sparse) {
+            if (!s->in_cage[dv]) continue;
+            self = s->index_offsets[dv];
+            /* the reference gates sparse TV with inCageInfo[indexOffsets[v]] */
+            if (!s->in_cage[self]) continue;
+            for (int k = 0; k < 6; k++) {
+                const uint32_t ci = s->index_offsets[nb[k]];
+                nb[k] = ci == 0 ? self : (int64_t)ci;
+            }
+        }
+        for (int e = 0; e < 1 + 3 * s->sh_dim; e++) {
+            double lam = lam_d;
+            if (e > 0) {
+                const int k = (e - 1) % s->sh_dim;
+                if (k < lo || k >= nsh) continue;
+                lam = lam_sh;
+            }
+            const double v = params[(int64_t)e * n + self];
+            double sum = 0., disp = 0.;
+            for (int k = 0; k < 6; k++) {
+                const double dlt = v - params[(int64_t)e * n + nb[k]];
+                sum += dlt * dlt;
+                disp += dlt;
+            }
+            grad[(int64_t)e * n + self] += lam * disp / (sqrt(sum) / 6. + 1e-6);
+        }
+    }
+}
+
+void orc64_adam(const orc_scene* s, double* params, double* grad, double* m, double* v,
+                double lr, double sh_lr, int timestep)
+{
+    const double b1 = 0.9, b2 = 0.999, eps = 1e-6;
+    const int64_t n = s->n_act;
+    const int na = 1 + 3 * s->sh_dim;
+    const int nsh = n_active_sh(s);
+    const double bc1 = 1. - pow(b1, timestep), bc2 = 1. - pow(b2, timestep);
+#pragma omp parallel for schedule(static) num_threads(orc_get_threads())
+    for (int64_t p = 0; p < n; p++) {
+        for (int e = 0; e < na; e++) {
+            if (e > 0 && s->hierarchy) {
+                const int k = (e - 1) % s->sh_dim;
+                if (k < s->band * s->band || k >= nsh) continue;
+            }
+            const int64_t i = (int64_t)e * n + p;
+            const double g = grad[i];
+            m[i] = b1 * m[i] + (1. - b1) * g;
+            v[i] = b2 * v[i] + (1. - b2) * g * g;
+            double lrp = e == 0 ? lr : sh_lr;
+            if (e == 0 && !s->sparse && s->adaptive_lr) lrp *= s->adaptive_lr[p];
+            double np = params[i] - lrp * (m[i] / bc1) / (sqrt(v[i] / bc2) + eps);
+            if (e == 0 && np < 0.) np = 0.;
+            params[i] = np;
+            grad[i] = 0.;
+        }
+    }
+}

@@ -140,6 +140,21 @@ void orc_composite_kat(const double* opacity, const double* colour /*[3][n]*/, i
                        double* weights /*[n]*/, double* opacity_grad /*[n]*/,
                        double* colour_grad /*[3][n]*/);
 
+/* ---- FP64 host oracle of the training step (every quantity in double) ----
+ * The same march, backward, TV (type 0, 6 neighbours) and Adam as the reference, with
+ * every operation in double: the yardstick the FP32 and the mixed 16-bit forms are both
+ * measured against.  pred [len][3] (background included), accw [len], losses [len],
+ * grad planar [n_arrays][n_act] (accumulated into). */
+void orc64_forward_backward(const orc_scene* s, const orc_rays* r, int start, int len,
+                            double mask_coef, double huber, double* pred, double* accw,
+                            double* losses, double* grad);
+/* TV type 0 / 6 neighbours in double, added into grad (same gating as orc_tv_grad). */
+void orc64_tv6(const orc_scene* s, const double* params, double* grad, double lam_d,
+               double lam_sh);
+/* Adam in double over planar params/moments (params updated in place, grad zeroed). */
+void orc64_adam(const orc_scene* s, double* params, double* grad, double* m, double* v,
+                double lr, double sh_lr, int timestep);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,10 @@ _fn("orc_compact", [_vp, C.c_int, C.c_int64, _vp, _vp, C.c_int64])
 _fn("orc_mse", [_vp, C.c_int], C.c_double)
 _fn("orc_composite_kat", [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _fn("orc_render_image", [C.POINTER(_Scene)] + [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
+_fn("orc64_forward_backward", [C.POINTER(_Scene), C.POINTER(_Rays), C.c_int, C.c_int, C.c_double, C.c_double,
+                               _vp, _vp, _vp, _vp])
+_fn("orc64_tv6", [C.POINTER(_Scene), _vp, _vp, C.c_double, C.c_double])
+_fn("orc64_adam", [C.POINTER(_Scene), _vp, _vp, _vp, _vp, C.c_double, C.c_double, C.c_int])
 
 
 def set_contract_mode(mode: int):
@@ -184,6 +188,33 @@ def render_image(scene: Scene, cam, bbox, width, height, white_bg=True):
                           int(height), 1 if white_bg else 0, _p(out["rgb"]), _p(out["rgb8"]), _p(out["depth"]),
                           _p(out["mask"]))
     return out
+
+
+def fp64_step(scene: Scene, rays: RaySet, mask_coef, huber, lam_d=None, lam_sh=None, lr=None, sh_lr=None,
+              timestep=1, start=0, length=None):
+    """The FP64 host oracle of one training batch: forward+backward over rays[start:start+length],
+    then (when lr is given) TV type 0 / 6 neighbours (when lam_d is given) and Adam from zero
+    moments.  Returns pred [len, 3], accw, losses, grad [n_arrays, n_act] (before TV/Adam) and
+    the post-step parameters (float64) or None."""
+    length = rays.n - start if length is None else length
+    na = 1 + 3 * scene.sh_dim
+    pred = np.zeros((length, 3), np.float64)
+    accw = np.zeros(length, np.float64)
+    losses = np.zeros(length, np.float64)
+    grad = np.zeros((na, scene.n_act), np.float64)
+    _lib.orc64_forward_backward(C.byref(scene.c), C.byref(rays.c), int(start), int(length), float(mask_coef),
+                                float(huber), _p(pred), _p(accw), _p(losses), _p(grad))
+    post = None
+    if lr is not None:
+        params = np.ascontiguousarray(scene.params, np.float64)
+        g = grad.copy()
+        if lam_d is not None:
+            _lib.orc64_tv6(C.byref(scene.c), _p(params), _p(g), float(lam_d), float(lam_sh))
+        m = np.zeros_like(params)
+        v = np.zeros_like(params)
+        _lib.orc64_adam(C.byref(scene.c), _p(params), _p(g), _p(m), _p(v), float(lr), float(sh_lr), int(timestep))
+        post = params
+    return pred, accw, losses, grad, post
 
 
 def render_forward(scene: Scene, rays: RaySet, sample_index=None, start=0, length=None):

@@ -155,3 +155,23 @@ def test_occupancy_x_face_flag_quirk():
     dens2[(n - 1) * n * n + 2 * n + (n - 1)] = 100.0  # occupies cells at z = D-2, x = W-2
     _, cage2, _, _, dropped2 = orc.occupancy(dens2, n, n, n, 8.0)
     assert dropped2 == 0 and cage2[(n - 1) * n * n + (n - 1)] == 1
+
+
+def test_fp64_oracle_agrees_with_the_reference_restatement(small):
+    """The all-FP64 oracle (the yardstick of the mixed forms) computes the same step as the
+    pinned restatement of the reference, up to the reference's float rounding."""
+    cfg, scene, rays = small
+    orc.render_forward(scene, rays)
+    losses32, grad32, _ = orc.render_backward(scene, rays, 1.0, 0.1)
+    pred64, accw64, losses64, grad64, post = orc.fp64_step(scene, rays, 1.0, 0.1, lam_d=1e-3, lam_sh=1e-3,
+                                                           lr=0.1, sh_lr=0.01)
+    pred32 = np.stack([rays["acc_r"], rays["acc_g"], rays["acc_b"]], 1)
+    assert np.abs(pred64 - pred32).max() < 2e-5
+    assert np.abs(accw64 - rays["acc_w"]).max() < 2e-5
+    assert np.abs(losses64 - losses32).max() < 255 * 2e-5
+    for blk in (slice(0, 1), slice(1, None)):
+        err = np.abs(grad64[blk] - grad32[blk]).max() / np.abs(grad64[blk]).max()
+        assert err < 1e-4, (blk, err)
+    # Adam from zero moments moves every updated parameter by about lr * sign(g) at t = 1
+    moved = np.abs(post - scene.params)
+    assert np.isfinite(post).all() and moved[0].max() <= 0.1 + 1e-9 and moved[1:].max() <= 0.01 + 1e-9
