@@ -49,6 +49,11 @@ WORKLOADS = {
     # CPU-runnable plain case shape, for quick runs
     "small128": dict(n=128, gt_n=128, n_blobs=8, gt_sh_std=0.3, cams=16, img=200, batch=4096,
                      pool_batches=8, init_density=0.1, seed=0),
+    # the precision configuration: 512^3 sparse grid whose occupancy is the hidden blob field
+    # thresholded at density 1.0 (about 10% of the cells), 16384-ray batches from 100 800x800
+    # views; the hidden grid is the same sparse structure with SH ~ N(0, 0.5)
+    "sparse512": dict(n=512, gt_n=512, n_blobs=4, gt_sh_std=0.5, cams=100, img=800, batch=16384,
+                      pool_batches=16, init_density=0.1, seed=1, sparse_threshold=1.0),
 }
 # the reference's shipped training constants (SparseVolumeRadianceField/config_linux.txt)
 STEP = dict(mask_coef=1.0, huber=0.1, lam_density=1e-5, lam_sh=1e-6, lr=0.3, sh_lr=1.0)
@@ -206,9 +211,14 @@ def run_ours(args, wl, world, rank, local):
 
     # ---- ground truth: render the pool pixels from the hidden grid with our forward
     gt_n = wl["gt_n"]
+    thr = wl.get("sparse_threshold")
     gt_scene = cpx.ObjectScene(gt_n, gt_n, gt_n, SH_DIM)
     gp = gt_params_device(wl, dev)
     gt_scene.upload_params_device(gp)
+    if thr is not None:
+        gt_scene.prune_self(thr, download=False)
+        gt_scene.make_sparse()
+    field = gp[0].clone() if thr is not None else None  # the training grid's occupancy source
     del gp
     torch.cuda.empty_cache()
     blank = [(np.zeros(wl["img"] ** 2, np.uint8),) * 3 + (None,) for _ in range(wl["cams"])]
@@ -227,10 +237,22 @@ def run_ours(args, wl, world, rank, local):
 
     # ---- training grid and the ray pool in its voxel space
     scene = cpx.ObjectScene(n, n, n, SH_DIM, precision=args.precision, sr_seed=wl["seed"] + 1)
-    init = torch.zeros((1 + 3 * SH_DIM, n ** 3), dtype=torch.float32, device=dev)
+    if thr is not None:
+        # occupancy from the hidden field, then density init_density and SH 0 on the in-cage
+        # vertices of the compact grid
+        init = torch.zeros((1 + 3 * SH_DIM, n ** 3), dtype=torch.float32, device=dev)
+        init[0] = field
+        scene.upload_params_device(init)
+        del init, field
+        torch.cuda.empty_cache()
+        scene.prune_self(thr, download=False)
+        scene.make_sparse()
+    n_act = scene.actual_grid_nums
+    init = torch.zeros((1 + 3 * SH_DIM, n_act), dtype=torch.float32, device=dev)
     init[0] = wl["init_density"]
     scene.upload_params_device(init)
     del init
+    torch.cuda.empty_cache()
     pool = cpx.Rays(P, white_bg=True)
     pool.initial_self(scene, [cpx.Camera.make(**S.look_at_camera(e, n, wl["img"], wl["img"])) for e in eyes],
                       blank, pix, wl["img"], wl["img"])
@@ -317,19 +339,23 @@ def run_ours(args, wl, world, rank, local):
     e2e_value = world * R * K / (e2e_ms / 1e3)
 
     # ---- roofline of the fused TV+Adam sweep
-    N = n ** 3
+    N = n_act
     rec = 28 * 4
     # gradient records are read and zeroed only for the vertices the batch touched
+    # dense grids read the density learning-rate multiplier (4 B); sparse grids read the
+    # compact->dense index (4 B) and the in-cage flag (1 B) of every active vertex
+    per_vertex_index = 4 if thr is None else 5
     if args.precision == "fp32":
-        # params r+w, m r+w, v r+w, density mirror w, LR mult r; grad r + zero-w where touched
-        alg_bytes = N * (6 * rec + 4 + 4) + touched * 2 * rec
-        sweep_kernel = "k_sweep<TV,dense> (fused TV type0/6 + Adam)"
+        # params r+w, m r+w, v r+w, density mirror w; grad r + zero-w where touched
+        alg_bytes = N * (6 * rec + 4 + per_vertex_index) + touched * 2 * rec
+        sweep_kernel = "k_sweep<TV,%s> (fused TV type0/6 + Adam)" % ("sparse" if thr is not None else "dense")
     else:
         # density r+w, 16-bit SH r+w, 16-bit m r+w, 16-bit v r+w, LR mult r; FP32 grad r +
         # zero-w where touched
         lrec = 28 * 2
-        alg_bytes = N * (8 + 6 * lrec + 4) + touched * 2 * rec
-        sweep_kernel = "k_sweep_lowp_dense<TV> (fused TV type0/6 + Adam, 16-bit storage, stochastic rounding)"
+        alg_bytes = N * (8 + 6 * lrec + per_vertex_index) + touched * 2 * rec
+        sweep_kernel = "k_sweep_lowp_%s<TV> (fused TV type0/6 + Adam, 16-bit storage, stochastic rounding)" % (
+            "sparse" if thr is not None else "dense")
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
     tpv = profiled_traffic_per_vertex() if args.precision == "fp32" else None
@@ -343,11 +369,14 @@ def run_ours(args, wl, world, rank, local):
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.precision == "fp32" else "f32 arithmetic, %s SH + bf16 moments" % args.precision,
-        "data": "synthetic: seeded 64-blob 512^3 hidden grid rendered by the plain forward; no dataset",
+        "data": "synthetic: seeded %d-blob %d^3 hidden grid rendered by the plain forward; no dataset"
+                % (wl["n_blobs"], wl["gt_n"]),
         "config": {
-            "workload": "plain FP32 training at scale: %d^3 grid SH band 2 (density 0.1, SH 0 init), %d-ray "
-                        "batches from %d %dx%d views of a hidden %d^3 64-blob grid, TV type 0/6 + Adam every batch"
-                        % (n, R, wl["cams"], wl["img"], wl["img"], wl["gt_n"]),
+            "workload": ("%s training: %d^3 %s grid SH band 2 (density 0.1, SH 0 init), %d-ray batches from %d "
+                         "%dx%d views of a hidden %d^3 %d-blob grid, TV type 0/6 + Adam every batch"
+                         % ("plain FP32" if args.precision == "fp32" else "mixed %s" % args.precision, n,
+                            "dense" if thr is None else "sparse (blob field > %.1f, %d active vertices)" % (thr, N),
+                            R, wl["cams"], wl["img"], wl["img"], wl["gt_n"], wl["n_blobs"])),
             "grid": n, "sh_dim": SH_DIM, "batch_rays": R, "pool_rays": P, "step_constants": STEP,
             "precision": args.precision,
             "l2": "inputs larger than L2: the sweep streams %.1f GB of grid state per step" % (alg_bytes / 1e9),
@@ -408,6 +437,9 @@ def run_reference(args, wl):
 
     if not RH.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libcpxref.so (reference built for sm_100a) missing"}
+    if wl.get("sparse_threshold") is not None:
+        return {"impl": "reference", "unavailable": "the reference arm runs the dense workloads (its sparse scene "
+                                                    "set-up takes the dense planar grid through host memory)"}
     n, R, P = wl["n"], wl["batch"], wl["batch"] * wl["pool_batches"]
     eyes, pix, order = camera_set(wl)
     img = wl["img"]
@@ -470,7 +502,7 @@ def run_reference(args, wl):
     return {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
         "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if args.precision == "fp32" else "f32 arithmetic, %s SH + bf16 moments" % args.precision, "impl": "reference",
+        "dtype": "f32", "impl": "reference",
         "data": "synthetic: seeded 64-blob 512^3 hidden grid rendered by the reference's forward; no dataset",
         "config": {"workload": "same as --impl ours", "grid": n, "batch_rays": R, "step_constants": STEP,
                    "entry_points": "RenderUtils::renderRays, renderRays_withGradients_RGB, losses D2H + "

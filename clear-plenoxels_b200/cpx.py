@@ -55,6 +55,9 @@ EXPORTED = [
     "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_grid_check",
     "cpx_last_sample_counts", "cpx_kernel_launches", "cpx_render_forward_backward_noalloc",
     "cpx_render_image", "cpx_image_mse", "cpx_grid_touched_count",
+    "cpx_proposal_param_count", "cpx_proposal_create", "cpx_proposal_destroy", "cpx_proposal_params",
+    "cpx_proposal_infer", "cpx_proposal_gradient", "cpx_proposal_train", "cpx_proposal_stats",
+    "cpx_render_forward_backward_guided", "cpx_train_step_proposal",
 ]
 
 
@@ -156,6 +159,31 @@ _sig("cpx_last_sample_counts", [_vp, _i32p, C.c_int])
 _sig("cpx_render_image", [_vp, C.POINTER(Camera), C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _sig("cpx_image_mse", [_vp, _vp, C.c_int64, C.POINTER(C.c_double), _vp])
 _sig("cpx_grid_touched_count", [_vp, C.POINTER(C.c_int64)])
+
+
+class ProposalDesc(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("confidence", C.c_float), ("label_weight", C.c_float),
+                ("learning_rate", C.c_float)]
+
+
+class ProposalSchedule(C.Structure):
+    _fields_ = [("warmup", C.c_int), ("train_every", C.c_int), ("train_steps", C.c_int),
+                ("rays_per_step", C.c_int)]
+
+
+_sig("cpx_proposal_param_count", [])
+_sig("cpx_proposal_create", [C.POINTER(ProposalDesc), C.POINTER(_vp)])
+_sig("cpx_proposal_destroy", [_vp])
+_sig("cpx_proposal_params", [_vp, _f32p, C.c_int])
+_sig("cpx_proposal_infer", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp])
+_sig("cpx_proposal_gradient", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _f32p, C.POINTER(C.c_double)])
+_sig("cpx_proposal_train", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.POINTER(C.c_double),
+                            _vp])
+_sig("cpx_proposal_stats", [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int)])
+_sig("cpx_render_forward_backward_guided", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_double, C.c_float, _vp, _vp,
+                                            _vp])
+_sig("cpx_train_step_proposal", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), C.POINTER(ProposalSchedule),
+                                 C.c_int, _vp, C.POINTER(C.c_double), _vp])
 
 
 def _check(rc: int, where: str):
@@ -324,12 +352,19 @@ class ObjectScene:
         _check(_lib.cpx_grid_set_optimize_step(self._h, int(step)), "cpx_grid_set_optimize_step")
 
     # -- occupancy (pruneSelf + getCagedNums, SceneUtils.cu:883, 1081)
-    def prune_self(self, threshold: float):
+    def prune_self(self, threshold: float, download: bool = True):
+        """objectScene::pruneSelf + getCagedNums on the device.  Returns (occupancy, in_cage,
+        index_offsets, in-cage count); with download=False only the count (the tables stay on
+        the device)."""
+        cnt = C.c_uint32()
+        if not download:
+            _check(_lib.cpx_occupancy_build(self._h, float(threshold), None, None, None, C.byref(cnt)),
+                   "cpx_occupancy_build")
+            return None, None, None, int(cnt.value)
         W, H, D = self.width, self.height, self.depth
         occ = np.empty((W - 1) * (H - 1) * (D - 1), np.uint8)
         cage = np.empty(W * H * D, np.uint8)
         idx = np.empty(W * H * D, np.uint32)
-        cnt = C.c_uint32()
         _check(_lib.cpx_occupancy_build(self._h, float(threshold), occ.ctypes.data, cage.ctypes.data,
                                         idx.ctypes.data, C.byref(cnt)), "cpx_occupancy_build")
         return occ, cage, idx, int(cnt.value)
@@ -554,6 +589,114 @@ def train_step(scene: ObjectScene, rays: Rays, losses, *, start: int = 0, length
 def lr_decay(lr: float, batch_count: int, epoch: int) -> float:
     """Per-batch learning-rate decay of the reference (Render.cu:499-500)."""
     return lr / (2.0 ** (1.0 / batch_count / (epoch + 1.0)))
+
+
+class Proposal:
+    """Learned sample-interval proposal (no reference counterpart): 32 segments per ray,
+    MLP 48 -> 64 -> 64 -> 64 -> 1 with BF16 tensor-core inference and FP32 training."""
+
+    SEGMENTS = 32
+
+    def __init__(self, seed=0, confidence=0.9, label_weight=1e-3, learning_rate=1e-3):
+        d = ProposalDesc()
+        d.seed, d.confidence, d.label_weight, d.learning_rate = int(seed), float(confidence), float(label_weight), \
+            float(learning_rate)
+        self.desc = d
+        h = _vp()
+        _check(_lib.cpx_proposal_create(C.byref(d), C.byref(h)), "cpx_proposal_create")
+        self._h = h
+        self.n_params = int(_lib.cpx_proposal_param_count())
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cpx_proposal_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        out = np.empty(self.n_params, np.float32)
+        _check(_lib.cpx_proposal_params(self._h, out, 0), "cpx_proposal_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32).copy()
+        _check(_lib.cpx_proposal_params(self._h, p, 1), "cpx_proposal_params")
+
+    def infer(self, scene, rays, start=0, length=None, sample_index=None, tensor_cores=True, stream=None):
+        """(logits [len, 32], masks [len] uint32 as int32) CUDA tensors."""
+        import torch
+
+        n = _len(rays, start, length)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        logits = torch.empty((n, self.SEGMENTS), dtype=torch.float32, device=dev)
+        masks = torch.empty(n, dtype=torch.int32, device=dev)
+        _check(_lib.cpx_proposal_infer(self._h, scene.handle, rays.handle, _ptr(sample_index), int(start), n,
+                                       _ptr(logits), _ptr(masks), 1 if tensor_cores else 0, _stream(stream)),
+               "cpx_proposal_infer")
+        return logits, masks
+
+    def gradient(self, scene, rays, seg_weights, start=0, length=None, sample_index=None):
+        n = _len(rays, start, length)
+        g = np.empty(self.n_params, np.float32)
+        loss = C.c_double()
+        _check(_lib.cpx_proposal_gradient(self._h, scene.handle, rays.handle, _ptr(sample_index), int(start), n,
+                                          _ptr(seg_weights), g, C.byref(loss)), "cpx_proposal_gradient")
+        return g, loss.value
+
+    def train(self, scene, rays, seg_weights, steps, rays_per_step=0, start=0, length=None, sample_index=None,
+              stream=None):
+        n = _len(rays, start, length)
+        loss = C.c_double()
+        _check(_lib.cpx_proposal_train(self._h, scene.handle, rays.handle, _ptr(sample_index), int(start), n,
+                                       _ptr(seg_weights), int(steps), int(rays_per_step), C.byref(loss),
+                                       _stream(stream)), "cpx_proposal_train")
+        return loss.value
+
+    def stats(self):
+        r, c, f = C.c_int(), C.c_int64(), C.c_int()
+        _check(_lib.cpx_proposal_stats(self._h, C.byref(r), C.byref(c), C.byref(f)), "cpx_proposal_stats")
+        return {"rounds": r.value, "confident_rays": c.value, "error_flags": f.value}
+
+
+def render_guided(scene: ObjectScene, rays: Rays, losses, start=0, length=None, sample_index=None, mask_coef=1.0,
+                  huber_delta=0.1, masks=None, seg_weights=None, stream=None):
+    """The mixed-form march guided by per-ray segment masks and/or recording segment weights."""
+    n = _len(rays, start, length)
+    _check(_lib.cpx_render_forward_backward_guided(scene.handle, rays.handle, _ptr(losses), _ptr(sample_index),
+                                                   int(start), n, float(mask_coef), float(huber_delta),
+                                                   _ptr(masks), _ptr(seg_weights), _stream(stream)),
+           "cpx_render_forward_backward_guided")
+
+
+def train_step_proposal(scene: ObjectScene, rays: Rays, proposal: Proposal, losses, iteration: int, *, start=0,
+                        length=None, sample_index=None, mask_coef=1.0, huber_delta=0.1, do_tv=True,
+                        lam_density=1e-5, lam_sh=1e-6, lr=0.3, sh_lr=1.0, timestep=1, warmup=0, train_every=50,
+                        train_steps=16, rays_per_step=1024, want_mse=True, stream=None):
+    """One batch of the mixed form with the learned proposal; returns the batch MSE."""
+    a = StepArgs()
+    a.mask_coef, a.huber_delta, a.do_tv, a.tv_type, a.tv_neighbours = float(mask_coef), float(huber_delta), \
+        1 if do_tv else 0, 0, 6
+    a.lam_density, a.lam_sh, a.lr, a.sh_lr, a.timestep = float(lam_density), float(lam_sh), float(lr), \
+        float(sh_lr), int(timestep)
+    sch = ProposalSchedule()
+    sch.warmup, sch.train_every, sch.train_steps, sch.rays_per_step = int(warmup), int(train_every), \
+        int(train_steps), int(rays_per_step)
+    n = _len(rays, start, length)
+    mse = C.c_double(0.0)
+    _check(_lib.cpx_train_step_proposal(scene.handle, rays.handle, proposal.handle, _ptr(sample_index), int(start), n,
+                                        C.byref(a), C.byref(sch), int(iteration), _ptr(losses),
+                                        C.byref(mse) if want_mse else None, _stream(stream)),
+           "cpx_train_step_proposal")
+    return mse.value if want_mse else None
 
 
 def image_mse(a, b, stream=None) -> float:

@@ -766,6 +766,76 @@ cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int sta
     return CPX_OK;
 }
 
+cpx_status cpx_render_forward_backward_guided(cpx_grid* g, cpx_rays* r, double* losses, const int32_t* sidx,
+                                              int start, int len, double mask_coef, float huber,
+                                              const uint32_t* masks, float* seg_w, cpx_stream stream)
+{
+    if (check_grid(g) || !r) return CPX_ERR_INVALID_ARGUMENT;
+    return march_launch_guided(g, r, sidx, start, len, losses, mask_coef, huber, masks, seg_w, (cudaStream_t)stream);
+}
+
+// Finishes a batch after its march: TV + Adam sweep and the optional batch MSE.
+static cpx_status finish_step(cpx_grid* g, const cpx_step_args* a, double* losses, int len, double* mse_out,
+                              cudaStream_t st)
+{
+    if (a->timestep < 1) {
+        set_error("timestep starts at 1");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    const bool fuse = a->do_tv && a->tv_type == 0 && a->tv_neighbours == 6;
+    cpx_status s = sweep_adam(g, fuse, a->lam_density, a->lam_sh, a->lr, a->sh_lr, a->timestep, st);
+    if (s != CPX_OK || !mse_out) return s;
+    s = mse_launch(losses, len, g->scratch.mse, st);
+    if (s != CPX_OK) return s;
+    cudaError_t e = cudaMemcpyAsync(mse_out, g->scratch.mse, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return cuda_status(e, "mse");
+}
+
+cpx_status cpx_train_step_proposal(cpx_grid* g, cpx_rays* r, cpx_proposal* p, const int32_t* sidx, int start,
+                                   int len, const cpx_step_args* a, const cpx_proposal_schedule* sch, int iteration,
+                                   double* losses, double* mse_out, cpx_stream stream)
+{
+    if (check_grid(g) || !r || !p || !a || !sch) return CPX_ERR_INVALID_ARGUMENT;
+    if (g->prec == kPrecFP32) {
+        set_error("the proposal form runs on the mixed-precision grid forms");
+        return CPX_ERR_UNSUPPORTED;
+    }
+    if (a->do_tv && !(a->tv_type == 0 && a->tv_neighbours == 6)) {
+        set_error("the mixed forms run TV type 0 / 6 neighbours fused into the optimizer sweep only");
+        return CPX_ERR_UNSUPPORTED;
+    }
+    if (sch->train_every < 1 || sch->train_steps < 0 || iteration < 0) {
+        set_error("invalid proposal schedule");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool label = iteration < sch->warmup || iteration % sch->train_every == 0;
+    cpx_status s;
+    if (label) {
+        // full march recording the segment weights, then a training round on them
+        float* seg_w = proposal_label_buffer(p, len);
+        if (!seg_w) {
+            set_error("proposal labels could not be allocated");
+            return CPX_ERR_OUT_OF_MEMORY;
+        }
+        s = march_launch_guided(g, r, sidx, start, len, losses, a->mask_coef, a->huber_delta, nullptr, seg_w, st);
+        if (s != CPX_OK) return s;
+        const bool train = iteration % sch->train_every == 0 || iteration + 1 == sch->warmup;
+        if (train && sch->train_steps > 0) {
+            s = proposal_train(p, g, r, sidx, start, len, seg_w, sch->train_steps, sch->rays_per_step, true, st);
+            if (s != CPX_OK) return s;
+        }
+    } else {
+        uint32_t* masks = nullptr;
+        s = proposal_masks(p, g, r, sidx, start, len, st, &masks);
+        if (s != CPX_OK) return s;
+        s = march_launch_guided(g, r, sidx, start, len, losses, a->mask_coef, a->huber_delta, masks, nullptr, st);
+        if (s != CPX_OK) return s;
+    }
+    return finish_step(g, a, losses, len, mse_out, st);
+}
+
 cpx_status cpx_grid_touched_count(cpx_grid* g, int64_t* count)
 {
     if (check_grid(g) || !count) return CPX_ERR_INVALID_ARGUMENT;

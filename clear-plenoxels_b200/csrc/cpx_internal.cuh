@@ -228,6 +228,15 @@ cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int 
                              int mode, double* losses, double mask_coef, float huber,
                              const MarchScratch& s, cudaStream_t st);
 int march_samples_per_ray(const cpx_grid* g);
+cpx_status march_launch_guided(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                               double* losses, double mask_coef, float huber, const uint32_t* masks,
+                               float* seg_w, cudaStream_t st);
+// proposal.cu
+cpx_status proposal_masks(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                          cudaStream_t st, uint32_t** masks_out);
+float* proposal_label_buffer(cpx_proposal* p, int len);
+cpx_status proposal_train(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                          const float* seg_w, int steps, int rays_per_step, bool adam, cudaStream_t st);
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
                       double sh_lr, int timestep, cudaStream_t s);
 cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
@@ -243,5 +252,8 @@ cpx_status rays_camera_launch(cpx_rays* r, const cpx_grid* g, const cpx_camera* 
 cpx_status mse_launch(const double* losses, int len, double* out, cudaStream_t s);
 
 enum MarchMode { kForward = 1, kBackward = 2, kForwardBackward = 3 };
+
+// Segments per ray of the learned proposal (proposal.cu).
+constexpr int kProposalSegments = 32;
 
 }  // namespace cpx

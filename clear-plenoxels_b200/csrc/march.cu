@@ -94,10 +94,15 @@ __device__ __forceinline__ float real_exp(float x) { return expf(x); }
 // recurrence operation for operation (the FP32 form); the mixed forms march in FP32
 // (Real = float): the same recurrence with t, transmittance and weights in float.
 // ---------------------------------------------------------------------------
-template <typename Real>
+// PROP: the proposal-aware march of the mixed forms.  seg_mask holds one bit per segment of
+// 32 equal segments of [near, far]: the march jumps over segments whose bit is clear and
+// stops after the last set one (all bits set = the full march).  seg_w, when non-null,
+// receives the summed sample weights of each segment (the proposal's labels).
+template <typename Real, bool PROP>
 __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
                                           SampleRec* samples, int maxs, int* counts,
-                                          double* acc_out, int* err, bool write_fwd)
+                                          double* acc_out, int* err, bool write_fwd,
+                                          uint32_t seg_mask, float* seg_w)
 {
     // renderRaysGPU zeroes the outputs first (RenderUtils.cu:1927-1941); the backward alone
     // leaves the forward's outputs as they are
@@ -118,7 +123,9 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
     // maxs bounds every ray inside the grid box; longer (or non-finite) rays stop there with
     // the error flag set instead of marching on.
     const double bound = floor(((double)far_t - (double)near_t + 2.0) / (double)step) + 4.0;
-    const int it_cap = bound < (double)(maxs + 16) ? (int)bound : maxs + 16;
+    // the guided march also spends an iteration on every jump over a skipped segment (two when
+    // the jump's end rounds back into the skipped segment)
+    const int it_cap = (bound < (double)(maxs + 16) ? (int)bound : maxs + 16) + (PROP ? 2 * kProposalSegments : 0);
 
     SampleRec* out = samples + (size_t)b * maxs;
     Real t = near_t;
@@ -130,10 +137,24 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
     // densities of the last cell visited (consecutive samples mostly share a cell)
     unsigned cb0 = 0xffffffffu, cb1 = 0, cb2 = 0;
     float cd[8];
+    const Real seg_len = PROP ? ((Real)far_t - (Real)near_t) * (Real)(1.0 / kProposalSegments) : (Real)0;
+    const Real inv_seg = PROP && seg_len > (Real)0 ? (Real)1 / seg_len : (Real)0;
     while (t < far_t) {
         if (++it > it_cap || n >= maxs) {
             atomicOr(err, 1);
             break;
+        }
+        int seg = 0;
+        if (PROP) {
+            seg = (int)((t - (Real)near_t) * inv_seg);
+            seg = seg < 0 ? 0 : (seg > kProposalSegments - 1 ? kProposalSegments - 1 : seg);
+            if (!((seg_mask >> seg) & 1u)) {
+                if ((seg_mask >> seg) == 0u) break;  // no predicted segment ahead
+                Real tn = (Real)near_t + (Real)(seg + 1) * seg_len;
+                t = tn > t ? tn : t + (Real)step;
+                ++intT;
+                continue;
+            }
         }
         Real ofx = 0, ofy = 0, ofz = 0;
         if (intT < g.n_off) {
@@ -201,6 +222,7 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
         acc += w;
         accDen += sigma;
         accD += sigma * step;
+        if (PROP && seg_w) seg_w[seg] += (float)w;
         const Real Tn = real_exp(-accD);
         SampleRec rec;
         rec.bx = (uint16_t)(b0 < 65535u ? b0 : 65535u);
@@ -604,10 +626,11 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
 // The two stages as kernels.  Placement is latency-bound per ray and needs only one thread
 // per ray, all resident in one wave; shading is throughput-bound and takes a warp per ray.
 // ---------------------------------------------------------------------------
-template <int MODE, typename Real>
+template <int MODE, typename Real, bool PROP>
 __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int32_t* sidx, int start,
                                                int len, int64_t n_rays, SampleRec* samples, int maxs,
-                                               int* counts, double* acc, int* err)
+                                               int* counts, double* acc, int* err, const uint32_t* seg_masks,
+                                               float* seg_w)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= len) return;
@@ -617,7 +640,9 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
         counts[b] = -2;  // invalid ray index: nothing is read or written for it
         return;
     }
-    place_ray<Real>(g, r, b, ri, samples, maxs, counts, acc, err, (MODE & kForward) != 0);
+    const uint32_t mask = PROP && seg_masks ? seg_masks[b] : 0xffffffffu;
+    float* sw = PROP && seg_w ? seg_w + (size_t)b * kProposalSegments : nullptr;
+    place_ray<Real, PROP>(g, r, b, ri, samples, maxs, counts, acc, err, (MODE & kForward) != 0, mask, sw);
 }
 
 constexpr int kShadeWarps = 4;
@@ -727,17 +752,28 @@ static cpx_status ensure_scratch(cpx_grid* g, int len)
     return CPX_OK;
 }
 
+// Proposal inputs of a march: per-ray segment masks and/or segment-weight output.
+struct Guide {
+    const uint32_t* masks = nullptr;
+    float* seg_w = nullptr;
+    bool on() const { return masks != nullptr || seg_w != nullptr; }
+};
+
 template <int MODE, int NSH, int PREC>
 static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv, const int32_t* sidx,
                         int start, int len, int64_t n_rays, const MarchScratch& s, double* losses,
-                        double mask_coef, float huber, uint32_t* touched)
+                        double mask_coef, float huber, uint32_t* touched, const Guide& guide)
 {
     using Real = typename std::conditional<PREC == kPrecFP32, double, float>::type;
     const dim3 pgrid((unsigned)((len + 31) / 32));
     const dim3 sgrid((unsigned)((len + kShadeWarps - 1) / kShadeWarps));
     const dim3 sblock(kShadeWarps * 32);
-    k_place<MODE, Real><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs, s.counts,
-                                              s.acc, s.err);
+    if (PREC != kPrecFP32 && guide.on())
+        k_place<MODE, Real, true><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
+                                                        s.counts, s.acc, s.err, guide.masks, guide.seg_w);
+    else
+        k_place<MODE, Real, false><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
+                                                         s.counts, s.acc, s.err, nullptr, nullptr);
     k_shade<NSH, MODE, PREC><<<sgrid, sblock, 0, st>>>(gv, rv, sidx, start, len, s.samples, s.colours, s.maxs,
                                                        s.counts, s.acc, losses, mask_coef, huber, touched);
 }
@@ -746,28 +782,28 @@ template <int NSH, int PREC>
 static void launch_march(int mode, cudaStream_t st, const GridView& gv, const RaysView& rv,
                          const int32_t* sidx, int start, int len, int64_t n_rays,
                          const MarchScratch& s, double* losses, double mask_coef, float huber,
-                         uint32_t* touched)
+                         uint32_t* touched, const Guide& guide)
 {
     if (mode == kForward)
         launch_mode<kForward, NSH, PREC>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber,
-                                         touched);
+                                         touched, guide);
     else if (mode == kBackward)
         launch_mode<kBackward, NSH, PREC>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber,
-                                          touched);
+                                          touched, guide);
     else
         launch_mode<kForwardBackward, NSH, PREC>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef,
-                                                 huber, touched);
+                                                 huber, touched, guide);
 }
 
 template <int PREC>
 static cpx_status launch_prec(int sh_dim, int mode, cudaStream_t st, const GridView& gv, const RaysView& rv,
                               const int32_t* sidx, int start, int len, int64_t n_rays, const MarchScratch& s,
-                              double* losses, double mask_coef, float huber, uint32_t* touched)
+                              double* losses, double mask_coef, float huber, uint32_t* touched, const Guide& guide)
 {
     switch (sh_dim) {
-    case 1: launch_march<1, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched); break;
-    case 4: launch_march<4, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched); break;
-    case 9: launch_march<9, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched); break;
+    case 1: launch_march<1, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched, guide); break;
+    case 4: launch_march<4, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched, guide); break;
+    case 9: launch_march<9, PREC>(mode, st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef, huber, touched, guide); break;
     default:
         set_error("sh_dim %d unsupported", sh_dim);
         return CPX_ERR_UNSUPPORTED;
@@ -799,24 +835,39 @@ static cpx_status march_check_args(cpx_grid* g, cpx_rays* r, const int32_t* sidx
 
 int march_samples_per_ray(const cpx_grid* g) { return max_samples_per_ray(g); }
 
+static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                                           int mode, double* losses, double mask_coef, float huber,
+                                           const MarchScratch& s, const Guide& guide, cudaStream_t st);
+
 cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                              int mode, double* losses, double mask_coef, float huber,
                              const MarchScratch& s, cudaStream_t st)
 {
+    return march_launch_guided_with(g, r, sidx, start, len, mode, losses, mask_coef, huber, s, Guide(), st);
+}
+
+static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                                           int mode, double* losses, double mask_coef, float huber,
+                                           const MarchScratch& s, const Guide& guide, cudaStream_t st)
+{
     cpx_status rc = march_check_args(g, r, sidx, start, len, mode, losses);
     if (rc != CPX_OK || len == 0) return rc;
+    if (guide.on() && g->prec == kPrecFP32) {
+        set_error("the proposal-guided march runs on the mixed forms (FP32 march) only");
+        return CPX_ERR_UNSUPPORTED;
+    }
     const GridView gv = grid_view(g);
     const RaysView rv = rays_view(r);
     uint32_t* touched = g->touched[g->tcur];
     if (g->prec == kPrecFP32)
         rc = launch_prec<kPrecFP32>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
-                                    touched);
+                                    touched, guide);
     else if (g->prec == kPrecBF16)
         rc = launch_prec<kPrecBF16>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
-                                    touched);
+                                    touched, guide);
     else
         rc = launch_prec<kPrecFP16>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
-                                    touched);
+                                    touched, guide);
     if (rc != CPX_OK) return rc;
     count_launch(2);
     return cuda_status(cudaGetLastError(), "march");
@@ -833,6 +884,27 @@ cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start
     rc = ensure_scratch(g, len);
     if (rc != CPX_OK) return rc;
     return march_launch_with(g, r, sidx, start, len, mode, losses, mask_coef, huber, g->scratch, st);
+}
+
+cpx_status march_launch_guided(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                               double* losses, double mask_coef, float huber, const uint32_t* masks,
+                               float* seg_w, cudaStream_t st)
+{
+    cpx_status rc = march_check_args(g, r, sidx, start, len, kForwardBackward, losses);
+    if (rc != CPX_OK) return rc;
+    g->last_len = len;
+    if (len == 0) return CPX_OK;
+    rc = ensure_scratch(g, len);
+    if (rc != CPX_OK) return rc;
+    if (seg_w) {
+        cudaError_t e = cudaMemsetAsync(seg_w, 0, (size_t)len * kProposalSegments * sizeof(float), st);
+        if (e != cudaSuccess) return cuda_status(e, "segment weights");
+    }
+    Guide guide;
+    guide.masks = masks;
+    guide.seg_w = seg_w;
+    return march_launch_guided_with(g, r, sidx, start, len, kForwardBackward, losses, mask_coef, huber, g->scratch,
+                                    guide, st);
 }
 
 }  // namespace cpx

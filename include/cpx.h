@@ -258,6 +258,69 @@ cpx_status cpx_last_sample_counts(const cpx_grid* g, int32_t* counts_host, int l
 /* Number of kernels this library launched since load (for launch accounting). */
 int64_t cpx_kernel_launches(void);
 
+/* ---- Learned sample-interval proposal (no reference counterpart) ----
+ * A small MLP (48 -> 64 -> 64 -> 64 -> 1, ReLU; BF16 tensor-core inference, FP32 training)
+ * predicts for each of 32 equal segments of a ray's [near, far] whether it holds visible
+ * density.  Input per segment: the midpoint in box coordinates with its 4-octave sin/cos
+ * encoding, the ray direction and the ray origin.  Label: the samples of a full march inside
+ * the segment carry total weight above label_weight (empty and occluded segments are 0).
+ * A ray all of whose 32 predictions are confident marches only the predicted segments;
+ * every other ray runs the full march. */
+typedef struct cpx_proposal cpx_proposal;
+typedef struct cpx_proposal_desc {
+    uint32_t seed;         /* parameter initialisation */
+    float confidence;      /* a segment is decided when sigmoid(logit) >= c or <= 1 - c (0.9) */
+    float label_weight;    /* segment label threshold on the summed sample weights (1e-3) */
+    float learning_rate;   /* Adam (1e-3) */
+} cpx_proposal_desc;
+
+int cpx_proposal_param_count(void);
+cpx_status cpx_proposal_create(const cpx_proposal_desc* desc, cpx_proposal** out);
+cpx_status cpx_proposal_destroy(cpx_proposal* p);
+/* FP32 parameters [cpx_proposal_param_count()] (W1 [64][48], b1, W2 [64][64], b2, W3, b3,
+ * w4 [64], b4) to (upload = 0) or from (upload = 1) host memory. */
+cpx_status cpx_proposal_params(cpx_proposal* p, float* host, int upload);
+/* Logits [len][32] and/or per-ray segment masks [len] (all ones = full march) of a batch;
+ * tensor_cores = 0 runs the FP32 CUDA-core forward instead (for checking). */
+cpx_status cpx_proposal_infer(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev,
+                              int start, int len, float* logits_dev, uint32_t* masks_dev, int tensor_cores,
+                              cpx_stream stream);
+/* Gradient of the mean binary cross-entropy over the batch's 32*len points against the
+ * labels of seg_weights_dev [len][32], to host memory, without an update.  Synchronous. */
+cpx_status cpx_proposal_gradient(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev,
+                                 int start, int len, const float* seg_weights_dev, float* grad_host,
+                                 double* loss_out);
+/* `steps` Adam steps over consecutive slices of rays_per_step rays of the batch. */
+cpx_status cpx_proposal_train(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev,
+                              int start, int len, const float* seg_weights_dev, int steps, int rays_per_step,
+                              double* loss_out, cpx_stream stream);
+/* Completed training rounds, rays that marched under a confident proposal so far, and the
+ * device error flags (4: a tensor-core wait ran out).  Synchronous. */
+cpx_status cpx_proposal_stats(cpx_proposal* p, int* rounds, int64_t* confident_rays, int* error_flags);
+/* The march of cpx_render_forward_backward with segment weights [len][32] recorded
+ * (seg_weights_dev, the proposal's labels) when non-NULL, or guided by per-ray segment masks
+ * [len] (masks_dev, from cpx_proposal_infer) when non-NULL.  The mixed-precision forms
+ * only (FP32 march).  With neither it equals cpx_render_forward_backward. */
+cpx_status cpx_render_forward_backward_guided(cpx_grid* g, cpx_rays* r, double* losses_dev,
+                                              const int32_t* sample_index_dev, int start, int len,
+                                              double mask_coef, float huber_delta,
+                                              const uint32_t* masks_dev, float* seg_weights_dev,
+                                              cpx_stream stream);
+/* One training batch of the mixed form with the proposal: every train_every-th iteration
+ * (and every iteration before warmup) runs the full march, records labels and then trains
+ * the proposal (train_steps Adam steps of rays_per_step rays); the other iterations infer
+ * the masks and run the guided march; then TV + Adam as cpx_train_step. */
+typedef struct cpx_proposal_schedule {
+    int warmup;          /* iterations of full march before the proposal is used */
+    int train_every;     /* label + training period (50) */
+    int train_steps;     /* Adam steps per training round */
+    int rays_per_step;   /* rays per Adam step */
+} cpx_proposal_schedule;
+cpx_status cpx_train_step_proposal(cpx_grid* g, cpx_rays* r, cpx_proposal* p, const int32_t* sample_index_dev,
+                                   int start, int len, const cpx_step_args* args,
+                                   const cpx_proposal_schedule* schedule, int iteration, double* losses_dev,
+                                   double* mse_out, cpx_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,182 @@
+"""The learned proposal on the GPU: tensor-core inference and FP32 training gradients against
+the FP64 oracle (oracle/proposal_ref.py), and the guided march of the mixed form.
+
+Tolerances: FP32 CUDA-core logits within 1e-4 (relative to the largest logit) of the FP64
+oracle; BF16 tensor-core logits within 2e-2 of the oracle run with the same BF16 roundings;
+training gradient within 1e-4 normwise of the FP64 gradient."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup(cuda):
+    import torch
+
+    import cpx
+    import cpx_scenes as S
+
+    cfg = S.small_config(seed=41, n=64, n_cams=8, img=96, n_rays=2048)
+    n = cfg["W"]
+    scene = cpx.ObjectScene(n, n, n, 9, precision="bf16", sr_seed=3)
+    scene.upload_params(cfg["params"])
+    nr = sum(len(p) for p in cfg["pix"])
+    rays = cpx.Rays(nr, white_bg=True)
+    rays.initial_self(scene, [cpx.Camera.make(**c) for c in cfg["cams"]], cfg["images"], cfg["pix"], 96, 96)
+    geo = rays.download(fields=("ox", "oy", "oz", "dx", "dy", "dz", "near", "far"))
+    return cfg, scene, rays, geo, torch
+
+
+def _feats(geo, n):
+    import proposal_ref as P
+
+    return P.features(geo["ox"], geo["oy"], geo["oz"], geo["dx"], geo["dy"], geo["dz"], geo["near"], geo["far"],
+                      (n, n, n))
+
+
+def _trained_like_params(seed):
+    """Parameters with logits spread over both signs (a fresh network sits near b4 = -2)."""
+    import proposal_ref as P
+
+    rng = np.random.default_rng(seed)
+    p = np.zeros(P.N_PARAMS, np.float32)
+    W1 = rng.uniform(-1, 1, (P.HID, P.N_IN)) * np.sqrt(6 / P.N_FEAT)
+    W1[:, P.N_FEAT:] = 0
+    p[P.O_W1:P.O_B1] = W1.reshape(-1)
+    p[P.O_W2:P.O_B2] = (rng.uniform(-1, 1, (P.HID, P.HID)) * np.sqrt(6 / P.HID)).reshape(-1)
+    p[P.O_W3:P.O_B3] = (rng.uniform(-1, 1, (P.HID, P.HID)) * np.sqrt(6 / P.HID)).reshape(-1)
+    p[P.O_B1:P.O_W2] = rng.normal(0, 0.1, P.HID)
+    p[P.O_W4:P.O_B4] = rng.normal(0, 0.5, P.HID)
+    return p
+
+
+def test_inference_matches_oracle(setup):
+    import cpx
+    import proposal_ref as P
+
+    cfg, scene, rays, geo, torch = setup
+    prop = cpx.Proposal(seed=1)
+    params = _trained_like_params(5)
+    prop.set_params(params)
+    x = _feats(geo, cfg["W"])
+    ref32 = P.forward(params, x)
+    ref16 = P.forward(params, x, bf16=True)
+    lf, mf = prop.infer(scene, rays, tensor_cores=False)
+    lt, mt = prop.infer(scene, rays, tensor_cores=True)
+    torch.cuda.synchronize()
+    lf, lt = lf.cpu().numpy().astype(np.float64), lt.cpu().numpy().astype(np.float64)
+    scale = max(np.abs(ref32).max(), 1.0)
+    assert np.abs(lf - ref32).max() <= 1e-4 * scale
+    assert np.abs(lt - ref16).max() <= 2e-2 * scale
+    assert np.abs(ref32).std() > 0.5  # the logits are spread, the check is not trivial
+    st = prop.stats()
+    assert st["error_flags"] == 0
+    # masks follow the logits: confident rays take the sign pattern, the others march in full
+    for logits, masks in ((lf, mf.cpu().numpy().view(np.uint32)), (lt, mt.cpu().numpy().view(np.uint32))):
+        conf = (np.abs(logits) >= np.log(0.9 / 0.1)).all(1)
+        bits = ((logits > 0) * (1 << np.arange(32, dtype=np.uint64))).sum(1).astype(np.uint32)
+        assert np.array_equal(masks[conf], bits[conf])
+        assert (masks[~conf] == 0xFFFFFFFF).all()
+    prop.close()
+
+
+def test_training_gradient_matches_oracle(setup):
+    import cpx
+    import proposal_ref as P
+
+    cfg, scene, rays, geo, torch = setup
+    prop = cpx.Proposal(seed=2)
+    params = _trained_like_params(6)
+    prop.set_params(params)
+    nr = rays.total_rays
+    rng = np.random.default_rng(0)
+    seg_w = rng.exponential(1e-2, (nr, 32)).astype(np.float32) * (rng.random((nr, 32)) < 0.3)
+    sw = torch.from_numpy(seg_w).cuda()
+    g, loss = prop.gradient(scene, rays, sw)
+    x = _feats(geo, cfg["W"])
+    y = seg_w > 1e-3
+    loss64, g64 = P.loss_and_grad(params.astype(np.float64), x, y)
+    assert abs(loss - loss64) <= 1e-5 * max(1.0, loss64)
+    assert np.abs(g - g64).max() <= 1e-4 * np.abs(g64).max()
+    # training on these labels lowers the loss
+    before = loss
+    for _ in range(4):
+        after = prop.train(scene, rays, sw, steps=25, rays_per_step=512)
+    assert after < 0.7 * before
+    prop.close()
+
+
+def test_guided_march_with_full_masks_equals_the_march(setup):
+    import cpx
+
+    cfg, scene, rays, geo, torch = setup
+    nr = rays.total_rays
+    zero = np.zeros((28, scene.actual_grid_nums), np.float32)
+    la = torch.zeros(nr, dtype=torch.float64, device="cuda")
+    scene.upload_grads(zero)
+    cpx.RenderUtils.renderRays_forwardBackward(scene, rays, la, maskRayLossCoefficient=1.0, huberDelta=0.1)
+    ca = scene.last_sample_counts(nr)
+    oa = rays.download(fields=cpx.RAY_OUTPUTS)
+    full = torch.full((nr,), -1, dtype=torch.int32, device="cuda")
+    seg_w = torch.zeros((nr, 32), dtype=torch.float32, device="cuda")
+    lb = torch.zeros(nr, dtype=torch.float64, device="cuda")
+    scene.upload_grads(zero)
+    cpx.render_guided(scene, rays, lb, masks=full, seg_weights=seg_w)
+    cb = scene.last_sample_counts(nr)
+    ob = rays.download(fields=cpx.RAY_OUTPUTS)
+    assert np.array_equal(ca, cb)
+    assert np.array_equal(oa["acc_weights"], ob["acc_weights"])
+    assert np.array_equal(oa["acc_density"], ob["acc_density"])
+    # the recorded segment weights sum to each ray's accumulated weight
+    assert np.abs(seg_w.sum(1).cpu().numpy() - ob["acc_weights"]).max() < 1e-5
+
+
+def test_guided_march_skips_masked_segments(setup):
+    import cpx
+
+    cfg, scene, rays, geo, torch = setup
+    nr = rays.total_rays
+    rng = np.random.default_rng(9)
+    masks = rng.integers(0, 2 ** 32, nr, dtype=np.uint64).astype(np.uint32)
+    masks[:64] = 0  # nothing predicted: no samples, background only
+    mt = torch.from_numpy(masks.view(np.int32)).cuda()
+    seg_w = torch.zeros((nr, 32), dtype=torch.float32, device="cuda")
+    losses = torch.zeros(nr, dtype=torch.float64, device="cuda")
+    scene.upload_grads(np.zeros((28, scene.actual_grid_nums), np.float32))
+    cpx.render_guided(scene, rays, losses, masks=mt, seg_weights=seg_w)
+    scene.check()
+    sw = seg_w.cpu().numpy()
+    bits = ((masks[:, None] >> np.arange(32, dtype=np.uint32)) & 1).astype(bool)
+    assert not sw[~bits].any()
+    assert sw[bits].any()
+    out = rays.download(fields=cpx.RAY_OUTPUTS)
+    counts = scene.last_sample_counts(nr)
+    hit = geo["near"] <= geo["far"]
+    assert (counts[:64][hit[:64]] == 0).all()
+    assert np.allclose(out["acc_r"][:64][hit[:64]], 1.0)  # white background
+
+
+def test_train_step_with_proposal(setup):
+    """A short run: full-march labels and training rounds, then guided batches; the loss
+    falls, no tensor-core wait runs out, and trained rounds are counted."""
+    import cpx
+
+    cfg, scene0, rays, geo, torch = setup
+    n = cfg["W"]
+    scene = cpx.ObjectScene(n, n, n, 9, precision="bf16", sr_seed=4)
+    scene.upload_params(cfg["params"])
+    nr = rays.total_rays
+    prop = cpx.Proposal(seed=3)
+    losses = torch.zeros(nr, dtype=torch.float64, device="cuda")
+    mses = []
+    for it in range(30):
+        mses.append(cpx.train_step_proposal(scene, rays, prop, losses, it, timestep=it + 1, warmup=10,
+                                            train_every=10, train_steps=8, rays_per_step=512, lam_density=1e-3,
+                                            lam_sh=1e-3, lr=0.1, sh_lr=0.01))
+    scene.check()
+    st = prop.stats()
+    assert st["error_flags"] == 0
+    assert st["rounds"] == 4  # iterations 0, 9 (end of warm-up), 10 and 20
+    assert mses[-1] < mses[0]
+    prop.close()
