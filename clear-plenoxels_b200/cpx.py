@@ -57,7 +57,8 @@ EXPORTED = [
     "cpx_render_image", "cpx_image_mse", "cpx_grid_touched_count",
     "cpx_proposal_param_count", "cpx_proposal_create", "cpx_proposal_destroy", "cpx_proposal_params",
     "cpx_proposal_infer", "cpx_proposal_gradient", "cpx_proposal_train", "cpx_proposal_stats",
-    "cpx_render_forward_backward_guided", "cpx_train_step_proposal",
+    "cpx_render_forward_backward_guided", "cpx_train_step_proposal", "cpx_render_forward_guided",
+    "cpx_grid_set_options",
 ]
 
 
@@ -182,6 +183,10 @@ _sig("cpx_proposal_train", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, C.c_int, 
 _sig("cpx_proposal_stats", [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int)])
 _sig("cpx_render_forward_backward_guided", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_double, C.c_float, _vp, _vp,
                                             _vp])
+_sig("cpx_render_forward_guided", [_vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
+_sig("cpx_grid_set_options", [_vp, C.c_int])
+OPT_NO_EMPTY_SKIP = 1  # the FP32 march steps through empty cells one step at a time
+OPT_FP32_MARCH = 2     # an FP32-storage grid marches like the mixed forms
 _sig("cpx_train_step_proposal", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), C.POINTER(ProposalSchedule),
                                  C.c_int, _vp, C.POINTER(C.c_double), _vp])
 
@@ -368,6 +373,10 @@ class ObjectScene:
         _check(_lib.cpx_occupancy_build(self._h, float(threshold), occ.ctypes.data, cage.ctypes.data,
                                         idx.ctypes.data, C.byref(cnt)), "cpx_occupancy_build")
         return occ, cage, idx, int(cnt.value)
+
+    def set_options(self, options: int):
+        """March options (OPT_NO_EMPTY_SKIP, OPT_FP32_MARCH)."""
+        _check(_lib.cpx_grid_set_options(self._h, int(options)), "cpx_grid_set_options")
 
     def touched_count(self) -> int:
         """Vertices whose gradient records the next optimizer sweep will read."""
@@ -644,6 +653,12 @@ class Proposal:
                "cpx_proposal_infer")
         return logits, masks
 
+    def masks_into(self, scene, rays, masks, start=0, length=None, sample_index=None, stream=None):
+        """Segment masks of a batch into a preallocated int32 CUDA tensor (no logits)."""
+        n = _len(rays, start, length)
+        _check(_lib.cpx_proposal_infer(self._h, scene.handle, rays.handle, _ptr(sample_index), int(start), n, None,
+                                       _ptr(masks), 1, _stream(stream)), "cpx_proposal_infer")
+
     def gradient(self, scene, rays, seg_weights, start=0, length=None, sample_index=None):
         n = _len(rays, start, length)
         g = np.empty(self.n_params, np.float32)
@@ -653,18 +668,19 @@ class Proposal:
         return g, loss.value
 
     def train(self, scene, rays, seg_weights, steps, rays_per_step=0, start=0, length=None, sample_index=None,
-              stream=None):
+              stream=None, want_loss=True):
+        """Adam steps on the labels of seg_weights; returns the mean loss (synchronises) or None."""
         n = _len(rays, start, length)
         loss = C.c_double()
         _check(_lib.cpx_proposal_train(self._h, scene.handle, rays.handle, _ptr(sample_index), int(start), n,
-                                       _ptr(seg_weights), int(steps), int(rays_per_step), C.byref(loss),
-                                       _stream(stream)), "cpx_proposal_train")
-        return loss.value
+                                       _ptr(seg_weights), int(steps), int(rays_per_step),
+                                       C.byref(loss) if want_loss else None, _stream(stream)), "cpx_proposal_train")
+        return loss.value if want_loss else None
 
     def stats(self):
         r, c, f = C.c_int(), C.c_int64(), C.c_int()
         _check(_lib.cpx_proposal_stats(self._h, C.byref(r), C.byref(c), C.byref(f)), "cpx_proposal_stats")
-        return {"rounds": r.value, "confident_rays": c.value, "error_flags": f.value}
+        return {"rounds": r.value, "skipped_segments": c.value, "error_flags": f.value}
 
 
 def render_guided(scene: ObjectScene, rays: Rays, losses, start=0, length=None, sample_index=None, mask_coef=1.0,
@@ -675,6 +691,14 @@ def render_guided(scene: ObjectScene, rays: Rays, losses, start=0, length=None, 
                                                    int(start), n, float(mask_coef), float(huber_delta),
                                                    _ptr(masks), _ptr(seg_weights), _stream(stream)),
            "cpx_render_forward_backward_guided")
+
+
+def render_forward_guided(scene: ObjectScene, rays: Rays, start=0, length=None, sample_index=None, masks=None,
+                          stream=None):
+    """Forward of the mixed forms' march (guided by segment masks when given)."""
+    n = _len(rays, start, length)
+    _check(_lib.cpx_render_forward_guided(scene.handle, rays.handle, _ptr(sample_index), int(start), n, _ptr(masks),
+                                          _stream(stream)), "cpx_render_forward_guided")
 
 
 def train_step_proposal(scene: ObjectScene, rays: Rays, proposal: Proposal, losses, iteration: int, *, start=0,

@@ -229,6 +229,7 @@ static void free_grid(cpx_grid* g)
     cudaFree(g->in_cage);
     cudaFree(g->index_offsets);
     cudaFree(g->compact_to_dense);
+    cudaFree(g->brick_bits);
     for (int i = 0; i < 3; i++) cudaFree(g->off[i]);
     cudaFree(g->scratch.samples);
     cudaFree(g->scratch.colours);
@@ -478,6 +479,13 @@ cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const doub
         if (e != cudaSuccess) return cuda_status(e, "sample offsets");
     }
     g->n_off = n;
+    return CPX_OK;
+}
+
+cpx_status cpx_grid_set_options(cpx_grid* g, int options)
+{
+    if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH))) return CPX_ERR_INVALID_ARGUMENT;
+    g->options = options;
     return CPX_OK;
 }
 
@@ -764,6 +772,14 @@ cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int sta
         if (e != cudaSuccess) return cuda_status(e, "mse");
     }
     return CPX_OK;
+}
+
+cpx_status cpx_render_forward_guided(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                                     const uint32_t* masks, cpx_stream stream)
+{
+    if (check_grid(g) || !r) return CPX_ERR_INVALID_ARGUMENT;
+    return march_launch_guided(g, r, sidx, start, len, nullptr, 0., 0.f, masks, nullptr, (cudaStream_t)stream,
+                               kForward);
 }
 
 cpx_status cpx_render_forward_backward_guided(cpx_grid* g, cpx_rays* r, double* losses, const int32_t* sidx,

@@ -130,6 +130,11 @@ struct cpx_grid {
     uint8_t* in_cage = nullptr;         // [n_dense]
     uint32_t* index_offsets = nullptr;  // [n_dense]
     uint32_t* compact_to_dense = nullptr;  // [n_act] when sparse
+    // bricks of 8x8x8 cells, one bit each (set when any cell of the brick is occupied): the
+    // FP32 march of the mixed forms crosses empty bricks in one jump
+    uint32_t* brick_bits = nullptr;
+    int bricks[3] = {0, 0, 0};
+    int options = 0;  // CPX_OPT_* march options
     // jitter
     double* off[3] = {nullptr, nullptr, nullptr};
     int n_off = 0;
@@ -216,6 +221,11 @@ inline RaysView rays_view(cpx_rays* r)
     return v;
 }
 
+enum MarchMode { kForward = 1, kBackward = 2, kForwardBackward = 3 };
+
+// Segments per ray of the learned proposal (proposal.cu).
+constexpr int kProposalSegments = 32;
+
 // Per-vertex state of the grid's storage form (api.cu).
 cudaError_t alloc_state(cpx_grid* g, int64_t n);
 void free_state(cpx_grid* g);
@@ -230,7 +240,7 @@ cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int 
 int march_samples_per_ray(const cpx_grid* g);
 cpx_status march_launch_guided(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                                double* losses, double mask_coef, float huber, const uint32_t* masks,
-                               float* seg_w, cudaStream_t st);
+                               float* seg_w, cudaStream_t st, int mode = kForwardBackward);
 // proposal.cu
 cpx_status proposal_masks(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                           cudaStream_t st, uint32_t** masks_out);
@@ -251,9 +261,6 @@ cpx_status rays_camera_launch(cpx_rays* r, const cpx_grid* g, const cpx_camera* 
                               int has_mask, cudaStream_t s);
 cpx_status mse_launch(const double* losses, int len, double* out, cudaStream_t s);
 
-enum MarchMode { kForward = 1, kBackward = 2, kForwardBackward = 3 };
 
-// Segments per ray of the learned proposal (proposal.cu).
-constexpr int kProposalSegments = 32;
 
 }  // namespace cpx

@@ -85,6 +85,48 @@ __device__ __forceinline__ void prefetch_cell(const GridView& g, unsigned b0, un
     for (int q = 0; q < 8; q += 2) asm volatile("prefetch.global.L1 [%0];" ::"l"(g.density + idx[q]));
 }
 
+// Brick occupancy of a sparse grid (8x8x8 cells per bit), read by the FP32 march.
+struct Skip {
+    const uint32_t* __restrict__ bits = nullptr;
+    int bx = 0, by = 0, bz = 0;
+};
+
+// FP32 march on a sparse grid, at an empty cell (b0, b1, b2) with position bc: the number of
+// steps that carry the sample position out of that cell -- or out of its whole 8x8x8 brick
+// when the brick is empty.  Every position the reference's step-by-step march would visit
+// before that point lies in the same empty cell or brick, so jumping by whole steps keeps
+// the reference's sample sequence: the samples after the jump sit where step-by-step
+// stepping would have put them.
+template <typename Real>
+__device__ __forceinline__ int empty_steps(const Skip& sk, const Real* bc, unsigned b0, unsigned b1, unsigned b2,
+                                           float dx, float dy, float dz, float step)
+{
+    int kx = (int)(b0 >> 3), ky = (int)(b1 >> 3), kz = (int)(b2 >> 3);
+    kx = kx < sk.bx ? kx : sk.bx - 1;
+    ky = ky < sk.by ? ky : sk.by - 1;
+    kz = kz < sk.bz ? kz : sk.bz - 1;
+    const unsigned k = ((unsigned)kz * sk.by + ky) * sk.bx + kx;
+    const bool brick_empty = !((__ldg(sk.bits + (k >> 5)) >> (k & 31u)) & 1u);
+    const unsigned base[3] = {b0, b1, b2};
+    const int kb[3] = {kx, ky, kz};
+    const float d[3] = {dx, dy, dz};
+    Real exit = (Real)3.0e38f;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const Real lo = brick_empty ? (Real)(8 * kb[a]) : (Real)base[a];
+        const Real hi = brick_empty ? (Real)(8 * kb[a] + 8) : (Real)(base[a] + 1u);
+        if (d[a] > 0.f) {
+            const Real e = (hi - bc[a]) / (Real)d[a];
+            exit = e < exit ? e : exit;
+        } else if (d[a] < 0.f) {
+            const Real e = (lo - bc[a]) / (Real)d[a];
+            exit = e < exit ? e : exit;
+        }
+    }
+    const Real n = ceil(exit / (Real)step);
+    return n < (Real)1 ? 1 : (n > (Real)1.0e6f ? 1000000 : (int)n);
+}
+
 // exp in the march's precision
 __device__ __forceinline__ double real_exp(double x) { return exp(x); }
 __device__ __forceinline__ float real_exp(float x) { return expf(x); }
@@ -102,7 +144,7 @@ template <typename Real, bool PROP>
 __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
                                           SampleRec* samples, int maxs, int* counts,
                                           double* acc_out, int* err, bool write_fwd,
-                                          uint32_t seg_mask, float* seg_w)
+                                          uint32_t seg_mask, float* seg_w, const Skip& sk)
 {
     // renderRaysGPU zeroes the outputs first (RenderUtils.cu:1927-1941); the backward alone
     // leaves the forward's outputs as they are
@@ -170,8 +212,16 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
         const unsigned b1 = (unsigned int)bc1;
         const unsigned b2 = (unsigned int)bc2;
         if (g.sparse && !cell_occupied(g, b0, b1, b2)) {  // RenderUtils.cu:1681-1686
-            t += step;
-            ++intT;
+            if (sizeof(Real) == sizeof(float) && sk.bits) {
+                // FP32 march: all the steps through the empty cell (or brick) at once
+                const Real bc[3] = {bc0, bc1, bc2};
+                const int k = empty_steps<Real>(sk, bc, b0, b1, b2, dx, dy, dz, step);
+                t += (Real)k * (Real)step;
+                intT += k;
+            } else {
+                t += step;
+                ++intT;
+            }
             continue;
         }
         if (b0 != cb0 || b1 != cb1 || b2 != cb2) {
@@ -630,7 +680,7 @@ template <int MODE, typename Real, bool PROP>
 __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int32_t* sidx, int start,
                                                int len, int64_t n_rays, SampleRec* samples, int maxs,
                                                int* counts, double* acc, int* err, const uint32_t* seg_masks,
-                                               float* seg_w)
+                                               float* seg_w, Skip sk)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= len) return;
@@ -642,7 +692,7 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
     }
     const uint32_t mask = PROP && seg_masks ? seg_masks[b] : 0xffffffffu;
     float* sw = PROP && seg_w ? seg_w + (size_t)b * kProposalSegments : nullptr;
-    place_ray<Real, PROP>(g, r, b, ri, samples, maxs, counts, acc, err, (MODE & kForward) != 0, mask, sw);
+    place_ray<Real, PROP>(g, r, b, ri, samples, maxs, counts, acc, err, (MODE & kForward) != 0, mask, sw, sk);
 }
 
 constexpr int kShadeWarps = 4;
@@ -756,6 +806,8 @@ static cpx_status ensure_scratch(cpx_grid* g, int len)
 struct Guide {
     const uint32_t* masks = nullptr;
     float* seg_w = nullptr;
+    Skip skip;
+    bool march32 = false;  // the FP32 march of the mixed forms (else the reference's sequence)
     bool on() const { return masks != nullptr || seg_w != nullptr; }
 };
 
@@ -764,16 +816,18 @@ static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv,
                         int start, int len, int64_t n_rays, const MarchScratch& s, double* losses,
                         double mask_coef, float huber, uint32_t* touched, const Guide& guide)
 {
-    using Real = typename std::conditional<PREC == kPrecFP32, double, float>::type;
     const dim3 pgrid((unsigned)((len + 31) / 32));
     const dim3 sgrid((unsigned)((len + kShadeWarps - 1) / kShadeWarps));
     const dim3 sblock(kShadeWarps * 32);
-    if (PREC != kPrecFP32 && guide.on())
-        k_place<MODE, Real, true><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
-                                                        s.counts, s.acc, s.err, guide.masks, guide.seg_w);
+    if (guide.march32 && guide.on())
+        k_place<MODE, float, true><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
+                                                         s.counts, s.acc, s.err, guide.masks, guide.seg_w, guide.skip);
+    else if (guide.march32)
+        k_place<MODE, float, false><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
+                                                          s.counts, s.acc, s.err, nullptr, nullptr, guide.skip);
     else
-        k_place<MODE, Real, false><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
-                                                         s.counts, s.acc, s.err, nullptr, nullptr);
+        k_place<MODE, double, false><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
+                                                           s.counts, s.acc, s.err, nullptr, nullptr, guide.skip);
     k_shade<NSH, MODE, PREC><<<sgrid, sblock, 0, st>>>(gv, rv, sidx, start, len, s.samples, s.colours, s.maxs,
                                                        s.counts, s.acc, losses, mask_coef, huber, touched);
 }
@@ -852,22 +906,31 @@ static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32
 {
     cpx_status rc = march_check_args(g, r, sidx, start, len, mode, losses);
     if (rc != CPX_OK || len == 0) return rc;
-    if (guide.on() && g->prec == kPrecFP32) {
-        set_error("the proposal-guided march runs on the mixed forms (FP32 march) only");
+    Guide gd = guide;
+    gd.march32 = g->prec != kPrecFP32 || (g->options & CPX_OPT_FP32_MARCH);
+    if (guide.on() && !gd.march32) {
+        set_error("the proposal-guided march runs on the FP32 march of the mixed forms only");
         return CPX_ERR_UNSUPPORTED;
+    }
+    // the FP32 march jumps over empty cells and bricks of a sparse grid
+    if (gd.march32 && !(g->options & CPX_OPT_NO_EMPTY_SKIP) && g->sparse && g->brick_bits) {
+        gd.skip.bits = g->brick_bits;
+        gd.skip.bx = g->bricks[0];
+        gd.skip.by = g->bricks[1];
+        gd.skip.bz = g->bricks[2];
     }
     const GridView gv = grid_view(g);
     const RaysView rv = rays_view(r);
     uint32_t* touched = g->touched[g->tcur];
     if (g->prec == kPrecFP32)
         rc = launch_prec<kPrecFP32>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
-                                    touched, guide);
+                                    touched, gd);
     else if (g->prec == kPrecBF16)
         rc = launch_prec<kPrecBF16>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
-                                    touched, guide);
+                                    touched, gd);
     else
         rc = launch_prec<kPrecFP16>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
-                                    touched, guide);
+                                    touched, gd);
     if (rc != CPX_OK) return rc;
     count_launch(2);
     return cuda_status(cudaGetLastError(), "march");
@@ -888,9 +951,9 @@ cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start
 
 cpx_status march_launch_guided(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                                double* losses, double mask_coef, float huber, const uint32_t* masks,
-                               float* seg_w, cudaStream_t st)
+                               float* seg_w, cudaStream_t st, int mode)
 {
-    cpx_status rc = march_check_args(g, r, sidx, start, len, kForwardBackward, losses);
+    cpx_status rc = march_check_args(g, r, sidx, start, len, mode, losses);
     if (rc != CPX_OK) return rc;
     g->last_len = len;
     if (len == 0) return CPX_OK;
@@ -903,8 +966,7 @@ cpx_status march_launch_guided(cpx_grid* g, cpx_rays* r, const int32_t* sidx, in
     Guide guide;
     guide.masks = masks;
     guide.seg_w = seg_w;
-    return march_launch_guided_with(g, r, sidx, start, len, kForwardBackward, losses, mask_coef, huber, g->scratch,
-                                    guide, st);
+    return march_launch_guided_with(g, r, sidx, start, len, mode, losses, mask_coef, huber, g->scratch, guide, st);
 }
 
 }  // namespace cpx

@@ -149,6 +149,30 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_write(const uint8_t* flag
     }
 }
 
+// Brick occupancy: bit k of the brick map is set when any cell of 8x8x8 brick k is occupied.
+// Thread per brick; a warp's 32 consecutive bricks form one word.
+constexpr int kBrick = 8;
+
+__global__ void k_bricks(const uint32_t* __restrict__ occ_bits, int cw, int ch, int cd, int bx, int by, int bz,
+                         uint32_t* brick_bits)
+{
+    const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nb = (int64_t)bx * by * bz;
+    bool any = false;
+    if (k < nb) {
+        const int x0 = (int)(k % bx) * kBrick, y0 = (int)((k / bx) % by) * kBrick;
+        const int z0 = (int)(k / ((int64_t)bx * by)) * kBrick;
+        for (int z = z0; z < min(z0 + kBrick, cd) && !any; z++)
+            for (int y = y0; y < min(y0 + kBrick, ch) && !any; y++)
+                for (int x = x0; x < min(x0 + kBrick, cw) && !any; x++) {
+                    const int64_t c = ((int64_t)z * ch + y) * cw + x;
+                    any = (occ_bits[c >> 5] >> (c & 31)) & 1u;
+                }
+    }
+    const unsigned word = __ballot_sync(0xffffffffu, any);
+    if ((threadIdx.x & 31) == 0 && k < nb) brick_bits[k >> 5] = word;
+}
+
 cpx_status occupancy_launch(cpx_grid* g, float threshold)
 {
     const int64_t N = g->n_dense;
@@ -190,6 +214,24 @@ cpx_status occupancy_launch(cpx_grid* g, float threshold)
                                                                threshold, g->occ_bytes,
                                                                g->occ_bits, g->in_cage, C,
                                                                dropped);
+    {
+        const int cw = g->W - 1, ch = g->H - 1, cd = g->D - 1;
+        const int bx = (cw + kBrick - 1) / kBrick, by = (ch + kBrick - 1) / kBrick, bz = (cd + kBrick - 1) / kBrick;
+        const int64_t nb = (int64_t)bx * by * bz;
+        if (!g->brick_bits && cudaMalloc((void**)&g->brick_bits, ((nb + 31) / 32) * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(tile_sums);
+            cudaFree(dropped);
+            set_error("brick map could not be allocated");
+            return CPX_ERR_OUT_OF_MEMORY;
+        }
+        g->bricks[0] = bx;
+        g->bricks[1] = by;
+        g->bricks[2] = bz;
+        // whole warps: the warp that writes the last word has no brick in its tail threads
+        k_bricks<<<(unsigned)((nb + 255) / 256), 256>>>(g->occ_bits, cw, ch, cd, bx, by, bz, g->brick_bits);
+        count_launch();
+    }
     k_scan_count<<<n_tiles, kScanThreads>>>(g->in_cage, N, tile_sums);
     k_scan_tiles<<<1, kScanThreads>>>(tile_sums, n_tiles, total);
     k_scan_write<<<n_tiles, kScanThreads>>>(g->in_cage, N, tile_sums, g->index_offsets);

@@ -4,9 +4,9 @@
 // -> 1, ReLU) predicts from the segment midpoint (position in box coordinates and its
 // 4-octave sin/cos encoding), the ray direction and the ray origin whether the segment holds
 // visible density (label: the samples of a full march inside the segment carry total weight
-// above a threshold -- empty and occluded segments are both 0).  A ray whose 32 predictions
-// are all confident (|logit| >= logit(confidence)) marches only the predicted segments; any
-// other ray runs the full march.
+// above a threshold -- empty and occluded segments are both 0).  The march skips the segments
+// predicted empty with confidence (sigmoid(logit) <= 1 - confidence) and marches every other
+// segment in full, so a ray whose predictions are all uncertain runs the plain full march.
 //
 // Inference runs on the 5th-generation tensor cores: a persistent CTA of 128 threads takes
 // tiles of 128 points (4 rays x 32 segments); each thread writes its point's features to
@@ -79,7 +79,7 @@ struct Args {
     uint32_t* seg_mask;  // [len] (or null)
     float* logits;       // [len][32] (or null)
     int* err;
-    unsigned long long* n_confident;
+    unsigned long long* n_skipped;  // segments predicted confidently empty
 };
 
 // ---------------------------------------------------------------------------
@@ -338,13 +338,13 @@ __global__ void __launch_bounds__(128, 1) k_infer_tc(Args a)
         }
         fence_before();
         __syncthreads();
-        const uint32_t mask = __ballot_sync(0xffffffffu, logit > 0.f);
-        const bool conf = __all_sync(0xffffffffu, fabsf(logit) >= a.conf_logit);
+        // march every segment that is not confidently empty
+        const uint32_t mask = __ballot_sync(0xffffffffu, !(logit <= -a.conf_logit));
         if (valid) {
             if (a.logits) a.logits[(size_t)b * kSeg + lane] = logit;
             if (lane == 0) {
-                if (a.seg_mask) a.seg_mask[b] = conf ? mask : 0xffffffffu;
-                if (conf && a.n_confident) atomicAdd(a.n_confident, 1ull);
+                if (a.seg_mask) a.seg_mask[b] = mask;
+                if (a.n_skipped) atomicAdd(a.n_skipped, (unsigned long long)(kSeg - __popc(mask)));
             }
         }
     }
@@ -401,11 +401,10 @@ __global__ void __launch_bounds__(128) k_infer_f32(Args a)
         float f[kIn], h1[kHid], h2[kHid], h3[kHid];
         features(a, ri, valid, lane, f);
         const float logit = forward_f32(sP, f, h1, h2, h3);
-        const uint32_t mask = __ballot_sync(0xffffffffu, logit > 0.f);
-        const bool conf = __all_sync(0xffffffffu, fabsf(logit) >= a.conf_logit);
+        const uint32_t mask = __ballot_sync(0xffffffffu, !(logit <= -a.conf_logit));
         if (valid) {
             if (a.logits) a.logits[(size_t)b * kSeg + lane] = logit;
-            if (lane == 0 && a.seg_mask) a.seg_mask[b] = conf ? mask : 0xffffffffu;
+            if (lane == 0 && a.seg_mask) a.seg_mask[b] = mask;
         }
     }
 }
@@ -586,7 +585,7 @@ struct cpx_proposal {
     uint16_t* wpack = nullptr;
     int* err = nullptr;
     double* loss = nullptr;
-    unsigned long long* n_confident = nullptr;
+    unsigned long long* n_skipped = nullptr;
     int adam_t = 0;
     int rounds = 0;  // completed training rounds
     uint32_t* seg_mask = nullptr;
@@ -647,7 +646,7 @@ static Args make_args(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int
     a.seg_mask = nullptr;
     a.logits = nullptr;
     a.err = p->err;
-    a.n_confident = p->n_confident;
+    a.n_skipped = p->n_skipped;
     return a;
 }
 
@@ -775,8 +774,8 @@ cpx_status cpx_proposal_create(const cpx_proposal_desc* d, cpx_proposal** out)
     if (e == cudaSuccess) e = cudaMalloc((void**)&p->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(p->err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc((void**)&p->loss, sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&p->n_confident, sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(p->n_confident, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&p->n_skipped, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(p->n_skipped, 0, sizeof(unsigned long long));
     if (e == cudaSuccess) {
         std::vector<float> P;
         init_params(d->seed, P);
@@ -805,7 +804,7 @@ cpx_status cpx_proposal_destroy(cpx_proposal* p)
     cudaFree(p->wpack);
     cudaFree(p->err);
     cudaFree(p->loss);
-    cudaFree(p->n_confident);
+    cudaFree(p->n_skipped);
     cudaFree(p->seg_mask);
     cudaFree(p->seg_w);
     delete p;
@@ -880,16 +879,16 @@ cpx_status cpx_proposal_train(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, c
     return cuda_status(e, "proposal training");
 }
 
-cpx_status cpx_proposal_stats(cpx_proposal* p, int* rounds, int64_t* confident_rays, int* error_flags)
+cpx_status cpx_proposal_stats(cpx_proposal* p, int* rounds, int64_t* skipped_segments, int* error_flags)
 {
     if (!p) return CPX_ERR_INVALID_ARGUMENT;
     cudaError_t e = cudaDeviceSynchronize();
     unsigned long long c = 0;
     int f = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&c, p->n_confident, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&c, p->n_skipped, sizeof(c), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(&f, p->err, sizeof(f), cudaMemcpyDeviceToHost);
     if (rounds) *rounds = p->rounds;
-    if (confident_rays) *confident_rays = (int64_t)c;
+    if (skipped_segments) *skipped_segments = (int64_t)c;
     if (error_flags) *error_flags = f;
     return cuda_status(e, "proposal stats");
 }

@@ -208,6 +208,15 @@ cpx_status cpx_render_image(cpx_grid* g, const cpx_camera* cam, int width, int h
  * summed in double on the device, for held-out PSNR; synchronises. */
 cpx_status cpx_image_mse(const float* a_dev, const float* b_dev, int64_t n, double* mse_out,
                          cpx_stream stream);
+/* March options (no reference counterpart; for studying the mixed forms):
+ * CPX_OPT_NO_EMPTY_SKIP  the FP32 march steps through every empty cell of a sparse grid as
+ *                        the reference does, instead of jumping over empty cells and bricks;
+ * CPX_OPT_FP32_MARCH     an FP32-storage grid marches like the mixed forms (FP32 arithmetic,
+ *                        empty-space jumps) instead of the reference's FP64/FP32 sequence. */
+#define CPX_OPT_NO_EMPTY_SKIP 1
+#define CPX_OPT_FP32_MARCH 2
+cpx_status cpx_grid_set_options(cpx_grid* g, int options);
+
 /* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,
  * type 2 both. */
 cpx_status cpx_tv_grad(cpx_grid* g, double lam_density, double lam_sh, int type,
@@ -264,12 +273,13 @@ int64_t cpx_kernel_launches(void);
  * density.  Input per segment: the midpoint in box coordinates with its 4-octave sin/cos
  * encoding, the ray direction and the ray origin.  Label: the samples of a full march inside
  * the segment carry total weight above label_weight (empty and occluded segments are 0).
- * A ray all of whose 32 predictions are confident marches only the predicted segments;
- * every other ray runs the full march. */
+ * The march skips the segments predicted empty with confidence (sigmoid(logit) <= 1 -
+ * confidence) and marches the others in full: a ray whose predictions are all uncertain
+ * runs the plain full march. */
 typedef struct cpx_proposal cpx_proposal;
 typedef struct cpx_proposal_desc {
     uint32_t seed;         /* parameter initialisation */
-    float confidence;      /* a segment is decided when sigmoid(logit) >= c or <= 1 - c (0.9) */
+    float confidence;      /* a segment is skipped when sigmoid(logit) <= 1 - confidence (0.9) */
     float label_weight;    /* segment label threshold on the summed sample weights (1e-3) */
     float learning_rate;   /* Adam (1e-3) */
 } cpx_proposal_desc;
@@ -294,9 +304,9 @@ cpx_status cpx_proposal_gradient(cpx_proposal* p, const cpx_grid* g, cpx_rays* r
 cpx_status cpx_proposal_train(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev,
                               int start, int len, const float* seg_weights_dev, int steps, int rays_per_step,
                               double* loss_out, cpx_stream stream);
-/* Completed training rounds, rays that marched under a confident proposal so far, and the
- * device error flags (4: a tensor-core wait ran out).  Synchronous. */
-cpx_status cpx_proposal_stats(cpx_proposal* p, int* rounds, int64_t* confident_rays, int* error_flags);
+/* Completed training rounds, segments predicted empty (and skipped) so far, and the device
+ * error flags (4: a tensor-core wait ran out).  Synchronous. */
+cpx_status cpx_proposal_stats(cpx_proposal* p, int* rounds, int64_t* skipped_segments, int* error_flags);
 /* The march of cpx_render_forward_backward with segment weights [len][32] recorded
  * (seg_weights_dev, the proposal's labels) when non-NULL, or guided by per-ray segment masks
  * [len] (masks_dev, from cpx_proposal_infer) when non-NULL.  The mixed-precision forms
@@ -306,6 +316,10 @@ cpx_status cpx_render_forward_backward_guided(cpx_grid* g, cpx_rays* r, double* 
                                               double mask_coef, float huber_delta,
                                               const uint32_t* masks_dev, float* seg_weights_dev,
                                               cpx_stream stream);
+/* The forward alone of cpx_render_forward_backward_guided (masks_dev may be NULL: the mixed
+ * forms' full march). */
+cpx_status cpx_render_forward_guided(cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev, int start, int len,
+                                     const uint32_t* masks_dev, cpx_stream stream);
 /* One training batch of the mixed form with the proposal: every train_every-th iteration
  * (and every iteration before warmup) runs the full march, records labels and then trains
  * the proposal (train_steps Adam steps of rays_per_step rays); the other iterations infer

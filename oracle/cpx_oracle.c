@@ -999,7 +999,33 @@ static int trilerp64(const orc_scene* s, const double bc[3], const double* shs, 
     return 1;
 }
 
-static void ray64(const orc_scene* s, const orc_rays* r, int tid, int ri, double mask_coef,
+/* FP32 march of the mixed forms on a sparse grid, at an empty cell: the whole steps that carry
+ * the position bc out of that cell, or out of its 8x8x8 brick when the brick is empty
+ * (bricks: one byte per brick). */
+static int empty_steps64(const orc_bricks* bk, const double bc[3], const double d[3], double step)
+{
+    uint32_t bi[3] = {sat_u32(bc[0]), sat_u32(bc[1]), sat_u32(bc[2])};
+    int kb[3];
+    const int bn[3] = {bk->bx, bk->by, bk->bz};
+    for (int a = 0; a < 3; a++) {
+        kb[a] = (int)(bi[a] >> 3);
+        if (kb[a] > bn[a] - 1) kb[a] = bn[a] - 1;
+    }
+    const int empty = !bk->bits[((int64_t)kb[2] * bk->by + kb[1]) * bk->bx + kb[0]];
+    double ex = 3.0e38;
+    for (int a = 0; a < 3; a++) {
+        const double lo = empty ? 8.0 * kb[a] : (double)bi[a];
+        const double hi = empty ? 8.0 * kb[a] + 8.0 : (double)bi[a] + 1.0;
+        double e = ex;
+        if (d[a] > 0.) e = (hi - bc[a]) / d[a];
+        else if (d[a] < 0.) e = (lo - bc[a]) / d[a];
+        if (e < ex) ex = e;
+    }
+    const double n = ceil(ex / step);
+    return n < 1. ? 1 : (n > 1e6 ? 1000000 : (int)n);
+}
+
+static void ray64(const orc_scene* s, const orc_rays* r, const orc_bricks* bk, int tid, int ri, double mask_coef,
                   double huber, double* pred, double* accw_out, double* losses, double* grad)
 {
     pred[3 * tid] = pred[3 * tid + 1] = pred[3 * tid + 2] = 0.;
@@ -1020,7 +1046,7 @@ static void ray64(const orc_scene* s, const orc_rays* r, int tid, int ri, double
         double bc[3];
         for (int a = 0; a < 3; a++) bc[a] = o[a] + t * d[a];
         if (!trilerp64(s, bc, shs, tri, wq, iq)) {
-            t += step;
+            t += bk ? empty_steps64(bk, bc, d, step) * step : step;
             continue;
         }
         const double sigma = softplus64(tri[0]);
@@ -1062,7 +1088,7 @@ static void ray64(const orc_scene* s, const orc_rays* r, int tid, int ri, double
         double bc[3];
         for (int a = 0; a < 3; a++) bc[a] = o[a] + t * d[a];
         if (!trilerp64(s, bc, shs, tri, wq, iq)) {
-            t += step;
+            t += bk ? empty_steps64(bk, bc, d, step) * step : step;
             continue;
         }
         const double sigma = softplus64(tri[0]);
@@ -1098,13 +1124,13 @@ static void ray64(const orc_scene* s, const orc_rays* r, int tid, int ri, double
     }
 }
 
-void orc64_forward_backward(const orc_scene* s, const orc_rays* r, int start, int len,
-                            double mask_coef, double huber, double* pred, double* accw,
+void orc64_forward_backward(const orc_scene* s, const orc_rays* r, const orc_bricks* bricks, int start,
+                            int len, double mask_coef, double huber, double* pred, double* accw,
                             double* losses, double* grad)
 {
 #pragma omp parallel for schedule(dynamic, 16) num_threads(orc_get_threads())
     for (int tid = 0; tid < len; tid++)
-        ray64(s, r, tid, tid + start, mask_coef, huber, pred, accw, losses, grad);
+        ray64(s, r, bricks, tid, tid + start, mask_coef, huber, pred, accw, losses, grad);
 }
 
 void orc64_tv6(const orc_scene* s, const double* params, double* grad, double lam_d, double lam_sh)

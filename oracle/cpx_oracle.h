@@ -145,8 +145,15 @@ void orc_composite_kat(const double* opacity, const double* colour /*[3][n]*/, i
  * every operation in double: the yardstick the FP32 and the mixed 16-bit forms are both
  * measured against.  pred [len][3] (background included), accw [len], losses [len],
  * grad planar [n_arrays][n_act] (accumulated into). */
-void orc64_forward_backward(const orc_scene* s, const orc_rays* r, int start, int len,
-                            double mask_coef, double huber, double* pred, double* accw,
+typedef struct orc_bricks {
+    const uint8_t* bits; /* one byte per 8x8x8-cell brick: any cell occupied */
+    int bx, by, bz;
+} orc_bricks;
+/* bricks non-NULL: the FP32 march of the mixed forms on a sparse grid, which moves through an
+ * empty cell (or through its whole brick when the brick is empty) in one jump of whole steps,
+ * leaving the sample sequence of step-by-step stepping unchanged. */
+void orc64_forward_backward(const orc_scene* s, const orc_rays* r, const orc_bricks* bricks, int start,
+                            int len, double mask_coef, double huber, double* pred, double* accw,
                             double* losses, double* grad);
 /* TV type 0 / 6 neighbours in double, added into grad (same gating as orc_tv_grad). */
 void orc64_tv6(const orc_scene* s, const double* params, double* grad, double lam_d,

@@ -71,8 +71,12 @@ _fn("orc_compact", [_vp, C.c_int, C.c_int64, _vp, _vp, C.c_int64])
 _fn("orc_mse", [_vp, C.c_int], C.c_double)
 _fn("orc_composite_kat", [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _fn("orc_render_image", [C.POINTER(_Scene)] + [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
-_fn("orc64_forward_backward", [C.POINTER(_Scene), C.POINTER(_Rays), C.c_int, C.c_int, C.c_double, C.c_double,
-                               _vp, _vp, _vp, _vp])
+class _Bricks(C.Structure):
+    _fields_ = [("bits", _vp), ("bx", C.c_int), ("by", C.c_int), ("bz", C.c_int)]
+
+
+_fn("orc64_forward_backward", [C.POINTER(_Scene), C.POINTER(_Rays), C.POINTER(_Bricks), C.c_int, C.c_int, C.c_double,
+                               C.c_double, _vp, _vp, _vp, _vp])
 _fn("orc64_tv6", [C.POINTER(_Scene), _vp, _vp, C.c_double, C.c_double])
 _fn("orc64_adam", [C.POINTER(_Scene), _vp, _vp, _vp, _vp, C.c_double, C.c_double, C.c_int])
 
@@ -100,6 +104,7 @@ class Scene:
                  occ=None, index_offsets=None, in_cage=None, adaptive_lr=None, offsets=None,
                  optimize_step=0):
         self.W, self.H, self.D, self.sh_dim = int(W), int(H), int(D), int(sh_dim)
+        self.sparse = bool(sparse)
         self.band = int(round(sh_dim ** 0.5)) - 1 if band is None else int(band)
         self.params = np.ascontiguousarray(params, np.float32).reshape(1 + 3 * self.sh_dim, -1).copy()
         self.n_act = self.params.shape[1]
@@ -190,11 +195,21 @@ def render_image(scene: Scene, cam, bbox, width, height, white_bg=True):
     return out
 
 
+def brick_map(occ, W, H, D):
+    """One byte per 8x8x8-cell brick: 1 when any of its cells is occupied."""
+    c = np.asarray(occ, np.uint8).reshape(D - 1, H - 1, W - 1)
+    bz, by, bx = (-(-(D - 1) // 8), -(-(H - 1) // 8), -(-(W - 1) // 8))
+    pad = np.zeros((bz * 8, by * 8, bx * 8), np.uint8)
+    pad[:D - 1, :H - 1, :W - 1] = c
+    b = pad.reshape(bz, 8, by, 8, bx, 8).max(axis=(1, 3, 5))
+    return np.ascontiguousarray(b.reshape(-1), np.uint8), (bx, by, bz)
+
+
 def fp64_step(scene: Scene, rays: RaySet, mask_coef, huber, lam_d=None, lam_sh=None, lr=None, sh_lr=None,
-              timestep=1, start=0, length=None):
-    """The FP64 host oracle of one training batch: forward+backward over rays[start:start+length],
-    then (when lr is given) TV type 0 / 6 neighbours (when lam_d is given) and Adam from zero
-    moments.  Returns pred [len, 3], accw, losses, grad [n_arrays, n_act] (before TV/Adam) and
+              timestep=1, start=0, length=None, skip_empty=False):
+    """The FP64 host oracle of one training batch: forward+backward over rays[start:start+length]
+    (skip_empty: the mixed forms' jumps over empty cells and bricks of a sparse grid), then (when
+    lr is given) TV type 0 / 6 neighbours (when lam_d is given) and Adam from zero moments.  Returns pred [len, 3], accw, losses, grad [n_arrays, n_act] (before TV/Adam) and
     the post-step parameters (float64) or None."""
     length = rays.n - start if length is None else length
     na = 1 + 3 * scene.sh_dim
@@ -202,8 +217,13 @@ def fp64_step(scene: Scene, rays: RaySet, mask_coef, huber, lam_d=None, lam_sh=N
     accw = np.zeros(length, np.float64)
     losses = np.zeros(length, np.float64)
     grad = np.zeros((na, scene.n_act), np.float64)
-    _lib.orc64_forward_backward(C.byref(scene.c), C.byref(rays.c), int(start), int(length), float(mask_coef),
-                                float(huber), _p(pred), _p(accw), _p(losses), _p(grad))
+    bk = None
+    if skip_empty and scene.sparse:
+        bits, (bx, by, bz) = brick_map(scene.occ, scene.W, scene.H, scene.D)
+        bk = _Bricks(bits.ctypes.data, bx, by, bz)
+    _lib.orc64_forward_backward(C.byref(scene.c), C.byref(rays.c), C.byref(bk) if bk is not None else None,
+                                int(start), int(length), float(mask_coef), float(huber), _p(pred), _p(accw),
+                                _p(losses), _p(grad))
     post = None
     if lr is not None:
         params = np.ascontiguousarray(scene.params, np.float64)

@@ -230,7 +230,8 @@ def test_sparse_mixed_form_against_fp64_oracle(cuda, case):
     osc = orc.Scene(n, n, n, 9, comp, step=case["step"], sparse=True, occ=occ, index_offsets=idx, in_cage=cage)
     _, orays = oracle(case, params)
     pred, accw, losses, grad = run_fb(scene, rays)
-    pred64, accw64, _, grad64, _ = orc.fp64_step(osc, orays, MASK_COEF, HUBER)
+    # the FP32 march jumps over empty cells and bricks of a sparse grid in whole steps
+    pred64, accw64, _, grad64, _ = orc.fp64_step(osc, orays, MASK_COEF, HUBER, skip_empty=True)
     assert np.abs(pred - pred64).max() < 1e-4
     assert normwise(grad[1:], grad64[1:]) < 2e-3
 

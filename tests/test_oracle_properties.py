@@ -175,3 +175,25 @@ def test_fp64_oracle_agrees_with_the_reference_restatement(small):
     # Adam from zero moments moves every updated parameter by about lr * sign(g) at t = 1
     moved = np.abs(post - scene.params)
     assert np.isfinite(post).all() and moved[0].max() <= 0.1 + 1e-9 and moved[1:].max() <= 0.01 + 1e-9
+
+
+def test_empty_space_jumps_keep_the_sample_sequence():
+    """The FP32 march's jumps over empty cells and bricks move by whole steps, so in the FP64
+    oracle a sparse march with jumps equals the step-by-step march up to rounding."""
+    cfg = S.small_config(seed=8, n=48, n_cams=4, img=40, n_rays=400)
+    n = cfg["W"]
+    occ, cage, idx, cnt, _ = orc.occupancy(cfg["params"][0], n, n, n, 4.0)
+    assert 0 < occ.mean() < 0.5
+    comp = orc.compact(cfg["params"], cage, cnt)
+    sc = orc.Scene(n, n, n, 9, comp, step=0.5, sparse=True, occ=occ, index_offsets=idx, in_cage=cage)
+    nr = sum(len(p) for p in cfg["pix"])
+    rays = orc.RaySet(nr, True)
+    off = 0
+    for cam, img, pix in zip(cfg["cams"], cfg["images"], cfg["pix"]):
+        orc.rays_from_camera(cam, cfg["bbox"], cfg["img_w"], *img, True, pix, rays, off)
+        off += len(pix)
+    a = orc.fp64_step(sc, rays, 1.0, 0.1)
+    b = orc.fp64_step(sc, rays, 1.0, 0.1, skip_empty=True)
+    assert np.abs(a[0] - b[0]).max() < 1e-9
+    assert np.abs(a[3] - b[3]).max() <= 1e-9 * np.abs(a[3]).max()
+    assert np.abs(a[0] - 1.0).max() > 0.05  # the rays see the blobs
