@@ -57,6 +57,10 @@ WORKLOADS = {
 }
 # the reference's shipped training constants (SparseVolumeRadianceField/config_linux.txt)
 STEP = dict(mask_coef=1.0, huber=0.1, lam_density=1e-5, lam_sh=1e-6, lr=0.3, sh_lr=1.0)
+# learned-proposal schedule: full-march labels for the first `warmup` batches, then a label
+# batch and a training round every `train_every` batches
+PROPOSAL = dict(warmup=100, train_every=50, train_steps=16, rays_per_step=1024)
+PROPOSAL_NET = dict(confidence=0.9, label_weight=1e-3, learning_rate=1e-3)
 SH_DIM = 9
 RAY_BYTES = 9 * 4  # packed ray record: 8 floats + rgba bytes
 
@@ -198,18 +202,15 @@ def profiled_traffic_per_vertex():
 
 
 # --------------------------------------------------------------------------- our arm
-def run_ours(args, wl, world, rank, local):
+def build_ground_truth(wl, dev, eyes, pix, P, keep_grid=False):
+    """Renders the pool pixels from the hidden grid with our plain forward.  Returns the
+    ground-truth bytes (r, g, b, mask), the hidden density field when the workload is sparse
+    (the training grid's occupancy source) and, with keep_grid, the hidden grid itself."""
     import torch
 
     import cpx
     import cpx_scenes as S
 
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    n, R, P = wl["n"], wl["batch"], wl["batch"] * wl["pool_batches"]
-    eyes, pix, order = camera_set(wl)
-
-    # ---- ground truth: render the pool pixels from the hidden grid with our forward
     gt_n = wl["gt_n"]
     thr = wl.get("sparse_threshold")
     gt_scene = cpx.ObjectScene(gt_n, gt_n, gt_n, SH_DIM)
@@ -218,7 +219,7 @@ def run_ours(args, wl, world, rank, local):
     if thr is not None:
         gt_scene.prune_self(thr, download=False)
         gt_scene.make_sparse()
-    field = gp[0].clone() if thr is not None else None  # the training grid's occupancy source
+    field = gp[0].clone() if thr is not None else None
     del gp
     torch.cuda.empty_cache()
     blank = [(np.zeros(wl["img"] ** 2, np.uint8),) * 3 + (None,) for _ in range(wl["cams"])]
@@ -230,20 +231,30 @@ def run_ours(args, wl, world, rank, local):
         cpx.RenderUtils.renderRays(gt_rays, gt_scene, startSampleIndex=s, len=min(chunk, P - s))
     gt_scene.check()
     go = gt_rays.download(fields=("acc_r", "acc_g", "acc_b", "acc_weights"))
-    gr, gg, gb, gm = to_gt_bytes(go["acc_r"], go["acc_g"], go["acc_b"], go["acc_weights"])
-    gt_scene.close()
+    gt = to_gt_bytes(go["acc_r"], go["acc_g"], go["acc_b"], go["acc_weights"])
     gt_rays.close()
+    if not keep_grid:
+        gt_scene.close()
+        gt_scene = None
     torch.cuda.empty_cache()
+    return gt, field, gt_scene
 
-    # ---- training grid and the ray pool in its voxel space
-    scene = cpx.ObjectScene(n, n, n, SH_DIM, precision=args.precision, sr_seed=wl["seed"] + 1)
+
+def build_training_grid(wl, dev, precision, field):
+    """The training grid: dense, or sparse with the hidden field's occupancy; density
+    init_density and SH 0 on every active vertex."""
+    import torch
+
+    import cpx
+
+    n = wl["n"]
+    thr = wl.get("sparse_threshold")
+    scene = cpx.ObjectScene(n, n, n, SH_DIM, precision=precision, sr_seed=wl["seed"] + 1)
     if thr is not None:
-        # occupancy from the hidden field, then density init_density and SH 0 on the in-cage
-        # vertices of the compact grid
         init = torch.zeros((1 + 3 * SH_DIM, n ** 3), dtype=torch.float32, device=dev)
         init[0] = field
         scene.upload_params_device(init)
-        del init, field
+        del init
         torch.cuda.empty_cache()
         scene.prune_self(thr, download=False)
         scene.make_sparse()
@@ -253,13 +264,43 @@ def run_ours(args, wl, world, rank, local):
     scene.upload_params_device(init)
     del init
     torch.cuda.empty_cache()
+    return scene
+
+
+def build_pool(scene, wl, eyes, pix, order, gt, P):
+    """The ray pool in the training grid's voxel space, in batch order, ground truth attached;
+    returns (pool, packed host records)."""
+    import cpx
+    import cpx_scenes as S
+
+    n = wl["n"]
+    blank = [(np.zeros(wl["img"] ** 2, np.uint8),) * 3 + (None,) for _ in range(wl["cams"])]
     pool = cpx.Rays(P, white_bg=True)
     pool.initial_self(scene, [cpx.Camera.make(**S.look_at_camera(e, n, wl["img"], wl["img"])) for e in eyes],
                       blank, pix, wl["img"], wl["img"])
     geo = pool.download(fields=("ox", "oy", "oz", "dx", "dy", "dz", "near", "far"))
+    gr, gg, gb, gm = gt
     packed = S.pack_rays(*[geo[k][order] for k in ("ox", "oy", "oz", "dx", "dy", "dz", "near", "far")],
                          gr[order], gg[order], gb[order], gm[order])
-    pool.upload_packed(packed)  # pool in batch order, ground truth attached
+    pool.upload_packed(packed)
+    return pool, packed
+
+
+def run_ours(args, wl, world, rank, local):
+    import torch
+
+    import cpx
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n, R, P = wl["n"], wl["batch"], wl["batch"] * wl["pool_batches"]
+    eyes, pix, order = camera_set(wl)
+    thr = wl.get("sparse_threshold")
+    gt, field, _ = build_ground_truth(wl, dev, eyes, pix, P)
+    scene = build_training_grid(wl, dev, args.precision, field)
+    del field
+    n_act = scene.actual_grid_nums
+    pool, packed = build_pool(scene, wl, eyes, pix, order, gt, P)
     host_pool = torch.from_numpy(packed).pin_memory()
     batch_rays = cpx.Rays(R, white_bg=True)
     losses = torch.zeros(R, dtype=torch.float64, device=dev)
@@ -268,10 +309,32 @@ def run_ours(args, wl, world, rank, local):
     lr = [STEP["lr"], STEP["sh_lr"]]
     K, W = args.steps, args.warmup
 
+    prop = None
+    if args.form == "proposal":
+        # the proposal is trained during the untimed warm-up and keeps its label batches and
+        # training rounds (every train_every batches) inside the timed region
+        prop = cpx.Proposal(seed=wl["seed"] + 11, **proposal_net(args))
+        W = max(W, PROPOSAL["warmup"] + 10)
+        seg_w = torch.zeros((R, cpx.Proposal.SEGMENTS), dtype=torch.float32, device=dev)
+        masks = torch.zeros(R, dtype=torch.int32, device=dev)
+
     def step(k, ev=None):
         b = k % wl["pool_batches"]
-        cpx.RenderUtils.renderRays_forwardBackward(scene, pool, losses, None, b * R, R, STEP["mask_coef"],
-                                                   STEP["huber"], stream=stream)
+        if prop is not None:
+            # the schedule of cpx_train_step_proposal, with the march and the sweep timed apart
+            if k < PROPOSAL["warmup"] or k % PROPOSAL["train_every"] == 0:
+                cpx.render_guided(scene, pool, losses, b * R, R, mask_coef=STEP["mask_coef"],
+                                  huber_delta=STEP["huber"], seg_weights=seg_w, stream=stream)
+                if k % PROPOSAL["train_every"] == 0 or k + 1 == PROPOSAL["warmup"]:
+                    prop.train(scene, pool, seg_w, PROPOSAL["train_steps"], PROPOSAL["rays_per_step"], start=b * R,
+                               length=R, stream=stream, want_loss=False)
+            else:
+                prop.masks_into(scene, pool, masks, start=b * R, length=R, stream=stream)
+                cpx.render_guided(scene, pool, losses, b * R, R, mask_coef=STEP["mask_coef"],
+                                  huber_delta=STEP["huber"], masks=masks, stream=stream)
+        else:
+            cpx.RenderUtils.renderRays_forwardBackward(scene, pool, losses, None, b * R, R, STEP["mask_coef"],
+                                                       STEP["huber"], stream=stream)
         if ev is not None:
             ev[1].record(stream)
         cpx.Optimizer.varianceAndUpdate(scene, STEP["lam_density"], STEP["lam_sh"], lr[0], lr[1], k + 1,
@@ -328,10 +391,18 @@ def run_ours(args, wl, world, rank, local):
     for k in range(K):
         b = k % wl["pool_batches"]
         batch_rays.upload_packed(host_pool[b * R:(b + 1) * R], stream=stream)
-        mses.append(cpx.train_step(scene, batch_rays, losses, start=0, length=R, mask_coef=STEP["mask_coef"],
-                                   huber_delta=STEP["huber"], lam_density=STEP["lam_density"],
-                                   lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1], timestep=W + K + 4 + k + 1,
-                                   want_mse=True, stream=stream))
+        it = W + K + 4 + k
+        if prop is not None:
+            mses.append(cpx.train_step_proposal(scene, batch_rays, prop, losses, it, start=0, length=R,
+                                                mask_coef=STEP["mask_coef"], huber_delta=STEP["huber"],
+                                                lam_density=STEP["lam_density"], lam_sh=STEP["lam_sh"], lr=lr[0],
+                                                sh_lr=lr[1], timestep=it + 1, want_mse=True, stream=stream,
+                                                **PROPOSAL))
+        else:
+            mses.append(cpx.train_step(scene, batch_rays, losses, start=0, length=R, mask_coef=STEP["mask_coef"],
+                                       huber_delta=STEP["huber"], lam_density=STEP["lam_density"],
+                                       lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1], timestep=it + 1,
+                                       want_mse=True, stream=stream))
     e1.record(stream)
     torch.cuda.synchronize()
     scene.check()
@@ -372,24 +443,176 @@ def run_ours(args, wl, world, rank, local):
         "data": "synthetic: seeded %d-blob %d^3 hidden grid rendered by the plain forward; no dataset"
                 % (wl["n_blobs"], wl["gt_n"]),
         "config": {
-            "workload": ("%s training: %d^3 %s grid SH band 2 (density 0.1, SH 0 init), %d-ray batches from %d "
+            "workload": ("%s%s training: %d^3 %s grid SH band 2 (density 0.1, SH 0 init), %d-ray batches from %d "
                          "%dx%d views of a hidden %d^3 %d-blob grid, TV type 0/6 + Adam every batch"
-                         % ("plain FP32" if args.precision == "fp32" else "mixed %s" % args.precision, n,
+                         % ("plain FP32" if args.precision == "fp32" else "mixed %s" % args.precision,
+                            " + learned proposal" if prop is not None else "", n,
                             "dense" if thr is None else "sparse (blob field > %.1f, %d active vertices)" % (thr, N),
                             R, wl["cams"], wl["img"], wl["img"], wl["gt_n"], wl["n_blobs"])),
             "grid": n, "sh_dim": SH_DIM, "batch_rays": R, "pool_rays": P, "step_constants": STEP,
-            "precision": args.precision,
+            "precision": args.precision, "form": args.form,
+            "proposal_schedule": PROPOSAL if prop is not None else None,
             "l2": "inputs larger than L2: the sweep streams %.1f GB of grid state per step" % (alg_bytes / 1e9),
             "parallelism": "replicas" if world > 1 else "single GPU",
         },
         "roofline": roofline,
-        "kernels_ms": {"march_fwd_bwd": round(march_ms, 4), "tv_adam_sweep": round(sweep_ms, 4)},
+        "kernels_ms": {"march_fwd_bwd" if prop is None else "proposal_and_march": round(march_ms, 4),
+                       "tv_adam_sweep": round(sweep_ms, 4)},
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": R * RAY_BYTES,
                 "d2h_bytes_per_step": 8, "last_mse": mses[-1]},
         "gpu_launches": int(launches),
+        "proposal": None if prop is None else prop.stats(),
         "clocks": clk,
     }
     return result, (scene, pool, R, wl)
+
+
+def proposal_net(args):
+    return dict(confidence=args.proposal_confidence, label_weight=args.proposal_label_weight,
+                learning_rate=PROPOSAL_NET["learning_rate"])
+
+
+def form_key(prec, form, run, args):
+    key = "%s/%s" % (prec, form)
+    if run == 1:
+        key += " (repeat)"
+    if run == 2 and args.march_options:
+        key += " options=%d" % args.march_options
+    return key
+
+
+def render_view_march(scene, cam, img, prec, prop):
+    """One view through the training march: every pixel a ray of the training grid's voxel
+    space; the FP32 form's reference march, or the mixed forms' march (guided by the proposal's
+    masks when given).  Returns the white-background colour [3, img*img] on the device."""
+    import torch
+
+    import cpx
+
+    n = img * img
+    rays = cpx.Rays(n, white_bg=True)
+    blank = [(np.zeros(n, np.uint8),) * 3 + (None,)]
+    rays.initial_self(scene, [cam], blank, [np.arange(n, dtype=np.int32)], img, img)
+    chunk = 65536
+    masks = torch.empty(chunk, dtype=torch.int32, device="cuda") if prop is not None else None
+    for s0 in range(0, n, chunk):
+        ln = min(chunk, n - s0)
+        if scene.precision == "fp32" and prop is None:
+            cpx.RenderUtils.renderRays(rays, scene, None, s0, ln)
+        else:
+            if prop is not None:
+                prop.masks_into(scene, rays, masks, start=s0, length=ln)
+            cpx.render_forward_guided(scene, rays, start=s0, length=ln, masks=masks[:ln] if prop is not None else None)
+    scene.check()
+    out = rays.download(fields=("acc_r", "acc_g", "acc_b", "near", "far"))
+    rays.close()
+    rgb = np.stack([out["acc_r"], out["acc_g"], out["acc_b"]])
+    # a ray that misses the box gets no background in the march (the reference's behaviour); the
+    # view shows white there, as the image path renders it
+    rgb[:, out["near"] > out["far"]] = 1.0
+    return torch.from_numpy(rgb).cuda()
+
+
+def quality_run(args, wl, local):
+    """Trains args.quality batches in the plain FP32 form and in the --precision/--form form
+    from the same initial grid and ray pool (with the reference's per-batch learning-rate decay),
+    renders held-out views of each (through the image path -- the reference's renderer, full
+    march -- and through the form's own training march) and of the hidden grid, and reports
+    the PSNR of each against the hidden grid's views and their difference."""
+    import torch
+
+    import cpx
+    import cpx_scenes as S
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    N, R = args.quality, wl["batch"]
+    wlq = dict(wl, pool_batches=min(N, 256))  # distinct batches of the run's ray pool
+    P = R * wlq["pool_batches"]
+    eyes, pix, order = camera_set(wlq)
+    gt, field, gt_scene = build_ground_truth(wlq, dev, eyes, pix, P, keep_grid=True)
+    img = wl["img"]
+    held = S.upper_hemisphere(8, 4.0, np.random.default_rng(wl["seed"] + 99))  # not among the training views
+    refs = [cpx.RenderUtils.renderImage(gt_scene, cpx.Camera.make(**S.look_at_camera(e, wl["gt_n"], img, img)), img,
+                                        img, outputs=("rgb",))["rgb"].clone() for e in held]
+    gt_scene.close()
+    torch.cuda.empty_cache()
+    forms = {}
+    net = proposal_net(args)
+    # the plain FP32 form twice: two runs differ only through the float atomics of the scatter,
+    # which sets the noise floor of the comparison
+    runs = [(0, "fp32", "plain"), (1, "fp32", "plain"), (2, args.precision, args.form)]
+    if args.no_repeat:
+        runs.pop(1)
+    for run, prec, form in runs:
+        lr = [STEP["lr"], STEP["sh_lr"]]
+        scene = build_training_grid(wl, dev, prec, field)
+        if run == 2 and args.march_options:
+            scene.set_options(args.march_options)
+        pool, _ = build_pool(scene, wlq, eyes, pix, order, gt, P)
+        losses = torch.zeros(R, dtype=torch.float64, device=dev)
+        prop = cpx.Proposal(seed=wl["seed"] + 11, **net) if form == "proposal" else None
+        batches = wlq["pool_batches"]
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for k in range(N):
+            b = k % batches
+            common = dict(start=b * R, length=R, mask_coef=STEP["mask_coef"], huber_delta=STEP["huber"],
+                          lam_density=STEP["lam_density"], lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1],
+                          timestep=k + 1, want_mse=False)
+            if prop is not None:
+                cpx.train_step_proposal(scene, pool, prop, losses, k, **common, **PROPOSAL)
+            else:
+                cpx.train_step(scene, pool, losses, **common)
+            # the reference's per-batch learning-rate decay (Render.cu:499-500)
+            lr = [cpx.lr_decay(x, batches, k // batches) for x in lr]
+        t1.record()
+        torch.cuda.synchronize()
+        scene.check()
+        ms = t0.elapsed_time(t1)
+        psnr, psnr_march, psnr_full, maxdiff = [], [], [], []
+        for e, ref in zip(held, refs):
+            cam = cpx.Camera.make(**S.look_at_camera(e, wl["n"], img, img))
+            im = cpx.RenderUtils.renderImage(scene, cam, img, img, outputs=("rgb",))["rgb"]
+            psnr.append(round(cpx.image_psnr(im, ref), 4))
+            own = render_view_march(scene, cam, img, prec, prop)
+            psnr_march.append(round(cpx.image_psnr(own, ref), 4))
+            if prop is not None:
+                full = render_view_march(scene, cam, img, prec, None)
+                psnr_full.append(round(cpx.image_psnr(full, ref), 4))
+                maxdiff.append(round(float((own - full).abs().max()), 5))
+        forms[form_key(prec, form, run, args)] = {
+            "march_options": args.march_options if run == 2 else 0,
+            "psnr_db": round(float(np.mean(psnr)), 4), "psnr_per_view": psnr,
+            "psnr_own_march_db": round(float(np.mean(psnr_march)), 4),
+            "psnr_full_march_db": round(float(np.mean(psnr_full)), 4) if psnr_full else None,
+            "max_pixel_diff_guided_vs_full": max(maxdiff) if maxdiff else None,
+            "train_ms": round(ms, 1), "train_rays_per_s": round(N * R / (ms / 1e3), 1),
+            "proposal": None if prop is None else prop.stats(),
+        }
+        if prop is not None:
+            prop.close()
+        pool.close()
+        scene.close()
+        torch.cuda.empty_cache()
+    base, rep = forms["fp32/plain"], forms.get("fp32/plain (repeat)")
+    other = forms[form_key(args.precision, args.form, 2, args)]
+    return {
+        "metric": "held-out view PSNR, plain FP32 minus %s/%s after %d batches" % (args.precision, args.form, N),
+        "value": round(base["psnr_db"] - other["psnr_db"], 4), "unit": "dB", "higher_is_better": False,
+        "delta_own_march_db": round(base["psnr_own_march_db"] - other["psnr_own_march_db"], 4),
+        "run_to_run_fp32_db": None if rep is None else round(base["psnr_db"] - rep["psnr_db"], 4),
+        "speedup_of_training": round(other["train_rays_per_s"] / base["train_rays_per_s"], 3),
+        "proposal_net": net if args.form == "proposal" else None,
+        "forms": forms, "held_out_views": len(held), "image": [img, img],
+        "config": {"workload": args.workload, "batch_rays": R, "pool_rays": P, "iterations": N,
+                   "step_constants": STEP, "lr_decay": "reference per batch (Render.cu:499-500)",
+                   "proposal_schedule": PROPOSAL if args.form == "proposal" else None},
+        "data": "synthetic: seeded %d-blob %d^3 hidden grid; held-out views on the upper hemisphere (another seed)"
+                % (wl["n_blobs"], wl["gt_n"]),
+    }
 
 
 def cpu_baseline(wl, scene, pool, R, args):
@@ -528,9 +751,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=("fp32", "bf16", "fp16"), default="fp32",
                     help="storage form of the training grid (fp32: the reference's)")
+    ap.add_argument("--form", choices=("plain", "proposal"), default="plain",
+                    help="proposal: the mixed form with the learned sample-interval proposal")
+    ap.add_argument("--proposal-confidence", type=float, default=PROPOSAL_NET["confidence"])
+    ap.add_argument("--proposal-label-weight", type=float, default=PROPOSAL_NET["label_weight"])
+    ap.add_argument("--quality", type=int, default=0, metavar="N",
+                    help="instead of timing, train N batches in the plain FP32 form and in the --precision/--form "
+                         "form and compare PSNR on held-out views")
+    ap.add_argument("--no-repeat", action="store_true", help="quality run: skip the second plain FP32 run")
+    ap.add_argument("--march-options", type=int, default=0,
+                    help="cpx_grid_set_options flags of the compared form's grid (quality run)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
+    if args.form == "proposal" and args.precision == "fp32":
+        ap.error("the proposal form runs on a mixed precision (--precision bf16 or fp16)")
     wl = WORKLOADS[args.workload]
     world, rank, local = dist_setup(use_cuda=True)
     if args.impl == "reference":
@@ -540,6 +775,10 @@ def main():
             import torch.distributed as dist
 
             dist.destroy_process_group()
+        return
+    if args.quality > 0:
+        if rank == 0:
+            print(json.dumps(quality_run(args, wl, local)), flush=True)
         return
     result, state = run_ours(args, wl, world, rank, local)
     if rank == 0:
