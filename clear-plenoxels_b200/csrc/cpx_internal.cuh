@@ -159,6 +159,51 @@ void set_error(const char* fmt, ...);
 cpx_status cuda_status(cudaError_t e, const char* where);
 void count_launch(int n = 1);
 
+// Sparse TV neighbourhood of compact vertex v (RenderUtils.cu:2663-2763): its six neighbours'
+// compact indices in the reference's order z-1, y-1, x-1, x+1, y+1, z+1, a bit per neighbour
+// whose compact index is 0 (it reads as the vertex itself), and whether v gets the term at all.
+// The reference gates sparse TV with inCageInfo[indexOffsets[v]] -- the dense flag array read
+// at the compact index (RenderUtils.cu:2669) -- so vertex c gets its term only when dense
+// vertex #c is in cage.
+struct SparseTv {
+    uint32_t nb[6];
+    uint32_t flags;  // bits 0..5: neighbour k reads the vertex itself; bit 6: the term applies
+};
+
+__device__ __forceinline__ SparseTv sparse_tv(uint32_t v, const uint32_t* __restrict__ c2d,
+                                              const uint8_t* __restrict__ in_cage,
+                                              const uint32_t* __restrict__ index_offsets, int W, int H, int D)
+{
+    SparseTv t;
+    t.flags = 0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) t.nb[k] = 0;
+    const uint32_t WH = (uint32_t)W * H;
+    const uint32_t dv = c2d[v];
+    const uint32_t x = dv % W, y = (dv / W) % H, z = dv / WH;
+    const bool on = x >= 1 && x + 2 <= (uint32_t)W && y >= 1 && y + 2 <= (uint32_t)H && z >= 1 &&
+                    z + 2 <= (uint32_t)D && in_cage[v] != 0;
+    if (!on) return t;
+    const uint32_t nbd[6] = {dv - WH, dv - W, dv - 1, dv + 1, dv + W, dv + WH};
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        t.nb[k] = index_offsets[nbd[k]];
+        if (t.nb[k] == 0) t.flags |= 1u << k;
+    }
+    t.flags |= 1u << 6;
+    return t;
+}
+
+// The SparseTv of vertex `from_lane`'s slot in a warp (every lane must call).
+__device__ __forceinline__ SparseTv shfl_tv(const SparseTv& mine, int from_lane)
+{
+    SparseTv t;
+#pragma unroll
+    for (int k = 0; k < 6; k++) t.nb[k] = __shfl_sync(0xffffffffu, mine.nb[k], from_lane);
+    t.flags = __shfl_sync(0xffffffffu, mine.flags, from_lane);
+    return t;
+}
+
 // Touched-map bit of vertex v (a null map means every vertex).
 __device__ __forceinline__ bool touched_bit(const uint32_t* __restrict__ map, uint32_t v)
 {

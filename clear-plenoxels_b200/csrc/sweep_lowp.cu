@@ -168,38 +168,32 @@ __global__ void __launch_bounds__(256) k_sweep_lowp_dense(LowpArgs a)
 template <int PREC, int S, bool TV>
 __global__ void __launch_bounds__(256) k_sweep_lowp_sparse(LowpArgs a)
 {
+    // A warp takes 32 consecutive compact vertices; each lane works out one vertex's TV
+    // neighbourhood and the warp's 32 * S quads take it by shuffle (as the FP32 sparse sweep).
     __shared__ float s_bc[2];
     lowp_bias_corrections(a.timestep, s_bc);
-    const uint32_t WH = (uint32_t)a.W * a.H;
-    const uint32_t total = a.n_act * S;
-    const uint32_t begin = blockIdx.x * blockDim.x * 8u;
-    const uint32_t end = min(begin + blockDim.x * 8u, total);
-    for (uint32_t li = begin + threadIdx.x; li < end; li += blockDim.x) {
-        const uint32_t v = li / S;
-        const int j = (int)(li - v * S);
-        bool tv_on = false;
-        uint32_t nb_v[6] = {0, 0, 0, 0, 0, 0};
-        bool nb_self[6] = {false, false, false, false, false, false};
-        if (TV) {
-            const uint32_t dv = a.compact_to_dense[v];
-            const uint32_t x = dv % a.W;
-            const uint32_t yy = (dv / a.W) % a.H;
-            const uint32_t zz = dv / WH;
-            // gated like the reference's sparse TV: inCageInfo read at the compact index
-            // (RenderUtils.cu:2669)
-            tv_on = x >= 1 && x + 2 <= (uint32_t)a.W && yy >= 1 && yy + 2 <= (uint32_t)a.H && zz >= 1 &&
-                    zz + 2 <= (uint32_t)a.D && a.in_cage[v] != 0;
-            if (tv_on) {
-                const uint32_t nbd[6] = {dv - WH, dv - a.W, dv - 1, dv + 1, dv + a.W, dv + WH};
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t v0 = warp * 32u;
+    if (v0 >= a.n_act) return;  // warp-uniform
+    SparseTv mine;
+    mine.flags = 0;
 #pragma unroll
-                for (int k = 0; k < 6; k++) {
-                    const uint32_t ci = a.index_offsets[nbd[k]];
-                    nb_self[k] = ci == 0;  // compact index 0 reads as the vertex itself
-                    nb_v[k] = ci;
-                }
-            }
-        }
-        lowp_quad<PREC, S, TV>(a, v, j, tv_on, nb_v, nb_self, s_bc[0], s_bc[1], a.lr);
+    for (int k = 0; k < 6; k++) mine.nb[k] = 0;
+    if (TV && v0 + lane < a.n_act)
+        mine = sparse_tv(v0 + lane, a.compact_to_dense, a.in_cage, a.index_offsets, a.W, a.H, a.D);
+#pragma unroll
+    for (int it = 0; it < S; it++) {
+        const uint32_t i = it * 32u + lane;
+        const uint32_t vl = i / S;
+        const int j = (int)(i - vl * S);
+        const SparseTv t = TV ? shfl_tv(mine, (int)vl) : mine;
+        const uint32_t v = v0 + vl;
+        if (v >= a.n_act) continue;
+        bool nb_self[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) nb_self[k] = (t.flags >> k) & 1u;
+        lowp_quad<PREC, S, TV>(a, v, j, (t.flags >> 6) & 1u, t.nb, nb_self, s_bc[0], s_bc[1], a.lr);
     }
 }
 
@@ -213,7 +207,7 @@ static void launch_lowp(const cpx_grid* g, const LowpArgs& a, bool tv, cudaStrea
         else
             k_sweep_lowp_dense<PREC, S, false><<<rows, 256, 0, st>>>(a);
     } else {
-        const unsigned blocks = (unsigned)(((int64_t)g->n_act * S + 2047) / 2048);
+        const unsigned blocks = (unsigned)(((int64_t)g->n_act + 255) / 256);  // a warp per 32 vertices
         if (tv)
             k_sweep_lowp_sparse<PREC, S, true><<<blocks, 256, 0, st>>>(a);
         else
