@@ -123,8 +123,16 @@ static void set_column(cpx_grid* g, Field f, const float* col, int64_t n, int a)
     } else if (g->prec == kPrecFP32) {
         float* dst = f == kParams ? g->params[g->cur] : (f == kMoment1 ? g->m : g->v);
         k_set_column<<<nb, 256>>>(dst, col, n, g->rec, a, (f == kParams && a == 0) ? g->density : nullptr);
+        if (f == kParams && a == 0) {
+            count_launch();
+            refresh_dense_mirror(g, 0);
+            return;
+        }
     } else if (f == kParams && a == 0) {
         k_set_column<<<nb, 256>>>(g->dens[g->cur], col, n, 1, 0, nullptr);
+        count_launch();
+        refresh_dense_mirror(g, 0);
+        return;
     } else if (f == kParams && g->prec == kPrecFP16) {
         k_set_column16<kPrecFP16><<<nb, 256>>>(g->sh16[g->cur], col, n, g->slots, a);
     } else {
@@ -230,6 +238,7 @@ static void free_grid(cpx_grid* g)
     cudaFree(g->index_offsets);
     cudaFree(g->compact_to_dense);
     cudaFree(g->brick_bits);
+    cudaFree(g->dense_mirror);
     for (int i = 0; i < 3; i++) cudaFree(g->off[i]);
     cudaFree(g->scratch.samples);
     cudaFree(g->scratch.colours);

@@ -132,6 +132,10 @@ struct cpx_grid {
     uint32_t* compact_to_dense = nullptr;  // [n_act] when sparse
     // bricks of 8x8x8 cells, one bit each (set when any cell of the brick is occupied): the
     // FP32 march of the mixed forms crosses empty bricks in one jump
+    // sparse grids: the density again at every dense vertex position, so the placement march
+    // reads a corner with one load instead of an index_offsets lookup and a dependent load;
+    // vertices outside the cage hold kMirrorEmpty and read compact vertex 0 as the reference does
+    float* dense_mirror = nullptr;
     uint32_t* brick_bits = nullptr;
     int bricks[3] = {0, 0, 0};
     int options = 0;  // CPX_OPT_* march options
@@ -270,6 +274,13 @@ enum MarchMode { kForward = 1, kBackward = 2, kForwardBackward = 3 };
 
 // Segments per ray of the learned proposal (proposal.cu).
 constexpr int kProposalSegments = 32;
+
+// Marker of a dense-mirror entry outside the cage (a quiet NaN with a payload no arithmetic
+// produces).
+constexpr uint32_t kMirrorEmpty = 0x7FBADA55u;
+
+// Rebuilds the dense density mirror of a sparse grid from its compact density (occupancy.cu).
+cpx_status refresh_dense_mirror(cpx_grid* g, cudaStream_t st);
 
 // Per-vertex state of the grid's storage form (api.cu).
 cudaError_t alloc_state(cpx_grid* g, int64_t n);

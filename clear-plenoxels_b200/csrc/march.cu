@@ -52,8 +52,8 @@ __device__ __forceinline__ int clamp_axis(unsigned b, int n)
 // The 8 corner vertices of cell (b0,b1,b2) in the reference's order 000,010,100,110,001,011,
 // 101,111 (x,y,z), each coordinate clamped to the grid as getSceneIndex does; sparse grids
 // map them through index_offsets (RenderUtils.cu:855-990).
-__device__ __forceinline__ void cell_corners(const GridView& g, unsigned b0, unsigned b1, unsigned b2,
-                                             unsigned* idx)
+__device__ __forceinline__ void cell_corners_dense(const GridView& g, unsigned b0, unsigned b1, unsigned b2,
+                                                   unsigned* idx)
 {
     const int x0 = clamp_axis(b0, g.W), x1 = clamp_axis(b0 + 1u, g.W);
     const int y0 = clamp_axis(b1, g.H), y1 = clamp_axis(b1 + 1u, g.H);
@@ -69,26 +69,37 @@ __device__ __forceinline__ void cell_corners(const GridView& g, unsigned b0, uns
     idx[5] = (unsigned)(r11 + x0);
     idx[6] = (unsigned)(r10 + x1);
     idx[7] = (unsigned)(r11 + x1);
+}
+
+__device__ __forceinline__ void cell_corners(const GridView& g, unsigned b0, unsigned b1, unsigned b2,
+                                             unsigned* idx)
+{
+    cell_corners_dense(g, b0, b1, b2, idx);
     if (g.sparse) {
 #pragma unroll
         for (int q = 0; q < 8; q++) idx[q] = g.index_offsets[idx[q]];
     }
 }
 
-// L1 prefetch of the four 32-byte density sectors that hold a cell's 8 corners (dense grids:
-// corners q and q+2 differ only in x and share a sector).
-__device__ __forceinline__ void prefetch_cell(const GridView& g, unsigned b0, unsigned b1, unsigned b2)
+// L1 prefetch of the four 32-byte sectors of a dense-indexed density array (the density of a
+// dense grid, or the dense mirror of a sparse one) that hold a cell's 8 corners (corners q and
+// q+2 differ only in x and share a sector).
+__device__ __forceinline__ void prefetch_cell(const GridView& g, const float* dens, unsigned b0, unsigned b1,
+                                              unsigned b2)
 {
     unsigned idx[8];
-    cell_corners(g, b0, b1, b2, idx);
+    cell_corners_dense(g, b0, b1, b2, idx);
 #pragma unroll
-    for (int q = 0; q < 8; q += 2) asm volatile("prefetch.global.L1 [%0];" ::"l"(g.density + idx[q]));
+    for (int q = 0; q < 8; q += 2) asm volatile("prefetch.global.L1 [%0];" ::"l"(dens + idx[q]));
 }
 
 // Brick occupancy of a sparse grid (8x8x8 cells per bit), read by the FP32 march.
 struct Skip {
     const uint32_t* __restrict__ bits = nullptr;
     int bx = 0, by = 0, bz = 0;
+    // sparse grids: the dense density mirror (kMirrorEmpty outside the cage), so a corner's
+    // density is one load; every march form reads it
+    const float* __restrict__ dense = nullptr;
 };
 
 // FP32 march on a sparse grid, at an empty cell (b0, b1, b2) with position bc: the number of
@@ -226,19 +237,30 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
         }
         if (b0 != cb0 || b1 != cb1 || b2 != cb2) {
             unsigned idx[8];
-            cell_corners(g, b0, b1, b2, idx);
+            if (g.sparse && sk.dense) {
+                // the same values as density[index_offsets[corner]], one load each
+                cell_corners_dense(g, b0, b1, b2, idx);
 #pragma unroll
-            for (int q = 0; q < 8; q++) cd[q] = g.density[idx[q]];
+                for (int q = 0; q < 8; q++) {
+                    const float v = __ldg(sk.dense + idx[q]);
+                    cd[q] = __float_as_uint(v) == kMirrorEmpty ? g.density[0] : v;
+                }
+            } else {
+                cell_corners(g, b0, b1, b2, idx);
+#pragma unroll
+                for (int q = 0; q < 8; q++) cd[q] = g.density[idx[q]];
+            }
             cb0 = b0;
             cb1 = b1;
             cb2 = b2;
             // the march waits on every new cell's densities; fetch the cells one and two
             // voxels further along the ray into L1 now, while this sample is evaluated
-            if (!g.sparse) {
+            if (!g.sparse || sk.dense) {
+                const float* src = g.sparse ? sk.dense : g.density;
 #pragma unroll
                 for (int k = 1; k <= 2; k++) {
                     const Real ta = t + (Real)k;
-                    prefetch_cell(g, (unsigned)(ox + ta * dx), (unsigned)(oy + ta * dy),
+                    prefetch_cell(g, src, (unsigned)(ox + ta * dx), (unsigned)(oy + ta * dy),
                                   (unsigned)(oz + ta * dz));
                 }
             }
@@ -912,6 +934,7 @@ static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32
         set_error("the proposal-guided march runs on the FP32 march of the mixed forms only");
         return CPX_ERR_UNSUPPORTED;
     }
+    if (g->sparse) gd.skip.dense = g->dense_mirror;
     // the FP32 march jumps over empty cells and bricks of a sparse grid
     if (gd.march32 && !(g->options & CPX_OPT_NO_EMPTY_SKIP) && g->sparse && g->brick_bits) {
         gd.skip.bits = g->brick_bits;

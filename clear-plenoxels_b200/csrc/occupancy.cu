@@ -273,6 +273,23 @@ __global__ void k_compact16(const float* __restrict__ dens_in, const uint2* __re
     c2d[c] = (uint32_t)v;
 }
 
+__global__ void k_dense_mirror(float* mirror, const float* __restrict__ density, const uint8_t* __restrict__ in_cage,
+                               const uint32_t* __restrict__ index_offsets, int64_t n)
+{
+    const int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    mirror[d] = in_cage[d] ? density[index_offsets[d]] : __uint_as_float(kMirrorEmpty);
+}
+
+cpx_status refresh_dense_mirror(cpx_grid* g, cudaStream_t st)
+{
+    if (!g->sparse || !g->dense_mirror) return CPX_OK;
+    k_dense_mirror<<<(unsigned)((g->n_dense + 255) / 256), 256, 0, st>>>(g->dense_mirror, g->density, g->in_cage,
+                                                                          g->index_offsets, g->n_dense);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "dense mirror");
+}
+
 cpx_status make_sparse_launch(cpx_grid* g)
 {
     if (!g->have_occupancy) {
@@ -293,6 +310,7 @@ cpx_status make_sparse_launch(cpx_grid* g)
     uint32_t* c2d = nullptr;
     cudaError_t e = alloc_state(&t, n);
     if (e == cudaSuccess) e = cudaMalloc((void**)&c2d, (n > 0 ? n : 1) * sizeof(uint32_t));
+    if (e == cudaSuccess && !g->dense_mirror) e = cudaMalloc((void**)&g->dense_mirror, g->n_dense * sizeof(float));
     if (e != cudaSuccess) {
         cudaGetLastError();
         free_state(&t);
@@ -339,7 +357,9 @@ cpx_status make_sparse_launch(cpx_grid* g)
     g->compact_to_dense = c2d;
     g->n_act = n;
     g->sparse = 1;
-    return CPX_OK;
+    cpx_status rc = refresh_dense_mirror(g, 0);
+    if (rc != CPX_OK) return rc;
+    return cuda_status(cudaDeviceSynchronize(), "dense mirror");
 }
 
 }  // namespace cpx

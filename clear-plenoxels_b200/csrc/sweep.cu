@@ -26,6 +26,7 @@ struct SweepArgs {
     float4* m;
     float4* v;
     float* density_out;
+    float* dense_mirror;  // sparse grids: density at dense positions (or null)
     const float* __restrict__ adaptive_lr;
     const uint32_t* __restrict__ index_offsets;
     const uint32_t* __restrict__ compact_to_dense;
@@ -115,7 +116,10 @@ __device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint
     a.m[sl] = m;
     a.v[sl] = vv;
     if (tch) a.grad[sl] = g;
-    if (j == 0) a.density_out[v] = pn.x;
+    if (j == 0) {
+        a.density_out[v] = pn.x;
+        if (a.dense_mirror) a.dense_mirror[a.compact_to_dense[v]] = pn.x;
+    }
 }
 
 __device__ __forceinline__ void bias_corrections(int t, float* s_bc)
@@ -263,6 +267,7 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
     a.m = reinterpret_cast<float4*>(g->m);
     a.v = reinterpret_cast<float4*>(g->v);
     a.density_out = g->density;
+    a.dense_mirror = g->sparse ? g->dense_mirror : nullptr;
     a.adaptive_lr = g->sparse ? nullptr : g->adaptive_lr;
     a.index_offsets = g->index_offsets;
     a.compact_to_dense = g->compact_to_dense;

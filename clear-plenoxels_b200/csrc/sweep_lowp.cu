@@ -18,6 +18,7 @@ struct LowpArgs {
     uint32_t n_act;
     const float* __restrict__ d_in;
     float* d_out;
+    float* dense_mirror;  // sparse grids: density at dense positions (or null)
     const uint2* __restrict__ sh_in;  // 4 x 16-bit per quad
     uint2* sh_out;
     float4* grad;  // FP32 gradient records, S float4 per vertex
@@ -116,6 +117,7 @@ __device__ __forceinline__ void lowp_quad(const LowpArgs& a, uint32_t v, int j, 
         if (e == 0) {
             np = np < 0.f ? 0.f : np;  // density clamp (Optimizer.cu:384)
             a.d_out[v] = np;
+            if (a.dense_mirror) a.dense_mirror[a.compact_to_dense[v]] = np;
         } else {
             sh_bits[c] = f_to_sh_sr<PREC>(np, r & 0xffffu);
         }
@@ -123,7 +125,10 @@ __device__ __forceinline__ void lowp_quad(const LowpArgs& a, uint32_t v, int j, 
         v_bits[c] = f_to_bf16_sr(vc, r >> 16);
         g[c] = 0.f;
     }
-    if (j == 0 && !(a.adam_mask & 1u)) a.d_out[v] = p[0];
+    if (j == 0 && !(a.adam_mask & 1u)) {
+        a.d_out[v] = p[0];
+        if (a.dense_mirror) a.dense_mirror[a.compact_to_dense[v]] = p[0];
+    }
     a.sh_out[q] = pack4(sh_bits);
     a.m[q] = pack4(m_bits);
     a.v[q] = pack4(v_bits);
@@ -244,6 +249,7 @@ cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_
     a.n_act = (uint32_t)g->n_act;
     a.d_in = g->dens[g->cur];
     a.d_out = g->dens[g->cur ^ 1];
+    a.dense_mirror = g->sparse ? g->dense_mirror : nullptr;
     a.sh_in = reinterpret_cast<const uint2*>(g->sh16[g->cur]);
     a.sh_out = reinterpret_cast<uint2*>(g->sh16[g->cur ^ 1]);
     a.grad = reinterpret_cast<float4*>(g->grad);
