@@ -58,7 +58,7 @@ EXPORTED = [
     "cpx_proposal_param_count", "cpx_proposal_create", "cpx_proposal_destroy", "cpx_proposal_params",
     "cpx_proposal_infer", "cpx_proposal_gradient", "cpx_proposal_train", "cpx_proposal_stats",
     "cpx_render_forward_backward_guided", "cpx_train_step_proposal", "cpx_render_forward_guided",
-    "cpx_grid_set_options",
+    "cpx_grid_set_options", "cpx_grid_upsample",
 ]
 
 
@@ -185,6 +185,7 @@ _sig("cpx_render_forward_backward_guided", [_vp, _vp, _vp, _vp, C.c_int, C.c_int
                                             _vp])
 _sig("cpx_render_forward_guided", [_vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
 _sig("cpx_grid_set_options", [_vp, C.c_int])
+_sig("cpx_grid_upsample", [_vp, _vp, C.c_float, C.c_int, _vp])
 OPT_NO_EMPTY_SKIP = 1  # the FP32 march steps through empty cells one step at a time
 OPT_FP32_MARCH = 2     # an FP32-storage grid marches like the mixed forms
 _sig("cpx_train_step_proposal", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), C.POINTER(ProposalSchedule),
@@ -373,6 +374,11 @@ class ObjectScene:
         _check(_lib.cpx_occupancy_build(self._h, float(threshold), occ.ctypes.data, cage.ctypes.data,
                                         idx.ctypes.data, C.byref(cnt)), "cpx_occupancy_build")
         return occ, cage, idx, int(cnt.value)
+
+    def init_by_upsample(self, src: "ObjectScene", threshold: float, low_band_only: bool = False, stream=None):
+        """upsampleScene of src into this (normally fresh) grid (SceneUtils.cu:419-485)."""
+        _check(_lib.cpx_grid_upsample(src.handle, self._h, float(threshold), 1 if low_band_only else 0,
+                                      _stream(stream)), "cpx_grid_upsample")
 
     def set_options(self, options: int):
         """March options (OPT_NO_EMPTY_SKIP, OPT_FP32_MARCH)."""

@@ -208,6 +208,18 @@ cpx_status cpx_render_image(cpx_grid* g, const cpx_camera* cam, int width, int h
  * summed in double on the device, for held-out PSNR; synchronises. */
 cpx_status cpx_image_mse(const float* a_dev, const float* b_dev, int64_t n, double* mse_out,
                          cpx_stream stream);
+/* Coarse-to-fine refinement (upsampleScene, SVRF/SceneUtils.cu:419-485, as
+ * objectScene::initSelfByUpsample runs it, SceneUtils.cu:487-657): every vertex of dst takes
+ * the trilinear interpolation of src at (col*srcW/dstW, row*srcH/dstH, depth*srcD/dstD);
+ * densities below threshold become 0.  low_band_only interpolates and writes only the first
+ * SH coefficient per channel (the reference's lowBoundOnly; otherwise dst->sh_dim must equal
+ * src->sh_dim).  A sparse src gives zeros in its unoccupied cells; a sparse dst (occupancy built,
+ * compacted) receives its in-cage vertices.  The reference's sparse target is reached by
+ * upsampling into a dense dst, then cpx_occupancy_build and cpx_grid_make_sparse.  FP32 form;
+ * dst is normally a fresh grid. */
+cpx_status cpx_grid_upsample(const cpx_grid* src, cpx_grid* dst, float threshold, int low_band_only,
+                             cpx_stream stream);
+
 /* March options (no reference counterpart; for studying the mixed forms):
  * CPX_OPT_NO_EMPTY_SKIP  the FP32 march steps through every empty cell of a sparse grid as
  *                        the reference does, instead of jumping over empty cells and bricks;

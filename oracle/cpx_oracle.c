@@ -1202,3 +1202,57 @@ void orc64_adam(const orc_scene* s, double* params, double* grad, double* m, dou
         }
     }
 }
+
+/* ------------------------------------------------------ coarse-to-fine upsampling */
+
+/* getIndex (SceneUtils.cu:250-260): clamped from above only. */
+static inline int64_t up_index(int col, int row, int depth, int W, int H, int D)
+{
+    col = col < W ? col : W - 1;
+    row = row < H ? row : H - 1;
+    depth = depth < D ? depth : D - 1;
+    return (int64_t)depth * W * H + (int64_t)row * W + col;
+}
+
+void orc_upsample(const orc_scene* s, int dW, int dH, int dD, int dst_sh, float threshold,
+                  int low_band_only, float* dst)
+{
+    const int64_t n = (int64_t)dW * dH * dD;
+    const int64_t na = s->n_act;
+    const int sh = s->sh_dim;
+#pragma omp parallel for schedule(static) num_threads(orc_get_threads())
+    for (int64_t p = 0; p < n; p++) {
+        const int col = (int)(p % dW), row = (int)((p / dW) % dH), depth = (int)(p / ((int64_t)dW * dH));
+        /* pixelCol * 1.f * src.sceneWidth / dest.sceneWidth, in float */
+        const float bc[3] = {(float)col * 1.f * (float)s->W / (float)dW, (float)row * 1.f * (float)s->H / (float)dH,
+                             (float)depth * 1.f * (float)s->D / (float)dD};
+        const uint32_t b[3] = {(uint32_t)bc[0], (uint32_t)bc[1], (uint32_t)bc[2]};
+        float tri[1 + 3 * 25];
+        for (int i = 0; i < 1 + 3 * sh; i++) tri[i] = 0.f;
+        int val = 1;
+        if (s->sparse) val = s->occ[up_index((int)b[0], (int)b[1], (int)b[2], s->W - 1, s->H - 1, s->D - 1)] != 0;
+        if (val) {
+            const double x = (double)(bc[0] - (float)b[0]);
+            const double y = (double)(bc[1] - (float)b[1]);
+            const double z = (double)(bc[2] - (float)b[2]);
+            const int nsh = low_band_only ? 1 : sh;
+            for (int q = 0; q < 8; q++) {
+                int64_t idx = up_index((int)(b[0] + k_corner[q][0]), (int)(b[1] + k_corner[q][1]),
+                                       (int)(b[2] + k_corner[q][2]), s->W, s->H, s->D);
+                if (s->sparse) idx = s->index_offsets[idx];
+                const double c = corner_weight(q, x, y, z);
+                tri[0] = (float)fma(c, (double)s->params[idx], (double)tri[0]);
+                for (int i = 0; i < nsh; i++)
+                    for (int ch = 0; ch < 3; ch++) {
+                        const int e = 1 + ch * sh + i;
+                        tri[e] = (float)fma(c, (double)s->params[(int64_t)e * na + idx], (double)tri[e]);
+                    }
+            }
+        }
+        dst[p] = (!val || tri[0] < threshold) ? 0.f : tri[0];
+        const int nw = low_band_only ? 1 : sh;
+        for (int i = 0; i < nw; i++)
+            for (int ch = 0; ch < 3; ch++)
+                dst[(int64_t)(1 + ch * dst_sh + i) * n + p] = tri[1 + ch * sh + i];
+    }
+}

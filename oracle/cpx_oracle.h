@@ -130,6 +130,12 @@ void orc_render_image(const orc_scene* s, const double* alpha, const double* pri
                       int height, int white_bg, float* rgb, uint8_t* rgb8, float* depth,
                       uint8_t* mask);
 
+/* Coarse-to-fine refinement: upsampleScene / upsample_trilinear (SceneUtils.cu:262-485).
+ * src: the oracle scene (dense or sparse); dst: planar [1 + 3*dst_sh][dW*dH*dD] (dense target,
+ * written for every vertex; entries beyond the written coefficients are left as they are). */
+void orc_upsample(const orc_scene* src, int dW, int dH, int dD, int dst_sh, float threshold,
+                  int low_band_only, float* dst);
+
 /* R11: batch MSE of the per-ray losses (Utils.cu:311-320). */
 double orc_mse(const double* losses, int n);
 

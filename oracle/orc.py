@@ -71,6 +71,7 @@ _fn("orc_compact", [_vp, C.c_int, C.c_int64, _vp, _vp, C.c_int64])
 _fn("orc_mse", [_vp, C.c_int], C.c_double)
 _fn("orc_composite_kat", [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _fn("orc_render_image", [C.POINTER(_Scene)] + [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
+_fn("orc_upsample", [C.POINTER(_Scene), C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp])
 class _Bricks(C.Structure):
     _fields_ = [("bits", _vp), ("bx", C.c_int), ("by", C.c_int), ("bz", C.c_int)]
 
@@ -235,6 +236,15 @@ def fp64_step(scene: Scene, rays: RaySet, mask_coef, huber, lam_d=None, lam_sh=N
         _lib.orc64_adam(C.byref(scene.c), _p(params), _p(g), _p(m), _p(v), float(lr), float(sh_lr), int(timestep))
         post = params
     return pred, accw, losses, grad, post
+
+
+def upsample(scene: Scene, dW, dH, dD, threshold, low_band_only=False, dst_sh=None):
+    """upsampleScene of the scene into a dense dW x dH x dD target: planar float32 params."""
+    dst_sh = (1 if low_band_only else scene.sh_dim) if dst_sh is None else int(dst_sh)
+    out = np.zeros((1 + 3 * dst_sh, dW * dH * dD), np.float32)
+    _lib.orc_upsample(C.byref(scene.c), int(dW), int(dH), int(dD), int(dst_sh), float(threshold),
+                      1 if low_band_only else 0, _p(out))
+    return out
 
 
 def render_forward(scene: Scene, rays: RaySet, sample_index=None, start=0, length=None):

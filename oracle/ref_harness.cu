@@ -311,6 +311,7 @@ int ref_rays_init(void* h, int ncam, const double* alpha, const double* principl
 
 int ref_rays_count(void* h) { return ((RefCtx*)h)->rays.totalRays; }
 
+
 // RenderUtils::renderImage (RenderUtils.cu:1802) of one camera into host buffers:
 // rgb float [3][w*h], rgb8 u8 [3][w*h], depth float [w*h], mask u8 [w*h].
 int ref_render_image(void* h, const double* alpha, const double* principle, const double* c2w,
@@ -467,6 +468,21 @@ static int copy_table(const std::vector<float*>& ptrs, int n_arrays, int64_t n, 
 }
 
 int64_t ref_n_active(void* h) { return ((RefCtx*)h)->scene.actualGridNums; }
+
+// objectScene::initSelfByUpsample of the handle's scene into a dense target (SceneUtils.cu:487-517):
+// the target's planar parameters [1 + 3 * its sh_dim][its vertices] to host memory.
+int ref_upsample(void* h, float threshold, int low_band_only, int target_sh, float* planar_out)
+{
+    RefCtx* c = (RefCtx*)h;
+    ObjectScene dst;
+    dst.initSelfByUpsample(c->scene, threshold, low_band_only != 0, false, target_sh);
+    int rc = fail(cudaDeviceSynchronize());
+    const int na = 1 + 3 * dst.sh_dim;
+    std::vector<float*> p(dst.totalVariableGPUPtrs, dst.totalVariableGPUPtrs + na);
+    if (!rc) rc = copy_table(p, na, dst.actualGridNums, planar_out, false);
+    dst.freeSelf();
+    return rc;
+}
 
 int ref_params(void* h, float* planar, int upload)
 {

@@ -53,6 +53,7 @@ def _setup(L):
     s("ref_rays_init", [_vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp, _vp, C.c_int])
     s("ref_rays_count", [_vp])
     s("ref_render_image", [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
+    s("ref_upsample", [_vp, C.c_float, C.c_int, C.c_int, _vp])
     s("ref_rays_download", [_vp] + [_vp] * 17)
     s("ref_render_forward", [_vp, C.c_int, C.c_int])
     s("ref_render_backward", [_vp, C.c_int, C.c_int, C.c_double, C.c_float, _vp])
@@ -144,6 +145,14 @@ class RefScene:
                  "acc_density", "acc_weights", "acc_r", "acc_g", "acc_b")
         out = {k: np.zeros(n, np.uint8 if k in ("mask", "r", "g", "b") else np.float32) for k in names}
         _ck(lib().ref_rays_download(self.h, *[_p(out[k]) for k in names]), "rays_download")
+        return out
+
+    def upsample(self, threshold, low_band_only=False, target_sh=None):
+        """objectScene::initSelfByUpsample into a dense target of doubled dimensions."""
+        target_sh = self.sh_dim if target_sh is None else int(target_sh)
+        sh = 1 if low_band_only else target_sh
+        out = np.zeros((1 + 3 * sh, 8 * self.W * self.H * self.D), np.float32)
+        _ck(lib().ref_upsample(self.h, float(threshold), 1 if low_band_only else 0, target_sh, _p(out)), "upsample")
         return out
 
     def render_image(self, cam, width, height, white_bg=True):
