@@ -59,6 +59,8 @@ EXPORTED = [
     "cpx_proposal_infer", "cpx_proposal_gradient", "cpx_proposal_train", "cpx_proposal_stats",
     "cpx_render_forward_backward_guided", "cpx_train_step_proposal", "cpx_render_forward_guided",
     "cpx_grid_set_options", "cpx_grid_upsample",
+    "cpx_batch_create", "cpx_batch_destroy", "cpx_batch_step", "cpx_batch_mse", "cpx_batch_check",
+    "cpx_batch_info", "cpx_batch_set_tuning", "cpx_batch_get_tuning", "cpx_batch_autotune",
 ]
 
 
@@ -190,6 +192,25 @@ OPT_NO_EMPTY_SKIP = 1  # the FP32 march steps through empty cells one step at a 
 OPT_FP32_MARCH = 2     # an FP32-storage grid marches like the mixed forms
 _sig("cpx_train_step_proposal", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), C.POINTER(ProposalSchedule),
                                  C.c_int, _vp, C.POINTER(C.c_double), _vp])
+
+
+class BatchScene(C.Structure):
+    _fields_ = [("grid", _vp), ("rays", _vp), ("rays_per_batch", C.c_int)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("place_block", C.c_int), ("shade_warps", C.c_int), ("grab", C.c_int)]
+
+
+_sig("cpx_batch_create", [C.POINTER(BatchScene), C.c_int, C.POINTER(StepArgs), C.POINTER(_vp)])
+_sig("cpx_batch_destroy", [_vp])
+_sig("cpx_batch_step", [_vp, C.c_int, _vp])
+_sig("cpx_batch_mse", [_vp, C.POINTER(C.c_double), _vp])
+_sig("cpx_batch_check", [_vp])
+_sig("cpx_batch_info", [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)])
+_sig("cpx_batch_set_tuning", [_vp, C.POINTER(BatchTuning)])
+_sig("cpx_batch_get_tuning", [_vp, C.POINTER(BatchTuning)])
+_sig("cpx_batch_autotune", [_vp, C.c_int, C.POINTER(BatchTuning), _vp])
 
 
 def _check(rc: int, where: str):
@@ -727,6 +748,84 @@ def train_step_proposal(scene: ObjectScene, rays: Rays, proposal: Proposal, loss
                                         C.byref(mse) if want_mse else None, _stream(stream)),
            "cpx_train_step_proposal")
     return mse.value if want_mse else None
+
+
+def step_args(*, mask_coef: float = 1.0, huber_delta: float = 0.1, do_tv: bool = True, tv_type: int = 0,
+              tv_neighbours: int = 6, lam_density: float = 1e-5, lam_sh: float = 1e-6, lr: float = 0.3,
+              sh_lr: float = 1.0, timestep: int = 1) -> StepArgs:
+    a = StepArgs()
+    a.mask_coef, a.huber_delta, a.do_tv = float(mask_coef), float(huber_delta), 1 if do_tv else 0
+    a.tv_type, a.tv_neighbours = int(tv_type), int(tv_neighbours)
+    a.lam_density, a.lam_sh, a.lr, a.sh_lr, a.timestep = float(lam_density), float(lam_sh), float(lr), \
+        float(sh_lr), int(timestep)
+    return a
+
+
+class Batch:
+    """Batched multi-scene training (no reference counterpart): every scene of the batch
+    steps together, one placement and one shading launch over all their rays, then each
+    scene's TV + Adam sweep.  Iteration i of a scene trains on rays
+    [(i % pool) * len, (i + 1) * len) of its ray table with Adam timestep i + 1, exactly as
+    train_step(start=(i % pool) * len, timestep=i + 1) on that scene alone."""
+
+    def __init__(self, scenes, **step_kw):
+        """scenes: (ObjectScene, Rays, rays_per_batch) triples; step_kw as train_step's."""
+        self.scenes = list(scenes)
+        arr = (BatchScene * len(self.scenes))()
+        for i, (sc, r, n) in enumerate(self.scenes):
+            arr[i].grid, arr[i].rays, arr[i].rays_per_batch = sc.handle, r.handle, int(n)
+        self.args = step_args(**step_kw)
+        h = _vp()
+        _check(_lib.cpx_batch_create(arr, len(self.scenes), C.byref(self.args), C.byref(h)), "cpx_batch_create")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cpx_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, graphs: bool = True, stream=None):
+        _check(_lib.cpx_batch_step(self._h, 1 if graphs else 0, _stream(stream)), "cpx_batch_step")
+
+    def mse(self, stream=None) -> np.ndarray:
+        out = (C.c_double * len(self.scenes))()
+        _check(_lib.cpx_batch_mse(self._h, out, _stream(stream)), "cpx_batch_mse")
+        return np.array(out[:], np.float64)
+
+    def check(self):
+        _check(_lib.cpx_batch_check(self._h), "cpx_batch_check")
+
+    def info(self) -> dict:
+        it, tot, lps = C.c_int(0), C.c_int(0), C.c_int(0)
+        _check(_lib.cpx_batch_info(self._h, C.byref(it), C.byref(tot), C.byref(lps)), "cpx_batch_info")
+        return {"iteration": it.value, "total_rays": tot.value, "launches_per_step": lps.value}
+
+    @property
+    def tuning(self) -> dict:
+        t = BatchTuning()
+        _check(_lib.cpx_batch_get_tuning(self._h, C.byref(t)), "cpx_batch_get_tuning")
+        return {"place_block": t.place_block, "shade_warps": t.shade_warps, "grab": t.grab}
+
+    def set_tuning(self, place_block: int, shade_warps: int, grab: int):
+        t = BatchTuning()
+        t.place_block, t.shade_warps, t.grab = int(place_block), int(shade_warps), int(grab)
+        _check(_lib.cpx_batch_set_tuning(self._h, C.byref(t)), "cpx_batch_set_tuning")
+
+    def autotune(self, steps_per_trial: int = 3, stream=None) -> dict:
+        t = BatchTuning()
+        _check(_lib.cpx_batch_autotune(self._h, int(steps_per_trial), C.byref(t), _stream(stream)),
+               "cpx_batch_autotune")
+        return {"place_block": t.place_block, "shade_warps": t.shade_warps, "grab": t.grab}
 
 
 def image_mse(a, b, stream=None) -> float:

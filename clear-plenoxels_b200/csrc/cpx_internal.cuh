@@ -282,6 +282,58 @@ constexpr uint32_t kMirrorEmpty = 0x7FBADA55u;
 // Rebuilds the dense density mirror of a sparse grid from its compact density (occupancy.cu).
 cpx_status refresh_dense_mirror(cpx_grid* g, cudaStream_t st);
 
+// ---- batched form (march.cu kernels, batch.cu host side)
+constexpr int kMaxBatchScenes = 64;
+
+// Brick occupancy and dense density mirror of a sparse grid, as the placement march reads them.
+struct Skip {
+    const uint32_t* __restrict__ bits = nullptr;
+    int bx = 0, by = 0, bz = 0;
+    // sparse grids: the dense density mirror (kMirrorEmpty outside the cage), so a corner's
+    // density is one load; every march form reads it
+    const float* __restrict__ dense = nullptr;
+};
+
+// One scene of a batch: its views as of the batch's step parity (the parameter and touched
+// buffers alternate every step).
+struct BatchScene {
+    GridView g;
+    RaysView r;
+    Skip skip;
+    uint32_t* touched;
+    int len;            // rays per batch
+    int pool_batches;   // batches in the scene's ray table; iteration i uses batch i % pool_batches
+    int maxs;           // sample slots per ray
+    int ray_base;       // first ray of the scene among the iteration's rays
+    int64_t n_rays;
+    int64_t sample_base;  // first sample slot of the scene
+};
+
+struct BatchArgs {
+    const BatchScene* scenes;
+    int n_scenes, total_rays;
+    SampleRec* samples;
+    float4* colours;
+    int* counts;
+    double* acc;
+    double* losses;
+    int* err;
+    int* queue;        // [2] work counters of the placement and shading launches, zeroed per step
+    const int* iter;   // the batch's iteration counter (device)
+    double mask_coef;
+    float huber;
+    int grab;          // rays a warp takes per work-counter access in shading
+};
+
+struct BatchTuning {
+    int place_block = 64;  // threads per block of the placement launch
+    int shade_warps = 4;   // warps per block of the shading launch
+    int grab = 1;          // rays per warp per work-counter access in shading
+};
+
+cpx_status batch_launch_march(int prec, const BatchArgs& a, const BatchTuning& tn, cudaStream_t st);
+BatchScene batch_scene_view(cpx_grid* g, cpx_rays* r, int len, int pool_batches, int ray_base, int64_t sample_base);
+
 // Per-vertex state of the grid's storage form (api.cu).
 cudaError_t alloc_state(cpx_grid* g, int64_t n);
 void free_state(cpx_grid* g);
@@ -304,9 +356,10 @@ float* proposal_label_buffer(cpx_proposal* p, int len);
 cpx_status proposal_train(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                           const float* seg_w, int steps, int rays_per_step, bool adam, cudaStream_t st);
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
-                      double sh_lr, int timestep, cudaStream_t s);
+                      double sh_lr, int timestep, cudaStream_t s, const int* t_dev = nullptr);
 cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
-                           int timestep, uint32_t tv_mask, uint32_t adam_mask, cudaStream_t st);
+                           int timestep, uint32_t tv_mask, uint32_t adam_mask, cudaStream_t st,
+                           const int* t_dev = nullptr);
 cpx_status tv_launch(cpx_grid* g, double lam_d, double lam_sh, int type, int nbrs,
                      cudaStream_t s);
 cpx_status occupancy_launch(cpx_grid* g, float threshold);

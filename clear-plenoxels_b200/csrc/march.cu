@@ -94,13 +94,7 @@ __device__ __forceinline__ void prefetch_cell(const GridView& g, const float* de
 }
 
 // Brick occupancy of a sparse grid (8x8x8 cells per bit), read by the FP32 march.
-struct Skip {
-    const uint32_t* __restrict__ bits = nullptr;
-    int bx = 0, by = 0, bz = 0;
-    // sparse grids: the dense density mirror (kMirrorEmpty outside the cage), so a corner's
-    // density is one load; every march form reads it
-    const float* __restrict__ dense = nullptr;
-};
+// (struct Skip: cpx_internal.cuh)
 
 // FP32 march on a sparse grid, at an empty cell (b0, b1, b2) with position bc: the number of
 // steps that carry the sample position out of that cell -- or out of its whole 8x8x8 brick
@@ -990,6 +984,147 @@ cpx_status march_launch_guided(cpx_grid* g, cpx_rays* r, const int32_t* sidx, in
     guide.masks = masks;
     guide.seg_w = seg_w;
     return march_launch_guided_with(g, r, sidx, start, len, mode, losses, mask_coef, huber, g->scratch, guide, st);
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: the batches of many scenes (grids of any size, any batch length) in one
+// placement launch and one shading launch.  Both kernels are persistent: a warp takes the
+// next rays from a global work counter, so scenes with long rays and scenes with short ones
+// share the GPU without one launch per scene.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int batch_scene_of(const int* s_base, int n, int gray)
+{
+    int lo = 0, hi = n - 1;  // the last scene whose first ray is <= gray
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_base[mid] <= gray) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <typename Real>
+__global__ void k_place_batched(BatchArgs a)
+{
+    __shared__ int s_base[kMaxBatchScenes];
+    for (int i = threadIdx.x; i < a.n_scenes; i += blockDim.x) s_base[i] = a.scenes[i].ray_base;
+    __syncthreads();
+    const int iter = *a.iter;
+    const int lane = threadIdx.x & 31;
+    while (true) {
+        int first = 0;
+        if (lane == 0) first = atomicAdd(a.queue, 32);
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (first >= a.total_rays) break;  // warp-uniform
+        const int gr = first + lane;
+        if (gr >= a.total_rays) continue;
+        const int si = batch_scene_of(s_base, a.n_scenes, gr);
+        const BatchScene& sc = a.scenes[si];
+        const int b = gr - sc.ray_base;
+        const int64_t ri = (int64_t)(iter % sc.pool_batches) * sc.len + b;
+        place_ray<Real, false>(sc.g, sc.r, b, ri, a.samples + sc.sample_base, sc.maxs, a.counts + sc.ray_base,
+                               a.acc + sc.ray_base, a.err, true, 0xffffffffu, nullptr, sc.skip);
+    }
+}
+
+template <int NSH, int PREC, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 20 / WARPS) k_shade_batched(BatchArgs a)
+{
+    __shared__ uint32_t h_keys[WARPS][kHashSlots];
+    __shared__ float h_vals[WARPS][4][kHashSlots];
+    __shared__ int s_base[kMaxBatchScenes];
+    for (int i = threadIdx.x; i < a.n_scenes; i += blockDim.x) s_base[i] = a.scenes[i].ray_base;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for (int s = lane; s < kHashSlots; s += 32) {
+        h_keys[warp][s] = kEmpty;
+        h_vals[warp][0][s] = h_vals[warp][1][s] = h_vals[warp][2][s] = h_vals[warp][3][s] = 0.f;
+    }
+    __syncthreads();
+    const WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
+    const int iter = *a.iter;
+    while (true) {
+        int first = 0;
+        if (lane == 0) first = atomicAdd(a.queue + 1, a.grab);
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (first >= a.total_rays) break;  // warp-uniform
+        for (int q = 0; q < a.grab; q++) {
+            const int gr = first + q;
+            if (gr >= a.total_rays) break;
+            const int si = batch_scene_of(s_base, a.n_scenes, gr);
+            const BatchScene& sc = a.scenes[si];
+            const int b = gr - sc.ray_base;
+            const int cnt = a.counts[gr];
+            if (cnt == -2) {
+                if (lane == 0) a.losses[gr] = 0.;
+                continue;
+            }
+            const int64_t ri = (int64_t)(iter % sc.pool_batches) * sc.len + b;
+            shade_ray<NSH, kForwardBackward, PREC>(sc.g, sc.r, b, ri, cnt, a.samples + sc.sample_base,
+                                                   a.colours + sc.sample_base, sc.maxs, a.acc + sc.ray_base,
+                                                   a.losses + sc.ray_base, a.mask_coef, a.huber, tab, sc.touched,
+                                                   lane);
+        }
+    }
+}
+
+static int batch_blocks(const void* fn, int threads, int smem)
+{
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem);
+    return sms * (per > 0 ? per : 1);
+}
+
+template <int PREC>
+static cpx_status batch_launch_prec(const BatchArgs& a, const BatchTuning& tn, cudaStream_t st)
+{
+    using Real = typename std::conditional<PREC == kPrecFP32, double, float>::type;
+    const int pb = batch_blocks((const void*)k_place_batched<Real>, tn.place_block, 0);
+    k_place_batched<Real><<<pb, tn.place_block, 0, st>>>(a);
+#define CPX_SHADE_B(W)                                                                              \
+    {                                                                                               \
+        const int sb = batch_blocks((const void*)k_shade_batched<9, PREC, W>, W * 32, 0);           \
+        k_shade_batched<9, PREC, W><<<sb, W * 32, 0, st>>>(a);                                      \
+    }
+    if (tn.shade_warps == 2) CPX_SHADE_B(2)
+    else if (tn.shade_warps == 8) CPX_SHADE_B(8)
+    else CPX_SHADE_B(4)
+#undef CPX_SHADE_B
+    count_launch(2);
+    return cuda_status(cudaGetLastError(), "batched march");
+}
+
+cpx_status batch_launch_march(int prec, const BatchArgs& a, const BatchTuning& tn, cudaStream_t st)
+{
+    if (prec == kPrecFP32) return batch_launch_prec<kPrecFP32>(a, tn, st);
+    if (prec == kPrecBF16) return batch_launch_prec<kPrecBF16>(a, tn, st);
+    return batch_launch_prec<kPrecFP16>(a, tn, st);
+}
+
+BatchScene batch_scene_view(cpx_grid* g, cpx_rays* r, int len, int pool_batches, int ray_base, int64_t sample_base)
+{
+    BatchScene sc;
+    sc.g = grid_view(g);
+    sc.r = rays_view(r);
+    sc.skip = Skip();
+    if (g->sparse) sc.skip.dense = g->dense_mirror;
+    const bool march32 = g->prec != kPrecFP32 || (g->options & CPX_OPT_FP32_MARCH);
+    if (march32 && !(g->options & CPX_OPT_NO_EMPTY_SKIP) && g->sparse && g->brick_bits) {
+        sc.skip.bits = g->brick_bits;
+        sc.skip.bx = g->bricks[0];
+        sc.skip.by = g->bricks[1];
+        sc.skip.bz = g->bricks[2];
+    }
+    sc.touched = g->touched[g->tcur];
+    sc.len = len;
+    sc.pool_batches = pool_batches;
+    sc.maxs = max_samples_per_ray(g);
+    sc.ray_base = ray_base;
+    sc.n_rays = r->n;
+    sc.sample_base = sample_base;
+    return sc;
 }
 
 }  // namespace cpx

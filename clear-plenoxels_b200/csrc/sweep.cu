@@ -38,6 +38,7 @@ struct SweepArgs {
     float lam_d, lam_sh;
     float lr, sh_lr;
     int timestep;
+    const int* t_dev;  // when set, the timestep is *t_dev + 1 (a replayed CUDA graph)
 };
 
 __device__ __forceinline__ float f4get(const float4& v, int c)
@@ -122,9 +123,10 @@ __device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint
     }
 }
 
-__device__ __forceinline__ void bias_corrections(int t, float* s_bc)
+__device__ __forceinline__ void bias_corrections(int t, const int* t_dev, float* s_bc)
 {
     if (threadIdx.x == 0) {
+        if (t_dev) t = *t_dev + 1;
         // bias corrections as the reference forms them (powf of the float betas)
         s_bc[0] = 1.f / (float)(1. - powf(0.9f, t));
         s_bc[1] = 1.f / (float)(1. - powf(0.999f, t));
@@ -137,7 +139,7 @@ template <int S, bool TV>
 __global__ void __launch_bounds__(256) k_sweep_dense(SweepArgs a)
 {
     __shared__ float s_bc[2];
-    bias_corrections(a.timestep, s_bc);
+    bias_corrections(a.timestep, a.t_dev, s_bc);
     const int row = blockIdx.x;
     const int y = row % a.H;
     const int z = row / a.H;
@@ -172,7 +174,7 @@ __global__ void __launch_bounds__(256) k_sweep_sparse(SweepArgs a)
     // neighbourhood once (the dense position, its flags and six neighbour lookups), and the
     // warp's 32 * S slots -- consecutive slots on consecutive lanes -- take it by shuffle.
     __shared__ float s_bc[2];
-    bias_corrections(a.timestep, s_bc);
+    bias_corrections(a.timestep, a.t_dev, s_bc);
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t v0 = warp * 32u;
@@ -243,13 +245,13 @@ static void element_masks(const cpx_grid* g, uint32_t* tv_mask, uint32_t* adam_m
 }
 
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
-                      double sh_lr, int timestep, cudaStream_t st)
+                      double sh_lr, int timestep, cudaStream_t st, const int* t_dev)
 {
     if (g->n_act == 0) return CPX_OK;
     if (g->prec != kPrecFP32) {
         uint32_t tvm, am;
         element_masks(g, &tvm, &am);
-        return sweep_adam_lowp(g, fused_tv, lam_d, lam_sh, lr, sh_lr, timestep, tvm, am, st);
+        return sweep_adam_lowp(g, fused_tv, lam_d, lam_sh, lr, sh_lr, timestep, tvm, am, st, t_dev);
     }
     const int S = g->rec / 4;
     if (g->n_act * S >= ((int64_t)1 << 32)) {
@@ -280,6 +282,7 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
     a.lr = (float)lr;
     a.sh_lr = (float)sh_lr;
     a.timestep = timestep;
+    a.t_dev = t_dev;
     switch (S) {
     case 1: launch_sweep<1>(g, a, fused_tv, st); break;
     case 4: launch_sweep<4>(g, a, fused_tv, st); break;

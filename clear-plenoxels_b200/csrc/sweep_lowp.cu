@@ -34,6 +34,8 @@ struct LowpArgs {
     float lam_d, lam_sh, lr, sh_lr;
     int timestep;
     uint32_t step_key;  // hash of (stochastic-rounding seed, timestep)
+    const int* t_dev;   // when set, the timestep is *t_dev + 1 (a replayed CUDA graph)
+    uint32_t seed;
 };
 
 __device__ __forceinline__ void bits4(const uint2& q, uint16_t* h)
@@ -53,7 +55,7 @@ __device__ __forceinline__ float fast_sqrt(float x) { return x > 0.f ? x * rsqrt
 template <int PREC, int S, bool TV>
 __device__ __forceinline__ void lowp_quad(const LowpArgs& a, uint32_t v, int j, bool tv_on,
                                           const uint32_t* nb_v, const bool* nb_self, float inv_bc1,
-                                          float inv_bc2, float lr_density)
+                                          float inv_bc2, float lr_density, uint32_t step_key)
 {
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
     const size_t q = (size_t)v * S + j;
@@ -101,7 +103,7 @@ __device__ __forceinline__ void lowp_quad(const LowpArgs& a, uint32_t v, int j, 
         }
     }
     // random bits: one hash of (launch key, vertex, quad), then one cheap draw per element
-    const uint32_t h1 = fmix32(a.step_key ^ (v * 0x632BE5ABu) ^ ((uint32_t)j << 28));
+    const uint32_t h1 = fmix32(step_key ^ (v * 0x632BE5ABu) ^ ((uint32_t)j << 28));
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const int e = 4 * j + c;
@@ -135,11 +137,14 @@ __device__ __forceinline__ void lowp_quad(const LowpArgs& a, uint32_t v, int j, 
     if (tch) a.grad[(size_t)v * S + j] = make_float4(g[0], g[1], g[2], g[3]);
 }
 
-__device__ __forceinline__ void lowp_bias_corrections(int t, float* s_bc)
+// Bias corrections and the stochastic-rounding key of this step into shared memory.
+__device__ __forceinline__ void lowp_bias_corrections(const LowpArgs& a, float* s_bc, uint32_t* s_key)
 {
     if (threadIdx.x == 0) {
+        const int t = a.t_dev ? *a.t_dev + 1 : a.timestep;
         s_bc[0] = 1.f / (float)(1. - powf(0.9f, t));
         s_bc[1] = 1.f / (float)(1. - powf(0.999f, t));
+        *s_key = a.t_dev ? fmix32(a.seed ^ ((uint32_t)t * 0x9E3779B9u)) : a.step_key;
     }
     __syncthreads();
 }
@@ -149,7 +154,8 @@ template <int PREC, int S, bool TV>
 __global__ void __launch_bounds__(256) k_sweep_lowp_dense(LowpArgs a)
 {
     __shared__ float s_bc[2];
-    lowp_bias_corrections(a.timestep, s_bc);
+    __shared__ uint32_t s_key;
+    lowp_bias_corrections(a, s_bc, &s_key);
     const int row = blockIdx.x;
     const int y = row % a.H;
     const int z = row / a.H;
@@ -165,7 +171,7 @@ __global__ void __launch_bounds__(256) k_sweep_lowp_dense(LowpArgs a)
         const uint32_t nb_v[6] = {v - WH, v - (uint32_t)a.W, v - 1u, v + 1u, v + (uint32_t)a.W, v + WH};
         const bool nb_self[6] = {false, false, false, false, false, false};
         const float lr_d = a.adaptive_lr ? a.lr * a.adaptive_lr[v] : a.lr;
-        lowp_quad<PREC, S, TV>(a, v, j, tv_on, nb_v, nb_self, s_bc[0], s_bc[1], lr_d);
+        lowp_quad<PREC, S, TV>(a, v, j, tv_on, nb_v, nb_self, s_bc[0], s_bc[1], lr_d, s_key);
     }
 }
 
@@ -176,7 +182,8 @@ __global__ void __launch_bounds__(256) k_sweep_lowp_sparse(LowpArgs a)
     // A warp takes 32 consecutive compact vertices; each lane works out one vertex's TV
     // neighbourhood and the warp's 32 * S quads take it by shuffle (as the FP32 sparse sweep).
     __shared__ float s_bc[2];
-    lowp_bias_corrections(a.timestep, s_bc);
+    __shared__ uint32_t s_key;
+    lowp_bias_corrections(a, s_bc, &s_key);
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t v0 = warp * 32u;
@@ -198,7 +205,7 @@ __global__ void __launch_bounds__(256) k_sweep_lowp_sparse(LowpArgs a)
         bool nb_self[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) nb_self[k] = (t.flags >> k) & 1u;
-        lowp_quad<PREC, S, TV>(a, v, j, (t.flags >> 6) & 1u, t.nb, nb_self, s_bc[0], s_bc[1], a.lr);
+        lowp_quad<PREC, S, TV>(a, v, j, (t.flags >> 6) & 1u, t.nb, nb_self, s_bc[0], s_bc[1], a.lr, s_key);
     }
 }
 
@@ -236,7 +243,7 @@ static cpx_status launch_lowp_shape(const cpx_grid* g, const LowpArgs& a, bool t
 }
 
 cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
-                           int timestep, uint32_t tv_mask, uint32_t adam_mask, cudaStream_t st)
+                           int timestep, uint32_t tv_mask, uint32_t adam_mask, cudaStream_t st, const int* t_dev)
 {
     if (g->n_act * (g->rec / 4) >= ((int64_t)1 << 32)) {
         set_error("grid too large for 32-bit quad indices");
@@ -269,6 +276,8 @@ cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_
     a.sh_lr = (float)sh_lr;
     a.timestep = timestep;
     a.step_key = fmix32(g->sr_seed ^ ((uint32_t)timestep * 0x9E3779B9u));
+    a.t_dev = t_dev;
+    a.seed = g->sr_seed;
     cpx_status rc = g->prec == kPrecFP16 ? launch_lowp_shape<kPrecFP16>(g, a, fused_tv, st)
                                          : launch_lowp_shape<kPrecBF16>(g, a, fused_tv, st);
     if (rc != CPX_OK) return rc;

@@ -347,6 +347,52 @@ cpx_status cpx_train_step_proposal(cpx_grid* g, cpx_rays* r, cpx_proposal* p, co
                                    const cpx_proposal_schedule* schedule, int iteration, double* losses_dev,
                                    double* mse_out, cpx_stream stream);
 
+/* ---- Batched multi-scene training (no reference counterpart: the reference trains one
+ * scene per process, Experiment.cu).  A batch holds scenes of any grid size and any batch
+ * length -- one precision form, SH band 2 -- and steps all of them together: one placement
+ * and one shading launch over every scene's rays (persistent kernels taking rays from a
+ * work counter), then each scene's TV + Adam sweep.  Iteration i of scene s reads rays
+ * [(i % pool) * len_s, (i + 1) * len_s) of its ray table, pool = floor(n_rays / len_s), and
+ * steps Adam with timestep i + 1: one batched step equals cpx_train_step on every scene with
+ * start = (i % pool) * len_s and no sample index (shuffle the ray table once, on upload).
+ * The iteration counter lives on the device, so a whole step can replay as a CUDA graph. */
+typedef struct cpx_batch cpx_batch;
+typedef struct cpx_batch_scene {
+    cpx_grid* grid;
+    cpx_rays* rays;
+    int rays_per_batch;
+} cpx_batch_scene;
+/* Launch shapes of the batched march: threads per placement block (32..256, a multiple of
+ * 32), warps per shading block (2, 4 or 8) and rays a shading warp takes per work-counter
+ * access (1..8). */
+typedef struct cpx_batch_tuning {
+    int place_block;
+    int shade_warps;
+    int grab;
+} cpx_batch_tuning;
+/* args->timestep is the first iteration's timestep; losses of every step stay on the device
+ * ([sum of rays_per_batch], scene after scene). */
+cpx_status cpx_batch_create(const cpx_batch_scene* scenes, int n_scenes, const cpx_step_args* args,
+                            cpx_batch** out);
+cpx_status cpx_batch_destroy(cpx_batch* b);
+/* One training iteration of every scene.  use_graphs: replay a captured CUDA graph of the
+ * whole iteration (captured on first use, one per parity of the grids' ping-pong buffers,
+ * and re-captured when a grid changed outside the batch). */
+cpx_status cpx_batch_step(cpx_batch* b, int use_graphs, cpx_stream stream);
+/* Per-scene batch MSE of the last step (getMSEError of each scene's losses) into
+ * mse_host[n_scenes].  Synchronous. */
+cpx_status cpx_batch_mse(cpx_batch* b, double* mse_host, cpx_stream stream);
+/* Synchronise and report the sticky device errors of the batch's marches, as cpx_grid_check. */
+cpx_status cpx_batch_check(cpx_batch* b);
+/* The iteration the next step runs (timestep - 1) and the per-step ray and launch totals. */
+cpx_status cpx_batch_info(const cpx_batch* b, int* iteration, int* total_rays, int* launches_per_step);
+cpx_status cpx_batch_set_tuning(cpx_batch* b, const cpx_batch_tuning* t);
+cpx_status cpx_batch_get_tuning(const cpx_batch* b, cpx_batch_tuning* t);
+/* Coordinate-descent search of the launch shapes: every candidate runs steps_per_trial real
+ * training iterations (they advance training like cpx_batch_step), timed with CUDA events;
+ * the fastest shapes are kept and written to best (may be NULL). */
+cpx_status cpx_batch_autotune(cpx_batch* b, int steps_per_trial, cpx_batch_tuning* best, cpx_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

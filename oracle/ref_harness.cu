@@ -474,6 +474,13 @@ int64_t ref_n_active(void* h) { return ((RefCtx*)h)->scene.actualGridNums; }
 int ref_upsample(void* h, float threshold, int low_band_only, int target_sh, float* planar_out)
 {
     RefCtx* c = (RefCtx*)h;
+    // The dense path of initSelfByUpsample (SceneUtils.cu:498-512) sizes the target by
+    // lowBandOnly but hands the kernel src.sh_dim != targetSH_dim as its low-band flag: with
+    // lowBandOnly set and targetSH_dim == src.sh_dim > 1 the kernel writes every coefficient
+    // into a one-coefficient target, past its arrays.  That combination is refused here; the
+    // reference's consistent low-band call is lowBandOnly with targetSH_dim = 1.
+    if (low_band_only && target_sh == c->scene.sh_dim && target_sh > 1) return 1;
+    if (target_sh < 1 || target_sh > c->scene.sh_dim) return 1;
     ObjectScene dst;
     dst.initSelfByUpsample(c->scene, threshold, low_band_only != 0, false, target_sh);
     int rc = fail(cudaDeviceSynchronize());

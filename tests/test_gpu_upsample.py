@@ -28,7 +28,9 @@ def test_upsample_matches_reference_and_oracle(cuda, low_band):
     dst.init_by_upsample(src, threshold=2.0, low_band_only=low_band)
     got = dst.download_params()
     ref = R.RefScene(n, n, n, 9, 2, 0.5, params)
-    want = ref.upsample(2.0, low_band_only=low_band)
+    # the reference's low-band refinement: lowBandOnly with a one-coefficient target (its dense
+    # path takes the kernel's low-band flag from src.sh_dim != targetSH_dim)
+    want = ref.upsample(2.0, low_band_only=low_band, target_sh=1 if low_band else None)
     ref.close()
     assert got.shape == want.shape
     assert np.array_equal(got, want)
