@@ -54,6 +54,12 @@ WORKLOADS = {
     # views; the hidden grid is the same sparse structure with SH ~ N(0, 0.5)
     "sparse512": dict(n=512, gt_n=512, n_blobs=4, gt_sh_std=0.5, cams=100, img=800, batch=16384,
                       pool_batches=16, init_density=0.1, seed=1, sparse_threshold=1.0),
+    # the batched form's workload: 24 dense scenes of uneven size (48^3 .. 192^3) and uneven batch
+    # length (512 .. 4096 rays), each fitted to 8 128x128 views of its own hidden 8-blob grid
+    "multi24": dict(multi=[dict(n=n, gt_n=n, n_blobs=8, gt_sh_std=0.5, cams=8, img=128, batch=b, pool_batches=4,
+                                init_density=0.1, seed=100 + i)
+                           for i, (n, b) in enumerate(zip([48, 64, 80, 96, 112, 128, 160, 192] * 3,
+                                                          [512, 1024, 2048, 768, 1536, 4096] * 4))]),
 }
 # the reference's shipped training constants (SparseVolumeRadianceField/config_linux.txt)
 STEP = dict(mask_coef=1.0, huber=0.1, lam_density=1e-5, lam_sh=1e-6, lr=0.3, sh_lr=1.0)
@@ -118,9 +124,15 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # the timed region starts once the sampler reports (short regions otherwise see none)
+        t_end = time.time() + 3.0
+        while time.time() < t_end and os.path.getsize(self.path) == 0:
+            time.sleep(0.02)
+        self.skip = len(open(self.path).read().splitlines())
 
     def stop(self):
         if not self.proc:
@@ -130,8 +142,12 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        lines = open(self.path).read().splitlines()
+        skip = getattr(self, "skip", 0)
+        # samples taken during the region; a region shorter than the period keeps the last one before it
+        region = lines[skip:] or lines[max(skip - 1, 0):skip]
         rows = []
-        for line in open(self.path).read().splitlines():
+        for line in region:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 9:
                 rows.append(parts)
@@ -467,6 +483,145 @@ def run_ours(args, wl, world, rank, local):
     return result, (scene, pool, R, wl)
 
 
+def run_batched(args, wl, world, rank, local):
+    """The batched multi-scene form: every scene of the workload steps in one batched iteration
+    (cpx_batch_step, graph replay, launch shapes autotuned during warm-up), against the same
+    scenes stepped one after another with cpx_train_step (a launch sequence per scene)."""
+    import torch
+
+    import cpx
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    specs = wl["multi"]
+    scenes, pools, hosts = [], [], []
+    for sw in specs:
+        P = sw["batch"] * sw["pool_batches"]
+        eyes, pix, order = camera_set(sw)
+        gt, _, _ = build_ground_truth(sw, dev, eyes, pix, P)
+        sc = build_training_grid(sw, dev, args.precision, None)
+        pool, packed = build_pool(sc, sw, eyes, pix, order, gt, P)
+        scenes.append(sc)
+        pools.append(pool)
+        hosts.append(torch.from_numpy(packed).pin_memory())
+    lens = [sw["batch"] for sw in specs]
+    total = sum(lens)
+    kw = dict(mask_coef=STEP["mask_coef"], huber_delta=STEP["huber"], lam_density=STEP["lam_density"],
+              lam_sh=STEP["lam_sh"], lr=STEP["lr"], sh_lr=STEP["sh_lr"])
+    K, W = args.steps, args.warmup
+    batch = cpx.Batch([(sc, pl, n) for sc, pl, n in zip(scenes, pools, lens)], timestep=1, **kw)
+    tuning = batch.autotune(steps_per_trial=3, stream=stream)
+    for _ in range(W):
+        batch.step(graphs=True, stream=stream)
+    torch.cuda.synchronize()
+    batch.check()
+
+    def timed(fn):
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for k in range(K):
+            fn(k)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return dist_max(t0.elapsed_time(t1), world, True)
+
+    # ---- timed: batched iterations by graph replay
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = cpx.kernel_launches()
+    ms = timed(lambda k: batch.step(graphs=True, stream=stream))
+    launches = cpx.kernel_launches() - launches0
+    clk = clocks.stop()
+    batch.check()
+    value = world * total * K / (ms / 1e3)
+    eager_ms = timed(lambda k: batch.step(graphs=False, stream=stream))
+    batch.check()
+
+    # ---- the same scenes one after another (cpx_train_step per scene)
+    losses = [torch.zeros(n, dtype=torch.float64, device=dev) for n in lens]
+    it0 = batch.info()["iteration"]
+
+    def sequential(k):
+        it = it0 + k
+        for sc, pl, n, ls, sw in zip(scenes, pools, lens, losses, specs):
+            cpx.train_step(sc, pl, ls, start=(it % sw["pool_batches"]) * n, length=n, timestep=it + 1,
+                           want_mse=False, stream=stream, **kw)
+
+    for k in range(W):
+        sequential(k)
+    seq_ms = timed(sequential)
+    for sc in scenes:
+        sc.check()
+
+    # ---- e2e: per iteration every scene's batch goes host->device into its ray table (pinned
+    # host memory), one batched step, the per-scene MSE back to the host
+    def e2e(k):
+        it = batch.info()["iteration"]
+        for pl, h, n, sw in zip(pools, hosts, lens, specs):
+            b = it % sw["pool_batches"]
+            pl.upload_packed(h[b * n:(b + 1) * n], offset=b * n, stream=stream)
+        batch.step(graphs=True, stream=stream)
+        e2e.mse = batch.mse(stream=stream)
+
+    batch.step(graphs=True, stream=stream)
+    e2e_ms = timed(e2e)
+    batch.check()
+    e2e_value = world * total * K / (e2e_ms / 1e3)
+
+    # ---- step-level roofline: the TV + Adam sweeps' algorithmic bytes (the step's floor) over
+    # the measured step time; touched vertices counted on untimed batches
+    rec = 28 * 4
+    alg = 0.0
+    for sc, pl, n, ls, sw in zip(scenes, pools, lens, losses, specs):
+        cpx.RenderUtils.renderRays_forwardBackward(sc, pl, ls, None, 0, n, STEP["mask_coef"], STEP["huber"],
+                                                   stream=stream)
+        touched = sc.touched_count()
+        N = sc.actual_grid_nums
+        if args.precision == "fp32":
+            alg += N * (6 * rec + 4 + 4) + touched * 2 * rec
+        else:
+            alg += N * (8 + 6 * 28 * 2 + 4) + touched * 2 * rec
+        cpx.Optimizer.varianceAndUpdate(sc, STEP["lam_density"], STEP["lam_sh"], STEP["lr"], STEP["sh_lr"],
+                                        it0 + K + W + 1, stream=stream)
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (ms / K / 1e3) / 1e9
+    info = batch.info()
+    batch.close()
+    sizes = [sw["n"] for sw in specs]
+    result = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.precision == "fp32" else "f32 arithmetic, %s SH + bf16 moments" % args.precision,
+        "data": "synthetic: each scene fitted to its own seeded 8-blob hidden grid rendered by the plain forward",
+        "config": {
+            "workload": "batched multi-scene training: %d dense scenes %d^3..%d^3 SH band 2, %d..%d-ray batches "
+                        "(%d rays per iteration), TV type 0/6 + Adam every iteration, one batched step"
+                        % (len(specs), min(sizes), max(sizes), min(lens), max(lens), total),
+            "scenes": [[sw["n"], sw["batch"]] for sw in specs], "precision": args.precision, "form": "batched",
+            "tuning": tuning, "launches_per_step": info["launches_per_step"],
+            "l2": "inputs larger than L2: the sweeps stream %.1f GB of grid state per step" % (alg / 1e9),
+            "parallelism": "replicas" if world > 1 else "single GPU",
+        },
+        "roofline": {"bound": "hbm", "kernel": "whole batched step against its TV+Adam sweep bytes",
+                     "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "alg_bytes_per_launch": int(alg), "traffic": None,
+                     "launch_ms": round(ms / K, 4)},
+        "batched_eager": {"value": round(world * total * K / (eager_ms / 1e3), 1), "ms_per_step": round(eager_ms / K, 4)},
+        "sequential": {"value": round(world * total * K / (seq_ms / 1e3), 1), "ms_per_step": round(seq_ms / K, 4),
+                       "what": "the same scenes stepped one after another with cpx_train_step"},
+        "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": total * RAY_BYTES,
+                "d2h_bytes_per_step": 8 * len(specs), "last_mse": [round(float(x), 3) for x in e2e.mse]},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "cpu_baseline": None,
+    }
+    return result
+
+
 def proposal_net(args):
     return dict(confidence=args.proposal_confidence, label_weight=args.proposal_label_weight,
                 learning_rate=PROPOSAL_NET["learning_rate"])
@@ -648,8 +803,9 @@ def cpu_baseline(wl, scene, pool, R, args):
 
 
 # --------------------------------------------------------------------------- reference arm
-def run_reference(args, wl):
-    """The reference's own kernels (oracle/_ref/libcpxref.so) through its entry points."""
+def ref_scene(wl):
+    """One training scene on the reference's own kernels: ground truth rendered by its
+    renderRays from the hidden grid, then the training grid and its ray table in batch order."""
     import torch
 
     sys.path.insert(0, str(REPO / "oracle"))
@@ -658,11 +814,6 @@ def run_reference(args, wl):
 
     import cpx_scenes as S
 
-    if not RH.available():
-        return {"impl": "reference", "unavailable": "oracle/_ref/libcpxref.so (reference built for sm_100a) missing"}
-    if wl.get("sparse_threshold") is not None:
-        return {"impl": "reference", "unavailable": "the reference arm runs the dense workloads (its sparse scene "
-                                                    "set-up takes the dense planar grid through host memory)"}
     n, R, P = wl["n"], wl["batch"], wl["batch"] * wl["pool_batches"]
     eyes, pix, order = camera_set(wl)
     img = wl["img"]
@@ -678,7 +829,6 @@ def run_reference(args, wl):
             off += len(p)
         return rays
 
-    # ground truth with the reference's renderRays on the hidden grid
     gt_n = wl["gt_n"]
     gp = gt_params_device(wl, torch.device("cuda")).cpu().numpy()
     torch.cuda.empty_cache()
@@ -691,7 +841,6 @@ def run_reference(args, wl):
     out = gt.rays_download()
     gt.close()
     gr, gg, gb, gm = to_gt_bytes(out["acc_r"], out["acc_g"], out["acc_b"], out["acc_weights"])
-    # training scene and ray table in batch order
     init = np.zeros((1 + 3 * SH_DIM, n ** 3), np.float32)
     init[0] = wl["init_density"]
     sc = RH.RefScene(n, n, n, SH_DIM, 2, 0.5, init)
@@ -701,33 +850,60 @@ def run_reference(args, wl):
     f = {k: tr[k][order] for k in ("ox", "oy", "oz", "dx", "dy", "dz", "near_t", "far_t")}
     sc.rays_create(True, *[f[k] for k in ("ox", "oy", "oz", "dx", "dy", "dz", "near_t", "far_t")],
                    gm[order], gr[order], gg[order], gb[order])
-    losses = np.zeros(R, np.float64)
+    return sc
+
+
+def run_reference(args, wl):
+    """The reference's own kernels (oracle/_ref/libcpxref.so) through its entry points.  A
+    multi-scene workload runs its scenes one after another, as the reference trains them."""
+    import torch
+
+    sys.path.insert(0, str(REPO / "oracle"))
+    import refharness as RH
+
+    if not RH.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcpxref.so (reference built for sm_100a) missing"}
+    if wl.get("sparse_threshold") is not None:
+        return {"impl": "reference", "unavailable": "the reference arm runs the dense workloads (its sparse scene "
+                                                    "set-up takes the dense planar grid through host memory)"}
+    specs = wl["multi"] if "multi" in wl else [wl]
+    scenes = [(ref_scene(sw), sw["batch"], sw["pool_batches"], np.zeros(sw["batch"], np.float64)) for sw in specs]
     K, W = args.steps, args.warmup
+
+    def step(k):
+        mse = None
+        for sc, R, pb, losses in scenes:
+            mse = sc.train_step((k % pb) * R, R, STEP["mask_coef"], STEP["huber"], STEP["lam_density"],
+                                STEP["lam_sh"], 0, 6, True, STEP["lr"], STEP["sh_lr"], k + 1, losses)
+        return mse
+
     for k in range(W):
-        sc.train_step((k % wl["pool_batches"]) * R, R, STEP["mask_coef"], STEP["huber"], STEP["lam_density"],
-                      STEP["lam_sh"], 0, 6, True, STEP["lr"], STEP["sh_lr"], k + 1, losses)
-    sc.sync()
+        step(k)
+    for sc, *_ in scenes:
+        sc.sync()
     clocks = ClockSampler(0)
     clocks.start()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
     for k in range(K):
-        mse = sc.train_step(((W + k) % wl["pool_batches"]) * R, R, STEP["mask_coef"], STEP["huber"],
-                            STEP["lam_density"], STEP["lam_sh"], 0, 6, True, STEP["lr"], STEP["sh_lr"], W + k + 1,
-                            losses)
+        mse = step(W + k)
     t1.record()
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms = t0.elapsed_time(t1)
-    value = R * K / (ms / 1e3)
-    sc.close()
+    total = sum(sw["batch"] for sw in specs)
+    value = total * K / (ms / 1e3)
+    for sc, *_ in scenes:
+        sc.close()
+    multi = "multi" in wl
     return {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
         "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "impl": "reference",
-        "data": "synthetic: seeded 64-blob 512^3 hidden grid rendered by the reference's forward; no dataset",
-        "config": {"workload": "same as --impl ours", "grid": n, "batch_rays": R, "step_constants": STEP,
+        "data": "synthetic: seeded blob hidden grids rendered by the reference's forward; no dataset",
+        "config": {"workload": "same as --impl ours" + (" (the scenes one after another)" if multi else ""),
+                   "grid": None if multi else wl["n"], "batch_rays": total, "step_constants": STEP,
                    "entry_points": "RenderUtils::renderRays, renderRays_withGradients_RGB, losses D2H + "
                                    "getMSEError, addVarianceLoss(type 0, 6), Optimizer::updateRGBScene"},
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": 0, "kind": "reference",
@@ -751,8 +927,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=("fp32", "bf16", "fp16"), default="fp32",
                     help="storage form of the training grid (fp32: the reference's)")
-    ap.add_argument("--form", choices=("plain", "proposal"), default="plain",
-                    help="proposal: the mixed form with the learned sample-interval proposal")
+    ap.add_argument("--form", choices=("plain", "proposal", "batched"), default="plain",
+                    help="proposal: the mixed form with the learned sample-interval proposal; batched: many "
+                         "scenes per step (--workload multi24)")
     ap.add_argument("--proposal-confidence", type=float, default=PROPOSAL_NET["confidence"])
     ap.add_argument("--proposal-label-weight", type=float, default=PROPOSAL_NET["label_weight"])
     ap.add_argument("--quality", type=int, default=0, metavar="N",
@@ -766,7 +943,11 @@ def main():
         ap.error("at least 3 warm-up steps")
     if args.form == "proposal" and args.precision == "fp32":
         ap.error("the proposal form runs on a mixed precision (--precision bf16 or fp16)")
+    if args.form == "batched" and args.workload == "plain256":
+        args.workload = "multi24"
     wl = WORKLOADS[args.workload]
+    if (args.form == "batched") != ("multi" in wl):
+        ap.error("--form batched runs the multi-scene workloads, and they run only batched")
     world, rank, local = dist_setup(use_cuda=True)
     if args.impl == "reference":
         if rank == 0:
@@ -774,6 +955,16 @@ def main():
         if world > 1:
             import torch.distributed as dist
 
+            dist.destroy_process_group()
+        return
+    if args.form == "batched":
+        result = run_batched(args, wl, world, rank, local)
+        if rank == 0:
+            print(json.dumps(result), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
             dist.destroy_process_group()
         return
     if args.quality > 0:
