@@ -190,6 +190,7 @@ _sig("cpx_grid_set_options", [_vp, C.c_int])
 _sig("cpx_grid_upsample", [_vp, _vp, C.c_float, C.c_int, _vp])
 OPT_NO_EMPTY_SKIP = 1  # the FP32 march steps through empty cells one step at a time
 OPT_FP32_MARCH = 2     # an FP32-storage grid marches like the mixed forms
+OPT_NO_EARLY_STOP = 4  # the FP32 march runs every ray to its far bound (no transmittance stop)
 _sig("cpx_train_step_proposal", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), C.POINTER(ProposalSchedule),
                                  C.c_int, _vp, C.POINTER(C.c_double), _vp])
 

@@ -239,6 +239,8 @@ static void free_grid(cpx_grid* g)
     cudaFree(g->compact_to_dense);
     cudaFree(g->brick_bits);
     cudaFree(g->dense_mirror);
+    cudaFree(g->dense_cells);
+    cudaFree(g->dense_bricks);
     for (int i = 0; i < 3; i++) cudaFree(g->off[i]);
     cudaFree(g->scratch.samples);
     cudaFree(g->scratch.colours);
@@ -370,6 +372,8 @@ cpx_status cpx_grid_create(const cpx_grid_desc* d, cpx_grid** out)
         count_launch();
         e = cudaDeviceSynchronize();
     }
+    if (e == cudaSuccess && refresh_dense_skip(g, 0) != CPX_OK) e = cudaErrorMemoryAllocation;
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         cudaGetLastError();
         free_grid(g);
@@ -493,9 +497,11 @@ cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const doub
 
 cpx_status cpx_grid_set_options(cpx_grid* g, int options)
 {
-    if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH))) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH | CPX_OPT_NO_EARLY_STOP))) return CPX_ERR_INVALID_ARGUMENT;
     g->options = options;
-    return CPX_OK;
+    cpx_status rc = refresh_dense_skip(g, 0);  // the maps of a grid now marched with jumps
+    if (rc != CPX_OK) return rc;
+    return cuda_status(cudaDeviceSynchronize(), "options");
 }
 
 cpx_status cpx_grid_set_optimize_step(cpx_grid* g, int optimize_step)

@@ -339,6 +339,11 @@ cpx_status cpx_batch_create(const cpx_batch_scene* scenes, int n_scenes, const c
             delete b;
             return CPX_ERR_INVALID_ARGUMENT;
         }
+        // the empty-space maps exist before any step is captured
+        if (refresh_dense_skip(g, 0) != CPX_OK) {
+            delete b;
+            return CPX_ERR_OUT_OF_MEMORY;
+        }
         b->grids.push_back(g);
         b->rays.push_back(r);
         b->len.push_back(len);

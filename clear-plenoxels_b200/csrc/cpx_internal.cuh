@@ -139,6 +139,11 @@ struct cpx_grid {
     uint32_t* brick_bits = nullptr;
     int bricks[3] = {0, 0, 0};
     int options = 0;  // CPX_OPT_* march options
+    // dense grids, FP32 march: one bit per cell, set unless all eight corner densities are at
+    // or below kEmptyDensity, and the 8x8x8 brick map of those bits (refreshed whenever the
+    // density changes); the march jumps over the cells and bricks they mark empty
+    uint32_t* dense_cells = nullptr;
+    uint32_t* dense_bricks = nullptr;
     // jitter
     double* off[3] = {nullptr, nullptr, nullptr};
     int n_off = 0;
@@ -281,6 +286,10 @@ constexpr uint32_t kMirrorEmpty = 0x7FBADA55u;
 
 // Rebuilds the dense density mirror of a sparse grid from its compact density (occupancy.cu).
 cpx_status refresh_dense_mirror(cpx_grid* g, cudaStream_t st);
+// Dense grids marched by the FP32 march with empty-space jumps: the cell and brick maps of
+// the current density (allocated on first use).  refresh_dense_mirror calls it too.
+bool dense_skip_on(const cpx_grid* g);
+cpx_status refresh_dense_skip(cpx_grid* g, cudaStream_t st);
 
 // ---- batched form (march.cu kernels, batch.cu host side)
 constexpr int kMaxBatchScenes = 64;
@@ -292,7 +301,21 @@ struct Skip {
     // sparse grids: the dense density mirror (kMirrorEmpty outside the cage), so a corner's
     // density is one load; every march form reads it
     const float* __restrict__ dense = nullptr;
+    // FP32 march: a ray stops once its transmittance falls below this (0: marches to far)
+    float t_stop = 0.f;
+    // FP32 march on a dense grid: the cell bits of cpx_grid::dense_cells (bits then holds
+    // their brick map), or null
+    const uint32_t* __restrict__ cells = nullptr;
 };
+
+// Density at or below which a dense grid's cell counts as empty for the FP32 march: the
+// softplus activation gives it at most softplus(-15) = 3.1e-7 per voxel of path, so a ray
+// that crosses a thousand such samples loses under 2e-4 of its transmittance.
+constexpr float kEmptyDensity = -2.0f;
+
+// Transmittance below which the FP32 march of the mixed forms ends a ray: what the samples
+// after it could still add to the colour or the accumulated weight is below this bound.
+constexpr float kStopTransmittance = 1.0e-4f;
 
 // One scene of a batch: its views as of the batch's step parity (the parameter and touched
 // buffers alternate every step).

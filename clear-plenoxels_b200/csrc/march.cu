@@ -43,6 +43,13 @@ __device__ __forceinline__ bool cell_occupied(const GridView& g, unsigned b0, un
     return (g.occ_bits[ci >> 5] >> (ci & 31)) & 1u;
 }
 
+__device__ __forceinline__ bool dense_cell_open(const uint32_t* __restrict__ cells, const GridView& g, unsigned b0,
+                                                unsigned b1, unsigned b2)
+{
+    const int ci = scene_index((int)b0, (int)b1, (int)b2, g.W - 1, g.H - 1, g.D - 1);
+    return (__ldg(cells + (ci >> 5)) >> (ci & 31)) & 1u;
+}
+
 __device__ __forceinline__ int clamp_axis(unsigned b, int n)
 {
     const int v = (int)b;  // getSceneIndex takes int coordinates (RenderUtils.cu:3-13)
@@ -216,7 +223,11 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
         const unsigned b0 = (unsigned int)bc0;
         const unsigned b1 = (unsigned int)bc1;
         const unsigned b2 = (unsigned int)bc2;
-        if (g.sparse && !cell_occupied(g, b0, b1, b2)) {  // RenderUtils.cu:1681-1686
+        // a sparse grid's unoccupied cell (RenderUtils.cu:1681-1686), or -- FP32 march on a
+        // dense grid -- a cell whose corner densities are all at or below kEmptyDensity
+        const bool empty = g.sparse ? !cell_occupied(g, b0, b1, b2)
+                                    : (sk.cells != nullptr && !dense_cell_open(sk.cells, g, b0, b1, b2));
+        if (empty) {
             if (sizeof(Real) == sizeof(float) && sk.bits) {
                 // FP32 march: all the steps through the empty cell (or brick) at once
                 const Real bc[3] = {bc0, bc1, bc2};
@@ -306,6 +317,7 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
         t += fabs(step - w);  // fabs(float) is the float overload
         ++intT;
         ++n;
+        if (Tn < (Real)sk.t_stop) break;  // FP32 march: nothing visible remains behind
     }
     if (write_fwd) {
         r.acc_den[ri] = accDen;
@@ -930,6 +942,14 @@ static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32
     }
     if (g->sparse) gd.skip.dense = g->dense_mirror;
     // the FP32 march jumps over empty cells and bricks of a sparse grid
+    if (gd.march32 && !(g->options & CPX_OPT_NO_EARLY_STOP)) gd.skip.t_stop = kStopTransmittance;
+    if (dense_skip_on(g) && g->dense_cells) {
+        gd.skip.cells = g->dense_cells;
+        gd.skip.bits = g->dense_bricks;
+        gd.skip.bx = (g->W - 1 + 7) / 8;
+        gd.skip.by = (g->H - 1 + 7) / 8;
+        gd.skip.bz = (g->D - 1 + 7) / 8;
+    }
     if (gd.march32 && !(g->options & CPX_OPT_NO_EMPTY_SKIP) && g->sparse && g->brick_bits) {
         gd.skip.bits = g->brick_bits;
         gd.skip.bx = g->bricks[0];
@@ -1111,6 +1131,14 @@ BatchScene batch_scene_view(cpx_grid* g, cpx_rays* r, int len, int pool_batches,
     sc.skip = Skip();
     if (g->sparse) sc.skip.dense = g->dense_mirror;
     const bool march32 = g->prec != kPrecFP32 || (g->options & CPX_OPT_FP32_MARCH);
+    if (march32 && !(g->options & CPX_OPT_NO_EARLY_STOP)) sc.skip.t_stop = kStopTransmittance;
+    if (dense_skip_on(g) && g->dense_cells) {
+        sc.skip.cells = g->dense_cells;
+        sc.skip.bits = g->dense_bricks;
+        sc.skip.bx = (g->W - 1 + 7) / 8;
+        sc.skip.by = (g->H - 1 + 7) / 8;
+        sc.skip.bz = (g->D - 1 + 7) / 8;
+    }
     if (march32 && !(g->options & CPX_OPT_NO_EMPTY_SKIP) && g->sparse && g->brick_bits) {
         sc.skip.bits = g->brick_bits;
         sc.skip.bx = g->bricks[0];

@@ -281,9 +281,62 @@ __global__ void k_dense_mirror(float* mirror, const float* __restrict__ density,
     mirror[d] = in_cage[d] ? density[index_offsets[d]] : __uint_as_float(kMirrorEmpty);
 }
 
+// Dense cell map: thread per cell (whole warps), bit set unless all eight corner densities are
+// at or below kEmptyDensity; a warp's 32 consecutive cells form one word.
+__global__ void k_dense_cells(const float* __restrict__ density, int W, int H, int D, int64_t n_cells,
+                              uint32_t* cells)
+{
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool open = false;
+    if (c < n_cells) {
+        const int cw = W - 1, ch = H - 1;
+        const int x = (int)(c % cw), y = (int)((c / cw) % ch), z = (int)(c / ((int64_t)cw * ch));
+        const int64_t v = ((int64_t)z * H + y) * W + x;
+        const int64_t WH = (int64_t)W * H;
+        const float d[8] = {density[v], density[v + 1], density[v + W], density[v + W + 1], density[v + WH],
+                            density[v + WH + 1], density[v + WH + W], density[v + WH + W + 1]};
+#pragma unroll
+        for (int q = 0; q < 8; q++) open |= d[q] > kEmptyDensity;
+    }
+    const unsigned word = __ballot_sync(0xffffffffu, open);
+    if ((threadIdx.x & 31) == 0 && c < n_cells) cells[c >> 5] = word;
+}
+
+bool dense_skip_on(const cpx_grid* g)
+{
+    const bool march32 = g->prec != kPrecFP32 || (g->options & CPX_OPT_FP32_MARCH);
+    return !g->sparse && march32 && !(g->options & CPX_OPT_NO_EMPTY_SKIP);
+}
+
+cpx_status refresh_dense_skip(cpx_grid* g, cudaStream_t st)
+{
+    if (!dense_skip_on(g)) return CPX_OK;
+    const int cw = g->W - 1, ch = g->H - 1, cd = g->D - 1;
+    const int64_t C = (int64_t)cw * ch * cd;
+    const int bx = (cw + kBrick - 1) / kBrick, by = (ch + kBrick - 1) / kBrick, bz = (cd + kBrick - 1) / kBrick;
+    const int64_t nb = (int64_t)bx * by * bz;
+    if (!g->dense_cells) {
+        if (cudaMalloc((void**)&g->dense_cells, ((C + 31) / 32) * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc((void**)&g->dense_bricks, ((nb + 31) / 32) * sizeof(uint32_t)) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(g->dense_cells);
+            g->dense_cells = nullptr;
+            set_error("empty-space maps could not be allocated");
+            return CPX_ERR_OUT_OF_MEMORY;
+        }
+    }
+    // whole warps in both launches: the warp that writes the last word has no cell (brick)
+    // in its tail threads
+    k_dense_cells<<<(unsigned)((C + 255) / 256), 256, 0, st>>>(g->density, g->W, g->H, g->D, C, g->dense_cells);
+    k_bricks<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(g->dense_cells, cw, ch, cd, bx, by, bz, g->dense_bricks);
+    count_launch(2);
+    return cuda_status(cudaGetLastError(), "empty-space maps");
+}
+
 cpx_status refresh_dense_mirror(cpx_grid* g, cudaStream_t st)
 {
-    if (!g->sparse || !g->dense_mirror) return CPX_OK;
+    if (!g->sparse) return refresh_dense_skip(g, st);
+    if (!g->dense_mirror) return CPX_OK;
     k_dense_mirror<<<(unsigned)((g->n_dense + 255) / 256), 256, 0, st>>>(g->dense_mirror, g->density, g->in_cage,
                                                                           g->index_offsets, g->n_dense);
     count_launch();

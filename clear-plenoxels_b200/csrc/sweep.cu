@@ -251,7 +251,8 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
     if (g->prec != kPrecFP32) {
         uint32_t tvm, am;
         element_masks(g, &tvm, &am);
-        return sweep_adam_lowp(g, fused_tv, lam_d, lam_sh, lr, sh_lr, timestep, tvm, am, st, t_dev);
+        cpx_status rc = sweep_adam_lowp(g, fused_tv, lam_d, lam_sh, lr, sh_lr, timestep, tvm, am, st, t_dev);
+        return rc == CPX_OK ? refresh_dense_skip(g, st) : rc;  // the new density's empty cells
     }
     const int S = g->rec / 4;
     if (g->n_act * S >= ((int64_t)1 << 32)) {
@@ -295,7 +296,8 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
     g->cur ^= 1;
     g->tcur ^= 1;
     g->all_touched = 0;
-    return cuda_status(cudaGetLastError(), "adam sweep");
+    cpx_status rc = cuda_status(cudaGetLastError(), "adam sweep");
+    return rc == CPX_OK ? refresh_dense_skip(g, st) : rc;
 }
 
 // ---------------------------------------------------------------------------

@@ -224,9 +224,14 @@ cpx_status cpx_grid_upsample(const cpx_grid* src, cpx_grid* dst, float threshold
  * CPX_OPT_NO_EMPTY_SKIP  the FP32 march steps through every empty cell of a sparse grid as
  *                        the reference does, instead of jumping over empty cells and bricks;
  * CPX_OPT_FP32_MARCH     an FP32-storage grid marches like the mixed forms (FP32 arithmetic,
- *                        empty-space jumps) instead of the reference's FP64/FP32 sequence. */
+ *                        empty-space jumps, early stop) instead of the reference's FP64/FP32
+ *                        sequence;
+ * CPX_OPT_NO_EARLY_STOP  the FP32 march runs every ray to its far bound, instead of ending it
+ *                        once its transmittance is below 1e-4 (what the rest of the ray could
+ *                        add to its colour and weight). */
 #define CPX_OPT_NO_EMPTY_SKIP 1
 #define CPX_OPT_FP32_MARCH 2
+#define CPX_OPT_NO_EARLY_STOP 4
 cpx_status cpx_grid_set_options(cpx_grid* g, int options);
 
 /* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,

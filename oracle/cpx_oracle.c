@@ -1025,6 +1025,18 @@ static int empty_steps64(const orc_bricks* bk, const double bc[3], const double 
     return n < 1. ? 1 : (n > 1e6 ? 1000000 : (int)n);
 }
 
+/* The dense empty-cell map of the FP32 march: is the cell at bc open?  Cell coordinates as
+ * the march truncates them, clamped to the cell range (getSceneIndex on cells). */
+static int dense_open64(const orc_scene* s, const orc_bricks* bk, const double bc[3])
+{
+    if (!bk || !bk->cells || s->sparse) return 1;
+    const int64_t cw = s->W - 1, ch = s->H - 1, cd = s->D - 1;
+    int64_t c[3] = {(int64_t)sat_u32(bc[0]), (int64_t)sat_u32(bc[1]), (int64_t)sat_u32(bc[2])};
+    const int64_t n[3] = {cw, ch, cd};
+    for (int a = 0; a < 3; a++) c[a] = c[a] > n[a] - 1 ? n[a] - 1 : c[a];
+    return bk->cells[(c[2] * ch + c[1]) * cw + c[0]] != 0;
+}
+
 static void ray64(const orc_scene* s, const orc_rays* r, const orc_bricks* bk, int tid, int ri, double mask_coef,
                   double huber, double* pred, double* accw_out, double* losses, double* grad)
 {
@@ -1045,8 +1057,8 @@ static void ray64(const orc_scene* s, const orc_rays* r, const orc_bricks* bk, i
     while (t < far_t) {
         double bc[3];
         for (int a = 0; a < 3; a++) bc[a] = o[a] + t * d[a];
-        if (!trilerp64(s, bc, shs, tri, wq, iq)) {
-            t += bk ? empty_steps64(bk, bc, d, step) * step : step;
+        if (!dense_open64(s, bk, bc) || !trilerp64(s, bc, shs, tri, wq, iq)) {
+            t += bk && bk->bits ? empty_steps64(bk, bc, d, step) * step : step;
             continue;
         }
         const double sigma = softplus64(tri[0]);
@@ -1055,6 +1067,7 @@ static void ray64(const orc_scene* s, const orc_rays* r, const orc_bricks* bk, i
         for (int c = 0; c < 3; c++) rgb[c] += w * sigmoid64(tri[1 + c]);
         accd += sigma * step;
         t += fabs(step - w);
+        if (bk && exp(-accd) < bk->t_stop) break;
     }
     const double bg = r->white_bg ? 1. - acc : 0.;
     for (int c = 0; c < 3; c++) pred[3 * tid + c] = rgb[c] + bg;
@@ -1087,8 +1100,8 @@ static void ray64(const orc_scene* s, const orc_rays* r, const orc_bricks* bk, i
     while (t < far_t) {
         double bc[3];
         for (int a = 0; a < 3; a++) bc[a] = o[a] + t * d[a];
-        if (!trilerp64(s, bc, shs, tri, wq, iq)) {
-            t += bk ? empty_steps64(bk, bc, d, step) * step : step;
+        if (!dense_open64(s, bk, bc) || !trilerp64(s, bc, shs, tri, wq, iq)) {
+            t += bk && bk->bits ? empty_steps64(bk, bc, d, step) * step : step;
             continue;
         }
         const double sigma = softplus64(tri[0]);
@@ -1121,6 +1134,7 @@ static void ray64(const orc_scene* s, const orc_rays* r, const orc_bricks* bk, i
             }
         }
         t += fabs(step - w);
+        if (bk && Tn < bk->t_stop) break;
     }
 }
 

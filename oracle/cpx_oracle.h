@@ -152,12 +152,17 @@ void orc_composite_kat(const double* opacity, const double* colour /*[3][n]*/, i
  * measured against.  pred [len][3] (background included), accw [len], losses [len],
  * grad planar [n_arrays][n_act] (accumulated into). */
 typedef struct orc_bricks {
-    const uint8_t* bits; /* one byte per 8x8x8-cell brick: any cell occupied */
+    const uint8_t* bits; /* one byte per 8x8x8-cell brick: any cell occupied (NULL: no jumps) */
     int bx, by, bz;
+    double t_stop;       /* a ray ends once its transmittance is below this (0: never) */
+    const uint8_t* cells; /* dense grid: one byte per cell, 0 when every corner density is at or
+                             below the empty bound -- such cells are jumped like unoccupied ones
+                             (NULL: none) */
 } orc_bricks;
-/* bricks non-NULL: the FP32 march of the mixed forms on a sparse grid, which moves through an
- * empty cell (or through its whole brick when the brick is empty) in one jump of whole steps,
- * leaving the sample sequence of step-by-step stepping unchanged. */
+/* bricks non-NULL: the FP32 march of the mixed forms.  With bits, on a sparse grid it moves
+ * through an empty cell (or through its whole brick when the brick is empty) in one jump of
+ * whole steps, leaving the sample sequence of step-by-step stepping unchanged; with t_stop it
+ * ends a ray after the sample that takes its transmittance below t_stop. */
 void orc64_forward_backward(const orc_scene* s, const orc_rays* r, const orc_bricks* bricks, int start,
                             int len, double mask_coef, double huber, double* pred, double* accw,
                             double* losses, double* grad);

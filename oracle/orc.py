@@ -73,7 +73,8 @@ _fn("orc_composite_kat", [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _fn("orc_render_image", [C.POINTER(_Scene)] + [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
 _fn("orc_upsample", [C.POINTER(_Scene), C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp])
 class _Bricks(C.Structure):
-    _fields_ = [("bits", _vp), ("bx", C.c_int), ("by", C.c_int), ("bz", C.c_int)]
+    _fields_ = [("bits", _vp), ("bx", C.c_int), ("by", C.c_int), ("bz", C.c_int), ("t_stop", C.c_double),
+                ("cells", _vp)]
 
 
 _fn("orc64_forward_backward", [C.POINTER(_Scene), C.POINTER(_Rays), C.POINTER(_Bricks), C.c_int, C.c_int, C.c_double,
@@ -206,12 +207,29 @@ def brick_map(occ, W, H, D):
     return np.ascontiguousarray(b.reshape(-1), np.uint8), (bx, by, bz)
 
 
+# transmittance below which the FP32 march of the mixed forms ends a ray (its default)
+MIXED_T_STOP = 1.0e-4
+# density at or below which a dense grid's cell is empty for the FP32 march (all 8 corners)
+EMPTY_DENSITY = np.float32(-2.0)
+
+
+def dense_open_cells(density, W, H, D):
+    """One byte per cell of a dense grid: 1 unless all eight corner densities are at or below
+    EMPTY_DENSITY (the FP32 march's dense empty-cell map)."""
+    d = np.asarray(density, np.float32).reshape(D, H, W) > EMPTY_DENSITY
+    o = (d[:-1, :-1, :-1] | d[:-1, :-1, 1:] | d[:-1, 1:, :-1] | d[:-1, 1:, 1:] | d[1:, :-1, :-1] | d[1:, :-1, 1:]
+         | d[1:, 1:, :-1] | d[1:, 1:, 1:])
+    return np.ascontiguousarray(o.reshape(-1), np.uint8)
+
+
 def fp64_step(scene: Scene, rays: RaySet, mask_coef, huber, lam_d=None, lam_sh=None, lr=None, sh_lr=None,
-              timestep=1, start=0, length=None, skip_empty=False):
+              timestep=1, start=0, length=None, skip_empty=False, t_stop=0.0):
     """The FP64 host oracle of one training batch: forward+backward over rays[start:start+length]
-    (skip_empty: the mixed forms' jumps over empty cells and bricks of a sparse grid), then (when
-    lr is given) TV type 0 / 6 neighbours (when lam_d is given) and Adam from zero moments.  Returns pred [len, 3], accw, losses, grad [n_arrays, n_act] (before TV/Adam) and
-    the post-step parameters (float64) or None."""
+    (skip_empty: the mixed forms' jumps over empty cells and bricks of a sparse grid; t_stop: their
+    end of a ray once its transmittance falls below t_stop), then (when lr is given) TV type 0 / 6
+    neighbours (when lam_d is given) and Adam from zero moments.  Returns pred [len, 3], accw,
+    losses, grad [n_arrays, n_act] (before TV/Adam) and the post-step parameters (float64) or
+    None."""
     length = rays.n - start if length is None else length
     na = 1 + 3 * scene.sh_dim
     pred = np.zeros((length, 3), np.float64)
@@ -221,7 +239,13 @@ def fp64_step(scene: Scene, rays: RaySet, mask_coef, huber, lam_d=None, lam_sh=N
     bk = None
     if skip_empty and scene.sparse:
         bits, (bx, by, bz) = brick_map(scene.occ, scene.W, scene.H, scene.D)
-        bk = _Bricks(bits.ctypes.data, bx, by, bz)
+        bk = _Bricks(bits.ctypes.data, bx, by, bz, float(t_stop), None)
+    elif skip_empty:
+        cells = dense_open_cells(scene.params[0], scene.W, scene.H, scene.D)
+        bits, (bx, by, bz) = brick_map(cells, scene.W, scene.H, scene.D)
+        bk = _Bricks(bits.ctypes.data, bx, by, bz, float(t_stop), cells.ctypes.data)
+    elif t_stop > 0:
+        bk = _Bricks(None, 0, 0, 0, float(t_stop), None)
     _lib.orc64_forward_backward(C.byref(scene.c), C.byref(rays.c), C.byref(bk) if bk is not None else None,
                                 int(start), int(length), float(mask_coef), float(huber), _p(pred), _p(accw),
                                 _p(losses), _p(grad))

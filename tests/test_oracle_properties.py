@@ -197,3 +197,57 @@ def test_empty_space_jumps_keep_the_sample_sequence():
     assert np.abs(a[0] - b[0]).max() < 1e-9
     assert np.abs(a[3] - b[3]).max() <= 1e-9 * np.abs(a[3]).max()
     assert np.abs(a[0] - 1.0).max() > 0.05  # the rays see the blobs
+
+
+def test_early_stop_bounds_the_colour_change():
+    """Ending a ray once its transmittance is below t_stop changes its colour and accumulated
+    weight by at most t_stop (all that the rest of the ray could add, against the white
+    background it would otherwise show); with t_stop 0 nothing changes."""
+    cfg = S.small_config(seed=9, n=48, n_cams=4, img=40, n_rays=400)
+    n = cfg["W"]
+    params = cfg["params"].copy()
+    params[0] *= 4.0  # opaque blobs: many rays end well before their far bound
+    sc = orc.Scene(n, n, n, 9, params, step=0.5)
+    nr = sum(len(p) for p in cfg["pix"])
+    rays = orc.RaySet(nr, True)
+    off = 0
+    for cam, img, pix in zip(cfg["cams"], cfg["images"], cfg["pix"]):
+        orc.rays_from_camera(cam, cfg["bbox"], cfg["img_w"], *img, True, pix, rays, off)
+        off += len(pix)
+    full = orc.fp64_step(sc, rays, 1.0, 0.1)
+    same = orc.fp64_step(sc, rays, 1.0, 0.1, t_stop=0.0)
+    # (the oracle's threads add gradients in any order: equal up to that rounding)
+    assert np.array_equal(full[0], same[0])
+    assert np.abs(full[3] - same[3]).max() <= 1e-12 * np.abs(full[3]).max()
+    stop = orc.fp64_step(sc, rays, 1.0, 0.1, t_stop=orc.MIXED_T_STOP)
+    assert np.abs(full[0] - stop[0]).max() <= orc.MIXED_T_STOP
+    assert np.abs(full[1] - stop[1]).max() <= orc.MIXED_T_STOP
+    assert (full[1] > 1 - orc.MIXED_T_STOP).mean() > 0.05  # some rays do end early
+    # the gradients change only through the samples past the stop and the loss they shift
+    assert np.linalg.norm(full[3] - stop[3]) <= 1e-2 * np.linalg.norm(full[3])
+
+
+def test_dense_empty_cells_change_little():
+    """On a dense grid the FP32 march jumps over cells whose eight corner densities are all at
+    or below EMPTY_DENSITY (-2): each such sample would add at most softplus(-15) * step to the
+    optical depth, so the image moves by far less than 1e-4 while the empty cells are skipped."""
+    cfg = S.small_config(seed=10, n=48, n_cams=4, img=40, n_rays=400)
+    n = cfg["W"]
+    params = cfg["params"].copy()
+    params[0] -= 6.0  # empty space well below the bound, blob cores above it
+    sc = orc.Scene(n, n, n, 9, params, step=0.5)
+    cells = orc.dense_open_cells(params[0], n, n, n)
+    assert 0.01 < cells.mean() < 0.6
+    nr = sum(len(p) for p in cfg["pix"])
+    rays = orc.RaySet(nr, True)
+    off = 0
+    for cam, img, pix in zip(cfg["cams"], cfg["images"], cfg["pix"]):
+        orc.rays_from_camera(cam, cfg["bbox"], cfg["img_w"], *img, True, pix, rays, off)
+        off += len(pix)
+    full = orc.fp64_step(sc, rays, 1.0, 0.1)
+    jump = orc.fp64_step(sc, rays, 1.0, 0.1, skip_empty=True)
+    assert np.abs(full[0] - jump[0]).max() < 2e-5
+    assert np.abs(full[1] - jump[1]).max() < 2e-5
+    assert np.abs(full[0] - 1.0).max() > 0.05  # the rays see the blobs
+    # the gradients agree on the vertices of open cells; the skipped ones lose tiny terms
+    assert np.linalg.norm(full[3] - jump[3]) <= 2e-3 * np.linalg.norm(full[3])
