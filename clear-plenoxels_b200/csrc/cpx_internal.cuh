@@ -308,10 +308,11 @@ struct Skip {
     const uint32_t* __restrict__ cells = nullptr;
 };
 
-// Density at or below which a dense grid's cell counts as empty for the FP32 march: the
-// softplus activation gives it at most softplus(-15) = 3.1e-7 per voxel of path, so a ray
-// that crosses a thousand such samples loses under 2e-4 of its transmittance.
-constexpr float kEmptyDensity = -2.0f;
+// Density at or below which a dense grid's cell counts as empty for the FP32 march.  The
+// optimizer clamps density at 0 (Optimizer.cu:384), so trained empty space sits exactly there;
+// the softplus activation gives it softplus(-13) = 2.3e-6 per voxel of path, so a sample there
+// carries a weight of at most 1.2e-6 (step 0.5).
+constexpr float kEmptyDensity = 0.0f;
 
 // Transmittance below which the FP32 march of the mixed forms ends a ray: what the samples
 // after it could still add to the colour or the accumulated weight is below this bound.

@@ -64,42 +64,11 @@ __device__ __forceinline__ uint16_t f_to_sh_rn(float x)
     return PREC == kPrecFP16 ? f_to_h16_rn(x) : f_to_bf16_rn(x);
 }
 
-// Stochastic rounding (both forms take 16 random bits in the low half of rnd).
-// To bfloat16: add the random bits below the kept mantissa and truncate (the magnitude
-// rounds up with probability equal to the dropped fraction).
-__device__ __forceinline__ uint16_t f_to_bf16_sr(float x, uint32_t rnd)
-{
-    const uint32_t b = __float_as_uint(x);
-    if ((b & 0x7f800000u) == 0x7f800000u) return f_to_bf16_rn(x);  // inf / NaN
-    return (uint16_t)((b + (rnd & 0xffffu)) >> 16);
-}
-
-// Stochastic rounding to half: between the value rounded toward zero and the next half
-// away from zero, pick the upper one with probability (|x| - |lo|) / (|hi| - |lo|)
-// (compared as u * (|hi| - |lo|) < |x| - |lo|, no division).
-__device__ __forceinline__ uint16_t f_to_h16_sr(float x, uint32_t rnd)
-{
-    const __half lo = __float2half_rz(x);
-    const float lf = __half2float(lo);
-    if (lf == x || !isfinite(x)) return f_to_h16_rn(x);
-    const uint16_t lb = __half_as_ushort(lo);
-    const uint16_t hb = (uint16_t)(lb + 1u);  // same sign, one unit further from zero
-    const float hf = __half2float(__ushort_as_half(hb));
-    const float u = (float)(rnd & 0xffffu) * (1.f / 65536.f);
-    return u * (fabsf(hf) - fabsf(lf)) < fabsf(x) - fabsf(lf) ? hb : lb;
-}
-
 // Cheap 32-bit mixer for words drawn from one hashed counter (multiply, xorshift).
 __device__ __forceinline__ uint32_t draw32(uint32_t h, uint32_t k)
 {
     uint32_t w = (h ^ (h >> 15)) * k;
     return w ^ (w >> 13);
-}
-
-template <int PREC>
-__device__ __forceinline__ uint16_t f_to_sh_sr(float x, uint32_t rnd)
-{
-    return PREC == kPrecFP16 ? f_to_h16_sr(x, rnd) : f_to_bf16_sr(x, rnd);
 }
 
 // 4 packed 16-bit values (one quad) <-> floats
@@ -110,6 +79,35 @@ __device__ __forceinline__ void unpack4(const uint2& q, float* f)
     f[1] = sh_to_f<PREC>((uint16_t)(q.x >> 16));
     f[2] = sh_to_f<PREC>((uint16_t)(q.y & 0xffffu));
     f[3] = sh_to_f<PREC>((uint16_t)(q.y >> 16));
+}
+
+// Two floats -> one 32-bit word of two 16-bit values (lo in bits 0..15) with stochastic
+// rounding by the sm_100a conversion cvt.rs, which rounds each magnitude up with probability
+// equal to the dropped fraction, drawing on the random word rbits.  Values already
+// representable convert exactly; NaN stays NaN and overflow goes to infinity.
+template <int PREC>
+__device__ __forceinline__ uint32_t sr_pack2(float lo, float hi, uint32_t rbits)
+{
+    uint32_t d;
+    if (PREC == kPrecFP16)
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    else
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+
+// One 32-bit word of two 16-bit values -> floats (lo from bits 0..15).
+template <int PREC>
+__device__ __forceinline__ void unpack2(uint32_t w, float& lo, float& hi)
+{
+    if (PREC == kPrecFP16) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w));
+        lo = f.x;
+        hi = f.y;
+    } else {
+        lo = __uint_as_float(w << 16);
+        hi = __uint_as_float(w & 0xffff0000u);
+    }
 }
 
 __device__ __forceinline__ uint2 pack4(const uint16_t* h)

@@ -3,12 +3,16 @@
 // Same order of operations as the FP32 sweep (TV term added to the gradient, then Adam
 // with the reference's bias corrections and density clamp, Optimizer.cu:359-415), over the
 // mixed storage: density FP32, SH in 16-bit records, gradients in FP32 records, moments in
-// bfloat16 records.  Like the FP32 sweep, a thread owns 4 consecutive parameters (one quad)
-// of one vertex: it reads their SH (8 B), gradients (16 B), moments (2 x 8 B), and for quad 0
-// the density, applies TV and Adam in FP32, and writes the new SH, moments and density back
-// with stochastic rounding to 16 bits, zeroing the gradients it consumed.  Per vertex at SH
-// band 2: density r+w 8 B, SH r+w 112 B, gradients r + zero-w 224 B, moments r+w 224 B
-// (+4 B learning-rate multiplier on dense grids): 572 B against the FP32 form's 904 B.
+// bfloat16 records.  A warp takes 32 consecutive vertices: each lane first works out one
+// vertex's own part (touched bit, learning rate, the FP32 density and its TV term), then the
+// warp's lanes each update one quad (4 consecutive slots) of those vertices, taking the vertex
+// part by shuffle: the quad's SH (8 B), gradients (16 B, touched vertices only), moments
+// (2 x 8 B) and its six TV neighbours' SH quads; TV and Adam run in FP32 (packed FP32 pairs
+// where every slot takes both), and the new SH and moments go back to 16 bits by the
+// hardware's stochastic-rounding conversion, the consumed gradients zeroed.  Per vertex at SH
+// band 2: density r+w 8 B, SH r+w 112 B, moments r+w 224 B (+4 B learning-rate multiplier on
+// dense grids), gradients r + zero-w 224 B where touched: 348 B (+224 B) against the FP32
+// form's 684 B (+224 B).
 #include "cpx_internal.cuh"
 
 namespace cpx {
@@ -36,105 +40,280 @@ struct LowpArgs {
     uint32_t step_key;  // hash of (stochastic-rounding seed, timestep)
     const int* t_dev;   // when set, the timestep is *t_dev + 1 (a replayed CUDA graph)
     uint32_t seed;
+    int full_masks;     // TV and Adam apply to every slot of every quad (no padding, no hierarchy)
 };
-
-__device__ __forceinline__ void bits4(const uint2& q, uint16_t* h)
-{
-    h[0] = (uint16_t)(q.x & 0xffffu);
-    h[1] = (uint16_t)(q.x >> 16);
-    h[2] = (uint16_t)(q.y & 0xffffu);
-    h[3] = (uint16_t)(q.y >> 16);
-}
 
 // Square root through the hardware reciprocal square root (about 2 ulp; the results are
 // stored in 16 bits), 0 for 0.
 __device__ __forceinline__ float fast_sqrt(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
 
-// Quad j (record slots 4j..4j+3) of vertex v; S quads per record.  The six-neighbour TV term (RenderUtils.cu:2672-2757, neighbours in
-// the reference's order z-1, y-1, x-1, x+1, y+1, z+1) streams one neighbour quad at a time.
-template <int PREC, int S, bool TV>
-__device__ __forceinline__ void lowp_quad(const LowpArgs& a, uint32_t v, int j, bool tv_on,
-                                          const uint32_t* nb_v, const bool* nb_self, float inv_bc1,
-                                          float inv_bc2, float lr_density, uint32_t step_key)
+// Per-vertex part of the sweep, worked out once by the lane that owns the vertex and handed
+// to the lanes of its quads by shuffle: the touched bit, whether the TV term applies, the
+// density learning rate, the density itself and its TV term (RenderUtils.cu:2672-2757,
+// neighbours in the reference's order z-1, y-1, x-1, x+1, y+1, z+1).
+struct LowpVertex {
+    float dens;     // FP32 density
+    float tv0;      // TV term of the density (0 when it does not apply)
+    float lr_d;     // density learning rate (adaptive multiplier included)
+    uint32_t bits;  // bit 0: touched; bit 1: TV applies; bits 2..7: neighbour k reads the vertex itself
+};
+
+template <bool TV>
+__device__ __forceinline__ LowpVertex lowp_vertex(const LowpArgs& a, uint32_t v, bool tv_on, const uint32_t* nb_v,
+                                                  uint32_t self_bits, float lr_d)
 {
-    const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
-    const size_t q = (size_t)v * S + j;
-    const uint2 sh_raw = a.sh_in[q];
-    uint16_t sh_bits[4];
-    bits4(sh_raw, sh_bits);
-    float p[4];
-    unpack4<PREC>(sh_raw, p);
-    if (j == 0) p[0] = a.d_in[v];  // slot 0 of an SH record is unused: density is FP32
-    // untouched vertices have zero gradients: their records are neither read nor written
-    const bool tch = touched_bit(a.touched, v);
-    if (a.clear && j == 0 && (v & 31u) == 0) a.clear[v >> 5] = 0u;
-    const float4 g4 = tch ? a.grad[(size_t)v * S + j] : make_float4(0.f, 0.f, 0.f, 0.f);
-    float g[4] = {g4.x, g4.y, g4.z, g4.w};
-    uint16_t m_bits[4], v_bits[4];
-    bits4(a.m[q], m_bits);
-    bits4(a.v[q], v_bits);
-    if (TV && tv_on) {
-        float sum[4] = {0.f, 0.f, 0.f, 0.f}, disp[4] = {0.f, 0.f, 0.f, 0.f};
+    LowpVertex r;
+    r.dens = __ldg(a.d_in + v);
+    r.lr_d = lr_d;
+    r.tv0 = 0.f;
+    r.bits = (touched_bit(a.touched, v) ? 1u : 0u) | (tv_on ? 2u : 0u) | (self_bits << 2);
+    if (TV && tv_on && (a.tv_mask & 1u)) {
+        float sum = 0.f, disp = 0.f;
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-            float nb[4];
-            if (nb_self[k]) {
+            const float nb = ((self_bits >> k) & 1u) ? r.dens : __ldg(a.d_in + nb_v[k]);
+            const float d = r.dens - nb;
+            sum += d * d;
+            disp = (k == 0) ? d : disp + d;
+        }
+        const float sd = fast_sqrt(sum) * (1.f / 6.f);
+        r.tv0 = __fdividef(a.lam_d * disp, sd + 1.e-6f);
+    }
+    return r;
+}
+
+__device__ __forceinline__ LowpVertex shfl_vertex(const LowpVertex& mine, int from_lane)
+{
+    LowpVertex r;
+    r.dens = __shfl_sync(0xffffffffu, mine.dens, from_lane);
+    r.tv0 = __shfl_sync(0xffffffffu, mine.tv0, from_lane);
+    r.lr_d = __shfl_sync(0xffffffffu, mine.lr_d, from_lane);
+    r.bits = __shfl_sync(0xffffffffu, mine.bits, from_lane);
+    return r;
+}
+
+// A thread's unit of a record: E = 4 slots (a quad: 8 B of 16-bit values, 16 B of gradients)
+// or E = 2 slots (a pair: 4 B and 8 B).
+template <int E> struct Unit;
+template <> struct Unit<4> {
+    using H = uint2;   // E 16-bit values
+    using F = float4;  // E floats
+    __device__ static void unpack_bf16(const H& w, float* f) { unpack2<kPrecBF16>(w.x, f[0], f[1]); unpack2<kPrecBF16>(w.y, f[2], f[3]); }
+    template <int PREC> __device__ static void unpack(const H& w, float* f) { unpack2<PREC>(w.x, f[0], f[1]); unpack2<PREC>(w.y, f[2], f[3]); }
+    template <int PREC> __device__ static H pack(const float* f, uint32_t r0, uint32_t r1)
+    {
+        return make_uint2(sr_pack2<PREC>(f[0], f[1], r0), sr_pack2<PREC>(f[2], f[3], r1));
+    }
+    __device__ static void floats(const F& g, float* f) { f[0] = g.x; f[1] = g.y; f[2] = g.z; f[3] = g.w; }
+    __device__ static F make(const float* f) { return make_float4(f[0], f[1], f[2], f[3]); }
+};
+template <> struct Unit<2> {
+    using H = uint32_t;
+    using F = float2;
+    __device__ static void unpack_bf16(const H& w, float* f) { unpack2<kPrecBF16>(w, f[0], f[1]); }
+    template <int PREC> __device__ static void unpack(const H& w, float* f) { unpack2<PREC>(w, f[0], f[1]); }
+    template <int PREC> __device__ static H pack(const float* f, uint32_t r0, uint32_t) { return sr_pack2<PREC>(f[0], f[1], r0); }
+    __device__ static void floats(const F& g, float* f) { f[0] = g.x; f[1] = g.y; }
+    __device__ static F make(const float* f) { return make_float2(f[0], f[1]); }
+};
+
+// Unit u (record slots E*u .. E*u+E-1) of vertex v, unit index q = v * U + u; nbq: the same
+// unit of the six TV neighbours.  Slot 0 is the density: its value, TV term and learning rate
+// come from the vertex's LowpVertex, its moments from the unit's moment records.
+template <int PREC, int E, bool TV>
+__device__ __forceinline__ void lowp_unit(const LowpArgs& a, uint32_t v, uint32_t q, int u, const LowpVertex& vx,
+                                          const uint32_t* nbq, float inv_bc1, float inv_bc2, uint32_t step_key)
+{
+    using UT = Unit<E>;
+    using H = typename UT::H;
+    using F = typename UT::F;
+    const H* sh_in = reinterpret_cast<const H*>(a.sh_in);
+    H* sh_out = reinterpret_cast<H*>(a.sh_out);
+    H* mrec = reinterpret_cast<H*>(a.m);
+    H* vrec = reinterpret_cast<H*>(a.v);
+    F* grad = reinterpret_cast<F*>(a.grad);
+    const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
+    // every record a unit reads is written only by the same thread after the read (or not at
+    // all), so all of them load through the non-coherent path
+    float p[E];
+    UT::template unpack<PREC>(__ldg(sh_in + q), p);
+    if (u == 0) p[0] = vx.dens;  // slot 0 of an SH record is unused: density is FP32
+    // untouched vertices have zero gradients: their records are neither read nor written
+    const bool tch = vx.bits & 1u;
+    float g[E];
+    if (tch) {
+        UT::floats(__ldg(grad + q), g);
+    } else {
 #pragma unroll
-                for (int c = 0; c < 4; c++) nb[c] = p[c];
+        for (int c = 0; c < E; c++) g[c] = 0.f;
+    }
+    float mo[E], vo[E];
+    UT::unpack_bf16(__ldg(mrec + q), mo);
+    UT::unpack_bf16(__ldg(vrec + q), vo);
+    if (TV && (vx.bits & 2u)) {
+        float sum[E], disp[E];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            float nb[E];
+            if ((vx.bits >> (2 + k)) & 1u) {
+#pragma unroll
+                for (int c = 0; c < E; c++) nb[c] = p[c];
             } else {
-                const size_t nq = (size_t)nb_v[k] * S + j;
-                unpack4<PREC>(a.sh_in[nq], nb);
-                if (j == 0) nb[0] = a.d_in[nb_v[k]];
+                UT::template unpack<PREC>(__ldg(sh_in + nbq[k]), nb);
             }
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
+            for (int c = 0; c < E; c++) {
                 const float d = p[c] - nb[c];
-                sum[c] += d * d;
+                sum[c] = (k == 0) ? d * d : fmaf(d, d, sum[c]);
                 disp[c] = (k == 0) ? d : disp[c] + d;
             }
         }
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const int e = 4 * j + c;
-            if ((a.tv_mask >> e) & 1u) {
+        for (int c = 0; c < E; c++) {
+            const int e = E * u + c;
+            if (e != 0 && ((a.tv_mask >> e) & 1u)) {
                 const float sd = fast_sqrt(sum[c]) * (1.f / 6.f);
-                g[c] += __fdividef((e == 0 ? a.lam_d : a.lam_sh) * disp[c], sd + 1.e-6f);
+                g[c] += __fdividef(a.lam_sh * disp[c], sd + 1.e-6f);
             }
         }
     }
-    // random bits: one hash of (launch key, vertex, quad), then one cheap draw per element
-    const uint32_t h1 = fmix32(step_key ^ (v * 0x632BE5ABu) ^ ((uint32_t)j << 28));
+    if (u == 0) g[0] += vx.tv0;
+    // Adam; elements outside the mask keep their values, which convert back exactly
+    float np[E], mn[E], vn[E];
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-        const int e = 4 * j + c;
+    for (int c = 0; c < E; c++) {
+        const int e = E * u + c;
+        np[c] = p[c];
+        mn[c] = mo[c];
+        vn[c] = vo[c];
         if (!((a.adam_mask >> e) & 1u)) continue;
         const float gc = g[c];
-        const float mc = fmaf(1.f - beta1, gc, beta1 * bf16_to_f(m_bits[c]));
-        const float vc = fmaf((1.f - beta2) * gc, gc, beta2 * bf16_to_f(v_bits[c]));
-        const float lr = e == 0 ? lr_density : a.sh_lr;
-        float np = p[c] - __fdividef(lr * (mc * inv_bc1), fast_sqrt(vc * inv_bc2) + eps);
-        // one 32-bit draw per element: the low half rounds the parameter, the high half
-        // both moments
-        const uint32_t r = draw32(h1 + (uint32_t)c * 0x9E3779B9u, 0x85EBCA6Bu);
-        if (e == 0) {
-            np = np < 0.f ? 0.f : np;  // density clamp (Optimizer.cu:384)
-            a.d_out[v] = np;
-            if (a.dense_mirror) a.dense_mirror[a.compact_to_dense[v]] = np;
-        } else {
-            sh_bits[c] = f_to_sh_sr<PREC>(np, r & 0xffffu);
-        }
-        m_bits[c] = f_to_bf16_sr(mc, r >> 16);
-        v_bits[c] = f_to_bf16_sr(vc, r >> 16);
+        mn[c] = fmaf(1.f - beta1, gc, beta1 * mo[c]);
+        vn[c] = fmaf((1.f - beta2) * gc, gc, beta2 * vo[c]);
+        const float lr = e == 0 ? vx.lr_d : a.sh_lr;
+        np[c] = p[c] - __fdividef(lr * (mn[c] * inv_bc1), fast_sqrt(vn[c] * inv_bc2) + eps);
         g[c] = 0.f;
     }
-    if (j == 0 && !(a.adam_mask & 1u)) {
-        a.d_out[v] = p[0];
-        if (a.dense_mirror) a.dense_mirror[a.compact_to_dense[v]] = p[0];
+    if (u == 0) {
+        const float d = (a.adam_mask & 1u) ? (np[0] < 0.f ? 0.f : np[0]) : p[0];  // density clamp (Optimizer.cu:384)
+        a.d_out[v] = d;
+        if (a.dense_mirror) a.dense_mirror[a.compact_to_dense[v]] = d;
     }
-    a.sh_out[q] = pack4(sh_bits);
-    a.m[q] = pack4(m_bits);
-    a.v[q] = pack4(v_bits);
-    if (tch) a.grad[(size_t)v * S + j] = make_float4(g[0], g[1], g[2], g[3]);
+    // random words: one hash of (launch key, vertex, unit) and one cheap draw; the parameters
+    // and the two moments take them in rotated forms
+    const uint32_t r0 = fmix32(step_key ^ (v * 0x632BE5ABu) ^ ((uint32_t)u << 27));
+    const uint32_t r1 = draw32(r0, 0x85EBCA6Bu);
+    sh_out[q] = UT::template pack<PREC>(np, r0, r1);
+    mrec[q] = UT::template pack<kPrecBF16>(mn, __funnelshift_l(r0, r0, 11), __funnelshift_l(r1, r1, 11));
+    vrec[q] = UT::template pack<kPrecBF16>(vn, __funnelshift_l(r0, r0, 22), __funnelshift_l(r1, r1, 22));
+    if (tch) grad[q] = UT::make(g);
+}
+
+// Hardware approximations (about 1 ulp) of the square root and of the reciprocal of each half
+// of a pair; the reciprocal takes arguments of at least 1e-6 here (no denormals to flush).
+__device__ __forceinline__ float2 sqrt2_approx(float2 x)
+{
+    float2 r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r.x) : "f"(x.x));
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r.y) : "f"(x.y));
+    return r;
+}
+__device__ __forceinline__ float2 rcp2_approx(float2 x)
+{
+    float2 r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(x.x));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(x.y));
+    return r;
+}
+
+// The quad update of lowp_unit<PREC, 4, TV> for records whose every slot takes TV and Adam,
+// with the element arithmetic in packed FP32 pairs (sm_100 FFMA2 / FMUL2 / FADD2: each pair
+// element rounds exactly as the scalar operation) and the square roots and reciprocals from the
+// hardware approximations.
+template <int PREC, bool TV>
+__device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint32_t q, int u, const LowpVertex& vx,
+                                             const uint32_t* nbq, float inv_bc1, float inv_bc2, uint32_t step_key)
+{
+    const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
+    const float2 neg1 = make_float2(-1.f, -1.f);
+    const uint2 sh_raw = __ldg(a.sh_in + q);
+    float2 p01, p23;
+    unpack2<PREC>(sh_raw.x, p01.x, p01.y);
+    unpack2<PREC>(sh_raw.y, p23.x, p23.y);
+    if (u == 0) p01.x = vx.dens;  // slot 0 of an SH record is unused: density is FP32
+    const bool tch = vx.bits & 1u;
+    float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tch) g4 = __ldg(a.grad + q);
+    float2 g01 = make_float2(g4.x, g4.y), g23 = make_float2(g4.z, g4.w);
+    const uint2 m_raw = __ldg(a.m + q), v_raw = __ldg(a.v + q);
+    float2 mo01, mo23, vo01, vo23;
+    unpack2<kPrecBF16>(m_raw.x, mo01.x, mo01.y);
+    unpack2<kPrecBF16>(m_raw.y, mo23.x, mo23.y);
+    unpack2<kPrecBF16>(v_raw.x, vo01.x, vo01.y);
+    unpack2<kPrecBF16>(v_raw.y, vo23.x, vo23.y);
+    if (TV && (vx.bits & 2u)) {
+        float2 s01, s23, d01s, d23s;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            float2 n01 = p01, n23 = p23;
+            if (!((vx.bits >> (2 + k)) & 1u)) {
+                const uint2 w = __ldg(a.sh_in + nbq[k]);
+                unpack2<PREC>(w.x, n01.x, n01.y);
+                unpack2<PREC>(w.y, n23.x, n23.y);
+            }
+            const float2 d01 = __ffma2_rn(n01, neg1, p01);  // p - n
+            const float2 d23 = __ffma2_rn(n23, neg1, p23);
+            s01 = k == 0 ? __fmul2_rn(d01, d01) : __ffma2_rn(d01, d01, s01);
+            s23 = k == 0 ? __fmul2_rn(d23, d23) : __ffma2_rn(d23, d23, s23);
+            d01s = k == 0 ? d01 : __fadd2_rn(d01s, d01);
+            d23s = k == 0 ? d23 : __fadd2_rn(d23s, d23);
+        }
+        // lam * disp / (sqrt(sum) / 6 + 1e-6), the denominator at least 1e-6
+        const float2 lam = make_float2(a.lam_sh, a.lam_sh);
+        const float2 sixth = make_float2(1.f / 6.f, 1.f / 6.f), tiny = make_float2(1.e-6f, 1.e-6f);
+        const float2 e01 = __ffma2_rn(sqrt2_approx(s01), sixth, tiny), e23 = __ffma2_rn(sqrt2_approx(s23), sixth, tiny);
+        g01 = __ffma2_rn(__fmul2_rn(lam, d01s), rcp2_approx(e01), g01);
+        g23 = __ffma2_rn(__fmul2_rn(lam, d23s), rcp2_approx(e23), g23);
+    }
+    if (u == 0) g01.x = g4.x + vx.tv0;  // the density's own TV term (slot 0 of the SH pass is void)
+    // Adam
+    const float2 b1 = make_float2(beta1, beta1), ob1 = make_float2(1.f - beta1, 1.f - beta1);
+    const float2 b2 = make_float2(beta2, beta2), ob2 = make_float2(1.f - beta2, 1.f - beta2);
+    const float2 bc1 = make_float2(inv_bc1, inv_bc1), bc2 = make_float2(inv_bc2, inv_bc2);
+    const float2 mn01 = __ffma2_rn(ob1, g01, __fmul2_rn(b1, mo01));
+    const float2 mn23 = __ffma2_rn(ob1, g23, __fmul2_rn(b1, mo23));
+    const float2 vn01 = __ffma2_rn(__fmul2_rn(ob2, g01), g01, __fmul2_rn(b2, vo01));
+    const float2 vn23 = __ffma2_rn(__fmul2_rn(ob2, g23), g23, __fmul2_rn(b2, vo23));
+    const float2 lr01 = make_float2(u == 0 ? vx.lr_d : a.sh_lr, a.sh_lr), lr23 = make_float2(a.sh_lr, a.sh_lr);
+    const float2 a01 = __fmul2_rn(lr01, __fmul2_rn(mn01, bc1)), a23 = __fmul2_rn(lr23, __fmul2_rn(mn23, bc1));
+    const float2 e2 = make_float2(eps, eps);
+    const float2 den01 = __fadd2_rn(sqrt2_approx(__fmul2_rn(vn01, bc2)), e2);
+    const float2 den23 = __fadd2_rn(sqrt2_approx(__fmul2_rn(vn23, bc2)), e2);
+    const float2 q01 = __fmul2_rn(a01, rcp2_approx(den01)), q23 = __fmul2_rn(a23, rcp2_approx(den23));
+    const float2 np01 = __ffma2_rn(q01, neg1, p01), np23 = __ffma2_rn(q23, neg1, p23);  // p - step
+    if (u == 0) {
+        const float d = np01.x < 0.f ? 0.f : np01.x;  // density clamp (Optimizer.cu:384)
+        a.d_out[v] = d;
+        if (a.dense_mirror) a.dense_mirror[a.compact_to_dense[v]] = d;
+    }
+    const uint32_t r0 = fmix32(step_key ^ (v * 0x632BE5ABu) ^ ((uint32_t)u << 27));
+    const uint32_t r1 = draw32(r0, 0x85EBCA6Bu);
+    a.sh_out[q] = make_uint2(sr_pack2<PREC>(np01.x, np01.y, r0), sr_pack2<PREC>(np23.x, np23.y, r1));
+    a.m[q] = make_uint2(sr_pack2<kPrecBF16>(mn01.x, mn01.y, __funnelshift_l(r0, r0, 11)),
+                        sr_pack2<kPrecBF16>(mn23.x, mn23.y, __funnelshift_l(r1, r1, 11)));
+    a.v[q] = make_uint2(sr_pack2<kPrecBF16>(vn01.x, vn01.y, __funnelshift_l(r0, r0, 22)),
+                        sr_pack2<kPrecBF16>(vn23.x, vn23.y, __funnelshift_l(r1, r1, 22)));
+    if (tch) a.grad[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+template <int PREC, int E, bool TV>
+__device__ __forceinline__ void lowp_step(const LowpArgs& a, uint32_t v, uint32_t q, int u, const LowpVertex& vx,
+                                          const uint32_t* nbq, float inv_bc1, float inv_bc2, uint32_t step_key)
+{
+    if (E == 4 && a.full_masks)
+        lowp_quad_x2<PREC, TV>(a, v, q, u, vx, nbq, inv_bc1, inv_bc2, step_key);
+    else
+        lowp_unit<PREC, E, TV>(a, v, q, u, vx, nbq, inv_bc1, inv_bc2, step_key);
 }
 
 // Bias corrections and the stochastic-rounding key of this step into shared memory.
@@ -149,38 +328,63 @@ __device__ __forceinline__ void lowp_bias_corrections(const LowpArgs& a, float* 
     __syncthreads();
 }
 
-// Dense grid: one block per (y, z) row of W vertices, S quads each.
-template <int PREC, int S, bool TV>
-__global__ void __launch_bounds__(256) k_sweep_lowp_dense(LowpArgs a)
+// Dense grid: one block per (y, z) row; a warp takes 32 consecutive vertices of the row, each
+// lane works out one vertex's LowpVertex, and the warp's 32 * U units (consecutive units on
+// consecutive lanes, U = 4 S / E per vertex) take it by shuffle.
+template <int PREC, int S, bool TV, int E>
+__global__ void __launch_bounds__(256, 4) k_sweep_lowp_dense(LowpArgs a)
 {
+    constexpr int U = 4 * S / E;
     __shared__ float s_bc[2];
     __shared__ uint32_t s_key;
     lowp_bias_corrections(a, s_bc, &s_key);
+    const int lane = threadIdx.x & 31;
     const int row = blockIdx.x;
     const int y = row % a.H;
     const int z = row / a.H;
     const uint32_t WH = (uint32_t)a.W * a.H;
     const uint32_t v0 = (uint32_t)z * WH + (uint32_t)y * a.W;
     const bool row_interior = y >= 1 && y <= a.H - 2 && z >= 1 && z <= a.D - 2;
-    const uint32_t n = (uint32_t)a.W * S;
-    for (uint32_t li = threadIdx.x; li < n; li += blockDim.x) {
-        const uint32_t x = li / S;
-        const int j = (int)(li - x * S);
+    // neighbour units lie a fixed number of units away (unsigned wrap-around; only read where
+    // the TV term applies, i.e. inside the grid)
+    const uint32_t off[6] = {0u - WH * U, 0u - (uint32_t)a.W * U, 0u - (uint32_t)U, (uint32_t)U,
+                             (uint32_t)a.W * U, WH * U};
+    for (uint32_t x0 = (threadIdx.x >> 5) * 32u; x0 < (uint32_t)a.W; x0 += blockDim.x) {
+        const uint32_t x = x0 + lane;
         const uint32_t v = v0 + x;
-        const bool tv_on = row_interior && x >= 1 && x + 2 <= (uint32_t)a.W;
-        const uint32_t nb_v[6] = {v - WH, v - (uint32_t)a.W, v - 1u, v + 1u, v + (uint32_t)a.W, v + WH};
-        const bool nb_self[6] = {false, false, false, false, false, false};
-        const float lr_d = a.adaptive_lr ? a.lr * a.adaptive_lr[v] : a.lr;
-        lowp_quad<PREC, S, TV>(a, v, j, tv_on, nb_v, nb_self, s_bc[0], s_bc[1], lr_d, s_key);
+        LowpVertex mine;
+        mine.dens = mine.tv0 = mine.lr_d = 0.f;
+        mine.bits = 0;
+        if (x < (uint32_t)a.W) {
+            const bool tv_on = row_interior && x >= 1 && x + 2 <= (uint32_t)a.W;
+            const uint32_t nb_v[6] = {v - WH, v - (uint32_t)a.W, v - 1u, v + 1u, v + (uint32_t)a.W, v + WH};
+            const float lr_d = a.adaptive_lr ? a.lr * a.adaptive_lr[v] : a.lr;
+            mine = lowp_vertex<TV>(a, v, tv_on, nb_v, 0u, lr_d);
+            if (a.clear && (v & 31u) == 0) a.clear[v >> 5] = 0u;
+        }
+        const uint32_t nx = min(32u, (uint32_t)a.W - x0);  // vertices of this chunk
+#pragma unroll
+        for (int it = 0; it < U; it++) {
+            const uint32_t i = it * 32u + lane;
+            const uint32_t vl = i / U;
+            const int u = (int)(i - vl * U);
+            const LowpVertex vx = shfl_vertex(mine, (int)vl);
+            if (vl >= nx) continue;
+            const uint32_t vv = v0 + x0 + vl;
+            const uint32_t q = vv * U + u;
+            const uint32_t nbq[6] = {q + off[0], q + off[1], q + off[2], q + off[3], q + off[4], q + off[5]};
+            lowp_step<PREC, E, TV>(a, vv, q, u, vx, nbq, s_bc[0], s_bc[1], s_key);
+        }
     }
 }
 
-// Sparse grid: blocks tile the compact (vertex, quad) pairs.
-template <int PREC, int S, bool TV>
+// Sparse grid: a warp takes 32 consecutive compact vertices; each lane works out one vertex's
+// TV neighbourhood and LowpVertex, and the warp's 32 * U units take them by shuffle (as the
+// FP32 sparse sweep).
+template <int PREC, int S, bool TV, int E>
 __global__ void __launch_bounds__(256) k_sweep_lowp_sparse(LowpArgs a)
 {
-    // A warp takes 32 consecutive compact vertices; each lane works out one vertex's TV
-    // neighbourhood and the warp's 32 * S quads take it by shuffle (as the FP32 sparse sweep).
+    constexpr int U = 4 * S / E;
     __shared__ float s_bc[2];
     __shared__ uint32_t s_key;
     lowp_bias_corrections(a, s_bc, &s_key);
@@ -192,22 +396,32 @@ __global__ void __launch_bounds__(256) k_sweep_lowp_sparse(LowpArgs a)
     mine.flags = 0;
 #pragma unroll
     for (int k = 0; k < 6; k++) mine.nb[k] = 0;
-    if (TV && v0 + lane < a.n_act)
-        mine = sparse_tv(v0 + lane, a.compact_to_dense, a.in_cage, a.index_offsets, a.W, a.H, a.D);
+    LowpVertex mv;
+    mv.dens = mv.tv0 = mv.lr_d = 0.f;
+    mv.bits = 0;
+    if (v0 + lane < a.n_act) {
+        if (TV) mine = sparse_tv(v0 + lane, a.compact_to_dense, a.in_cage, a.index_offsets, a.W, a.H, a.D);
+        mv = lowp_vertex<TV>(a, v0 + lane, (mine.flags >> 6) & 1u, mine.nb, mine.flags & 63u, a.lr);
+        if (a.clear && ((v0 + lane) & 31u) == 0) a.clear[(v0 + lane) >> 5] = 0u;
+    }
 #pragma unroll
-    for (int it = 0; it < S; it++) {
+    for (int it = 0; it < U; it++) {
         const uint32_t i = it * 32u + lane;
-        const uint32_t vl = i / S;
-        const int j = (int)(i - vl * S);
+        const uint32_t vl = i / U;
+        const int u = (int)(i - vl * U);
         const SparseTv t = TV ? shfl_tv(mine, (int)vl) : mine;
+        const LowpVertex vx = shfl_vertex(mv, (int)vl);
         const uint32_t v = v0 + vl;
         if (v >= a.n_act) continue;
-        bool nb_self[6];
+        uint32_t nbq[6];
 #pragma unroll
-        for (int k = 0; k < 6; k++) nb_self[k] = (t.flags >> k) & 1u;
-        lowp_quad<PREC, S, TV>(a, v, j, (t.flags >> 6) & 1u, t.nb, nb_self, s_bc[0], s_bc[1], a.lr, s_key);
+        for (int k = 0; k < 6; k++) nbq[k] = t.nb[k] * U + u;
+        lowp_step<PREC, E, TV>(a, v, v * U + u, u, vx, nbq, s_bc[0], s_bc[1], s_key);
     }
 }
+
+// slots a thread updates: quads (pairs measured slower: twice the loads for the same bytes)
+constexpr int kLowpUnit = 4;
 
 template <int PREC, int S>
 static void launch_lowp(const cpx_grid* g, const LowpArgs& a, bool tv, cudaStream_t st)
@@ -215,15 +429,15 @@ static void launch_lowp(const cpx_grid* g, const LowpArgs& a, bool tv, cudaStrea
     if (!g->sparse) {
         const unsigned rows = (unsigned)((int64_t)g->H * g->D);
         if (tv)
-            k_sweep_lowp_dense<PREC, S, true><<<rows, 256, 0, st>>>(a);
+            k_sweep_lowp_dense<PREC, S, true, kLowpUnit><<<rows, 256, 0, st>>>(a);
         else
-            k_sweep_lowp_dense<PREC, S, false><<<rows, 256, 0, st>>>(a);
+            k_sweep_lowp_dense<PREC, S, false, kLowpUnit><<<rows, 256, 0, st>>>(a);
     } else {
         const unsigned blocks = (unsigned)(((int64_t)g->n_act + 255) / 256);  // a warp per 32 vertices
         if (tv)
-            k_sweep_lowp_sparse<PREC, S, true><<<blocks, 256, 0, st>>>(a);
+            k_sweep_lowp_sparse<PREC, S, true, kLowpUnit><<<blocks, 256, 0, st>>>(a);
         else
-            k_sweep_lowp_sparse<PREC, S, false><<<blocks, 256, 0, st>>>(a);
+            k_sweep_lowp_sparse<PREC, S, false, kLowpUnit><<<blocks, 256, 0, st>>>(a);
     }
 }
 
@@ -278,6 +492,8 @@ cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_
     a.step_key = fmix32(g->sr_seed ^ ((uint32_t)timestep * 0x9E3779B9u));
     a.t_dev = t_dev;
     a.seed = g->sr_seed;
+    const uint32_t all = (g->rec >= 32) ? 0xffffffffu : ((1u << g->rec) - 1u);
+    a.full_masks = (tv_mask & all) == all && (adam_mask & all) == all ? 1 : 0;
     cpx_status rc = g->prec == kPrecFP16 ? launch_lowp_shape<kPrecFP16>(g, a, fused_tv, st)
                                          : launch_lowp_shape<kPrecBF16>(g, a, fused_tv, st);
     if (rc != CPX_OK) return rc;

@@ -209,8 +209,9 @@ def brick_map(occ, W, H, D):
 
 # transmittance below which the FP32 march of the mixed forms ends a ray (its default)
 MIXED_T_STOP = 1.0e-4
-# density at or below which a dense grid's cell is empty for the FP32 march (all 8 corners)
-EMPTY_DENSITY = np.float32(-2.0)
+# density at or below which a dense grid's cell is empty for the FP32 march (all 8 corners):
+# the optimizer's density clamp, where trained empty space sits
+EMPTY_DENSITY = np.float32(0.0)
 
 
 def dense_open_cells(density, W, H, D):

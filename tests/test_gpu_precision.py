@@ -111,14 +111,16 @@ def test_upload_rounds_to_nearest_and_downloads_exactly(cuda, case, precision):
 @pytest.mark.parametrize("precision", ["bf16", "fp16"])
 def test_fp32_march_against_fp64_oracle(cuda, case, precision):
     """SH values exactly representable in 16 bits: the remaining difference to the FP64
-    oracle is the FP32 march alone."""
+    oracle is the FP32 march alone (the oracle marching as the FP32 march does: empty cells
+    at the density clamp jumped, rays ended below transmittance 1e-4)."""
     import orc
 
     params = to_storage(case["params"], precision)
     scene, rays = make(case, precision, params)
     pred, accw, losses, grad = run_fb(scene, rays)
     osc, orays = oracle(case, params)
-    pred64, accw64, losses64, grad64, _ = orc.fp64_step(osc, orays, MASK_COEF, HUBER, t_stop=orc.MIXED_T_STOP)
+    pred64, accw64, losses64, grad64, _ = orc.fp64_step(osc, orays, MASK_COEF, HUBER, skip_empty=True,
+                                                        t_stop=orc.MIXED_T_STOP)
     assert np.abs(pred - pred64).max() < 1e-4
     assert np.abs(accw - accw64).max() < 1e-4
     assert normwise(grad[0], grad64[0]) < 2e-3
@@ -241,14 +243,14 @@ def test_dense_empty_jumps_and_early_stop_against_fp64_oracle(cuda, case):
     """A dense mixed grid whose empty space lies below the empty-density bound: the FP32 march
     jumps over those cells and stops rays behind opaque content, exactly as the FP64 oracle
     with the same map and stop; the march without them (options) is the plain FP32 march, and
-    the two differ by less than 2e-4 in colour (1e-4 from the stop, the rest from the skipped
-    samples' optical depth) while the jumping march keeps far fewer samples."""
+    the two differ by less than 5e-4 in colour (1e-4 from the stop, the rest from the skipped
+    samples' optical depth, 1.2e-6 each) while the jumping march keeps far fewer samples."""
     import orc
 
     import cpx
 
     params = to_storage(case["params"], "bf16")
-    params[0] = params[0] * 4.0 - 6.0  # opaque blob cores, empty space at -6
+    params[0] = np.maximum(params[0] * 4.0 - 6.0, 0.0)  # opaque blob cores, empty space at the clamp
     scene, rays = make(case, "bf16", params)
     pred, accw, losses, grad = run_fb(scene, rays)
     n_jump = scene.last_sample_counts(rays.total_rays)
@@ -262,7 +264,7 @@ def test_dense_empty_jumps_and_early_stop_against_fp64_oracle(cuda, case):
     scene.set_options(cpx.OPT_NO_EMPTY_SKIP | cpx.OPT_NO_EARLY_STOP)
     pred_full, _, _, _ = run_fb(scene, rays)
     n_full = scene.last_sample_counts(rays.total_rays)
-    assert np.abs(pred - pred_full).max() < 2e-4
+    assert np.abs(pred - pred_full).max() < 5e-4
     assert n_jump.sum() < 0.8 * n_full.sum()
     assert np.all(n_jump <= n_full)
 

@@ -229,12 +229,13 @@ def test_early_stop_bounds_the_colour_change():
 
 def test_dense_empty_cells_change_little():
     """On a dense grid the FP32 march jumps over cells whose eight corner densities are all at
-    or below EMPTY_DENSITY (-2): each such sample would add at most softplus(-15) * step to the
-    optical depth, so the image moves by far less than 1e-4 while the empty cells are skipped."""
+    or below EMPTY_DENSITY (0, the optimizer's clamp): each such sample would add at most
+    softplus(-13) * step to the optical depth; with empty space at the clamp the image moves
+    by less than 2e-4 while the empty cells are skipped."""
     cfg = S.small_config(seed=10, n=48, n_cams=4, img=40, n_rays=400)
     n = cfg["W"]
     params = cfg["params"].copy()
-    params[0] -= 6.0  # empty space well below the bound, blob cores above it
+    params[0] = np.maximum(params[0] - 6.0, 0.0)  # empty space at the clamp, blob cores above it
     sc = orc.Scene(n, n, n, 9, params, step=0.5)
     cells = orc.dense_open_cells(params[0], n, n, n)
     assert 0.01 < cells.mean() < 0.6
@@ -246,8 +247,8 @@ def test_dense_empty_cells_change_little():
         off += len(pix)
     full = orc.fp64_step(sc, rays, 1.0, 0.1)
     jump = orc.fp64_step(sc, rays, 1.0, 0.1, skip_empty=True)
-    assert np.abs(full[0] - jump[0]).max() < 2e-5
-    assert np.abs(full[1] - jump[1]).max() < 2e-5
+    assert np.abs(full[0] - jump[0]).max() < 2e-4
+    assert np.abs(full[1] - jump[1]).max() < 2e-4
     assert np.abs(full[0] - 1.0).max() > 0.05  # the rays see the blobs
     # the gradients agree on the vertices of open cells; the skipped ones lose tiny terms
     assert np.linalg.norm(full[3] - jump[3]) <= 2e-3 * np.linalg.norm(full[3])
