@@ -367,6 +367,10 @@ cpx_status cpx_grid_create(const cpx_grid_desc* d, cpx_grid** out)
     g->slots = lowp_slots(g->n_arrays);
     cudaError_t e = alloc_state(g, n);
     if (e == cudaSuccess) e = cudaMalloc((void**)&g->adaptive_lr, n * sizeof(float));
+    // device error flags of the marches and sweeps
+    if (e == cudaSuccess) e = cudaMalloc((void**)&g->scratch.err, sizeof(int) * 4);
+    if (e == cudaSuccess) e = cudaMemset(g->scratch.err, 0, sizeof(int) * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&g->scratch.mse, sizeof(double));
     if (e == cudaSuccess) {
         k_fill<<<blocks_for(n), 256>>>(g->adaptive_lr, n, 1.f);
         count_launch();
