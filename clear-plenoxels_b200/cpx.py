@@ -61,6 +61,7 @@ EXPORTED = [
     "cpx_grid_set_options", "cpx_grid_upsample",
     "cpx_batch_create", "cpx_batch_destroy", "cpx_batch_step", "cpx_batch_mse", "cpx_batch_check",
     "cpx_batch_info", "cpx_batch_set_tuning", "cpx_batch_get_tuning", "cpx_batch_autotune",
+    "cpx_carve_silhouette", "cpx_grid_bbox",
 ]
 
 
@@ -203,6 +204,8 @@ class BatchTuning(C.Structure):
     _fields_ = [("place_block", C.c_int), ("shade_warps", C.c_int), ("grab", C.c_int)]
 
 
+_sig("cpx_carve_silhouette", [_vp, C.POINTER(C.c_double), C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp])
+_sig("cpx_grid_bbox", [_vp, C.POINTER(C.c_int), C.POINTER(C.c_double)])
 _sig("cpx_batch_create", [C.POINTER(BatchScene), C.c_int, C.POINTER(StepArgs), C.POINTER(_vp)])
 _sig("cpx_batch_destroy", [_vp])
 _sig("cpx_batch_step", [_vp, C.c_int, _vp])
@@ -525,6 +528,19 @@ class RenderUtils:
     """Per-batch march entry points (RenderUtils.cuh:7-85)."""
 
     @staticmethod
+    def bbox_silhouette(projections, images, scene: "ObjectScene", img_w: int, img_h: int, radius: int = 0,
+                        isGettingScaleRatio: bool = False, skipIndex=()):
+        """RenderUtils::bbox_silhouette (RenderUtils.cu:323-478): carve with every camera not in
+        skipIndex, then the bounding box (set as the grid's ray box); returns the scale ratio
+        (0.0 unless isGettingScaleRatio)."""
+        skip = set(int(i) for i in skipIndex)
+        for i, (P, img) in enumerate(zip(projections, images)):
+            if i not in skip:
+                carve_silhouette(scene, P, img, img_w, img_h, radius)
+        _, sr = grid_bbox(scene, isGettingScaleRatio)
+        return sr if isGettingScaleRatio else 0.0
+
+    @staticmethod
     def renderRays(rays: Rays, scene: ObjectScene, sampleIndex=None, startSampleIndex: int = 0,
                    len: int | None = None, stream=None):
         n = _len(rays, startSampleIndex, len)
@@ -578,6 +594,37 @@ class RenderUtils:
                         neighboorNums: int = 6, stream=None):
         _check(_lib.cpx_tv_grad(scene.handle, float(varianceCoefficient), float(shCoefficient),
                                 int(varianceType), int(neighboorNums), _stream(stream)), "addVarianceLoss")
+
+
+def _plane(p, n):
+    if p is None:
+        return None
+    a = np.ascontiguousarray(p, np.uint8).reshape(-1)
+    if a.size != n:
+        raise ValueError(f"image plane of {a.size} bytes, expected {n}")
+    return a
+
+
+def carve_silhouette(scene: "ObjectScene", projection, image, img_w: int, img_h: int, radius: int = 0, stream=None):
+    """silhouetteCarving (RenderUtils.cu:181-254) of one camera: projection is the camera's
+    3x4 world-to-pixel matrix, image = (r, g, b, mask) planes of img_h*img_w bytes."""
+    P = np.ascontiguousarray(projection, np.float64).reshape(12)
+    n = int(img_w) * int(img_h)
+    r, g, b, m = (_plane(p, n) for p in image)
+    _check(_lib.cpx_carve_silhouette(scene.handle, P.ctypes.data_as(C.POINTER(C.c_double)), int(img_w), int(img_h),
+                                     r.ctypes.data, g.ctypes.data, b.ctypes.data,
+                                     None if m is None else m.ctypes.data, int(radius), _stream(stream)),
+           "cpx_carve_silhouette")
+
+
+def grid_bbox(scene: "ObjectScene", scale_ratio: bool = False):
+    """Bounding box of the uncarved vertices (getBoundingBoxZ + bbox_silhouette's reduction);
+    it becomes the grid's ray box.  Returns (bbox tuple, scale ratio or None)."""
+    box = (C.c_int * 6)()
+    sr = C.c_double(0.0)
+    _check(_lib.cpx_grid_bbox(scene.handle, box, C.byref(sr) if scale_ratio else None), "cpx_grid_bbox")
+    scene.bbox = tuple(box[:])
+    return tuple(box[:]), (sr.value if scale_ratio else None)
 
 
 class Optimizer:

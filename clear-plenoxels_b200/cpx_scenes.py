@@ -60,6 +60,17 @@ def look_at_camera(eye_world, n_vox: int, img_w: int, img_h: int, fov_deg: float
     }
 
 
+def projection_matrix(cam) -> np.ndarray:
+    """The camera's 3x4 world-to-pixel matrix K [I|0] w2c (Camera::formulateProjectionMat's
+    product), consistent with getBound's pixel rays: a point on pixel (row, col)'s centre ray
+    projects to (col + 0.5, row + 0.5)."""
+    ax, ay = cam["alpha"]
+    px, py = cam["principle"]
+    K = np.array([[ax, 0.0, px], [0.0, ay, py], [0.0, 0.0, 1.0]])
+    w2c = np.linalg.inv(np.asarray(cam["c2w"], np.float64))
+    return K @ w2c[:3, :]
+
+
 def fibonacci_sphere(n: int, radius: float):
     i = np.arange(n) + 0.5
     phi = np.arccos(1 - 2 * i / n)

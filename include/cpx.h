@@ -220,6 +220,24 @@ cpx_status cpx_image_mse(const float* a_dev, const float* b_dev, int64_t n, doub
 cpx_status cpx_grid_upsample(const cpx_grid* src, cpx_grid* dst, float threshold, int low_band_only,
                              cpx_stream stream);
 
+/* Silhouette carving, one camera (silhouetteCarving, SVRF/RenderUtils.cu:181-254, as
+ * RenderUtils::bbox_silhouette runs it per training image): every vertex (x, y, z) of the dense
+ * grid projects its point (x + 0.5, y + 0.5, z) through `projection` (the camera's 3x4
+ * row-major world-to-pixel matrix, Camera::projectionMatHost) and, when no pixel within
+ * `radius` of the truncated image position has a nonzero mask or colour byte, gets density 0
+ * and density-LR multiplier 0.  Image planes are host arrays of img_w*img_h bytes (mask may be
+ * NULL: all zero).  Dense grids.  Synchronous. */
+cpx_status cpx_carve_silhouette(cpx_grid* g, const double* projection, int img_w, int img_h,
+                                const uint8_t* red, const uint8_t* green, const uint8_t* blue,
+                                const uint8_t* mask, int radius, cpx_stream stream);
+/* Bounding box of the vertices whose density-LR multiplier exceeds 1e-6 (getBoundingBoxZ and
+ * the reduction of bbox_silhouette, SVRF/RenderUtils.cu:256-286, 372-464): bbox_out[6] =
+ * wmin, wmax, hmin, hmax, dmin, dmax, which also becomes the grid's ray box (as the reference
+ * sets scene->bbox_*).  scale_ratio_out (may be NULL): getMaxRadius's largest distance of such
+ * a vertex from the grid centre, / width * 2 (bbox_silhouette's return value).  Dense grids.
+ * Synchronous. */
+cpx_status cpx_grid_bbox(cpx_grid* g, int* bbox_out, double* scale_ratio_out);
+
 /* March options (no reference counterpart; for studying the mixed forms):
  * CPX_OPT_NO_EMPTY_SKIP  the FP32 march steps through every empty cell of a sparse grid as
  *                        the reference does, instead of jumping over empty cells and bricks;

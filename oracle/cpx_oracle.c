@@ -1270,3 +1270,95 @@ void orc_upsample(const orc_scene* s, int dW, int dH, int dD, int dst_sh, float 
                 dst[(int64_t)(1 + ch * dst_sh + i) * n + p] = tri[1 + ch * sh + i];
     }
 }
+
+
+/* ------------------------------------------------------------------ carving, bounding box */
+/* The device's double -> int conversion (cvt.rzi.s32.f64): truncation, saturating, NaN -> 0. */
+static int sat_i32(double v)
+{
+    if (v != v) return 0;
+    if (v >= 2147483647.0) return 2147483647;
+    if (v <= -2147483648.0) return (int)-2147483647 - 1;
+    return (int)v;
+}
+
+/* silhouetteCarving (SVRF/RenderUtils.cu:181-254); projectWorld2Image (:120-132) accumulates
+ * each image coordinate with fused multiply-adds from 0, as nvcc compiles it. */
+void orc_carve_silhouette(float* density, float* lr, int W, int H, int D, const double* P, int img_w,
+                          int img_h, const uint8_t* red, const uint8_t* green, const uint8_t* blue,
+                          const uint8_t* mask, int radius)
+{
+    const int64_t WH = (int64_t)W * H;
+#pragma omp parallel for schedule(static)
+    for (int64_t pix = 0; pix < WH; pix++) {
+        const int row = (int)(pix / W), col = (int)(pix % W);
+        for (int depth = 0; depth < D; depth++) {
+            const double world[4] = {col + 0.5, row + 0.5, (double)depth, 1.};
+            double image[3];
+            for (int r = 0; r < 3; r++) {
+                image[r] = 0.;
+                for (int c = 0; c < 4; c++) image[r] = fma(P[r * 4 + c], world[c], image[r]);
+            }
+            image[0] /= image[2];
+            image[1] /= image[2];
+            const int imageRow = sat_i32(image[1]), imageCol = sat_i32(image[0]);
+            int save = 0;
+            for (int nr = -radius; nr < radius + 1 && !save; nr++) {
+                const double pr = (double)imageRow + nr;
+                for (int nc = -radius; nc < radius + 1; nc++) {
+                    const double pc = (double)imageCol + nc;
+                    if (pc < 0 || pc >= img_w || pr < 0 || pr >= img_h) continue;
+                    const int p = sat_i32(pr * img_w + pc);
+                    if ((mask && mask[p]) || red[p] || green[p] || blue[p]) {
+                        save = 1;
+                        break;
+                    }
+                }
+            }
+            if (!save) {
+                const int64_t v = depth * WH + pix;
+                density[v] = 0.f;
+                lr[v] = 0.f;
+            }
+        }
+    }
+}
+
+/* getBoundingBoxZ (RenderUtils.cu:256-286), getMaxRadius (:288-321) and the host reduction
+ * (:351-464); the radius terms compile to fused multiply-adds on the device. */
+double orc_bbox(const float* lr, int W, int H, int D, int* bbox)
+{
+    const int64_t WH = (int64_t)W * H;
+    int b[6] = {W, -1, H, -1, D, -1};
+    double best = 0.;
+    for (int64_t pix = 0; pix < WH; pix++) {
+        const int row = (int)(pix / W), col = (int)(pix % W);
+        int depth = 0;
+        while (lr[depth * WH + pix] < 1e-6 && depth + 1 < D) ++depth;
+        const int rmin = depth;
+        int rmax = depth;
+        while (depth + 1 < D) {
+            ++depth;
+            if (lr[depth * WH + pix] > 1e-6) rmax = depth;
+        }
+        if (rmin != depth) {
+            if (col < b[0]) b[0] = col;
+            if (col > b[1]) b[1] = col;
+            if (row < b[2]) b[2] = row;
+            if (row > b[3]) b[3] = row;
+            if (rmin < b[4]) b[4] = rmin;
+            if (rmax > b[5]) b[5] = rmax;
+        }
+        const double dr = row - H / 2., dc = col - W / 2.;
+        const double temp = fma(dr, dr, dc * dc);
+        for (int d = 0; d < D; d++) {
+            if (lr[d * WH + pix] > 1e-6) {
+                const double dd = d - D / 2.;
+                const double distance = sqrt(fma(dd, dd, temp));
+                if (distance > best) best = distance;
+            }
+        }
+    }
+    for (int i = 0; i < 6; i++) bbox[i] = b[i];
+    return best / W * 2.;
+}

@@ -133,6 +133,16 @@ void orc_render_image(const orc_scene* s, const double* alpha, const double* pri
 /* Coarse-to-fine refinement: upsampleScene / upsample_trilinear (SceneUtils.cu:262-485).
  * src: the oracle scene (dense or sparse); dst: planar [1 + 3*dst_sh][dW*dH*dD] (dense target,
  * written for every vertex; entries beyond the written coefficients are left as they are). */
+/* silhouetteCarving (SVRF/RenderUtils.cu:181-254) of one camera on a dense W x H x D grid:
+ * density[v] and lr[v] become 0 where no pixel within `radius` of the vertex's projection has a
+ * nonzero byte (mask may be NULL). */
+void orc_carve_silhouette(float* density, float* lr, int W, int H, int D, const double* P, int img_w,
+                          int img_h, const uint8_t* red, const uint8_t* green, const uint8_t* blue,
+                          const uint8_t* mask, int radius);
+/* getBoundingBoxZ + getMaxRadius + bbox_silhouette's reduction (SVRF/RenderUtils.cu:256-478):
+ * bbox[6] = wmin, wmax, hmin, hmax, dmin, dmax of the vertices with lr > 1e-6; returns the
+ * scale ratio (max radius / W * 2). */
+double orc_bbox(const float* lr, int W, int H, int D, int* bbox);
 void orc_upsample(const orc_scene* src, int dW, int dH, int dD, int dst_sh, float threshold,
                   int low_band_only, float* dst);
 

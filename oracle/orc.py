@@ -72,6 +72,8 @@ _fn("orc_mse", [_vp, C.c_int], C.c_double)
 _fn("orc_composite_kat", [_vp, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _fn("orc_render_image", [C.POINTER(_Scene)] + [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
 _fn("orc_upsample", [C.POINTER(_Scene), C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp])
+_fn("orc_carve_silhouette", [_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int])
+_fn("orc_bbox", [_vp, C.c_int, C.c_int, C.c_int, _vp], C.c_double)
 class _Bricks(C.Structure):
     _fields_ = [("bits", _vp), ("bx", C.c_int), ("by", C.c_int), ("bz", C.c_int), ("t_stop", C.c_double),
                 ("cells", _vp)]
@@ -344,3 +346,21 @@ def activations(x):
     x = np.asarray(x, np.float32).reshape(-1)
     f = [_lib.orc_density_activation, _lib.orc_density_derivation, _lib.orc_sigmoid, _lib.orc_sigmoid_derivative]
     return [np.array([fn(float(v)) for v in x], np.float32) for fn in f]
+
+
+def carve_silhouette(density, lr, W, H, D, projection, image, img_w, img_h, radius=0):
+    """silhouetteCarving of one camera, in place on float32 density / lr arrays [W*H*D]."""
+    assert density.dtype == np.float32 and lr.dtype == np.float32
+    assert density.flags.c_contiguous and lr.flags.c_contiguous
+    P = np.ascontiguousarray(projection, np.float64).reshape(12)
+    planes = [None if p is None else np.ascontiguousarray(p, np.uint8).reshape(-1) for p in image]
+    _lib.orc_carve_silhouette(_p(density), _p(lr), int(W), int(H), int(D), _p(P), int(img_w), int(img_h),
+                              _p(planes[0]), _p(planes[1]), _p(planes[2]),
+                              None if planes[3] is None else _p(planes[3]), int(radius))
+
+
+def bbox(lr, W, H, D):
+    """(bbox tuple, scale ratio) of the vertices with lr > 1e-6."""
+    out = np.zeros(6, np.int32)
+    sr = _lib.orc_bbox(_p(np.ascontiguousarray(lr, np.float32)), int(W), int(H), int(D), _p(out))
+    return tuple(int(x) for x in out), float(sr)

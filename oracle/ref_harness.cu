@@ -491,6 +491,60 @@ int ref_upsample(void* h, float threshold, int low_band_only, int target_sh, flo
     return rc;
 }
 
+// RenderUtils::bbox_silhouette (RenderUtils.cu:323-478) over ncam cameras given by their 3x4
+// world-to-pixel matrices (12 doubles each) and images of 4 planes (r, g, b, mask) of
+// img_w*img_h bytes: carving, then the bounding box into bbox_out[6] (wmin, wmax, hmin, hmax,
+// dmin, dmax) and the returned scale ratio into scale_out.  Dense scenes.
+int ref_bbox_silhouette(void* h, int ncam, const double* proj, const uint8_t* images, int img_w, int img_h,
+                        int radius, int get_scale, int* bbox_out, double* scale_out)
+{
+    RefCtx* c = (RefCtx*)h;
+    std::vector<Camera> cams(ncam);
+    std::vector<Image> imgs(ncam);
+    const size_t plane = (size_t)img_w * img_h;
+    for (int i = 0; i < ncam; i++) {
+        cudaMalloc((void**)&cams[i].projectionMatDevice, sizeof(double) * 12);
+        cudaMemcpy(cams[i].projectionMatDevice, proj + 12 * i, sizeof(double) * 12, cudaMemcpyHostToDevice);
+        Image& im = imgs[i];
+        im.width = img_w;
+        im.height = img_h;
+        im.grayImage = false;
+        uint8_t* planes[4];
+        for (int p = 0; p < 4; p++) {
+            cudaMalloc((void**)&planes[p], plane);
+            cudaMemcpy(planes[p], images + ((size_t)i * 4 + p) * plane, plane, cudaMemcpyHostToDevice);
+        }
+        im.redDevice = planes[0];
+        im.greenDevice = planes[1];
+        im.blueDevice = planes[2];
+        im.maskDevice = planes[3];
+    }
+    *scale_out = RenderUtils::bbox_silhouette(cams.data(), imgs.data(), &c->scene, ncam, radius, get_scale != 0,
+                                              nullptr, 0);
+    bbox_out[0] = c->scene.bbox_width_min;
+    bbox_out[1] = c->scene.bbox_width_max;
+    bbox_out[2] = c->scene.bbox_height_min;
+    bbox_out[3] = c->scene.bbox_height_max;
+    bbox_out[4] = c->scene.bbox_depth_min;
+    bbox_out[5] = c->scene.bbox_depth_max;
+    for (int i = 0; i < ncam; i++) {
+        cudaFree(cams[i].projectionMatDevice);
+        cudaFree(imgs[i].redDevice);
+        cudaFree(imgs[i].greenDevice);
+        cudaFree(imgs[i].blueDevice);
+        cudaFree(imgs[i].maskDevice);
+    }
+    return fail(cudaDeviceSynchronize());
+}
+
+// The scene's density-LR multipliers (dense) to host memory.
+int ref_adaptive_lr(void* h, float* out)
+{
+    RefCtx* c = (RefCtx*)h;
+    const size_t n = (size_t)c->scene.sceneWidth * c->scene.sceneHeight * c->scene.sceneDepth;
+    return fail(cudaMemcpy(out, c->scene.adaptiveLRDevice, sizeof(float) * n, cudaMemcpyDeviceToHost));
+}
+
 int ref_params(void* h, float* planar, int upload)
 {
     RefCtx* c = (RefCtx*)h;

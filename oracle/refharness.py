@@ -54,6 +54,9 @@ def _setup(L):
     s("ref_rays_count", [_vp])
     s("ref_render_image", [_vp] * 5 + [C.c_int] * 3 + [_vp] * 4)
     s("ref_upsample", [_vp, C.c_float, C.c_int, C.c_int, _vp])
+    s("ref_bbox_silhouette", [_vp, C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
+                              C.POINTER(C.c_double)])
+    s("ref_adaptive_lr", [_vp, _vp])
     s("ref_rays_download", [_vp] + [_vp] * 17)
     s("ref_render_forward", [_vp, C.c_int, C.c_int])
     s("ref_render_backward", [_vp, C.c_int, C.c_int, C.c_double, C.c_float, _vp])
@@ -193,6 +196,24 @@ class RefScene:
                                  float(lam_sh), int(tv_type), int(nbrs), 1 if do_tv else 0, float(lr),
                                  float(sh_lr), int(timestep), _p(losses), C.byref(mse)), "train_step")
         return mse.value
+
+    def bbox_silhouette(self, projections, images, img_w, img_h, radius=0, get_scale=False):
+        """RenderUtils::bbox_silhouette: carving with every camera, then the box; returns
+        (bbox tuple, scale ratio)."""
+        P = np.ascontiguousarray(np.stack([np.asarray(p, np.float64).reshape(12) for p in projections]))
+        planes = np.ascontiguousarray(np.stack([np.stack([np.asarray(q, np.uint8).reshape(-1) for q in img])
+                                                for img in images]))
+        box = np.zeros(6, np.int32)
+        sr = C.c_double()
+        _ck(lib().ref_bbox_silhouette(self.h, len(projections), _p(P), _p(planes), int(img_w), int(img_h),
+                                      int(radius), 1 if get_scale else 0, _p(box), C.byref(sr)),
+            "bbox_silhouette")
+        return tuple(int(x) for x in box), sr.value
+
+    def adaptive_lr(self):
+        out = np.zeros(self.W * self.H * self.D, np.float32)
+        _ck(lib().ref_adaptive_lr(self.h, _p(out)), "adaptive_lr")
+        return out
 
     def params(self):
         out = np.zeros((self.n_arrays, self.n_act), np.float32)
