@@ -62,6 +62,8 @@ EXPORTED = [
     "cpx_batch_create", "cpx_batch_destroy", "cpx_batch_step", "cpx_batch_mse", "cpx_batch_check",
     "cpx_batch_info", "cpx_batch_set_tuning", "cpx_batch_get_tuning", "cpx_batch_autotune",
     "cpx_carve_silhouette", "cpx_grid_bbox",
+    "cpx_ray_source_create", "cpx_ray_source_destroy", "cpx_ray_source_count", "cpx_ray_source_shuffle",
+    "cpx_ray_source_keys", "cpx_ray_source_generate", "cpx_ray_source_check",
 ]
 
 
@@ -204,6 +206,14 @@ class BatchTuning(C.Structure):
     _fields_ = [("place_block", C.c_int), ("shade_warps", C.c_int), ("grab", C.c_int)]
 
 
+_sig("cpx_ray_source_create", [C.c_void_p, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int,
+                              C.POINTER(_vp)])
+_sig("cpx_ray_source_destroy", [_vp])
+_sig("cpx_ray_source_count", [_vp, C.POINTER(C.c_int64)])
+_sig("cpx_ray_source_shuffle", [_vp, C.c_uint64, C.c_int])
+_sig("cpx_ray_source_keys", [_vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int)])
+_sig("cpx_ray_source_generate", [_vp, _vp, C.c_int64, C.c_int, _vp, _vp])
+_sig("cpx_ray_source_check", [_vp])
 _sig("cpx_carve_silhouette", [_vp, C.POINTER(C.c_double), C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp])
 _sig("cpx_grid_bbox", [_vp, C.POINTER(C.c_int), C.POINTER(C.c_double)])
 _sig("cpx_batch_create", [C.POINTER(BatchScene), C.c_int, C.POINTER(StepArgs), C.POINTER(_vp)])
@@ -518,6 +528,71 @@ class Rays:
                                              pix.size, off), "cpx_rays_init_camera")
             off += pix.size
         return off
+
+
+class RaySource:
+    """Training samples (camera, pixel) whose rays are generated per batch on the device (no
+    ray table); a drop-in for _rays::initialSelf + the training shuffle (Rays.cu:187-287)."""
+
+    def __init__(self, cameras, images, img_w: int, img_h: int, pixel_lists=None, white_bg: bool = True):
+        n = int(img_w) * int(img_h)
+        cams = (Camera * len(cameras))(*cameras)
+        planes = []
+        for q in range(4):
+            if q == 3 and any(img[3] is None for img in images):
+                planes.append(None)
+                continue
+            planes.append(np.ascontiguousarray(np.stack([np.asarray(img[q], np.uint8).reshape(n) for img in images])))
+        pix = npx = None
+        if pixel_lists is not None:
+            pix = np.ascontiguousarray(np.concatenate([np.asarray(p, np.int32).reshape(-1) for p in pixel_lists]))
+            npx = np.ascontiguousarray([len(p) for p in pixel_lists], np.int64)
+        h = _vp()
+        _check(_lib.cpx_ray_source_create(C.cast(cams, C.c_void_p), len(cameras), int(img_w), int(img_h),
+                                          planes[0].ctypes.data, planes[1].ctypes.data, planes[2].ctypes.data,
+                                          None if planes[3] is None else planes[3].ctypes.data,
+                                          None if pix is None else pix.ctypes.data,
+                                          None if npx is None else npx.ctypes.data, 1 if white_bg else 0,
+                                          C.byref(h)), "cpx_ray_source_create")
+        self._h = h
+        self.white_bg = bool(white_bg)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __len__(self):
+        n = C.c_int64()
+        _check(_lib.cpx_ray_source_count(self._h, C.byref(n)), "cpx_ray_source_count")
+        return int(n.value)
+
+    def shuffle(self, seed: int, shuffled: bool = True):
+        _check(_lib.cpx_ray_source_shuffle(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, 1 if shuffled else 0),
+               "cpx_ray_source_shuffle")
+
+    def keys(self):
+        k = (C.c_uint32 * 4)()
+        hb = C.c_int()
+        _check(_lib.cpx_ray_source_keys(self._h, k, C.byref(hb)), "cpx_ray_source_keys")
+        return [int(x) for x in k], int(hb.value)
+
+    def generate(self, scene: ObjectScene, start: int, length: int, batch: Rays, stream=None):
+        _check(_lib.cpx_ray_source_generate(self._h, scene.handle, int(start), int(length), batch.handle,
+                                            _stream(stream)), "cpx_ray_source_generate")
+
+    def check(self):
+        _check(_lib.cpx_ray_source_check(self._h), "cpx_ray_source_check")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cpx_ray_source_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _len(rays: Rays, start: int, length):

@@ -163,6 +163,32 @@ cpx_status cpx_rays_init_camera(cpx_rays* r, const cpx_grid* g, const cpx_camera
                                 const uint8_t* blue, const uint8_t* gt_mask,
                                 const int32_t* pixel_index, int64_t n_pix, int64_t offset);
 
+/* Ray source (no ray table): the training samples (camera, pixel) of n_cams cameras whose
+ * images stay on the device; each batch's rays are generated on the device, bit for bit the
+ * rays cpx_rays_init_camera makes (getBound + initialRays, SVRF/Rays.cu:22-144), replacing
+ * _rays::initialSelf's table of every ray and the host shuffle (ShuffleRank + shuffleTo,
+ * SVRF/Utils.cu:488, Rays.cu:242).  Planes are host arrays [n_cams][img_w*img_h] (gt_mask may
+ * be NULL: 255); pixel_index concatenates each camera's pixel list (n_pix[c] entries; NULL:
+ * every pixel of every camera).  Sample i of an epoch is permute(i): the identity, or after
+ * cpx_ray_source_shuffle(seed, 1) a keyed bijection of [0, n) (4-round Feistel network with
+ * cycle walking; the keys come from seed through SplitMix64). */
+typedef struct cpx_ray_source cpx_ray_source;
+cpx_status cpx_ray_source_create(const cpx_camera* cams, int n_cams, int img_w, int img_h, const uint8_t* red,
+                                 const uint8_t* green, const uint8_t* blue, const uint8_t* gt_mask,
+                                 const int32_t* pixel_index, const int64_t* n_pix, int white_bg,
+                                 cpx_ray_source** out);
+cpx_status cpx_ray_source_destroy(cpx_ray_source* s);
+cpx_status cpx_ray_source_count(const cpx_ray_source* s, int64_t* n);
+/* New epoch order: shuffled = 0 restores the identity. */
+cpx_status cpx_ray_source_shuffle(cpx_ray_source* s, uint64_t seed, int shuffled);
+/* The permutation's round keys [4] and half width (for checking it on the host). */
+cpx_status cpx_ray_source_keys(const cpx_ray_source* s, uint32_t* keys, int* half_bits);
+/* Rays of samples permute(start .. start+len) into batch[0 .. len), with the grid's ray box. */
+cpx_status cpx_ray_source_generate(cpx_ray_source* s, const cpx_grid* g, int64_t start, int len, cpx_rays* batch,
+                                   cpx_stream stream);
+/* Synchronise and report a shuffle whose cycle walk ran out of steps (none expected). */
+cpx_status cpx_ray_source_check(cpx_ray_source* s);
+
 /* ------------------------------------------------------------------ per-batch path */
 /* Batch = rays sample_index_dev[start .. start+len) (identity when NULL).
  * Forward march: accumulated density, weight and RGB (+white background) per ray. */
