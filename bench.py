@@ -397,6 +397,12 @@ def run_ours(args, wl, world, rank, local):
     sweep_ms = float(np.mean([evs[k][1].elapsed_time(evs[k][2]) for k in range(K)]))
     value = world * R * K / (ms / 1e3)
 
+    # ---- the table-free path: each batch's rays generated on the device from (camera, pixel)
+    # samples of images held on the device (cpx_ray_source), then the same training step
+    src_result = None
+    if prop is None:
+        src_result = ray_source_leg(args, wl, scene, eyes, pix, gt, R, K, W + K + 4, stream, world, dev)
+
     # ---- e2e: host buffers through the public API (H2D batch, step, MSE back)
     mses = []
     dist_barrier(world)
@@ -477,6 +483,7 @@ def run_ours(args, wl, world, rank, local):
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": R * RAY_BYTES,
                 "d2h_bytes_per_step": 8, "last_mse": mses[-1]},
         "gpu_launches": int(launches),
+        "ray_source": src_result,
         "proposal": None if prop is None else prop.stats(),
         "clocks": clk,
     }
@@ -620,6 +627,59 @@ def run_batched(args, wl, world, rank, local):
         "cpu_baseline": None,
     }
     return result
+
+
+def ray_source_leg(args, wl, scene, eyes, pix, gt, R, K, it0, stream, world, dev):
+    """K training steps whose R rays are generated on the device per batch from a shuffled
+    ray source over the pool's (camera, pixel) samples: no ray table."""
+    import torch
+
+    import cpx
+    import cpx_scenes as S
+
+    img = wl["img"]
+    n = wl["n"]
+    plane = img * img
+    gr, gg, gb, gm = gt
+    images, off = [], 0
+    for p in pix:  # the pool's ground truth bytes back into image planes (camera order)
+        planes = [np.zeros(plane, np.uint8) for _ in range(4)]
+        for q, src in enumerate((gr, gg, gb, gm)):
+            planes[q][p] = src[off:off + len(p)]
+        images.append(tuple(planes))
+        off += len(p)
+    cams = [cpx.Camera.make(**S.look_at_camera(e, n, img, img)) for e in eyes]
+    rsrc = cpx.RaySource(cams, images, img, img, pixel_lists=pix, white_bg=True)
+    rsrc.shuffle(wl["seed"] + 3)
+    batch = cpx.Rays(R, white_bg=True)
+    losses = torch.zeros(R, dtype=torch.float64, device=dev)
+    total = len(rsrc)
+    lr = [STEP["lr"], STEP["sh_lr"]]
+
+    def step(k):
+        rsrc.generate(scene, (k * R) % (total - R + 1), R, batch, stream=stream)
+        cpx.train_step(scene, batch, losses, start=0, length=R, mask_coef=STEP["mask_coef"],
+                       huber_delta=STEP["huber"], lam_density=STEP["lam_density"], lam_sh=STEP["lam_sh"],
+                       lr=lr[0], sh_lr=lr[1], timestep=it0 + k + 1, want_mse=False, stream=stream)
+
+    for k in range(3):
+        step(k)
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(K):
+        step(3 + k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    rsrc.check()
+    ms = dist_max(e0.elapsed_time(e1), world, True)
+    rsrc.close()
+    return {"value": round(world * R * K / (ms / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms / K, 4),
+            "samples": total, "what": "rays generated per batch on the device (cpx_ray_source, shuffled), "
+                                      "no ray table; images %d x %dx%d bytes x 4 planes on the device"
+                                      % (len(cams), img, img)}
 
 
 def proposal_net(args):
