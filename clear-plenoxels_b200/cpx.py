@@ -64,6 +64,7 @@ EXPORTED = [
     "cpx_carve_silhouette", "cpx_grid_bbox",
     "cpx_ray_source_create", "cpx_ray_source_destroy", "cpx_ray_source_count", "cpx_ray_source_shuffle",
     "cpx_ray_source_keys", "cpx_ray_source_generate", "cpx_ray_source_check",
+    "cpx_grid_save_text", "cpx_grid_load_text", "cpx_image_load_text", "cpx_image_mask_pixels",
 ]
 
 
@@ -214,6 +215,10 @@ _sig("cpx_ray_source_shuffle", [_vp, C.c_uint64, C.c_int])
 _sig("cpx_ray_source_keys", [_vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int)])
 _sig("cpx_ray_source_generate", [_vp, _vp, C.c_int64, C.c_int, _vp, _vp])
 _sig("cpx_ray_source_check", [_vp])
+_sig("cpx_grid_save_text", [_vp, C.c_char_p, C.c_int, C.c_int, C.c_int])
+_sig("cpx_grid_load_text", [_vp, C.c_char_p, C.c_int])
+_sig("cpx_image_load_text", [C.c_char_p, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int)])
+_sig("cpx_image_mask_pixels", [C.POINTER(C.c_int), C.c_int, _vp, C.POINTER(C.c_int64)])
 _sig("cpx_carve_silhouette", [_vp, C.POINTER(C.c_double), C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp])
 _sig("cpx_grid_bbox", [_vp, C.POINTER(C.c_int), C.POINTER(C.c_double)])
 _sig("cpx_batch_create", [C.POINTER(BatchScene), C.c_int, C.POINTER(StepArgs), C.POINTER(_vp)])
@@ -690,6 +695,37 @@ def carve_silhouette(scene: "ObjectScene", projection, image, img_w: int, img_h:
                                      r.ctypes.data, g.ctypes.data, b.ctypes.data,
                                      None if m is None else m.ctypes.data, int(radius), _stream(stream)),
            "cpx_carve_silhouette")
+
+
+def save_text(scene: "ObjectScene", directory: str, band: int, density_only: bool = False,
+              hierarchy_mode: bool = False):
+    """objectScene::saveSelf (SceneUtils.cu:1246-1300): the reference's text checkpoint."""
+    _check(_lib.cpx_grid_save_text(scene.handle, str(directory).encode(), int(band), 1 if density_only else 0,
+                                   1 if hierarchy_mode else 0), "cpx_grid_save_text")
+
+
+def load_text(scene: "ObjectScene", directory: str, file_sh_dim: int):
+    """objectScene::initFromFile (SceneUtils.cu:703-790), dense."""
+    _check(_lib.cpx_grid_load_text(scene.handle, str(directory).encode(), int(file_sh_dim)), "cpx_grid_load_text")
+
+
+def load_image_text(prefix: str, width: int, height: int, gray_only: bool = False, use_mask: bool = True):
+    """Image::initSelfFromFile (ImageUtils.cu:84-128): planes (r, g, b, mask) or (gray, mask),
+    the mask bounds, and the mask-area pixel list (processMasksInfo) when use_mask."""
+    n = int(width) * int(height)
+    planes = [np.zeros(n, np.uint8) for _ in range(5)]
+    box = (C.c_int * 4)()
+    _check(_lib.cpx_image_load_text(str(prefix).encode(), int(width), int(height), 1 if gray_only else 0,
+                                    planes[0].ctypes.data, planes[1].ctypes.data, planes[2].ctypes.data,
+                                    planes[3].ctypes.data, planes[4].ctypes.data, box), "cpx_image_load_text")
+    pix = None
+    if use_mask:
+        cnt = C.c_int64()
+        _check(_lib.cpx_image_mask_pixels(box, int(width), None, C.byref(cnt)), "cpx_image_mask_pixels")
+        pix = np.zeros(cnt.value, np.int32)
+        _check(_lib.cpx_image_mask_pixels(box, int(width), pix.ctypes.data, C.byref(cnt)), "cpx_image_mask_pixels")
+    img = (planes[3], planes[4]) if gray_only else (planes[0], planes[1], planes[2], planes[4])
+    return img, tuple(box[:]), pix
 
 
 def grid_bbox(scene: "ObjectScene", scale_ratio: bool = False):

@@ -264,6 +264,26 @@ cpx_status cpx_carve_silhouette(cpx_grid* g, const double* projection, int img_w
  * Synchronous. */
 cpx_status cpx_grid_bbox(cpx_grid* g, int* bbox_out, double* scale_ratio_out);
 
+/* ------------------------------------------------------------------ text formats */
+/* objectScene::saveSelf (SVRF/SceneUtils.cu:1246-1300) into the existing directory `dir`:
+ * occupancy.txt, opacity_band<band>.txt and <red|green|blue>_<k>.txt for the first (band+1)^2
+ * coefficients (from band^2 with hierarchy_mode), or the sparse files; rows of "%.6lf " values
+ * as the reference writes them (saveFloaters2File, SVRF/Utils.cu:648).  Synchronous. */
+cpx_status cpx_grid_save_text(const cpx_grid* g, const char* dir, int band, int density_only, int hierarchy_mode);
+/* objectScene::initFromFile (SVRF/SceneUtils.cu:703-790), dense: the density and the first
+ * file_sh_dim SH coefficients per channel from `dir` into a dense grid of at least that many
+ * (the rest zero); values parsed as the reference's fscanf("%f ").  Synchronous. */
+cpx_status cpx_grid_load_text(cpx_grid* g, const char* dir, int file_sh_dim);
+/* Image::initSelfFromFile (SVRF/ImageUtils.cu:84-128): <prefix>_mask.txt and
+ * <prefix>_{red,green,blue}.txt (or <prefix>.txt when gray_only) into host planes of
+ * width*height bytes; bbox[4] = the rows and columns bounding the nonzero mask pixels
+ * (row min, row max, col min, col max; readMask, SVRF/Utils.cu:508). */
+cpx_status cpx_image_load_text(const char* prefix, int width, int height, int gray_only, uint8_t* red, uint8_t* green,
+                               uint8_t* blue, uint8_t* gray, uint8_t* mask, int* bbox);
+/* processMasksInfo's masksIndex (SVRF/ImageUtils.cu:130-146): the pixels of the bbox rectangle,
+ * row by row -- the mask-area rays' pixel list.  index_out NULL: only the count. */
+cpx_status cpx_image_mask_pixels(const int* bbox, int width, int32_t* index_out, int64_t* n_out);
+
 /* March options (no reference counterpart; for studying the mixed forms):
  * CPX_OPT_NO_EMPTY_SKIP  the FP32 march steps through every empty cell of a sparse grid as
  *                        the reference does, instead of jumping over empty cells and bricks;

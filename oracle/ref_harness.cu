@@ -537,6 +537,55 @@ int ref_bbox_silhouette(void* h, int ncam, const double* proj, const uint8_t* im
     return fail(cudaDeviceSynchronize());
 }
 
+// objectScene::saveSelf (SceneUtils.cu:1246-1300) of the harness scene into `dir`.
+int ref_save_text(void* h, const char* dir, int density_only, int band, int hierarchy_mode)
+{
+    RefCtx* c = (RefCtx*)h;
+    ObjectScene& s = c->scene;
+    if (s.sparse) {
+        // the host copies of the sparse tables that initSelfByUpsample allocates
+        // (SceneUtils.cu:542, 548) and copy2HostMemory fills before saving
+        const size_t N = (size_t)s.sceneWidth * s.sceneHeight * s.sceneDepth;
+        if (!s.inCageInfoHost) s.inCageInfoHost = (uchar*)calloc(N, sizeof(uchar));
+        if (!s.indexOffsetsHost) s.indexOffsetsHost = (unsigned int*)malloc(sizeof(unsigned int) * N);
+    }
+    s.saveSelf(dir, density_only != 0, band, hierarchy_mode != 0);
+    return fail(cudaDeviceSynchronize());
+}
+
+// objectScene::initFromFile (SceneUtils.cu:703-790) of a dense checkpoint in `dir` into a
+// fresh scene, its planar parameters [1 + 3 target_sh][W*H*D] to host memory.
+int ref_load_text(const char* dir, int W, int H, int D, float step, int sh_dim, int target_sh, float* planar_out)
+{
+    ObjectScene sc;
+    sc.initFromFile(dir, W, H, D, false, step, sh_dim, target_sh, false, false);
+    int rc = fail(cudaDeviceSynchronize());
+    const int na = 1 + 3 * sc.sh_dim;
+    std::vector<float*> p(sc.totalVariableGPUPtrs, sc.totalVariableGPUPtrs + na);
+    if (!rc) rc = copy_table(p, na, sc.actualGridNums, planar_out, false);
+    sc.freeSelf();
+    return rc;
+}
+
+// Image::initSelfFromFile (ImageUtils.cu:84-128) of the colour image at `prefix` with its mask:
+// planes r, g, b, mask (w*h bytes each) into planes_out, bbox[4], and the mask-area pixel list
+// (masksIndex, up to w*h entries) with its length.
+int ref_image_load_text(const char* prefix, int w, int h, uint8_t* planes_out, int* bbox_out, int* index_out,
+                        int* n_out)
+{
+    Image im;
+    im.initSelfFromFile(prefix, w, h, false, true);
+    const size_t n = (size_t)w * h;
+    std::memcpy(planes_out, im.redHost, n);
+    std::memcpy(planes_out + n, im.greenHost, n);
+    std::memcpy(planes_out + 2 * n, im.blueHost, n);
+    std::memcpy(planes_out + 3 * n, im.maskHost, n);
+    for (int i = 0; i < 4; i++) bbox_out[i] = im.bbox[i];
+    *n_out = im.masksLen;
+    std::memcpy(index_out, im.masksIndex, sizeof(int) * (size_t)im.masksLen);
+    return fail(cudaDeviceSynchronize());
+}
+
 // The scene's density-LR multipliers (dense) to host memory.
 int ref_adaptive_lr(void* h, float* out)
 {

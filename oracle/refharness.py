@@ -57,6 +57,9 @@ def _setup(L):
     s("ref_bbox_silhouette", [_vp, C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
                               C.POINTER(C.c_double)])
     s("ref_adaptive_lr", [_vp, _vp])
+    s("ref_save_text", [_vp, C.c_char_p, C.c_int, C.c_int, C.c_int])
+    s("ref_load_text", [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, _vp])
+    s("ref_image_load_text", [C.c_char_p, C.c_int, C.c_int, _vp, _vp, _vp, C.POINTER(C.c_int)])
     s("ref_rays_download", [_vp] + [_vp] * 17)
     s("ref_render_forward", [_vp, C.c_int, C.c_int])
     s("ref_render_backward", [_vp, C.c_int, C.c_int, C.c_double, C.c_float, _vp])
@@ -210,6 +213,10 @@ class RefScene:
             "bbox_silhouette")
         return tuple(int(x) for x in box), sr.value
 
+    def save_text(self, directory, band, density_only=False, hierarchy_mode=False):
+        _ck(lib().ref_save_text(self.h, str(directory).encode(), 1 if density_only else 0, int(band),
+                                1 if hierarchy_mode else 0), "save_text")
+
     def adaptive_lr(self):
         out = np.zeros(self.W * self.H * self.D, np.float32)
         _ck(lib().ref_adaptive_lr(self.h, _p(out)), "adaptive_lr")
@@ -253,3 +260,22 @@ class RefScene:
             self.close()
         except Exception:
             pass
+
+
+def load_text(directory, W, H, D, step, sh_dim, target_sh):
+    """objectScene::initFromFile of a dense checkpoint: planar parameters [1 + 3 target_sh][W*H*D]."""
+    out = np.zeros((1 + 3 * target_sh, W * H * D), np.float32)
+    _ck(lib().ref_load_text(str(directory).encode(), W, H, D, float(step), int(sh_dim), int(target_sh), _p(out)),
+        "load_text")
+    return out
+
+
+def image_load_text(prefix, w, h):
+    """Image::initSelfFromFile with mask: (r, g, b, mask) planes, bbox, masksIndex."""
+    planes = np.zeros((4, w * h), np.uint8)
+    box = np.zeros(4, np.int32)
+    idx = np.zeros(w * h, np.int32)
+    n = C.c_int()
+    _ck(lib().ref_image_load_text(str(prefix).encode(), int(w), int(h), _p(planes), _p(box), _p(idx), C.byref(n)),
+        "image_load_text")
+    return tuple(planes), tuple(int(x) for x in box), idx[:n.value].copy()
