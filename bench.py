@@ -54,6 +54,15 @@ WORKLOADS = {
     # views; the hidden grid is the same sparse structure with SH ~ N(0, 0.5)
     "sparse512": dict(n=512, gt_n=512, n_blobs=4, gt_sh_std=0.5, cams=100, img=800, batch=16384,
                       pool_batches=16, init_density=0.1, seed=1, sparse_threshold=1.0),
+    # the batched form's configuration: 16 scenes, grids 64^3..384^3, 8-128 blobs, 1024-16384-ray
+    # batches (seeded choices, held under about 135 M vertices in total so the FP32 form fits)
+    "multi16": dict(multi=[dict(n=n, gt_n=n, n_blobs=b, gt_sh_std=0.5, cams=8, img=256, batch=r, pool_batches=2,
+                                init_density=0.1, seed=200 + i)
+                           for i, (n, b, r) in enumerate(zip(
+                               [64, 384, 96, 128, 192, 64, 256, 96, 128, 320, 64, 160, 96, 192, 128, 64],
+                               [8, 64, 16, 32, 96, 8, 128, 24, 40, 112, 12, 48, 20, 72, 36, 10],
+                               [1024, 16384, 2048, 4096, 8192, 1024, 16384, 2048, 4096, 16384, 1024, 4096,
+                                2048, 8192, 4096, 1024]))]),
     # the batched form's workload: 24 dense scenes of uneven size (48^3 .. 192^3) and uneven batch
     # length (512 .. 4096 rays), each fitted to 8 128x128 views of its own hidden 8-blob grid
     "multi24": dict(multi=[dict(n=n, gt_n=n, n_blobs=8, gt_sh_std=0.5, cams=8, img=128, batch=b, pool_batches=4,
@@ -603,7 +612,8 @@ def run_batched(args, wl, world, rank, local):
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.precision == "fp32" else "f32 arithmetic, %s SH + bf16 moments" % args.precision,
-        "data": "synthetic: each scene fitted to its own seeded 8-blob hidden grid rendered by the plain forward",
+        "data": "synthetic: each scene fitted to its own seeded blob hidden grid (%d-%d blobs) rendered by the "
+                "plain forward" % (min(sw["n_blobs"] for sw in specs), max(sw["n_blobs"] for sw in specs)),
         "config": {
             "workload": "batched multi-scene training: %d dense scenes %d^3..%d^3 SH band 2, %d..%d-ray batches "
                         "(%d rays per iteration), TV type 0/6 + Adam every iteration, one batched step"
@@ -1004,7 +1014,7 @@ def main():
     if args.form == "proposal" and args.precision == "fp32":
         ap.error("the proposal form runs on a mixed precision (--precision bf16 or fp16)")
     if args.form == "batched" and args.workload == "plain256":
-        args.workload = "multi24"
+        args.workload = "multi16"
     wl = WORKLOADS[args.workload]
     if (args.form == "batched") != ("multi" in wl):
         ap.error("--form batched runs the multi-scene workloads, and they run only batched")

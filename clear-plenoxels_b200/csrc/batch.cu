@@ -146,7 +146,7 @@ static std::vector<SceneSig> batch_sig(const cpx_batch* b)
 
 static bool valid_tuning(const BatchTuning& t)
 {
-    return t.place_block >= 32 && t.place_block <= 256 && t.place_block % 32 == 0 &&
+    return t.place_block >= 32 && t.place_block <= 512 && t.place_block % 32 == 0 &&
            (t.shade_warps == 2 || t.shade_warps == 4 || t.shade_warps == 8) && t.grab >= 1 && t.grab <= 8;
 }
 
@@ -475,7 +475,7 @@ cpx_status cpx_batch_set_tuning(cpx_batch* b, const cpx_batch_tuning* t)
     n.shade_warps = t->shade_warps;
     n.grab = t->grab;
     if (!valid_tuning(n)) {
-        set_error("tuning outside place_block 32..256 (multiple of 32), shade_warps 2/4/8, grab 1..8");
+        set_error("tuning outside place_block 32..512 (multiple of 32), shade_warps 2/4/8, grab 1..8");
         return CPX_ERR_INVALID_ARGUMENT;
     }
     b->tuning = n;
@@ -520,16 +520,16 @@ cpx_status cpx_batch_autotune(cpx_batch* b, int steps_per_trial, cpx_batch_tunin
         cudaEventElapsedTime(ms, e0, e1);
         return CPX_OK;
     };
-    const int places[] = {32, 64, 128, 256};
+    const int places[] = {64, 128, 256, 512};
     const int warps[] = {2, 4, 8};
-    const int grabs[] = {1, 2, 4};
+    const int grabs[] = {1, 2, 4, 8};
     BatchTuning cur = b->tuning;
     float best_ms = 0.f;
     cpx_status s = trial(cur, &best_ms);
     for (int round = 0; round < 2 && s == CPX_OK; round++) {
         for (int dim = 0; dim < 3 && s == CPX_OK; dim++) {
             const int* vals = dim == 0 ? places : dim == 1 ? warps : grabs;
-            const int nv = dim == 0 ? 4 : 3;
+            const int nv = dim == 1 ? 3 : 4;
             for (int k = 0; k < nv && s == CPX_OK; k++) {
                 BatchTuning t = cur;
                 int& field = dim == 0 ? t.place_block : dim == 1 ? t.shade_warps : t.grab;

@@ -431,7 +431,7 @@ typedef struct cpx_batch_scene {
     cpx_rays* rays;
     int rays_per_batch;
 } cpx_batch_scene;
-/* Launch shapes of the batched march: threads per placement block (32..256, a multiple of
+/* Launch shapes of the batched march: threads per placement block (32..512, a multiple of
  * 32), warps per shading block (2, 4 or 8) and rays a shading warp takes per work-counter
  * access (1..8). */
 typedef struct cpx_batch_tuning {
@@ -457,7 +457,8 @@ cpx_status cpx_batch_check(cpx_batch* b);
 cpx_status cpx_batch_info(const cpx_batch* b, int* iteration, int* total_rays, int* launches_per_step);
 cpx_status cpx_batch_set_tuning(cpx_batch* b, const cpx_batch_tuning* t);
 cpx_status cpx_batch_get_tuning(const cpx_batch* b, cpx_batch_tuning* t);
-/* Coordinate-descent search of the launch shapes: every candidate runs steps_per_trial real
+/* Coordinate-descent search of the launch shapes (placement blocks of 64/128/256/512 threads,
+ * shading blocks of 2/4/8 warps, 1/2/4/8 rays per access): every candidate runs steps_per_trial real
  * training iterations (they advance training like cpx_batch_step), timed with CUDA events;
  * the fastest shapes are kept and written to best (may be NULL). */
 cpx_status cpx_batch_autotune(cpx_batch* b, int steps_per_trial, cpx_batch_tuning* best, cpx_stream stream);
