@@ -12,7 +12,7 @@
 // hardware's stochastic-rounding conversion, the consumed gradients zeroed.  Per vertex at SH
 // band 2: density r+w 8 B, SH r+w 112 B, moments r+w 224 B (+4 B learning-rate multiplier on
 // dense grids), gradients r + zero-w 224 B where touched: 348 B (+224 B) against the FP32
-// form's 684 B (+224 B).
+// form's 680 B (+224 B).
 #include "cpx_internal.cuh"
 
 namespace cpx {
@@ -230,44 +230,22 @@ __device__ __forceinline__ float2 rcp2_approx(float2 x)
 // with the element arithmetic in packed FP32 pairs (sm_100 FFMA2 / FMUL2 / FADD2: each pair
 // element rounds exactly as the scalar operation) and the square roots and reciprocals from the
 // hardware approximations.
-// The loaded operands of one quad: its SH, moments, gradients (touched vertices only) and the
-// six TV neighbours' SH (where the term applies).  Every record a quad reads is written only
-// by the same thread after the read, or not at all, so all load through the non-coherent path.
-struct QuadOps {
-    uint2 self, m, v;
-    uint2 nb[6];
-    float4 g;
-};
-
-template <bool TV>
-__device__ __forceinline__ void load_quad(const LowpArgs& a, uint32_t q, const LowpVertex& vx, const uint32_t* nbq,
-                                          QuadOps& o)
-{
-    o.self = __ldg(a.sh_in + q);
-    o.m = __ldg(a.m + q);
-    o.v = __ldg(a.v + q);
-    o.g = (vx.bits & 1u) ? __ldg(a.grad + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-    if (TV && (vx.bits & 2u)) {
-#pragma unroll
-        for (int k = 0; k < 6; k++) o.nb[k] = ((vx.bits >> (2 + k)) & 1u) ? o.self : __ldg(a.sh_in + nbq[k]);
-    }
-}
-
 template <int PREC, bool TV>
 __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint32_t q, int u, const LowpVertex& vx,
-                                             const QuadOps& o, float inv_bc1, float inv_bc2, uint32_t step_key)
+                                             const uint32_t* nbq, float inv_bc1, float inv_bc2, uint32_t step_key)
 {
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
     const float2 neg1 = make_float2(-1.f, -1.f);
-    const uint2 sh_raw = o.self;
+    const uint2 sh_raw = __ldg(a.sh_in + q);
     float2 p01, p23;
     unpack2<PREC>(sh_raw.x, p01.x, p01.y);
     unpack2<PREC>(sh_raw.y, p23.x, p23.y);
     if (u == 0) p01.x = vx.dens;  // slot 0 of an SH record is unused: density is FP32
     const bool tch = vx.bits & 1u;
-    const float4 g4 = o.g;
+    float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tch) g4 = __ldg(a.grad + q);
     float2 g01 = make_float2(g4.x, g4.y), g23 = make_float2(g4.z, g4.w);
-    const uint2 m_raw = o.m, v_raw = o.v;
+    const uint2 m_raw = __ldg(a.m + q), v_raw = __ldg(a.v + q);
     float2 mo01, mo23, vo01, vo23;
     unpack2<kPrecBF16>(m_raw.x, mo01.x, mo01.y);
     unpack2<kPrecBF16>(m_raw.y, mo23.x, mo23.y);
@@ -279,7 +257,7 @@ __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint
         for (int k = 0; k < 6; k++) {
             float2 n01 = p01, n23 = p23;
             if (!((vx.bits >> (2 + k)) & 1u)) {
-                const uint2 w = o.nb[k];
+                const uint2 w = __ldg(a.sh_in + nbq[k]);
                 unpack2<PREC>(w.x, n01.x, n01.y);
                 unpack2<PREC>(w.y, n23.x, n23.y);
             }
@@ -332,13 +310,10 @@ template <int PREC, int E, bool TV>
 __device__ __forceinline__ void lowp_step(const LowpArgs& a, uint32_t v, uint32_t q, int u, const LowpVertex& vx,
                                           const uint32_t* nbq, float inv_bc1, float inv_bc2, uint32_t step_key)
 {
-    if (E == 4 && a.full_masks) {
-        QuadOps o;
-        load_quad<TV>(a, q, vx, nbq, o);
-        lowp_quad_x2<PREC, TV>(a, v, q, u, vx, o, inv_bc1, inv_bc2, step_key);
-    } else {
+    if (E == 4 && a.full_masks)
+        lowp_quad_x2<PREC, TV>(a, v, q, u, vx, nbq, inv_bc1, inv_bc2, step_key);
+    else
         lowp_unit<PREC, E, TV>(a, v, q, u, vx, nbq, inv_bc1, inv_bc2, step_key);
-    }
 }
 
 // Bias corrections and the stochastic-rounding key of this step into shared memory.
@@ -388,39 +363,6 @@ __global__ void __launch_bounds__(256, 4) k_sweep_lowp_dense(LowpArgs a)
             if (a.clear && (v & 31u) == 0) a.clear[v >> 5] = 0u;
         }
         const uint32_t nx = min(32u, (uint32_t)a.W - x0);  // vertices of this chunk
-        if (E == 4 && a.full_masks) {
-            // two quads per step: both quads' loads are issued before either's arithmetic, so
-            // twice the bytes are in flight per warp
-#pragma unroll
-            for (int it = 0; it < U; it += 2) {
-                const int nq = it + 1 < U ? 2 : 1;
-                QuadOps o[2];
-                LowpVertex vx[2];
-                uint32_t vv[2], q[2];
-                int u[2];
-                bool ok[2];
-#pragma unroll
-                for (int k = 0; k < 2; k++) {
-                    if (k >= nq) break;
-                    const uint32_t i = (it + k) * 32u + lane;
-                    const uint32_t vl = i / U;
-                    u[k] = (int)(i - vl * U);
-                    vx[k] = shfl_vertex(mine, (int)vl);
-                    ok[k] = vl < nx;
-                    vv[k] = v0 + x0 + vl;
-                    q[k] = vv[k] * U + u[k];
-                    const uint32_t nbq[6] = {q[k] + off[0], q[k] + off[1], q[k] + off[2],
-                                             q[k] + off[3], q[k] + off[4], q[k] + off[5]};
-                    if (ok[k]) load_quad<TV>(a, q[k], vx[k], nbq, o[k]);
-                }
-#pragma unroll
-                for (int k = 0; k < 2; k++) {
-                    if (k >= nq) break;
-                    if (ok[k]) lowp_quad_x2<PREC, TV>(a, vv[k], q[k], u[k], vx[k], o[k], s_bc[0], s_bc[1], s_key);
-                }
-            }
-            continue;
-        }
 #pragma unroll
         for (int it = 0; it < U; it++) {
             const uint32_t i = it * 32u + lane;
