@@ -180,3 +180,46 @@ def test_train_step_with_proposal(setup):
     assert st["rounds"] == 4  # iterations 0, 9 (end of warm-up), 10 and 20
     assert mses[-1] < mses[0]
     prop.close()
+
+
+def test_trained_network_gains_over_the_untrained(setup):
+    """What the trained network buys over the method without it: the same guided march, masks
+    from an untrained network and from one trained on the full march's labels, each against
+    the full march.  The trained masks keep the colours close to the full march's while
+    skipping a large share of the samples; the untrained masks skip content at random."""
+    import cpx
+
+    cfg, scene, rays, geo, torch = setup
+    nr = rays.total_rays
+    fields = ("acc_r", "acc_g", "acc_b")
+
+    def forward(masks):
+        cpx.render_forward_guided(scene, rays, masks=masks)
+        scene.check()
+        out = rays.download(fields=fields)
+        return np.stack([out[k] for k in fields], 1), scene.last_sample_counts(nr)
+
+    rgb_full, n_full = forward(None)
+    prop = cpx.Proposal(seed=5)
+    masks = torch.zeros(nr, dtype=torch.int32, device="cuda")
+
+    def guided():
+        prop.masks_into(scene, rays, masks)
+        rgb, n = forward(masks)
+        return 1.0 - n.sum() / n_full.sum(), np.abs(rgb - rgb_full)
+
+    saved_u, err_u = guided()
+    seg_w = torch.zeros((nr, cpx.Proposal.SEGMENTS), dtype=torch.float32, device="cuda")
+    losses = torch.zeros(nr, dtype=torch.float64, device="cuda")
+    cpx.render_guided(scene, rays, losses, seg_weights=seg_w)  # the full march's labels
+    for _ in range(40):
+        prop.train(scene, rays, seg_w, 16, rays_per_step=1024)
+    saved_t, err_t = guided()
+    print(f"untrained: saved {saved_u:.3f} error mean {err_u.mean():.2e} max {err_u.max():.3f}; "
+          f"trained: saved {saved_t:.3f} error mean {err_t.mean():.2e} max {err_t.max():.3f}")
+    # measured: untrained 6% saved, colour error up to 0.26; trained 90% saved, error 1.9e-4
+    # mean, 2e-3 max
+    assert saved_t > 0.5
+    assert err_t.mean() < 1e-3 and err_t.max() < 0.02 and err_t.max() < err_u.max()
+    assert prop.stats()["error_flags"] == 0
+    prop.close()
