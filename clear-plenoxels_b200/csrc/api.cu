@@ -376,6 +376,7 @@ cpx_status cpx_grid_create(const cpx_grid_desc* d, cpx_grid** out)
         count_launch();
         e = cudaDeviceSynchronize();
     }
+    if (e == cudaSuccess && g->prec != kPrecFP32) lowp_prepare();
     if (e == cudaSuccess && refresh_dense_skip(g, 0) != CPX_OK) e = cudaErrorMemoryAllocation;
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {

@@ -381,6 +381,9 @@ cpx_status proposal_train(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const
                           const float* seg_w, int steps, int rays_per_step, bool adam, cudaStream_t st);
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
                       double sh_lr, int timestep, cudaStream_t s, const int* t_dev = nullptr);
+// Once per process, before any graph capture (grid creation of a mixed form calls it): the
+// shared-memory opt-in of the mixed forms' pipelined dense sweep.
+cpx_status lowp_prepare();
 cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
                            int timestep, uint32_t tv_mask, uint32_t adam_mask, cudaStream_t st,
                            const int* t_dev = nullptr);

@@ -230,22 +230,58 @@ __device__ __forceinline__ float2 rcp2_approx(float2 x)
 // with the element arithmetic in packed FP32 pairs (sm_100 FFMA2 / FMUL2 / FADD2: each pair
 // element rounds exactly as the scalar operation) and the square roots and reciprocals from the
 // hardware approximations.
-template <int PREC, bool TV>
+// Operand sources of lowp_quad_x2.  From global memory: every record a quad reads is written
+// only by the same thread after the read, or not at all, so all of them load through the
+// non-coherent path.
+struct QuadGlobal {
+    const LowpArgs& a;
+    uint32_t q;
+    const uint32_t* nbq;
+    __device__ uint2 self() const { return __ldg(a.sh_in + q); }
+    __device__ uint2 nb(int k) const { return __ldg(a.sh_in + nbq[k]); }
+    __device__ uint2 m() const { return __ldg(a.m + q); }
+    __device__ uint2 v() const { return __ldg(a.v + q); }
+    __device__ float4 grad() const { return __ldg(a.grad + q); }
+};
+
+// From the lane's own shared-memory slots, filled by its cp.async copies: slot k of 8 bytes at
+// s8 + k * stride (SH, m, v, the six neighbours), the gradient quad at g16.
+struct QuadStaged {
+    uint32_t s8, stride, g16;
+    __device__ static uint2 ld8(uint32_t addr)
+    {
+        uint2 r;
+        asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(r.x), "=r"(r.y) : "r"(addr));
+        return r;
+    }
+    __device__ uint2 self() const { return ld8(s8); }
+    __device__ uint2 m() const { return ld8(s8 + stride); }
+    __device__ uint2 v() const { return ld8(s8 + 2 * stride); }
+    __device__ uint2 nb(int k) const { return ld8(s8 + (3 + k) * stride); }
+    __device__ float4 grad() const
+    {
+        float4 r;
+        asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w) : "r"(g16));
+        return r;
+    }
+};
+
+template <int PREC, bool TV, class Src>
 __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint32_t q, int u, const LowpVertex& vx,
-                                             const uint32_t* nbq, float inv_bc1, float inv_bc2, uint32_t step_key)
+                                             const Src& src, float inv_bc1, float inv_bc2, uint32_t step_key)
 {
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
     const float2 neg1 = make_float2(-1.f, -1.f);
-    const uint2 sh_raw = __ldg(a.sh_in + q);
+    const uint2 sh_raw = src.self();
     float2 p01, p23;
     unpack2<PREC>(sh_raw.x, p01.x, p01.y);
     unpack2<PREC>(sh_raw.y, p23.x, p23.y);
     if (u == 0) p01.x = vx.dens;  // slot 0 of an SH record is unused: density is FP32
     const bool tch = vx.bits & 1u;
     float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (tch) g4 = __ldg(a.grad + q);
+    if (tch) g4 = src.grad();
     float2 g01 = make_float2(g4.x, g4.y), g23 = make_float2(g4.z, g4.w);
-    const uint2 m_raw = __ldg(a.m + q), v_raw = __ldg(a.v + q);
+    const uint2 m_raw = src.m(), v_raw = src.v();
     float2 mo01, mo23, vo01, vo23;
     unpack2<kPrecBF16>(m_raw.x, mo01.x, mo01.y);
     unpack2<kPrecBF16>(m_raw.y, mo23.x, mo23.y);
@@ -257,7 +293,7 @@ __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint
         for (int k = 0; k < 6; k++) {
             float2 n01 = p01, n23 = p23;
             if (!((vx.bits >> (2 + k)) & 1u)) {
-                const uint2 w = __ldg(a.sh_in + nbq[k]);
+                const uint2 w = src.nb(k);
                 unpack2<PREC>(w.x, n01.x, n01.y);
                 unpack2<PREC>(w.y, n23.x, n23.y);
             }
@@ -311,7 +347,7 @@ __device__ __forceinline__ void lowp_step(const LowpArgs& a, uint32_t v, uint32_
                                           const uint32_t* nbq, float inv_bc1, float inv_bc2, uint32_t step_key)
 {
     if (E == 4 && a.full_masks)
-        lowp_quad_x2<PREC, TV>(a, v, q, u, vx, nbq, inv_bc1, inv_bc2, step_key);
+        lowp_quad_x2<PREC, TV>(a, v, q, u, vx, QuadGlobal{a, q, nbq}, inv_bc1, inv_bc2, step_key);
     else
         lowp_unit<PREC, E, TV>(a, v, q, u, vx, nbq, inv_bc1, inv_bc2, step_key);
 }
@@ -420,12 +456,156 @@ __global__ void __launch_bounds__(256) k_sweep_lowp_sparse(LowpArgs a)
     }
 }
 
+// Dense grid, every slot under TV and Adam, copies one quad ahead.  The layout of work is that
+// of k_sweep_lowp_dense (block per row, warp per 32 vertices, lane per quad); each lane copies
+// its next quad's operands -- SH, moments, the gradients of a touched vertex, the six TV
+// neighbours' SH -- into its own shared-memory slots with cp.async while it updates the
+// current quad from the slots the previous copies filled.  A lane reads only the slots it
+// filled itself (after cp.async.wait_group), so no barrier is involved, and the operands in
+// flight take no registers.
+constexpr int kAsyncThreads = 256;
+constexpr int kAsyncSlots = 9;  // 8-byte slots per quad: SH, m, v, six neighbours
+
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+// Waits until at most n of this thread's copy groups are still in flight (n a constant once
+// the caller's loop is unrolled).
+__device__ __forceinline__ void cp_async_wait(int n)
+{
+    switch (n) {
+    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+    default: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+    }
+}
+
+// Quads in flight per lane, the one in use included.  Measured at 256^3: 2 stages (4 blocks per
+// SM) 1.56 ms, 3 or 4 stages (fewer resident blocks) 1.89 ms.
+constexpr int kAsyncStages = 2;
+constexpr int kAsyncStageBytes = kAsyncSlots * kAsyncThreads * 8 + kAsyncThreads * 16;
+constexpr int kAsyncSmem = kAsyncStages * kAsyncStageBytes;
+constexpr int kAsyncBlocks = (226 * 1024) / (kAsyncSmem + 1152) < 4 ? (226 * 1024) / (kAsyncSmem + 1152) : 4;
+
+template <int PREC, int S, bool TV>
+__global__ void __launch_bounds__(kAsyncThreads, kAsyncBlocks) k_sweep_lowp_dense_async(LowpArgs a)
+{
+    constexpr int U = S;  // quads per vertex
+    constexpr int NS = kAsyncStages;
+    extern __shared__ __align__(16) unsigned char async_smem[];
+    __shared__ float s_bc[2];
+    __shared__ uint32_t s_key;
+    lowp_bias_corrections(a, s_bc, &s_key);
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x;
+    const int y = row % a.H;
+    const int z = row / a.H;
+    const uint32_t WH = (uint32_t)a.W * a.H;
+    const uint32_t v0 = (uint32_t)z * WH + (uint32_t)y * a.W;
+    const bool row_interior = y >= 1 && y <= a.H - 2 && z >= 1 && z <= a.D - 2;
+    const uint32_t off[6] = {0u - WH * U, 0u - (uint32_t)a.W * U, 0u - (uint32_t)U, (uint32_t)U,
+                             (uint32_t)a.W * U, WH * U};
+    // stage k: 9 slot rows of 8 bytes per thread, then the thread's 16-byte gradient slot
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(async_smem);
+    const uint32_t stride = kAsyncThreads * 8;  // bytes between a thread's slots
+    const uint32_t slot0 = base + threadIdx.x * 8;
+    const uint32_t g0 = base + kAsyncSlots * kAsyncThreads * 8 + threadIdx.x * 16;
+    for (uint32_t x0 = (threadIdx.x >> 5) * 32u; x0 < (uint32_t)a.W; x0 += blockDim.x) {
+        const uint32_t x = x0 + lane;
+        const uint32_t v = v0 + x;
+        LowpVertex mine;
+        mine.dens = mine.tv0 = mine.lr_d = 0.f;
+        mine.bits = 0;
+        if (x < (uint32_t)a.W) {
+            const bool tv_on = row_interior && x >= 1 && x + 2 <= (uint32_t)a.W;
+            const uint32_t nb_v[6] = {v - WH, v - (uint32_t)a.W, v - 1u, v + 1u, v + (uint32_t)a.W, v + WH};
+            const float lr_d = a.adaptive_lr ? a.lr * a.adaptive_lr[v] : a.lr;
+            mine = lowp_vertex<TV>(a, v, tv_on, nb_v, 0u, lr_d);
+            if (a.clear && (v & 31u) == 0) a.clear[v >> 5] = 0u;
+        }
+        const uint32_t nx = min(32u, (uint32_t)a.W - x0);
+        // the copies of quad `it` into stage it % NS (every lane commits a group, empty or not)
+        auto issue = [&](int it) {
+            const uint32_t i = it * 32u + lane;
+            const uint32_t vl = i / U;
+            const LowpVertex vx = shfl_vertex(mine, (int)vl);
+            if (vl < nx) {
+                const uint32_t q = (v0 + x0 + vl) * U + (i - vl * U);
+                const uint32_t d = slot0 + (it % NS) * kAsyncStageBytes;
+                cp_async8(d, a.sh_in + q);
+                cp_async8(d + stride, a.m + q);
+                cp_async8(d + 2 * stride, a.v + q);
+                if (vx.bits & 1u) cp_async16(g0 + (it % NS) * kAsyncStageBytes, a.grad + q);
+                if (TV && (vx.bits & 2u)) {
+#pragma unroll
+                    for (int k = 0; k < 6; k++) cp_async8(d + (3 + k) * stride, a.sh_in + (q + off[k]));
+                }
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+#pragma unroll
+        for (int it = 0; it < NS - 1 && it < U; it++) issue(it);
+#pragma unroll
+        for (int it = 0; it < U; it++) {
+            if (it + NS - 1 < U) issue(it + NS - 1);
+            // groups committed after quad it's: min(NS - 1, U - 1 - it)
+            cp_async_wait(U - 1 - it < NS - 1 ? U - 1 - it : NS - 1);
+            const uint32_t i = it * 32u + lane;
+            const uint32_t vl = i / U;
+            const int u = (int)(i - vl * U);
+            const LowpVertex vx = shfl_vertex(mine, (int)vl);
+            if (vl >= nx) continue;
+            const uint32_t vv = v0 + x0 + vl;
+            const uint32_t q = vv * U + u;
+            const QuadStaged src{slot0 + (it % NS) * kAsyncStageBytes, stride, g0 + (it % NS) * kAsyncStageBytes};
+            lowp_quad_x2<PREC, TV>(a, vv, q, u, vx, src, s_bc[0], s_bc[1], s_key);
+        }
+    }
+}
+
+// Once per process, before any graph capture: the async sweep's dynamic shared-memory opt-in.
+template <int PREC, int S>
+static bool async_opt_in()
+{
+    return cudaFuncSetAttribute(k_sweep_lowp_dense_async<PREC, S, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kAsyncSmem) == cudaSuccess &&
+           cudaFuncSetAttribute(k_sweep_lowp_dense_async<PREC, S, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kAsyncSmem) == cudaSuccess;
+}
+
+static int g_async_ready = -1;  // -1: not yet asked; 0: unavailable (the row sweep serves); 1: ready
+
+cpx_status lowp_prepare()
+{
+    if (g_async_ready >= 0) return CPX_OK;
+    const bool ok = async_opt_in<kPrecBF16, 1>() && async_opt_in<kPrecBF16, 4>() && async_opt_in<kPrecBF16, 7>() &&
+                    async_opt_in<kPrecFP16, 1>() && async_opt_in<kPrecFP16, 4>() && async_opt_in<kPrecFP16, 7>();
+    if (!ok) cudaGetLastError();
+    g_async_ready = ok ? 1 : 0;
+    return CPX_OK;
+}
+
 // slots a thread updates: quads (pairs measured slower: twice the loads for the same bytes)
 constexpr int kLowpUnit = 4;
 
 template <int PREC, int S>
 static void launch_lowp(const cpx_grid* g, const LowpArgs& a, bool tv, cudaStream_t st)
 {
+    if (!g->sparse && a.full_masks && g_async_ready == 1) {
+        const unsigned rows = (unsigned)((int64_t)g->H * g->D);
+        if (tv)
+            k_sweep_lowp_dense_async<PREC, S, true><<<rows, kAsyncThreads, kAsyncSmem, st>>>(a);
+        else
+            k_sweep_lowp_dense_async<PREC, S, false><<<rows, kAsyncThreads, kAsyncSmem, st>>>(a);
+        return;
+    }
     if (!g->sparse) {
         const unsigned rows = (unsigned)((int64_t)g->H * g->D);
         if (tv)
