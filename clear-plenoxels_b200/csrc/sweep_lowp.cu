@@ -570,6 +570,78 @@ __global__ void __launch_bounds__(kAsyncThreads, kAsyncBlocks) k_sweep_lowp_dens
     }
 }
 
+// Sparse grid, copies one quad ahead: the work of k_sweep_lowp_sparse (a warp per 32 compact
+// vertices, lane per quad, neighbourhoods shared by shuffle) with the operands of each lane's
+// next quad -- including its gathered TV neighbours -- copied into its own shared-memory slots
+// by cp.async while it updates the current one (as k_sweep_lowp_dense_async).
+template <int PREC, int S, bool TV>
+__global__ void __launch_bounds__(kAsyncThreads, kAsyncBlocks) k_sweep_lowp_sparse_async(LowpArgs a)
+{
+    constexpr int U = S;
+    constexpr int NS = kAsyncStages;
+    extern __shared__ __align__(16) unsigned char async_smem[];
+    __shared__ float s_bc[2];
+    __shared__ uint32_t s_key;
+    lowp_bias_corrections(a, s_bc, &s_key);
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t v0 = warp * 32u;
+    if (v0 >= a.n_act) return;  // warp-uniform; no copy is in flight yet
+    SparseTv mine;
+    mine.flags = 0;
+#pragma unroll
+    for (int k = 0; k < 6; k++) mine.nb[k] = 0;
+    LowpVertex mv;
+    mv.dens = mv.tv0 = mv.lr_d = 0.f;
+    mv.bits = 0;
+    if (v0 + lane < a.n_act) {
+        if (TV) mine = sparse_tv(v0 + lane, a.compact_to_dense, a.in_cage, a.index_offsets, a.W, a.H, a.D);
+        mv = lowp_vertex<TV>(a, v0 + lane, (mine.flags >> 6) & 1u, mine.nb, mine.flags & 63u, a.lr);
+        if (a.clear && ((v0 + lane) & 31u) == 0) a.clear[(v0 + lane) >> 5] = 0u;
+    }
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(async_smem);
+    const uint32_t stride = kAsyncThreads * 8;
+    const uint32_t slot0 = base + threadIdx.x * 8;
+    const uint32_t g0 = base + kAsyncSlots * kAsyncThreads * 8 + threadIdx.x * 16;
+    auto issue = [&](int it) {
+        const uint32_t i = it * 32u + lane;
+        const uint32_t vl = i / U;
+        const uint32_t u = i - vl * U;
+        const SparseTv t = TV ? shfl_tv(mine, (int)vl) : mine;
+        const LowpVertex vx = shfl_vertex(mv, (int)vl);
+        const uint32_t v = v0 + vl;
+        if (v < a.n_act) {
+            const uint32_t q = v * U + u;
+            const uint32_t d = slot0 + (it % NS) * kAsyncStageBytes;
+            cp_async8(d, a.sh_in + q);
+            cp_async8(d + stride, a.m + q);
+            cp_async8(d + 2 * stride, a.v + q);
+            if (vx.bits & 1u) cp_async16(g0 + (it % NS) * kAsyncStageBytes, a.grad + q);
+            if (TV && (vx.bits & 2u)) {
+#pragma unroll
+                for (int k = 0; k < 6; k++)
+                    if (!((vx.bits >> (2 + k)) & 1u)) cp_async8(d + (3 + k) * stride, a.sh_in + (t.nb[k] * U + u));
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+#pragma unroll
+    for (int it = 0; it < NS - 1 && it < U; it++) issue(it);
+#pragma unroll
+    for (int it = 0; it < U; it++) {
+        if (it + NS - 1 < U) issue(it + NS - 1);
+        cp_async_wait(U - 1 - it < NS - 1 ? U - 1 - it : NS - 1);
+        const uint32_t i = it * 32u + lane;
+        const uint32_t vl = i / U;
+        const int u = (int)(i - vl * U);
+        const LowpVertex vx = shfl_vertex(mv, (int)vl);
+        const uint32_t v = v0 + vl;
+        if (v >= a.n_act) continue;
+        const QuadStaged src{slot0 + (it % NS) * kAsyncStageBytes, stride, g0 + (it % NS) * kAsyncStageBytes};
+        lowp_quad_x2<PREC, TV>(a, v, v * U + u, u, vx, src, s_bc[0], s_bc[1], s_key);
+    }
+}
+
 // Once per process, before any graph capture: the async sweep's dynamic shared-memory opt-in.
 template <int PREC, int S>
 static bool async_opt_in()
@@ -577,6 +649,10 @@ static bool async_opt_in()
     return cudaFuncSetAttribute(k_sweep_lowp_dense_async<PREC, S, true>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kAsyncSmem) == cudaSuccess &&
            cudaFuncSetAttribute(k_sweep_lowp_dense_async<PREC, S, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kAsyncSmem) == cudaSuccess &&
+           cudaFuncSetAttribute(k_sweep_lowp_sparse_async<PREC, S, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kAsyncSmem) == cudaSuccess &&
+           cudaFuncSetAttribute(k_sweep_lowp_sparse_async<PREC, S, false>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kAsyncSmem) == cudaSuccess;
 }
 
@@ -612,6 +688,12 @@ static void launch_lowp(const cpx_grid* g, const LowpArgs& a, bool tv, cudaStrea
             k_sweep_lowp_dense<PREC, S, true, kLowpUnit><<<rows, 256, 0, st>>>(a);
         else
             k_sweep_lowp_dense<PREC, S, false, kLowpUnit><<<rows, 256, 0, st>>>(a);
+    } else if (a.full_masks && g_async_ready == 1) {
+        const unsigned blocks = (unsigned)(((int64_t)g->n_act + kAsyncThreads - 1) / kAsyncThreads);
+        if (tv)
+            k_sweep_lowp_sparse_async<PREC, S, true><<<blocks, kAsyncThreads, kAsyncSmem, st>>>(a);
+        else
+            k_sweep_lowp_sparse_async<PREC, S, false><<<blocks, kAsyncThreads, kAsyncSmem, st>>>(a);
     } else {
         const unsigned blocks = (unsigned)(((int64_t)g->n_act + 255) / 256);  // a warp per 32 vertices
         if (tv)
