@@ -54,7 +54,7 @@ EXPORTED = [
     "cpx_render_forward", "cpx_render_backward", "cpx_render_forward_backward", "cpx_tv_grad",
     "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_grid_check",
     "cpx_last_sample_counts", "cpx_kernel_launches", "cpx_render_forward_backward_noalloc",
-    "cpx_render_image", "cpx_image_mse", "cpx_grid_touched_count",
+    "cpx_render_image", "cpx_image_mse", "cpx_grid_touched_count", "cpx_grid_download_cell_map",
     "cpx_proposal_param_count", "cpx_proposal_create", "cpx_proposal_destroy", "cpx_proposal_params",
     "cpx_proposal_infer", "cpx_proposal_gradient", "cpx_proposal_train", "cpx_proposal_stats",
     "cpx_render_forward_backward_guided", "cpx_train_step_proposal", "cpx_render_forward_guided",
@@ -166,6 +166,7 @@ _sig("cpx_last_sample_counts", [_vp, _i32p, C.c_int])
 _sig("cpx_render_image", [_vp, C.POINTER(Camera), C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _sig("cpx_image_mse", [_vp, _vp, C.c_int64, C.POINTER(C.c_double), _vp])
 _sig("cpx_grid_touched_count", [_vp, C.POINTER(C.c_int64)])
+_sig("cpx_grid_download_cell_map", [_vp, _vp, C.c_int64])
 
 
 class ProposalDesc(C.Structure):
@@ -429,6 +430,13 @@ class ObjectScene:
         t = C.c_int64()
         _check(_lib.cpx_grid_touched_count(self._h, C.byref(t)), "cpx_grid_touched_count")
         return int(t.value)
+
+    def cell_map(self) -> np.ndarray:
+        """The march's dense empty-space map, one uint8 per cell (1 = open) in x-fastest order."""
+        cells = (self.width - 1) * (self.height - 1) * (self.depth - 1)
+        words = np.zeros((cells + 31) // 32, np.uint32)
+        _check(_lib.cpx_grid_download_cell_map(self._h, words.ctypes.data, words.size), "cpx_grid_download_cell_map")
+        return np.unpackbits(words.view(np.uint8), bitorder="little")[:cells]
 
     def make_sparse(self):
         _check(_lib.cpx_grid_make_sparse(self._h), "cpx_grid_make_sparse")

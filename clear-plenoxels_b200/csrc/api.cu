@@ -893,6 +893,28 @@ cpx_status cpx_grid_touched_count(cpx_grid* g, int64_t* count)
     return cuda_status(e, "touched count");
 }
 
+cpx_status cpx_grid_download_cell_map(cpx_grid* g, uint32_t* words, int64_t n_words)
+{
+    if (check_grid(g) || !words) return CPX_ERR_INVALID_ARGUMENT;
+    if (!dense_skip_on(g)) {
+        set_error("this grid's march keeps no dense empty-space map");
+        return CPX_ERR_UNSUPPORTED;
+    }
+    const int64_t cells = (int64_t)(g->W - 1) * (g->H - 1) * (g->D - 1);
+    const int64_t need = (cells + 31) / 32;
+    if (n_words < need) {
+        set_error("the map needs %lld words, %lld given", (long long)need, (long long)n_words);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (!g->dense_cells) {
+        set_error("no density uploaded yet");
+        return CPX_ERR_NOT_READY;
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(words, g->dense_cells, need * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    return cuda_status(e, "cell map download");
+}
+
 cpx_status cpx_grid_check(cpx_grid* g)
 {
     if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;

@@ -281,25 +281,58 @@ __global__ void k_dense_mirror(float* mirror, const float* __restrict__ density,
     mirror[d] = in_cage[d] ? density[index_offsets[d]] : __uint_as_float(kMirrorEmpty);
 }
 
-// Dense cell map: thread per cell (whole warps), bit set unless all eight corner densities are
-// at or below kEmptyDensity; a warp's 32 consecutive cells form one word.
+// Dense cell map: bit set unless all eight corner densities of the cell are at or below
+// kEmptyDensity; 32 consecutive cells form one word.  A warp builds kCellWords consecutive
+// words with every corner load of all of them issued before the first compare, so each
+// thread keeps 8 x kCellWords loads in flight: with one cell per thread the kernel waited a
+// full memory latency per wave of threads.
+constexpr int kCellWords = 4;
+
 __global__ void k_dense_cells(const float* __restrict__ density, int W, int H, int D, int64_t n_cells,
                               uint32_t* cells)
 {
-    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    bool open = false;
-    if (c < n_cells) {
-        const int cw = W - 1, ch = H - 1;
-        const int x = (int)(c % cw), y = (int)((c / cw) % ch), z = (int)(c / ((int64_t)cw * ch));
-        const int64_t v = ((int64_t)z * H + y) * W + x;
-        const int64_t WH = (int64_t)W * H;
-        const float d[8] = {density[v], density[v + 1], density[v + W], density[v + W + 1], density[v + WH],
-                            density[v + WH + 1], density[v + WH + W], density[v + WH + W + 1]};
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32 * kCellWords;
+    const int cw = W - 1, ch = H - 1;
+    const int64_t WH = (int64_t)W * H;
+    float d[kCellWords][8];
+    bool in[kCellWords];
 #pragma unroll
-        for (int q = 0; q < 8; q++) open |= d[q] > kEmptyDensity;
+    for (int u = 0; u < kCellWords; u++) {
+        const int64_t c = (w0 + u) * 32 + lane;
+        in[u] = c < n_cells;
+        if (!in[u]) continue;
+        int x, y, z;
+        if (n_cells <= 0xffffffffll) {  // 32-bit division: a 64-bit one costs several times more
+            const uint32_t c32 = (uint32_t)c, row = c32 / (uint32_t)cw;
+            x = (int)(c32 - row * (uint32_t)cw);
+            y = (int)(row % (uint32_t)ch);
+            z = (int)(row / (uint32_t)ch);
+        } else {
+            x = (int)(c % cw);
+            y = (int)((c / cw) % ch);
+            z = (int)(c / ((int64_t)cw * ch));
+        }
+        const int64_t v = ((int64_t)z * H + y) * W + x;
+        d[u][0] = density[v];
+        d[u][1] = density[v + 1];
+        d[u][2] = density[v + W];
+        d[u][3] = density[v + W + 1];
+        d[u][4] = density[v + WH];
+        d[u][5] = density[v + WH + 1];
+        d[u][6] = density[v + WH + W];
+        d[u][7] = density[v + WH + W + 1];
     }
-    const unsigned word = __ballot_sync(0xffffffffu, open);
-    if ((threadIdx.x & 31) == 0 && c < n_cells) cells[c >> 5] = word;
+#pragma unroll
+    for (int u = 0; u < kCellWords; u++) {
+        bool open = false;
+        if (in[u]) {
+#pragma unroll
+            for (int q = 0; q < 8; q++) open |= d[u][q] > kEmptyDensity;
+        }
+        const unsigned word = __ballot_sync(0xffffffffu, open);
+        if (lane == 0 && (w0 + u) * 32 < n_cells) cells[w0 + u] = word;
+    }
 }
 
 bool dense_skip_on(const cpx_grid* g)
@@ -327,7 +360,8 @@ cpx_status refresh_dense_skip(cpx_grid* g, cudaStream_t st)
     }
     // whole warps in both launches: the warp that writes the last word has no cell (brick)
     // in its tail threads
-    k_dense_cells<<<(unsigned)((C + 255) / 256), 256, 0, st>>>(g->density, g->W, g->H, g->D, C, g->dense_cells);
+    const int64_t cell_warps = ((C + 31) / 32 + kCellWords - 1) / kCellWords;
+    k_dense_cells<<<(unsigned)((cell_warps + 7) / 8), 256, 0, st>>>(g->density, g->W, g->H, g->D, C, g->dense_cells);
     k_bricks<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(g->dense_cells, cw, ch, cd, bx, by, bz, g->dense_bricks);
     count_launch(2);
     return cuda_status(cudaGetLastError(), "empty-space maps");

@@ -421,75 +421,181 @@ struct TrainArgs {
     double* loss;            // sum of the points' losses, accumulated
 };
 
-// dynamic shared memory of k_train (floats)
+// Dynamic shared memory of k_train (floats): the parameter block, then one row per point of
+// the input and of every hidden activation.  Row strides are odd, so the 32 lanes of a warp,
+// each reading its own row at the same column, fall in 32 different banks.
+constexpr int kSX = kIn + 1;
+constexpr int kSH = kHid + 1;
 constexpr int tP = 0;
 constexpr int tX = tP + ((kParams + 3) & ~3);
-constexpr int tH1 = tX + kRows * kIn;
-constexpr int tH2 = tH1 + kRows * kHid;
-constexpr int tH3 = tH2 + kRows * kHid;
-constexpr int tD = tH3 + kRows * kHid;
-constexpr int tDz = tD + kRows * kHid;
+constexpr int tH1 = tX + kRows * kSX;
+constexpr int tH2 = tH1 + kRows * kSH;
+constexpr int tH3 = tH2 + kRows * kSH;
+constexpr int tD = tH3 + kRows * kSH;
+constexpr int tDz = tD + kRows * kSH;
 constexpr int kTrainSmemFloats = tDz + kRows;
+static_assert(kTrainSmemFloats * 4 <= 227 * 1024, "k_train shared memory");
+static_assert(oW1 % 4 == 0 && oW2 % 4 == 0 && oW3 % 4 == 0 && kIn % 4 == 0, "float4 weight rows");
 
-// out[i][j] += sum_p A[p][i] * B[p][j] for i < NI, j < NJ (row strides sa, sb), split over
-// the 128 threads; written with atomics to the global gradient.
-template <int NI, int NJ>
-__device__ __forceinline__ void outer_reduce(const float* A, int sa, const float* B, int sb, float* out, int rows)
+// out[n] = relu(b[n] + sum_k W[n][k] r[k]) for the thread's own point, its input row r held in
+// registers.  Four outputs advance together (four independent FMA chains) on float4 broadcast
+// loads of the weight rows; each output still sums bias first, then k ascending, as
+// forward_f32 does.  With Z, also returns b4 + sum_n out[n] w4[n] in n order.
+template <int KI, bool Z>
+__device__ __forceinline__ float layer_fwd(const float* P, int oW, int oB, const float (&r)[KI], float* out)
 {
-    constexpr int PER = (NI * NJ) / kRows;  // outputs per thread (contiguous in j)
-    static_assert((NI * NJ) % kRows == 0 && NJ % PER == 0, "shape");
-    const int o0 = threadIdx.x * PER;
-    const int i = o0 / NJ, j0 = o0 % NJ;
-    float acc[PER];
+    float z = Z ? P[oB4] : 0.f;
+#pragma unroll 1
+    for (int n = 0; n < kHid; n += 4) {
+        float s[4];
 #pragma unroll
-    for (int q = 0; q < PER; q++) acc[q] = 0.f;
-    for (int p = 0; p < rows; p++) {
-        const float av = A[p * sa + i];
-        if (av == 0.f) continue;
+        for (int u = 0; u < 4; u++) s[u] = P[oB + n + u];
 #pragma unroll
-        for (int q = 0; q < PER; q++) acc[q] = fmaf(av, B[p * sb + j0 + q], acc[q]);
+        for (int k = 0; k < KI; k += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const float4 w = *reinterpret_cast<const float4*>(P + oW + (n + u) * KI + k);
+                s[u] = fmaf(w.x, r[k], s[u]);
+                s[u] = fmaf(w.y, r[k + 1], s[u]);
+                s[u] = fmaf(w.z, r[k + 2], s[u]);
+                s[u] = fmaf(w.w, r[k + 3], s[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const float h = fmaxf(s[u], 0.f);
+            out[n + u] = h;
+            if (Z) z = fmaf(h, P[oW4 + n + u], z);
+        }
+    }
+    return z;
+}
+
+// out[k] = act[k] > 0 ? sum_n W[n][k] g[n] : 0 (W is kHid x kHid, row n = output), the
+// back-propagated gradient of one point, g in registers; four k together on float4 loads, n
+// ascending.
+__device__ __forceinline__ void layer_bwd(const float* P, int oW, const float (&g)[kHid], const float* act, float* out)
+{
+#pragma unroll 1
+    for (int k = 0; k < kHid; k += 4) {
+        float s[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int n = 0; n < kHid; n++) {
+            const float4 w = *reinterpret_cast<const float4*>(P + oW + n * kHid + k);
+            s[0] = fmaf(w.x, g[n], s[0]);
+            s[1] = fmaf(w.y, g[n], s[1]);
+            s[2] = fmaf(w.z, g[n], s[2]);
+            s[3] = fmaf(w.w, g[n], s[3]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) out[k + u] = act[k + u] > 0.f ? s[u] : 0.f;
+    }
+}
+
+// out[i][j] += sum_p A[p][i] * B[p][j] for i < kHid, j < NJ over the block's 128 points (row
+// strides sa, sb): each thread sums a 4 x NJ/8 tile in registers, p ascending, and adds it to
+// the global gradient with atomics.  Points whose four A values are all zero (ReLU) are
+// skipped; a zero A value adds nothing to the other sums either.
+template <int NJ>
+__device__ __forceinline__ void outer_reduce(const float* A, int sa, const float* B, int sb, float* out)
+{
+    constexpr int TJ = NJ / 8;
+    static_assert(NJ % 8 == 0 && kHid == 4 * 16 && kRows == 128, "tile split");
+    const int i0 = (threadIdx.x >> 3) * 4, j0 = (threadIdx.x & 7) * TJ;
+    float acc[4][TJ];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < TJ; b++) acc[a][b] = 0.f;
+    for (int p = 0; p < kRows; p++) {
+        float av[4], bv[TJ];
+#pragma unroll
+        for (int a = 0; a < 4; a++) av[a] = A[p * sa + i0 + a];
+        if (av[0] == 0.f && av[1] == 0.f && av[2] == 0.f && av[3] == 0.f) continue;
+#pragma unroll
+        for (int b = 0; b < TJ; b++) bv[b] = B[p * sb + j0 + b];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < TJ; b++) acc[a][b] = fmaf(av[a], bv[b], acc[a][b]);
     }
 #pragma unroll
-    for (int q = 0; q < PER; q++)
-        if (acc[q] != 0.f) atomicAdd(out + i * NJ + j0 + q, acc[q]);
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < TJ; b++)
+            if (acc[a][b] != 0.f) atomicAdd(out + (i0 + a) * NJ + j0 + b, acc[a][b]);
+}
+
+// column sum over the block's points of a hidden-activation region (bias gradients)
+__device__ __forceinline__ void column_sum(const float* R, float* out)
+{
+    const int tid = threadIdx.x;
+    if (tid < kHid) {
+        float s = 0.f;
+        for (int p = 0; p < kRows; p++) s += R[p * kSH + tid];
+        if (s != 0.f) atomicAdd(out + tid, s);
+    }
 }
 
 __global__ void __launch_bounds__(128) k_train(TrainArgs t)
 {
-    extern __shared__ float sm[];
+    extern __shared__ float4 train_smem[];
+    float* sm = reinterpret_cast<float*>(train_smem);
     const Args& a = t.a;
     float* P = sm + tP;
     for (int i = threadIdx.x; i < kParams; i += blockDim.x) P[i] = a.params[i];
     __syncthreads();
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int b = blockIdx.x * 4 + warp;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int b = blockIdx.x * 4 + (tid >> 5);
     int64_t ri;
-    bool valid;
+    bool valid;  // one ray per warp: uniform across the warp
     ray_of(a, b, ri, valid);
-    float* x = sm + tX + tid * kIn;
-    float* h1 = sm + tH1 + tid * kHid;
-    float* h2 = sm + tH2 + tid * kHid;
-    float* h3 = sm + tH3 + tid * kHid;
-    float* d = sm + tD + tid * kHid;
-    features(a, ri, valid, lane, x);
-    const float z = forward_f32(P, x, h1, h2, h3);
+    float* x = sm + tX + tid * kSX;
+    float* h1 = sm + tH1 + tid * kSH;
+    float* h2 = sm + tH2 + tid * kSH;
+    float* h3 = sm + tH3 + tid * kSH;
+    float* d = sm + tD + tid * kSH;
+    float z;
+    {
+        float r[kIn];
+        features(a, ri, valid, lane, r);
+#pragma unroll
+        for (int k = 0; k < kIn; k++) x[k] = r[k];
+        layer_fwd<kIn, false>(P, oW1, oB1, r, h1);
+    }
+    {
+        float r[kHid];
+#pragma unroll
+        for (int k = 0; k < kHid; k++) r[k] = h1[k];
+        layer_fwd<kHid, false>(P, oW2, oB2, r, h2);
+    }
+    {
+        float r[kHid];
+#pragma unroll
+        for (int k = 0; k < kHid; k++) r[k] = h2[k];
+        z = layer_fwd<kHid, true>(P, oW3, oB3, r, h3);
+    }
     float dz = 0.f;
+    double l = 0.;
     if (valid) {
         const float y = t.seg_w[(size_t)b * kSeg + lane] > t.label_weight ? 1.f : 0.f;
         const float sg = 1.f / (1.f + expf(-z));
         dz = (sg - y) * t.inv_points;
         // binary cross-entropy with logits: softplus(z) - y z
-        const float l = fmaxf(z, 0.f) - y * z + log1pf(expf(-fabsf(z)));
-        atomicAdd(t.loss, (double)l);
+        l = fmaxf(z, 0.f) - y * z + log1pf(expf(-fabsf(z)));
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if (valid && lane == 0) atomicAdd(t.loss, l);
     sm[tDz + tid] = dz;
     // layer 4 and d3 = dz * w4 * relu'(h3)
+#pragma unroll 4
     for (int n = 0; n < kHid; n++) d[n] = h3[n] > 0.f ? dz * P[oW4 + n] : 0.f;
     __syncthreads();
     // dW4 = sum dz h3, db4 = sum dz
     if (tid < kHid) {
         float s = 0.f;
-        for (int p = 0; p < kRows; p++) s = fmaf(sm[tDz + p], sm[tH3 + p * kHid + tid], s);
+        for (int p = 0; p < kRows; p++) s = fmaf(sm[tDz + p], sm[tH3 + p * kSH + tid], s);
         if (s != 0.f) atomicAdd(t.grad + oW4 + tid, s);
     } else if (tid == kHid) {
         float s = 0.f;
@@ -497,42 +603,30 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs t)
         if (s != 0.f) atomicAdd(t.grad + oB4, s);
     }
     // dW3 = sum d3 x h2, db3 = sum d3
-    outer_reduce<kHid, kHid>(sm + tD, kHid, sm + tH2, kHid, t.grad + oW3, kRows);
-    if (tid < kHid) {
-        float s = 0.f;
-        for (int p = 0; p < kRows; p++) s += sm[tD + p * kHid + tid];
-        if (s != 0.f) atomicAdd(t.grad + oB3 + tid, s);
-    }
+    outer_reduce<kHid>(sm + tD, kSH, sm + tH2, kSH, t.grad + oW3);
+    column_sum(sm + tD, t.grad + oB3);
     __syncthreads();
     // d2 = (W3^T d3) * relu'(h2), kept in h3's place
-    for (int k = 0; k < kHid; k++) {
-        float s = 0.f;
-        if (h2[k] > 0.f)
-            for (int n = 0; n < kHid; n++) s = fmaf(P[oW3 + n * kHid + k], d[n], s);
-        h3[k] = s;
+    {
+        float g[kHid];
+#pragma unroll
+        for (int n = 0; n < kHid; n++) g[n] = d[n];
+        layer_bwd(P, oW3, g, h2, h3);
     }
     __syncthreads();
-    outer_reduce<kHid, kHid>(sm + tH3, kHid, sm + tH1, kHid, t.grad + oW2, kRows);
-    if (tid < kHid) {
-        float s = 0.f;
-        for (int p = 0; p < kRows; p++) s += sm[tH3 + p * kHid + tid];
-        if (s != 0.f) atomicAdd(t.grad + oB2 + tid, s);
-    }
+    outer_reduce<kHid>(sm + tH3, kSH, sm + tH1, kSH, t.grad + oW2);
+    column_sum(sm + tH3, t.grad + oB2);
     __syncthreads();
     // d1 = (W2^T d2) * relu'(h1), kept in d
-    for (int k = 0; k < kHid; k++) {
-        float s = 0.f;
-        if (h1[k] > 0.f)
-            for (int n = 0; n < kHid; n++) s = fmaf(P[oW2 + n * kHid + k], h3[n], s);
-        d[k] = s;
+    {
+        float g[kHid];
+#pragma unroll
+        for (int n = 0; n < kHid; n++) g[n] = h3[n];
+        layer_bwd(P, oW2, g, h1, d);
     }
     __syncthreads();
-    outer_reduce<kHid, kIn>(sm + tD, kHid, sm + tX, kIn, t.grad + oW1, kRows);
-    if (tid < kHid) {
-        float s = 0.f;
-        for (int p = 0; p < kRows; p++) s += sm[tD + p * kHid + tid];
-        if (s != 0.f) atomicAdd(t.grad + oB1 + tid, s);
-    }
+    outer_reduce<kIn>(sm + tD, kSH, sm + tX, kSX, t.grad + oW1);
+    column_sum(sm + tD, t.grad + oB1);
 }
 
 __global__ void k_adam(float* p, float* g, float* m, float* v, int n, float lr, float inv_bc1, float inv_bc2)

@@ -266,7 +266,10 @@ struct QuadStaged {
     }
 };
 
-template <int PREC, bool TV, class Src>
+// NB_SELF: a TV neighbour may be the vertex itself (bits 2..7 of the LowpVertex, the sparse
+// grid's missing neighbours); false where no neighbour ever is (the dense grid applies TV to
+// interior vertices only), which drops the per-neighbour tests.
+template <int PREC, bool TV, class Src, bool NB_SELF = true>
 __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint32_t q, int u, const LowpVertex& vx,
                                              const Src& src, float inv_bc1, float inv_bc2, uint32_t step_key)
 {
@@ -292,7 +295,7 @@ __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint
 #pragma unroll
         for (int k = 0; k < 6; k++) {
             float2 n01 = p01, n23 = p23;
-            if (!((vx.bits >> (2 + k)) & 1u)) {
+            if (!NB_SELF || !((vx.bits >> (2 + k)) & 1u)) {
                 const uint2 w = src.nb(k);
                 unpack2<PREC>(w.x, n01.x, n01.y);
                 unpack2<PREC>(w.y, n23.x, n23.y);
@@ -565,7 +568,7 @@ __global__ void __launch_bounds__(kAsyncThreads, kAsyncBlocks) k_sweep_lowp_dens
             const uint32_t vv = v0 + x0 + vl;
             const uint32_t q = vv * U + u;
             const QuadStaged src{slot0 + (it % NS) * kAsyncStageBytes, stride, g0 + (it % NS) * kAsyncStageBytes};
-            lowp_quad_x2<PREC, TV>(a, vv, q, u, vx, src, s_bc[0], s_bc[1], s_key);
+            lowp_quad_x2<PREC, TV, QuadStaged, false>(a, vv, q, u, vx, src, s_bc[0], s_bc[1], s_key);
         }
     }
 }

@@ -340,6 +340,15 @@ cpx_status cpx_grid_check(cpx_grid* g);
  * into and a sweep reads and clears gradient records only there; after
  * cpx_grid_upload_grads or a standalone cpx_tv_grad every vertex counts.  Synchronous. */
 cpx_status cpx_grid_touched_count(cpx_grid* g, int64_t* count);
+/* No reference counterpart (a diagnostic): the dense empty-space map the mixed forms' march
+ * (and the FP32 march under CPX_OPT_FP32_MARCH) jumps by -- one bit per cell, set unless all
+ * eight corner densities are at or below 0; cell (x, y, z) of the (W-1) x (H-1) x (D-1) cells
+ * is bit c % 32 of word c / 32, c = (z (H-1) + y) (W-1) + x.  The map follows every density
+ * change (upload, sweep, carving).  n_words must be at least ceil(cells / 32).
+ * CPX_ERR_UNSUPPORTED for a grid whose march keeps no such map (sparse, the FP32 form's
+ * march, CPX_OPT_NO_EMPTY_SKIP); CPX_ERR_NOT_READY before the first density upload.
+ * Synchronous. */
+cpx_status cpx_grid_download_cell_map(cpx_grid* g, uint32_t* words, int64_t n_words);
 
 /* Per-ray sample counts of the last forward/backward batch (device int32[len], or a
  * host copy) -- the march's sample sequence, for bit-exact checks. */

@@ -288,3 +288,38 @@ def test_mixed_training_tracks_fp32_training(cuda, case):
         curves[form] = np.array(curve)
     assert curves["fp32"][-1] < curves["fp32"][0]
     assert np.all(np.abs(curves["bf16"] - curves["fp32"]) <= 0.02 * curves["fp32"])
+
+
+@pytest.mark.parametrize("dims", [(37, 30, 45), (66, 17, 9)])
+def test_dense_cell_map_is_bit_exact(cuda, dims):
+    """The dense empty-space map the mixed march jumps by, bit for bit against the oracle's
+    (a cell is open unless all eight corner densities are at or below 0): after an upload and
+    after a sweep that moves densities across 0, on uneven grids whose cell counts leave a
+    ragged last word.  The FP32 form's march keeps no map."""
+    import orc
+
+    import cpx
+
+    W, H, D = dims
+    n = W * H * D
+    rng = np.random.default_rng(W * 1000 + H)
+    params = rng.normal(0.0, 0.05, (28, n)).astype(np.float32)
+    dens = rng.normal(0.0, 1.0, n).astype(np.float32)
+    dens[rng.random(n) < 0.9] = 0.0  # mostly at the clamp: about two thirds of the cells empty
+    params[0] = dens
+    scene = cpx.ObjectScene(W, H, D, 9, precision="bf16", sr_seed=3)
+    scene.upload_params(params)
+    got = scene.cell_map()
+    want = orc.dense_open_cells(dens, W, H, D)
+    assert 0.1 < want.mean() < 0.9
+    assert np.array_equal(got, want)
+    grads = rng.normal(0.0, 1.0, params.shape).astype(np.float32)
+    scene.upload_grads(grads)
+    cpx.Optimizer.varianceAndUpdate(scene, 1e-4, 1e-5, 0.3, 0.1, 1)
+    after = scene.download_params()[0]
+    assert np.mean((after > 0) != (dens > 0)) > 0.05  # the sweep moved densities across 0
+    assert np.array_equal(scene.cell_map(), orc.dense_open_cells(after, W, H, D))
+    fp32 = cpx.ObjectScene(W, H, D, 9, precision="fp32")
+    fp32.upload_params(params)
+    with pytest.raises(cpx.CpxError):
+        fp32.cell_map()
