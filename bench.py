@@ -347,6 +347,11 @@ def run_ours(args, wl, world, rank, local):
         # training rounds (every train_every batches) inside the timed region
         prop = cpx.Proposal(seed=wl["seed"] + 11, **proposal_net(args))
         W = max(W, PROPOSAL["warmup"] + 10)
+    # --start-batch: the timed window starts after that many untimed training batches, every
+    # batch with the reference's per-batch learning-rate decay, as in a real run at that point
+    decay = args.start_batch is not None
+    if decay:
+        W = max(W, args.start_batch)
         seg_w = torch.zeros((R, cpx.Proposal.SEGMENTS), dtype=torch.float32, device=dev)
         masks = torch.zeros(R, dtype=torch.int32, device=dev)
 
@@ -371,6 +376,8 @@ def run_ours(args, wl, world, rank, local):
             ev[1].record(stream)
         cpx.Optimizer.varianceAndUpdate(scene, STEP["lam_density"], STEP["lam_sh"], lr[0], lr[1], k + 1,
                                         stream=stream)
+        if decay:  # Render.cu:499-500
+            lr[:] = [cpx.lr_decay(x, wl["pool_batches"], k // wl["pool_batches"]) for x in lr]
 
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
     for k in range(W):
@@ -386,12 +393,14 @@ def run_ours(args, wl, world, rank, local):
     launches0 = cpx.kernel_launches()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")  # lets a profiler capture the timed steps alone (--nvtx-include timed/)
     t0.record(stream)
     for k in range(K):
         evs[k][0].record(stream)
         step(W + k, evs[k])
         evs[k][2].record(stream)
     t1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     launches = cpx.kernel_launches() - launches0
     clk = clocks.stop()
@@ -490,6 +499,7 @@ def run_ours(args, wl, world, rank, local):
             "grid": n, "sh_dim": SH_DIM, "batch_rays": R, "pool_rays": P, "step_constants": STEP,
             "precision": args.precision, "form": args.form,
             "proposal_schedule": PROPOSAL if prop is not None else None,
+            "start_batch": W, "lr_decay": "reference per batch (Render.cu:499-500)" if decay else "none",
             "l2": "inputs larger than L2: the sweep streams %.1f GB of grid state per step" % (alg_bytes / 1e9),
             "parallelism": "replicas" if world > 1 else "single GPU",
         },
@@ -1014,6 +1024,9 @@ def main():
     ap.add_argument("--quality", type=int, default=0, metavar="N",
                     help="instead of timing, train N batches in the plain FP32 form and in the --precision/--form "
                          "form and compare PSNR on held-out views")
+    ap.add_argument("--start-batch", type=int, default=None, metavar="N",
+                    help="time the window after N untimed training batches with the reference's learning-rate "
+                         "decay (a mid-run step; the proposal form otherwise times batches 110-130)")
     ap.add_argument("--no-repeat", action="store_true", help="quality run: skip the second plain FP32 run")
     ap.add_argument("--march-options", type=int, default=0,
                     help="cpx_grid_set_options flags of the compared form's grid (quality run)")
@@ -1022,6 +1035,8 @@ def main():
         ap.error("at least 3 warm-up steps")
     if args.form == "proposal" and args.precision == "fp32":
         ap.error("the proposal form runs on a mixed precision (--precision bf16 or fp16)")
+    if args.start_batch is not None and (args.form == "batched" or args.quality):
+        ap.error("--start-batch applies to the timed plain and proposal forms")
     if args.form == "batched" and args.workload == "plain256":
         args.workload = "multi16"
     wl = WORKLOADS[args.workload]
