@@ -282,12 +282,10 @@ __global__ void k_dense_mirror(float* mirror, const float* __restrict__ density,
 }
 
 // Dense cell map: bit set unless all eight corner densities of the cell are at or below
-// kEmptyDensity; 32 consecutive cells form one word.  A lane loads the four corners of its
-// cell's x column (x; y, y+1; z, z+1); the x+1 column is the next lane's x column, taken from a
-// ballot, except for lane 31 and for a cell at the end of its row, which load it themselves.
-// A warp builds kCellWords consecutive words with all of their loads issued before the first
-// compare, so each thread keeps 4 x kCellWords loads in flight (one cell per thread waited a
-// full memory latency per wave of threads).
+// kEmptyDensity; 32 consecutive cells form one word.  A warp builds kCellWords consecutive
+// words with every corner load of all of them issued before the first compare, so each
+// thread keeps 8 x kCellWords loads in flight: with one cell per thread the kernel waited a
+// full memory latency per wave of threads.
 constexpr int kCellWords = 4;
 
 __global__ void k_dense_cells(const float* __restrict__ density, int W, int H, int D, int64_t n_cells,
@@ -297,13 +295,12 @@ __global__ void k_dense_cells(const float* __restrict__ density, int W, int H, i
     const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32 * kCellWords;
     const int cw = W - 1, ch = H - 1;
     const int64_t WH = (int64_t)W * H;
-    float d[kCellWords][4], e[kCellWords][4];
-    bool in[kCellWords], own[kCellWords];
+    float d[kCellWords][8];
+    bool in[kCellWords];
 #pragma unroll
     for (int u = 0; u < kCellWords; u++) {
         const int64_t c = (w0 + u) * 32 + lane;
         in[u] = c < n_cells;
-        own[u] = false;
         if (!in[u]) continue;
         int x, y, z;
         if (n_cells <= 0xffffffffll) {  // 32-bit division: a 64-bit one costs several times more
@@ -318,35 +315,22 @@ __global__ void k_dense_cells(const float* __restrict__ density, int W, int H, i
         }
         const int64_t v = ((int64_t)z * H + y) * W + x;
         d[u][0] = density[v];
-        d[u][1] = density[v + W];
-        d[u][2] = density[v + WH];
-        d[u][3] = density[v + WH + W];
-        own[u] = lane == 31 || x + 1 == cw;  // the next lane's column is not this cell's x+1
-        if (own[u]) {
-            e[u][0] = density[v + 1];
-            e[u][1] = density[v + W + 1];
-            e[u][2] = density[v + WH + 1];
-            e[u][3] = density[v + WH + W + 1];
-        }
+        d[u][1] = density[v + 1];
+        d[u][2] = density[v + W];
+        d[u][3] = density[v + W + 1];
+        d[u][4] = density[v + WH];
+        d[u][5] = density[v + WH + 1];
+        d[u][6] = density[v + WH + W];
+        d[u][7] = density[v + WH + W + 1];
     }
 #pragma unroll
     for (int u = 0; u < kCellWords; u++) {
-        bool col = false;  // the lane's x column holds a density above the bound
+        bool open = false;
         if (in[u]) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) col |= d[u][q] > kEmptyDensity;
+            for (int q = 0; q < 8; q++) open |= d[u][q] > kEmptyDensity;
         }
-        const unsigned cols = __ballot_sync(0xffffffffu, col);
-        bool open = col;
-        if (in[u]) {
-            if (own[u]) {
-#pragma unroll
-                for (int q = 0; q < 4; q++) open |= e[u][q] > kEmptyDensity;
-            } else {
-                open |= (cols >> (lane + 1)) & 1u;
-            }
-        }
-        const unsigned word = __ballot_sync(0xffffffffu, open && in[u]);
+        const unsigned word = __ballot_sync(0xffffffffu, open);
         if (lane == 0 && (w0 + u) * 32 < n_cells) cells[w0 + u] = word;
     }
 }
