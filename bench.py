@@ -1024,6 +1024,10 @@ def main():
     ap.add_argument("--quality", type=int, default=0, metavar="N",
                     help="instead of timing, train N batches in the plain FP32 form and in the --precision/--form "
                          "form and compare PSNR on held-out views")
+    ap.add_argument("--proposal-warmup", type=int, default=None,
+                    help="batches of full march before the proposal guides (default %d)" % PROPOSAL["warmup"])
+    ap.add_argument("--proposal-train-every", type=int, default=None,
+                    help="a label batch and a training round every N batches (default %d)" % PROPOSAL["train_every"])
     ap.add_argument("--start-batch", type=int, default=None, metavar="N",
                     help="time the window after N untimed training batches with the reference's learning-rate "
                          "decay (a mid-run step; the proposal form otherwise times batches 110-130)")
@@ -1040,6 +1044,10 @@ def main():
     if args.form == "batched" and args.workload == "plain256":
         args.workload = "multi16"
     wl = WORKLOADS[args.workload]
+    if args.proposal_warmup is not None:
+        PROPOSAL["warmup"] = args.proposal_warmup
+    if args.proposal_train_every is not None:
+        PROPOSAL["train_every"] = args.proposal_train_every
     net = dict(PROPOSAL_NET, **PROPOSAL_NET_BY_WORKLOAD.get(args.workload, {}))
     if args.proposal_confidence is None:
         args.proposal_confidence = net["confidence"]
