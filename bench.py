@@ -347,13 +347,13 @@ def run_ours(args, wl, world, rank, local):
         # training rounds (every train_every batches) inside the timed region
         prop = cpx.Proposal(seed=wl["seed"] + 11, **proposal_net(args))
         W = max(W, PROPOSAL["warmup"] + 10)
+        seg_w = torch.zeros((R, cpx.Proposal.SEGMENTS), dtype=torch.float32, device=dev)
+        masks = torch.zeros(R, dtype=torch.int32, device=dev)
     # --start-batch: the timed window starts after that many untimed training batches, every
     # batch with the reference's per-batch learning-rate decay, as in a real run at that point
     decay = args.start_batch is not None
     if decay:
         W = max(W, args.start_batch)
-        seg_w = torch.zeros((R, cpx.Proposal.SEGMENTS), dtype=torch.float32, device=dev)
-        masks = torch.zeros(R, dtype=torch.int32, device=dev)
 
     def step(k, ev=None):
         b = k % wl["pool_batches"]
