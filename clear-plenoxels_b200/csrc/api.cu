@@ -240,6 +240,7 @@ static void free_grid(cpx_grid* g)
     cudaFree(g->brick_bits);
     cudaFree(g->dense_mirror);
     cudaFree(g->dense_cells);
+    cudaFree(g->dense_vbits);
     cudaFree(g->dense_bricks);
     for (int i = 0; i < 3; i++) cudaFree(g->off[i]);
     cudaFree(g->scratch.samples);

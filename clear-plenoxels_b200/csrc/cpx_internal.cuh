@@ -143,6 +143,7 @@ struct cpx_grid {
     // or below kEmptyDensity, and the 8x8x8 brick map of those bits (refreshed whenever the
     // density changes); the march jumps over the cells and bricks they mark empty
     uint32_t* dense_cells = nullptr;
+    uint32_t* dense_vbits = nullptr;   // vertex bits the cell map is built from (rows of ceil(W / 32) words)
     uint32_t* dense_bricks = nullptr;
     // jitter
     double* off[3] = {nullptr, nullptr, nullptr};

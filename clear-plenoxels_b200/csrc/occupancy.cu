@@ -281,58 +281,64 @@ __global__ void k_dense_mirror(float* mirror, const float* __restrict__ density,
     mirror[d] = in_cage[d] ? density[index_offsets[d]] : __uint_as_float(kMirrorEmpty);
 }
 
-// Dense cell map: bit set unless all eight corner densities of the cell are at or below
-// kEmptyDensity; 32 consecutive cells form one word.  A warp builds kCellWords consecutive
-// words with every corner load of all of them issued before the first compare, so each
-// thread keeps 8 x kCellWords loads in flight: with one cell per thread the kernel waited a
-// full memory latency per wave of threads.
-constexpr int kCellWords = 4;
+// Dense cell map, in two passes.  First a vertex map: bit x % 32 of word (z H + y) wpr + x / 32
+// is set when vertex (x, y, z) has a density above kEmptyDensity (wpr = ceil(W / 32) words per
+// row of vertices, padding bits clear).  Each density is read once, coalesced; a thread reads
+// one column of kVertexRows rows, all loads in flight before the ballots.
+constexpr int kVertexRows = 8;
 
-__global__ void k_dense_cells(const float* __restrict__ density, int W, int H, int D, int64_t n_cells,
-                              uint32_t* cells)
+__global__ void k_vertex_bits(const float* __restrict__ density, int W, int64_t rows, int wpr, uint32_t* vbits)
 {
+    const int x = blockIdx.y * blockDim.x + threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.x * kVertexRows;
     const int lane = threadIdx.x & 31;
-    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32 * kCellWords;
+    float d[kVertexRows];
+#pragma unroll
+    for (int u = 0; u < kVertexRows; u++) d[u] = (r0 + u < rows && x < W) ? density[(r0 + u) * W + x] : 0.f;
+#pragma unroll
+    for (int u = 0; u < kVertexRows; u++) {
+        const unsigned word = __ballot_sync(0xffffffffu, x < W && d[u] > kEmptyDensity);
+        if (lane == 0 && r0 + u < rows && (x >> 5) < wpr) vbits[(r0 + u) * wpr + (x >> 5)] = word;
+    }
+}
+
+// Then the cell map: bit c % 32 of word c / 32 is set unless all eight corner densities of cell
+// c = (z (H-1) + y) (W-1) + x are at or below kEmptyDensity, i.e. when vertex column x or x+1 is
+// open in any of the vertex rows (y, z), (y+1, z), (y, z+1), (y+1, z+1).  A thread per word; the
+// word's cells fall in one or more cell rows, each segment taken from the four vertex rows
+// with 64-bit funnel shifts (the segment and its x+1 column span at most 33 bits).
+__global__ void k_cells_from_bits(const uint32_t* __restrict__ vbits, int W, int H, int wpr, int64_t n_cells,
+                                  uint32_t* cells)
+{
+    const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (w >= (n_cells + 31) / 32) return;
     const int cw = W - 1, ch = H - 1;
-    const int64_t WH = (int64_t)W * H;
-    float d[kCellWords][8];
-    bool in[kCellWords];
+    int64_t c = w * 32;
+    const int64_t c_end = c + 32 < n_cells ? c + 32 : n_cells;
+    uint32_t word = 0;
+    int bit = 0;
+    while (c < c_end) {
+        const int64_t row = c / cw;
+        const int x = (int)(c - row * cw);
+        const int64_t y = row % ch, z = row / ch;
+        const int len = (int)(cw - x < c_end - c ? cw - x : c_end - c);  // 1..32
+        const int64_t r = z * H + y;
+        const int64_t vrows[4] = {r, r + 1, r + H, r + H + 1};
+        const int k = x >> 5, s = x & 31;
+        uint64_t o = 0;
 #pragma unroll
-    for (int u = 0; u < kCellWords; u++) {
-        const int64_t c = (w0 + u) * 32 + lane;
-        in[u] = c < n_cells;
-        if (!in[u]) continue;
-        int x, y, z;
-        if (n_cells <= 0xffffffffll) {  // 32-bit division: a 64-bit one costs several times more
-            const uint32_t c32 = (uint32_t)c, row = c32 / (uint32_t)cw;
-            x = (int)(c32 - row * (uint32_t)cw);
-            y = (int)(row % (uint32_t)ch);
-            z = (int)(row / (uint32_t)ch);
-        } else {
-            x = (int)(c % cw);
-            y = (int)((c / cw) % ch);
-            z = (int)(c / ((int64_t)cw * ch));
+        for (int q = 0; q < 4; q++) {
+            const uint32_t* rb = vbits + vrows[q] * wpr;
+            const uint64_t lo = rb[k];
+            const uint64_t hi = k + 1 < wpr ? rb[k + 1] : 0u;
+            o |= ((hi << 32) | lo) >> s;
         }
-        const int64_t v = ((int64_t)z * H + y) * W + x;
-        d[u][0] = density[v];
-        d[u][1] = density[v + 1];
-        d[u][2] = density[v + W];
-        d[u][3] = density[v + W + 1];
-        d[u][4] = density[v + WH];
-        d[u][5] = density[v + WH + 1];
-        d[u][6] = density[v + WH + W];
-        d[u][7] = density[v + WH + W + 1];
+        const uint32_t seg = (uint32_t)((o | (o >> 1)) & ((1ull << len) - 1));
+        word |= seg << bit;  // bit + len <= 32
+        bit += len;
+        c += len;
     }
-#pragma unroll
-    for (int u = 0; u < kCellWords; u++) {
-        bool open = false;
-        if (in[u]) {
-#pragma unroll
-            for (int q = 0; q < 8; q++) open |= d[u][q] > kEmptyDensity;
-        }
-        const unsigned word = __ballot_sync(0xffffffffu, open);
-        if (lane == 0 && (w0 + u) * 32 < n_cells) cells[w0 + u] = word;
-    }
+    cells[w] = word;
 }
 
 bool dense_skip_on(const cpx_grid* g)
@@ -348,22 +354,30 @@ cpx_status refresh_dense_skip(cpx_grid* g, cudaStream_t st)
     const int64_t C = (int64_t)cw * ch * cd;
     const int bx = (cw + kBrick - 1) / kBrick, by = (ch + kBrick - 1) / kBrick, bz = (cd + kBrick - 1) / kBrick;
     const int64_t nb = (int64_t)bx * by * bz;
+    const int64_t rows = (int64_t)g->H * g->D;
+    const int wpr = (g->W + 31) / 32;
     if (!g->dense_cells) {
         if (cudaMalloc((void**)&g->dense_cells, ((C + 31) / 32) * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc((void**)&g->dense_vbits, rows * wpr * sizeof(uint32_t)) != cudaSuccess ||
             cudaMalloc((void**)&g->dense_bricks, ((nb + 31) / 32) * sizeof(uint32_t)) != cudaSuccess) {
             cudaGetLastError();
             cudaFree(g->dense_cells);
+            cudaFree(g->dense_vbits);
             g->dense_cells = nullptr;
+            g->dense_vbits = nullptr;
             set_error("empty-space maps could not be allocated");
             return CPX_ERR_OUT_OF_MEMORY;
         }
     }
-    // whole warps in both launches: the warp that writes the last word has no cell (brick)
-    // in its tail threads
-    const int64_t cell_warps = ((C + 31) / 32 + kCellWords - 1) / kCellWords;
-    k_dense_cells<<<(unsigned)((cell_warps + 7) / 8), 256, 0, st>>>(g->density, g->W, g->H, g->D, C, g->dense_cells);
+    // whole warps in the vertex and brick launches: the warp that writes the last word has no
+    // vertex (brick) in its tail threads
+    const dim3 vgrid((unsigned)((rows + kVertexRows - 1) / kVertexRows), (unsigned)((g->W + 255) / 256));
+    k_vertex_bits<<<vgrid, 256, 0, st>>>(g->density, g->W, rows, wpr, g->dense_vbits);
+    const int64_t words = (C + 31) / 32;
+    k_cells_from_bits<<<(unsigned)((words + 255) / 256), 256, 0, st>>>(g->dense_vbits, g->W, g->H, wpr, C,
+                                                                        g->dense_cells);
     k_bricks<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(g->dense_cells, cw, ch, cd, bx, by, bz, g->dense_bricks);
-    count_launch(2);
+    count_launch(3);
     return cuda_status(cudaGetLastError(), "empty-space maps");
 }
 

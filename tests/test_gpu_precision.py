@@ -290,12 +290,13 @@ def test_mixed_training_tracks_fp32_training(cuda, case):
     assert np.all(np.abs(curves["bf16"] - curves["fp32"]) <= 0.02 * curves["fp32"])
 
 
-@pytest.mark.parametrize("dims", [(37, 30, 45), (66, 17, 9)])
+@pytest.mark.parametrize("dims", [(37, 30, 45), (66, 17, 9), (5, 4, 40), (33, 9, 5), (65, 2, 6)])
 def test_dense_cell_map_is_bit_exact(cuda, dims):
     """The dense empty-space map the mixed march jumps by, bit for bit against the oracle's
     (a cell is open unless all eight corner densities are at or below 0): after an upload and
     after a sweep that moves densities across 0, on uneven grids whose cell counts leave a
-    ragged last word.  The FP32 form's march keeps no map."""
+    ragged last word, whose cell rows are shorter than a word (W = 5) or exactly one (W = 33),
+    or one vertex longer than two words (W = 65).  The FP32 form's march keeps no map."""
     import orc
 
     import cpx
