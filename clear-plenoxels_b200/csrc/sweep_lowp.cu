@@ -269,6 +269,21 @@ struct QuadStaged {
 // NB_SELF: a TV neighbour may be the vertex itself (bits 2..7 of the LowpVertex, the sparse
 // grid's missing neighbours); false where no neighbour ever is (the dense grid applies TV to
 // interior vertices only), which drops the per-neighbour tests.
+// (lo(w) + a.x, hi(w) + a.y) for a word of two 16-bit values: the mixed-precision add converts
+// the 16-bit operand exactly and rounds the sum once
+template <int PREC>
+__device__ __forceinline__ float2 add2_h16(uint32_t w, float2 a)
+{
+    float2 r;
+    if (PREC == kPrecBF16)
+        asm("{.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\tadd.rn.f32.bf16 %0, lo, %3;\n\tadd.rn.f32.bf16 %1, hi, %4;}"
+            : "=f"(r.x), "=f"(r.y) : "r"(w), "f"(a.x), "f"(a.y));
+    else
+        asm("{.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\tadd.rn.f32.f16 %0, lo, %3;\n\tadd.rn.f32.f16 %1, hi, %4;}"
+            : "=f"(r.x), "=f"(r.y) : "r"(w), "f"(a.x), "f"(a.y));
+    return r;
+}
+
 template <int PREC, bool TV, class Src, bool NB_SELF = true>
 __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint32_t q, int u, const LowpVertex& vx,
                                              const Src& src, float inv_bc1, float inv_bc2, uint32_t step_key)
@@ -292,23 +307,24 @@ __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint
     unpack2<kPrecBF16>(v_raw.y, vo23.x, vo23.y);
     if (TV && (vx.bits & 2u)) {
         float2 s01, s23, d01s, d23s;
+        const float2 mp01 = __fmul2_rn(p01, neg1), mp23 = __fmul2_rn(p23, neg1);
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-            float2 n01 = p01, n23 = p23;
+            // n - p, exactly the negation of p - n (one rounding either way); a neighbour that is
+            // the vertex itself gives +0, as p - p does
+            float2 d01 = make_float2(0.f, 0.f), d23 = make_float2(0.f, 0.f);
             if (!NB_SELF || !((vx.bits >> (2 + k)) & 1u)) {
                 const uint2 w = src.nb(k);
-                unpack2<PREC>(w.x, n01.x, n01.y);
-                unpack2<PREC>(w.y, n23.x, n23.y);
+                d01 = add2_h16<PREC>(w.x, mp01);
+                d23 = add2_h16<PREC>(w.y, mp23);
             }
-            const float2 d01 = __ffma2_rn(n01, neg1, p01);  // p - n
-            const float2 d23 = __ffma2_rn(n23, neg1, p23);
             s01 = k == 0 ? __fmul2_rn(d01, d01) : __ffma2_rn(d01, d01, s01);
             s23 = k == 0 ? __fmul2_rn(d23, d23) : __ffma2_rn(d23, d23, s23);
             d01s = k == 0 ? d01 : __fadd2_rn(d01s, d01);
             d23s = k == 0 ? d23 : __fadd2_rn(d23s, d23);
         }
         // lam * disp / (sqrt(sum) / 6 + 1e-6), the denominator at least 1e-6
-        const float2 lam = make_float2(a.lam_sh, a.lam_sh);
+        const float2 lam = make_float2(-a.lam_sh, -a.lam_sh);  // the sums hold n - p
         const float2 sixth = make_float2(1.f / 6.f, 1.f / 6.f), tiny = make_float2(1.e-6f, 1.e-6f);
         const float2 e01 = __ffma2_rn(sqrt2_approx(s01), sixth, tiny), e23 = __ffma2_rn(sqrt2_approx(s23), sixth, tiny);
         g01 = __ffma2_rn(__fmul2_rn(lam, d01s), rcp2_approx(e01), g01);
