@@ -11,15 +11,7 @@ from conftest import GOLDEN
 
 import make_ref_golden as G  # noqa: E402  (tests/golden is on sys.path via this file's conftest)
 import orc
-
-RGB_ABS = 1e-5      # rendered RGB, absolute
-GRAD_REL = 1e-4     # gradients, normwise relative (max |a-b| / max |b| per parameter block)
-
-
-def normwise(a, b):
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
-    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+from tolerances import GRAD_REL, RGB_ABS, assert_grads_close, normwise  # noqa: F401
 
 
 def oracle_rays(case, bbox):
@@ -67,8 +59,7 @@ def test_backward_matches_reference(dense):
         rays.a[{"acc_density": "acc_den", "acc_weights": "acc_w"}.get(k, k)][:] = ref[f"fwd_{k}"]
     losses, grad, _ = orc.render_backward(sc, rays, G.MASK_COEF, G.HUBER)
     assert np.abs(losses - ref["losses"]).max() <= 255 * RGB_ABS
-    assert normwise(grad[0], ref["grad_bwd"][0]) <= GRAD_REL
-    assert normwise(grad[1:], ref["grad_bwd"][1:]) <= GRAD_REL
+    assert_grads_close(grad, ref["grad_bwd"])
 
 
 def test_tv_and_adam_match_reference(dense):
@@ -161,7 +152,7 @@ def test_sparse_tables_and_march_match_reference():
         rays.a[{"acc_density": "acc_den", "acc_weights": "acc_w"}.get(k, k)][:] = ref[f"fwd_{k}"]
     losses, grad, _ = orc.render_backward(sc, rays, G.MASK_COEF, G.HUBER)
     assert np.abs(losses - ref["losses"]).max() <= 255 * RGB_ABS
-    assert normwise(grad, ref["grad_bwd"]) <= GRAD_REL
+    assert_grads_close(grad, ref["grad_bwd"])
     g = ref["grad_bwd"].copy()
     orc.tv_grad(sc, g, 1e-3, 1e-3, 0, 6)
     assert normwise(g - ref["grad_bwd"], ref["grad_tv"] - ref["grad_bwd"]) <= 1e-5

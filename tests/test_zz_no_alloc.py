@@ -10,10 +10,9 @@ import ctypes as C
 import numpy as np
 import pytest
 
-pytestmark = pytest.mark.gpu
+from tolerances import RGB_ABS, assert_grads_close
 
-RGB_ABS = 1e-5
-GRAD_REL = 1e-4
+pytestmark = pytest.mark.gpu
 
 
 def _noalloc():
@@ -24,10 +23,6 @@ def _noalloc():
                    C.c_void_p]
     fn.restype = C.c_int
     return fn
-
-
-def normwise(a, b):
-    return np.abs(np.asarray(a, np.float64) - b).max() / max(np.abs(b).max(), 1e-30)
 
 
 def test_noalloc_matches_allocating_entry_point_twice(cuda):
@@ -75,8 +70,7 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda):
         for c in "rgb":
             assert np.abs(out[f"acc_{c}"] - ref_out[f"acc_{c}"]).max() <= RGB_ABS
         assert np.abs(losses.cpu().numpy() - ref_losses.cpu().numpy()).max() <= 255 * RGB_ABS
-        assert normwise(grad[0], ref_grad[0]) <= GRAD_REL
-        assert normwise(grad[1:], ref_grad[1:]) <= GRAD_REL
+        assert_grads_close(grad, ref_grad)
     assert torch.cuda.mem_get_info()[0] >= free_before - (2 << 20)
 
 

@@ -1,0 +1,65 @@
+"""Tolerance checks shared by the parity tests.
+
+The hot-path contract: rendered RGB within 1e-5 absolute; density and SH
+gradients within 1e-4 relative; ray/AABB hits, sample counts and occupancy
+index lists bit-exact.
+
+Gradients are sums of float atomics whose order differs between any two runs
+(and between this library and the reference), so "1e-4 relative" is checked
+per parameter array, two ways:
+
+* normwise: max|got - want| / max|want| <= rel, for every array on its own
+  (density, and each of the 3*sh_dim SH arrays), so a small-magnitude SH array
+  cannot hide behind a large one;
+* elementwise: |got - want| <= rel * |want| for every element whose reference
+  magnitude is at least `floor_frac` of its array's largest magnitude.  Below
+  that floor an element is a near-cancelling sum of much larger per-sample
+  contributions, and its relative error is set by the accumulation order, not
+  by the arithmetic; the normwise check still bounds it.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+RGB_ABS = 1e-5
+GRAD_REL = 1e-4
+GRAD_FLOOR_FRAC = 1e-2
+
+
+def normwise(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def grad_report(got, want, rel=GRAD_REL, floor_frac=GRAD_FLOOR_FRAC):
+    """Per-array worst normwise and elementwise errors: list of
+    (array, normwise, worst elementwise relative above the floor, elements checked)."""
+    got = np.asarray(got, np.float64)
+    want = np.asarray(want, np.float64)
+    if got.ndim == 1:
+        got, want = got[None], want[None]
+    rows = []
+    for k in range(want.shape[0]):
+        a, b = got[k], want[k]
+        top = np.abs(b).max()
+        if top == 0.0:
+            rows.append((k, float(np.abs(a).max()), 0.0, 0))
+            continue
+        nw = float(np.abs(a - b).max() / top)
+        sel = np.abs(b) >= floor_frac * top
+        ew = float((np.abs(a[sel] - b[sel]) / np.abs(b[sel])).max()) if sel.any() else 0.0
+        rows.append((k, nw, ew, int(sel.sum())))
+    return rows
+
+
+def assert_grads_close(got, want, rel=GRAD_REL, floor_frac=GRAD_FLOOR_FRAC, what="gradient"):
+    """Every array within `rel` normwise, and every element above the floor within `rel`
+    relative.  An all-zero reference array must come back all zero."""
+    bad = []
+    for k, nw, ew, n in grad_report(got, want, rel, floor_frac):
+        if n == 0 and nw != 0.0:
+            bad.append(f"array {k}: reference is zero, got max |g| {nw:.3e}")
+        elif nw > rel or ew > rel:
+            bad.append(f"array {k}: normwise {nw:.3e}, elementwise {ew:.3e} over {n} elements")
+    assert not bad, f"{what} outside {rel} relative: " + "; ".join(bad)
