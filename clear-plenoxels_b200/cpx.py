@@ -48,8 +48,10 @@ EXPORTED = [
     "cpx_status_string", "cpx_last_error", "cpx_version", "cpx_grid_create", "cpx_grid_destroy",
     "cpx_grid_info", "cpx_grid_upload_params", "cpx_grid_upload_params_device", "cpx_grid_download_params", "cpx_grid_upload_grads",
     "cpx_grid_download_grads", "cpx_grid_upload_moments", "cpx_grid_download_moments",
-    "cpx_grid_set_adaptive_lr", "cpx_grid_set_sample_offsets", "cpx_grid_set_optimize_step",
-    "cpx_occupancy_build", "cpx_grid_make_sparse", "cpx_rays_create", "cpx_rays_destroy",
+    "cpx_grid_set_adaptive_lr", "cpx_grid_set_sample_offsets", "cpx_grid_fill_sample_offsets",
+    "cpx_grid_download_sample_offsets",
+    "cpx_grid_set_optimize_step",
+    "cpx_occupancy_build", "cpx_grid_download_occupancy", "cpx_grid_make_sparse", "cpx_rays_create", "cpx_rays_destroy",
     "cpx_rays_upload", "cpx_rays_upload_packed", "cpx_rays_download", "cpx_rays_init_camera",
     "cpx_render_forward", "cpx_render_backward", "cpx_render_forward_backward", "cpx_tv_grad",
     "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_grid_check",
@@ -64,7 +66,7 @@ EXPORTED = [
     "cpx_carve_silhouette", "cpx_grid_bbox",
     "cpx_ray_source_create", "cpx_ray_source_destroy", "cpx_ray_source_count", "cpx_ray_source_shuffle",
     "cpx_ray_source_keys", "cpx_ray_source_generate", "cpx_ray_source_check",
-    "cpx_grid_save_text", "cpx_grid_load_text", "cpx_image_load_text", "cpx_image_mask_pixels",
+    "cpx_grid_save_text", "cpx_grid_load_text", "cpx_grid_load_text_sparse", "cpx_config_read", "cpx_image_load_text", "cpx_image_mask_pixels",
 ]
 
 
@@ -143,6 +145,8 @@ _sig("cpx_grid_upload_moments", [_vp, _f32p, _f32p, C.c_int64])
 _sig("cpx_grid_download_moments", [_vp, _f32p, _f32p, C.c_int64])
 _sig("cpx_grid_set_adaptive_lr", [_vp, _f32p, C.c_int64])
 _sig("cpx_grid_set_sample_offsets", [_vp, _vp, _vp, _vp, C.c_int])
+_sig("cpx_grid_fill_sample_offsets", [_vp, C.c_float, _vp, _vp])
+_sig("cpx_grid_download_sample_offsets", [_vp, _vp, _vp, _vp, C.c_int])
 _sig("cpx_grid_set_optimize_step", [_vp, C.c_int])
 _sig("cpx_occupancy_build", [_vp, C.c_float, _vp, _vp, _vp, C.POINTER(C.c_uint32)])
 _sig("cpx_grid_make_sparse", [_vp])
@@ -196,6 +200,7 @@ _sig("cpx_grid_upsample", [_vp, _vp, C.c_float, C.c_int, _vp])
 OPT_NO_EMPTY_SKIP = 1  # the FP32 march steps through empty cells one step at a time
 OPT_FP32_MARCH = 2     # an FP32-storage grid marches like the mixed forms
 OPT_NO_EARLY_STOP = 4  # the FP32 march runs every ray to its far bound (no transmittance stop)
+OPT_TWO_STAGE_MARCH = 8  # placement and shading as two launches instead of the fused march
 _sig("cpx_train_step_proposal", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), C.POINTER(ProposalSchedule),
                                  C.c_int, _vp, C.POINTER(C.c_double), _vp])
 
@@ -218,6 +223,8 @@ _sig("cpx_ray_source_generate", [_vp, _vp, C.c_int64, C.c_int, _vp, _vp])
 _sig("cpx_ray_source_check", [_vp])
 _sig("cpx_grid_save_text", [_vp, C.c_char_p, C.c_int, C.c_int, C.c_int])
 _sig("cpx_grid_load_text", [_vp, C.c_char_p, C.c_int])
+_sig("cpx_grid_load_text_sparse", [_vp, C.c_char_p, C.c_int])
+_sig("cpx_grid_download_occupancy", [_vp, _vp, _vp, _vp, C.POINTER(C.c_uint32)])
 _sig("cpx_image_load_text", [C.c_char_p, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(C.c_int)])
 _sig("cpx_image_mask_pixels", [C.POINTER(C.c_int), C.c_int, _vp, C.POINTER(C.c_int64)])
 _sig("cpx_carve_silhouette", [_vp, C.POINTER(C.c_double), C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp])
@@ -395,6 +402,22 @@ class ObjectScene:
         _check(_lib.cpx_grid_set_sample_offsets(self._h, *[a.ctypes.data for a in arrs], len(arrs[0])),
                "cpx_grid_set_sample_offsets")
 
+    def fill_sample_offsets(self, radius: float, seeds, stream=None):
+        """setSelfSampleOffset(radius) (SceneUtils.cu:792-798): the reference's scrambled-Sobol
+        jitter offsets, from the three host rand() values its randGPU calls would draw."""
+        sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+        if sd.size != 3:
+            raise ValueError("three seeds, one per axis")
+        _check(_lib.cpx_grid_fill_sample_offsets(self._h, C.c_float(radius), sd.ctypes.data, _stream(stream)),
+               "cpx_grid_fill_sample_offsets")
+
+    def sample_offsets(self, n: int):
+        """The first n jitter offsets per axis: (x, y, z) float64 arrays."""
+        out = [np.zeros(n, np.float64) for _ in range(3)]
+        _check(_lib.cpx_grid_download_sample_offsets(self._h, *[a.ctypes.data for a in out], int(n)),
+               "cpx_grid_download_sample_offsets")
+        return tuple(out)
+
     def set_optimize_step(self, step: int):
         _check(_lib.cpx_grid_set_optimize_step(self._h, int(step)), "cpx_grid_set_optimize_step")
 
@@ -416,13 +439,24 @@ class ObjectScene:
                                         idx.ctypes.data, C.byref(cnt)), "cpx_occupancy_build")
         return occ, cage, idx, int(cnt.value)
 
+    def occupancy_tables(self):
+        """The grid's current (occupancy, in_cage, index_offsets) tables."""
+        W, H, D = self.width, self.height, self.depth
+        occ = np.empty((W - 1) * (H - 1) * (D - 1), np.uint8)
+        cage = np.empty(W * H * D, np.uint8)
+        idx = np.empty(W * H * D, np.uint32)
+        cnt = C.c_uint32()
+        _check(_lib.cpx_grid_download_occupancy(self._h, occ.ctypes.data, cage.ctypes.data, idx.ctypes.data,
+                                                C.byref(cnt)), "cpx_grid_download_occupancy")
+        return occ, cage, idx
+
     def init_by_upsample(self, src: "ObjectScene", threshold: float, low_band_only: bool = False, stream=None):
         """upsampleScene of src into this (normally fresh) grid (SceneUtils.cu:419-485)."""
         _check(_lib.cpx_grid_upsample(src.handle, self._h, float(threshold), 1 if low_band_only else 0,
                                       _stream(stream)), "cpx_grid_upsample")
 
     def set_options(self, options: int):
-        """March options (OPT_NO_EMPTY_SKIP, OPT_FP32_MARCH)."""
+        """March options (OPT_NO_EMPTY_SKIP, OPT_FP32_MARCH, OPT_NO_EARLY_STOP, OPT_TWO_STAGE_MARCH)."""
         _check(_lib.cpx_grid_set_options(self._h, int(options)), "cpx_grid_set_options")
 
     def touched_count(self) -> int:
@@ -715,6 +749,63 @@ def save_text(scene: "ObjectScene", directory: str, band: int, density_only: boo
 def load_text(scene: "ObjectScene", directory: str, file_sh_dim: int):
     """objectScene::initFromFile (SceneUtils.cu:703-790), dense."""
     _check(_lib.cpx_grid_load_text(scene.handle, str(directory).encode(), int(file_sh_dim)), "cpx_grid_load_text")
+
+
+def load_text_sparse(scene: "ObjectScene", directory: str, file_sh_dim: int):
+    """objectScene::initFromFile (SceneUtils.cu:703-790), sparse with occupancy, into a fresh dense
+    grid of the checkpoint's dimensions (which becomes sparse)."""
+    _check(_lib.cpx_grid_load_text_sparse(scene.handle, str(directory).encode(), int(file_sh_dim)),
+           "cpx_grid_load_text_sparse")
+
+
+CONFIG_MAX_SKIPS = 256
+
+
+class Config(C.Structure):
+    """cpx_config: the reference's positional config.txt (readConfig, Utils.cu:765-932)."""
+    _fields_ = [(n, C.c_int) for n in ("width", "height", "depth", "render_width", "render_height", "graylized",
+                                       "sh_band", "hierarchy_band_strategy", "shs_for_target_resolution_only",
+                                       "hierarchy", "minimum_hierarchy", "to_sparse_hierarchy", "silhouette_bound",
+                                       "silhouette_initial", "silhouette_radius", "mask_area_only",
+                                       "initial_from_file")] + [
+        ("initial_file_dir_base", C.c_char * 512), ("available_sh_bands", C.c_int), ("render_only", C.c_int),
+        ("views_directory", C.c_char * 512), ("camera_pose_file", C.c_char * 512),
+        ("validation_pose_file", C.c_char * 512), ("novel_view_pose_file", C.c_char * 512),
+        ("camera_distance", C.c_double)] + [(n, C.c_int) for n in (
+            "view_count", "validation_count", "test_count", "train_process_view_index", "white_bg", "test_skip",
+            "repeat_layers", "random_seed")] + [
+        ("learning_rate", C.c_double), ("sh_learning_rate", C.c_double), ("density_optimizer", C.c_int),
+        ("color_channel_optimizer", C.c_int), ("momentum", C.c_double), ("epochs", C.c_int),
+        ("validation_interval", C.c_int), ("batch_size", C.c_int), ("fix_batch_size", C.c_int),
+        ("base_dir", C.c_char * 512), ("save_intervals", C.c_int), ("half_lr_intervals", C.c_int),
+        ("lowest_lr", C.c_double), ("prune_epoch", C.c_int), ("prune_threshold", C.c_float), ("skips", C.c_int),
+        ("skip_index", C.c_int * CONFIG_MAX_SKIPS), ("step_size", C.c_float), ("solid_strategy", C.c_int),
+        ("initial_density", C.c_float), ("initial_color", C.c_float), ("variance_loss_interval", C.c_int),
+        ("variance_coefficient", C.c_double), ("sh_coefficient", C.c_double),
+        ("mask_ray_coefficient", C.c_double), ("variance_type", C.c_int), ("neighbour_nums", C.c_int),
+        ("diffuse_ratio", C.c_double), ("export_model", C.c_int), ("shuffle_rays", C.c_int),
+        ("just_model", C.c_int), ("huber_delta", C.c_float)]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            if isinstance(v, bytes):
+                v = v.decode()
+            elif name == "skip_index":
+                v = [int(x) for x in v[:self.skips]]
+            out[name] = v
+        return out
+
+
+_sig("cpx_config_read", [C.c_char_p, C.POINTER(Config)])
+
+
+def read_config(path) -> dict:
+    """readConfig (Utils.cu:765-932) without its side effects: the fields of config.txt."""
+    c = Config()
+    _check(_lib.cpx_config_read(str(path).encode(), C.byref(c)), "cpx_config_read")
+    return c.as_dict()
 
 
 def load_image_text(prefix: str, width: int, height: int, gray_only: bool = False, use_mask: bool = True):

@@ -243,10 +243,13 @@ static void free_grid(cpx_grid* g)
     cudaFree(g->dense_vbits);
     cudaFree(g->dense_bricks);
     for (int i = 0; i < 3; i++) cudaFree(g->off[i]);
+    cudaFree(g->sobol_dirs);
+    cudaFree(g->sobol_scramble);
     cudaFree(g->scratch.samples);
     cudaFree(g->scratch.colours);
     cudaFree(g->scratch.counts);
     cudaFree(g->scratch.acc);
+    cudaFree(g->scratch.queue);
     cudaFree(g->scratch.err);
     cudaFree(g->scratch.mse);
 }
@@ -503,7 +506,7 @@ cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const doub
 
 cpx_status cpx_grid_set_options(cpx_grid* g, int options)
 {
-    if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH | CPX_OPT_NO_EARLY_STOP))) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH | CPX_OPT_NO_EARLY_STOP | CPX_OPT_TWO_STAGE_MARCH))) return CPX_ERR_INVALID_ARGUMENT;
     g->options = options;
     cpx_status rc = refresh_dense_skip(g, 0);  // the maps of a grid now marched with jumps
     if (rc != CPX_OK) return rc;
@@ -933,6 +936,10 @@ cpx_status cpx_grid_check(cpx_grid* g)
     if (flags[0] & 1) {
         set_error("a ray's march exceeded its sample bound (near/far beyond the grid box?)");
         return CPX_ERR_ITERATION_CAP;
+    }
+    if (flags[0] & 8) {
+        set_error("a shading warp of the fused march gave up waiting for a ray's placement");
+        return CPX_ERR_NOT_READY;
     }
     return CPX_OK;
 }

@@ -88,6 +88,7 @@ struct MarchScratch {
     double* acc = nullptr;         // [cap_rays]: sum of weights (double, for the background)
     int* err = nullptr;            // [4] device error flags
     double* mse = nullptr;         // [1]
+    int* queue = nullptr;          // [cap_rays + 4]: work counters and ready slots of the fused march
 };
 
 }  // namespace cpx
@@ -148,6 +149,11 @@ struct cpx_grid {
     // jitter
     double* off[3] = {nullptr, nullptr, nullptr};
     int n_off = 0;
+    // cuRAND's scrambled Sobol direction numbers (64 words per state) and 32-bit scramble
+    // words of the jitter generator (jitter.cu), for sobol_n states
+    unsigned long long* sobol_dirs = nullptr;
+    uint32_t* sobol_scramble = nullptr;
+    int sobol_n = 0;
     cpx::MarchScratch scratch;
     int last_len = 0;
 };
@@ -391,6 +397,8 @@ cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_
 cpx_status tv_launch(cpx_grid* g, double lam_d, double lam_sh, int type, int nbrs,
                      cudaStream_t s);
 cpx_status occupancy_launch(cpx_grid* g, float threshold);
+// The occupancy tables from given cell bytes (device, one per cell) instead of the density.
+cpx_status occupancy_build(cpx_grid* g, float threshold, const uint8_t* occ_in_dev);
 cpx_status make_sparse_launch(cpx_grid* g);
 cpx_status rays_camera_launch(cpx_rays* r, const cpx_grid* g, const cpx_camera* cam,
                               int img_w, int64_t plane_bytes, const uint8_t* planes_dev,

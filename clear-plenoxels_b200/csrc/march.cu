@@ -152,11 +152,31 @@ __device__ __forceinline__ float real_exp(float x) { return expf(x); }
 // 32 equal segments of [near, far]: the march jumps over segments whose bit is clear and
 // stops after the last set one (all bits set = the full march).  seg_w, when non-null,
 // receives the summed sample weights of each segment (the proposal's labels).
+//
+// The march of one ray is a state (PlaceRay) with three steps -- begin, one iteration of the
+// sample loop, end -- so that the same arithmetic runs either as a loop per ray (place_ray)
+// or inside the fused march, where a lane that finishes a ray takes the next one without
+// waiting for the other lanes of its warp.
+template <typename Real>
+struct PlaceRay {
+    float ox, oy, oz, dx, dy, dz, near_t, far_t;
+    Real t, Ti, acc, accD, seg_len, inv_seg;
+    float accDen;
+    int intT, n, it, it_cap, b;
+    int64_t ri;
+    unsigned cb0, cb1, cb2;
+    float cd[8];
+    uint32_t seg_mask;
+    float* seg_w;
+    SampleRec* out;
+};
+
+// renderRaysGPU's set-up of one ray (RenderUtils.cu:1927-1946).  Returns false for a ray with
+// no samples (near > far), whose outputs are then complete.
 template <typename Real, bool PROP>
-__device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
-                                          SampleRec* samples, int maxs, int* counts,
-                                          double* acc_out, int* err, bool write_fwd,
-                                          uint32_t seg_mask, float* seg_w, const Skip& sk)
+__device__ __forceinline__ bool place_begin(PlaceRay<Real>& st, const GridView& g, const RaysView& r, int b,
+                                            int64_t ri, SampleRec* samples, int maxs, int* counts,
+                                            double* acc_out, bool write_fwd, uint32_t seg_mask, float* seg_w)
 {
     // renderRaysGPU zeroes the outputs first (RenderUtils.cu:1927-1941); the backward alone
     // leaves the forward's outputs as they are
@@ -164,167 +184,206 @@ __device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, 
         r.acc_den[ri] = 0.f;
         r.acc_w[ri] = 0.f;
     }
-    const float near_t = r.near_t[ri];
-    const float far_t = r.far_t[ri];
-    if (near_t > far_t) {  // RenderUtils.cu:1943-1946: no samples, no background
+    st.near_t = r.near_t[ri];
+    st.far_t = r.far_t[ri];
+    if (st.near_t > st.far_t) {  // RenderUtils.cu:1943-1946: no samples, no background
         counts[b] = -1;
         acc_out[b] = 0.;
-        return;
+        return false;
     }
-    const float ox = r.ox[ri], oy = r.oy[ri], oz = r.oz[ri];
-    const float dx = r.dx[ri], dy = r.dy[ri], dz = r.dz[ri];
-    const float step = g.step;
+    st.b = b;
+    st.ri = ri;
+    st.ox = r.ox[ri];
+    st.oy = r.oy[ri];
+    st.oz = r.oz[ri];
+    st.dx = r.dx[ri];
+    st.dy = r.dy[ri];
+    st.dz = r.dz[ri];
     // maxs bounds every ray inside the grid box; longer (or non-finite) rays stop there with
     // the error flag set instead of marching on.
-    const double bound = floor(((double)far_t - (double)near_t + 2.0) / (double)step) + 4.0;
+    const double bound = floor(((double)st.far_t - (double)st.near_t + 2.0) / (double)g.step) + 4.0;
     // the guided march also spends an iteration on every jump over a skipped segment (two when
     // the jump's end rounds back into the skipped segment)
-    const int it_cap = (bound < (double)(maxs + 16) ? (int)bound : maxs + 16) + (PROP ? 2 * kProposalSegments : 0);
-
-    SampleRec* out = samples + (size_t)b * maxs;
-    Real t = near_t;
-    Real Ti = 1;
-    Real acc = 0;
-    Real accD = 0;
-    float accDen = 0.f;
-    int intT = 0, n = 0, it = 0;
+    st.it_cap = (bound < (double)(maxs + 16) ? (int)bound : maxs + 16) + (PROP ? 2 * kProposalSegments : 0);
+    st.out = samples + (size_t)b * maxs;
+    st.t = st.near_t;
+    st.Ti = 1;
+    st.acc = 0;
+    st.accD = 0;
+    st.accDen = 0.f;
+    st.intT = 0;
+    st.n = 0;
+    st.it = 0;
     // densities of the last cell visited (consecutive samples mostly share a cell)
-    unsigned cb0 = 0xffffffffu, cb1 = 0, cb2 = 0;
-    float cd[8];
-    const Real seg_len = PROP ? ((Real)far_t - (Real)near_t) * (Real)(1.0 / kProposalSegments) : (Real)0;
-    const Real inv_seg = PROP && seg_len > (Real)0 ? (Real)1 / seg_len : (Real)0;
-    while (t < far_t) {
-        if (++it > it_cap || n >= maxs) {
-            atomicOr(err, 1);
-            break;
-        }
-        int seg = 0;
-        if (PROP) {
-            seg = (int)((t - (Real)near_t) * inv_seg);
-            seg = seg < 0 ? 0 : (seg > kProposalSegments - 1 ? kProposalSegments - 1 : seg);
-            if (!((seg_mask >> seg) & 1u)) {
-                if ((seg_mask >> seg) == 0u) break;  // no predicted segment ahead
-                Real tn = (Real)near_t + (Real)(seg + 1) * seg_len;
-                t = tn > t ? tn : t + (Real)step;
-                ++intT;
-                continue;
-            }
-        }
-        Real ofx = 0, ofy = 0, ofz = 0;
-        if (intT < g.n_off) {
-            ofx = (Real)g.off_x[intT];
-            ofy = (Real)g.off_y[intT];
-            ofz = (Real)g.off_z[intT];
-        }
-        // RenderUtils.cu:1676-1678
-        const Real bc0 = ox + t * dx + ofx;
-        const Real bc1 = oy + t * dy + ofy;
-        const Real bc2 = oz + t * dz + ofz;
-        const unsigned b0 = (unsigned int)bc0;
-        const unsigned b1 = (unsigned int)bc1;
-        const unsigned b2 = (unsigned int)bc2;
-        // a sparse grid's unoccupied cell (RenderUtils.cu:1681-1686), or -- FP32 march on a
-        // dense grid -- a cell whose corner densities are all at or below kEmptyDensity
-        const bool empty = g.sparse ? !cell_occupied(g, b0, b1, b2)
-                                    : (sk.cells != nullptr && !dense_cell_open(sk.cells, g, b0, b1, b2));
-        if (empty) {
-            if (sizeof(Real) == sizeof(float) && sk.bits) {
-                // FP32 march: all the steps through the empty cell (or brick) at once
-                const Real bc[3] = {bc0, bc1, bc2};
-                const int k = empty_steps<Real>(sk, bc, b0, b1, b2, dx, dy, dz, step);
-                t += (Real)k * (Real)step;
-                intT += k;
-            } else {
-                t += step;
-                ++intT;
-            }
-            continue;
-        }
-        if (b0 != cb0 || b1 != cb1 || b2 != cb2) {
-            unsigned idx[8];
-            if (g.sparse && sk.dense) {
-                // the same values as density[index_offsets[corner]], one load each
-                cell_corners_dense(g, b0, b1, b2, idx);
-#pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    const float v = __ldg(sk.dense + idx[q]);
-                    cd[q] = __float_as_uint(v) == kMirrorEmpty ? g.density[0] : v;
-                }
-            } else {
-                cell_corners(g, b0, b1, b2, idx);
-#pragma unroll
-                for (int q = 0; q < 8; q++) cd[q] = g.density[idx[q]];
-            }
-            cb0 = b0;
-            cb1 = b1;
-            cb2 = b2;
-            // the march waits on every new cell's densities; fetch the cells one and two
-            // voxels further along the ray into L1 now, while this sample is evaluated
-            if (!g.sparse || sk.dense) {
-                const float* src = g.sparse ? sk.dense : g.density;
-#pragma unroll
-                for (int k = 1; k <= 2; k++) {
-                    const Real ta = t + (Real)k;
-                    prefetch_cell(g, src, (unsigned)(ox + ta * dx), (unsigned)(oy + ta * dy),
-                                  (unsigned)(oz + ta * dz));
-                }
-            }
-        }
-        const Real x = bc0 - b0;
-        const Real y = bc1 - b1;
-        const Real z = bc2 - b2;
-        const Real one = 1;
-        // trilerpRGB density term (RenderUtils.cu:855-990), corners in the reference's order
-        float tri0 = 0.f;
-        Real c;
-        c = (one - x) * (one - y) * (one - z);
-        tri0 += c * cd[0];
-        c = (one - x) * y * (one - z);
-        tri0 += c * cd[1];
-        c = x * (one - y) * (one - z);
-        tri0 += c * cd[2];
-        c = x * y * (one - z);
-        tri0 += c * cd[3];
-        c = (one - x) * (one - y) * z;
-        tri0 += c * cd[4];
-        c = (one - x) * y * z;
-        tri0 += c * cd[5];
-        c = x * (one - y) * z;
-        tri0 += c * cd[6];
-        c = x * y * z;
-        tri0 += c * cd[7];
-        // density_activation (RenderUtils.cu:491) and the weight (RenderUtils.cu:1693-1704)
-        const float sigma = logf(1.f + expf(tri0 - 13.f));
-        const Real w = Ti * (one - expf(-sigma * step));
-        acc += w;
-        accDen += sigma;
-        accD += sigma * step;
-        if (PROP && seg_w) seg_w[seg] += (float)w;
-        const Real Tn = real_exp(-accD);
-        SampleRec rec;
-        rec.bx = (uint16_t)(b0 < 65535u ? b0 : 65535u);
-        rec.by = (uint16_t)(b1 < 65535u ? b1 : 65535u);
-        rec.bz = (uint16_t)(b2 < 65535u ? b2 : 65535u);
-        rec.pad = 0;
-        rec.fx = (float)x;
-        rec.fy = (float)y;
-        rec.fz = (float)z;
-        rec.raw = tri0;
-        rec.w = (float)w;
-        rec.tn = (float)Tn;
-        out[n] = rec;
-        Ti = Tn;
-        t += fabs(step - w);  // fabs(float) is the float overload
-        ++intT;
-        ++n;
-        if (Tn < (Real)sk.t_stop) break;  // FP32 march: nothing visible remains behind
+    st.cb0 = 0xffffffffu;
+    st.cb1 = 0;
+    st.cb2 = 0;
+    st.seg_mask = seg_mask;
+    st.seg_w = seg_w;
+    st.seg_len = PROP ? ((Real)st.far_t - (Real)st.near_t) * (Real)(1.0 / kProposalSegments) : (Real)0;
+    st.inv_seg = PROP && st.seg_len > (Real)0 ? (Real)1 / st.seg_len : (Real)0;
+    return true;
+}
+
+// One iteration of the sample loop (RenderUtils.cu:1674-1705), entered with t < far.  Returns
+// true when the ray ends here (the loop's breaks).
+template <typename Real, bool PROP>
+__device__ __forceinline__ bool place_iter(PlaceRay<Real>& st, const GridView& g, int maxs, int* err,
+                                           const Skip& sk)
+{
+    const float step = g.step;
+    if (++st.it > st.it_cap || st.n >= maxs) {
+        atomicOr(err, 1);
+        return true;
     }
+    Real t = st.t;
+    int seg = 0;
+    if (PROP) {
+        seg = (int)((t - (Real)st.near_t) * st.inv_seg);
+        seg = seg < 0 ? 0 : (seg > kProposalSegments - 1 ? kProposalSegments - 1 : seg);
+        if (!((st.seg_mask >> seg) & 1u)) {
+            if ((st.seg_mask >> seg) == 0u) return true;  // no predicted segment ahead
+            Real tn = (Real)st.near_t + (Real)(seg + 1) * st.seg_len;
+            st.t = tn > t ? tn : t + (Real)step;
+            ++st.intT;
+            return false;
+        }
+    }
+    Real ofx = 0, ofy = 0, ofz = 0;
+    if (st.intT < g.n_off) {
+        ofx = (Real)g.off_x[st.intT];
+        ofy = (Real)g.off_y[st.intT];
+        ofz = (Real)g.off_z[st.intT];
+    }
+    // RenderUtils.cu:1676-1678
+    const Real bc0 = st.ox + t * st.dx + ofx;
+    const Real bc1 = st.oy + t * st.dy + ofy;
+    const Real bc2 = st.oz + t * st.dz + ofz;
+    const unsigned b0 = (unsigned int)bc0;
+    const unsigned b1 = (unsigned int)bc1;
+    const unsigned b2 = (unsigned int)bc2;
+    // a sparse grid's unoccupied cell (RenderUtils.cu:1681-1686), or -- FP32 march on a
+    // dense grid -- a cell whose corner densities are all at or below kEmptyDensity
+    const bool empty = g.sparse ? !cell_occupied(g, b0, b1, b2)
+                                : (sk.cells != nullptr && !dense_cell_open(sk.cells, g, b0, b1, b2));
+    if (empty) {
+        if (sizeof(Real) == sizeof(float) && sk.bits) {
+            // FP32 march: all the steps through the empty cell (or brick) at once
+            const Real bc[3] = {bc0, bc1, bc2};
+            const int k = empty_steps<Real>(sk, bc, b0, b1, b2, st.dx, st.dy, st.dz, step);
+            st.t = t + (Real)k * (Real)step;
+            st.intT += k;
+        } else {
+            st.t = t + step;
+            ++st.intT;
+        }
+        return false;
+    }
+    if (b0 != st.cb0 || b1 != st.cb1 || b2 != st.cb2) {
+        unsigned idx[8];
+        if (g.sparse && sk.dense) {
+            // the same values as density[index_offsets[corner]], one load each
+            cell_corners_dense(g, b0, b1, b2, idx);
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const float v = __ldg(sk.dense + idx[q]);
+                st.cd[q] = __float_as_uint(v) == kMirrorEmpty ? g.density[0] : v;
+            }
+        } else {
+            cell_corners(g, b0, b1, b2, idx);
+#pragma unroll
+            for (int q = 0; q < 8; q++) st.cd[q] = g.density[idx[q]];
+        }
+        st.cb0 = b0;
+        st.cb1 = b1;
+        st.cb2 = b2;
+        // the march waits on every new cell's densities; fetch the cells one and two
+        // voxels further along the ray into L1 now, while this sample is evaluated
+        if (!g.sparse || sk.dense) {
+            const float* src = g.sparse ? sk.dense : g.density;
+#pragma unroll
+            for (int k = 1; k <= 2; k++) {
+                const Real ta = t + (Real)k;
+                prefetch_cell(g, src, (unsigned)(st.ox + ta * st.dx), (unsigned)(st.oy + ta * st.dy),
+                              (unsigned)(st.oz + ta * st.dz));
+            }
+        }
+    }
+    const Real x = bc0 - b0;
+    const Real y = bc1 - b1;
+    const Real z = bc2 - b2;
+    const Real one = 1;
+    // trilerpRGB density term (RenderUtils.cu:855-990), corners in the reference's order
+    float tri0 = 0.f;
+    Real c;
+    c = (one - x) * (one - y) * (one - z);
+    tri0 += c * st.cd[0];
+    c = (one - x) * y * (one - z);
+    tri0 += c * st.cd[1];
+    c = x * (one - y) * (one - z);
+    tri0 += c * st.cd[2];
+    c = x * y * (one - z);
+    tri0 += c * st.cd[3];
+    c = (one - x) * (one - y) * z;
+    tri0 += c * st.cd[4];
+    c = (one - x) * y * z;
+    tri0 += c * st.cd[5];
+    c = x * (one - y) * z;
+    tri0 += c * st.cd[6];
+    c = x * y * z;
+    tri0 += c * st.cd[7];
+    // density_activation (RenderUtils.cu:491) and the weight (RenderUtils.cu:1693-1704)
+    const float sigma = logf(1.f + expf(tri0 - 13.f));
+    const Real w = st.Ti * (one - expf(-sigma * step));
+    st.acc += w;
+    st.accDen += sigma;
+    st.accD += sigma * step;
+    if (PROP && st.seg_w) st.seg_w[seg] += (float)w;
+    const Real Tn = real_exp(-st.accD);
+    SampleRec rec;
+    rec.bx = (uint16_t)(b0 < 65535u ? b0 : 65535u);
+    rec.by = (uint16_t)(b1 < 65535u ? b1 : 65535u);
+    rec.bz = (uint16_t)(b2 < 65535u ? b2 : 65535u);
+    rec.pad = 0;
+    rec.fx = (float)x;
+    rec.fy = (float)y;
+    rec.fz = (float)z;
+    rec.raw = tri0;
+    rec.w = (float)w;
+    rec.tn = (float)Tn;
+    st.out[st.n] = rec;
+    st.Ti = Tn;
+    st.t = t + fabs(step - w);  // fabs(float) is the float overload
+    ++st.intT;
+    ++st.n;
+    return Tn < (Real)sk.t_stop;  // FP32 march: nothing visible remains behind
+}
+
+template <typename Real>
+__device__ __forceinline__ void place_end(const PlaceRay<Real>& st, const RaysView& r, int* counts,
+                                          double* acc_out, bool write_fwd)
+{
     if (write_fwd) {
-        r.acc_den[ri] = accDen;
-        r.acc_w[ri] = (float)acc;
+        r.acc_den[st.ri] = st.accDen;
+        r.acc_w[st.ri] = (float)st.acc;
     }
-    acc_out[b] = (double)acc;
-    counts[b] = n;
+    acc_out[st.b] = (double)st.acc;
+    counts[st.b] = st.n;
+}
+
+template <typename Real, bool PROP>
+__device__ __forceinline__ void place_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
+                                          SampleRec* samples, int maxs, int* counts,
+                                          double* acc_out, int* err, bool write_fwd,
+                                          uint32_t seg_mask, float* seg_w, const Skip& sk)
+{
+    PlaceRay<Real> st;
+    if (!place_begin<Real, PROP>(st, g, r, b, ri, samples, maxs, counts, acc_out, write_fwd, seg_mask, seg_w))
+        return;
+    while (st.t < st.far_t) {
+        if (place_iter<Real, PROP>(st, g, maxs, err, sk)) break;
+    }
+    place_end<Real>(st, r, counts, acc_out, write_fwd);
 }
 
 // ---------------------------------------------------------------------------
@@ -597,7 +656,9 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
         if (miss) {
             pred[0] = pred[1] = pred[2] = 0.f;
         } else {
-            const double bg = r.white_bg ? 1. - acc_in[b] : 0.;  // RenderUtils.cu:1709-1716
+            // per-ray values the placement wrote are read from L2 (__ldcg): in the fused march a
+            // neighbouring ray's placement on another SM may have written the same cache line
+            const double bg = r.white_bg ? 1. - __ldcg(acc_in + b) : 0.;  // RenderUtils.cu:1709-1716
             pred[0] = (float)(s0 + bg);
             pred[1] = (float)(s1 + bg);
             pred[2] = (float)(s2 + bg);
@@ -637,7 +698,7 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
         else if (res[i] < -huber)
             res[i] = 0.5 * huber * huber - huber;
     }
-    const float accw_f = r.acc_w[ri];
+    const float accw_f = __ldcg(r.acc_w + ri);
     float mask_loss = 0.f;
     const uint8_t gm = r.mask[ri];
     if (gm && accw_f < 1.) mask_loss = (gm / 255.0 - accw_f) * mask_coef;
@@ -757,6 +818,123 @@ __global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysV
 }
 
 // ---------------------------------------------------------------------------
+// The fused march: placement and shading in one launch, overlapped.  Placement is one
+// dependent chain per ray and keeps only a warp or two per SM busy; shading is a warp per ray
+// and wants the SM's throughput.  Warp 0 of every block runs placement lanes: a lane takes the
+// next ray from a work counter, marches it, publishes it to a ready queue and takes another
+// ray at once (the sample loop and the ray loop are one loop, so a lane never waits for the
+// other lanes of its warp).  The other warps take ready rays in publication order and shade
+// them, so shading runs while the long rays are still being placed.
+//
+// Progress: placement never waits on anything, and rays are handed out by the counter only
+// to lanes that are running, so every ray is published whatever the scheduling of the
+// blocks; a shading warp waits only for a slot that some running lane will fill.  The wait
+// is still bounded (kSpinLimit polls); a warp that gives up sets error bit 8 and stops.
+//
+// queue[0]: next ray to place; queue[1]: next free ready slot; queue[2]: next slot to
+// shade; queue[4 + s]: 1 + the ray published in slot s (0 = not yet).  Zeroed before every
+// launch.  Per-ray values the placement writes (count, weight sum, accumulated weight) are
+// read from L2; each ray's sample records start on a 128-byte line (maxs is a multiple of
+// 4), so no SM holds a stale line of a ray it has not yet read.
+// ---------------------------------------------------------------------------
+constexpr int kFusedShadeWarps = 7;
+constexpr int kFusedThreads = (1 + kFusedShadeWarps) * 32;
+constexpr int kSpinLimit = 1 << 22;  // polls with 128-ns sleeps: well over a second
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void publish_ray(int* queue, int b)
+{
+    __threadfence();  // the ray's samples, count and sums before its ready entry
+    const int slot = atomicAdd(queue + 1, 1);
+    atomicExch(queue + 4 + slot, b + 1);
+}
+
+template <int NSH, int MODE, int PREC, typename Real, bool PROP>
+__global__ void __launch_bounds__(kFusedThreads, 2)
+    k_march(GridView g, RaysView r, const int32_t* sidx, int start, int len, int64_t n_rays, SampleRec* samples,
+            float4* colours, int maxs, int* counts, double* acc, int* err, const uint32_t* seg_masks,
+            float* seg_w, Skip sk, double* losses, double mask_coef, float huber, uint32_t* touched, int* queue)
+{
+    __shared__ uint32_t h_keys[kFusedShadeWarps][kHashSlots];
+    __shared__ float h_vals[kFusedShadeWarps][4][kHashSlots];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    constexpr bool kFwd = (MODE & kForward) != 0;
+    if (warp == 0) {
+        PlaceRay<Real> st;
+        bool active = false;
+        while (true) {
+            if (!active) {
+                const int b = atomicAdd(queue, 1);
+                if (b >= len) break;
+                const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
+                if (ri < 0 || ri >= n_rays) {
+                    atomicOr(err, 2);
+                    counts[b] = -2;  // invalid ray index: nothing is read or written for it
+                    publish_ray(queue, b);
+                    continue;
+                }
+                const uint32_t mask = PROP && seg_masks ? seg_masks[b] : 0xffffffffu;
+                float* sw = PROP && seg_w ? seg_w + (size_t)b * kProposalSegments : nullptr;
+                if (!place_begin<Real, PROP>(st, g, r, b, ri, samples, maxs, counts, acc, kFwd, mask, sw)) {
+                    publish_ray(queue, b);
+                    continue;
+                }
+                active = true;
+            }
+            if (!(st.t < st.far_t) || place_iter<Real, PROP>(st, g, maxs, err, sk)) {
+                place_end<Real>(st, r, counts, acc, kFwd);
+                publish_ray(queue, st.b);
+                active = false;
+            }
+        }
+        return;
+    }
+    const int sw = warp - 1;
+    for (int s = lane; s < kHashSlots; s += 32) {
+        h_keys[sw][s] = kEmpty;
+        h_vals[sw][0][s] = h_vals[sw][1][s] = h_vals[sw][2][s] = h_vals[sw][3][s] = 0.f;
+    }
+    __syncwarp();
+    const WarpTable tab{h_keys[sw], h_vals[sw][0], h_vals[sw][1], h_vals[sw][2], h_vals[sw][3]};
+    while (true) {
+        int s = 0;
+        if (lane == 0) s = atomicAdd(queue + 2, 1);
+        s = __shfl_sync(0xffffffffu, s, 0);
+        if (s >= len) break;  // warp-uniform
+        int v = 0;
+        if (lane == 0) {
+            for (int spin = 0;; ++spin) {
+                v = ld_acquire_gpu(queue + 4 + s);
+                if (v != 0 || spin >= kSpinLimit) break;
+                __nanosleep(128);
+            }
+        }
+        v = __shfl_sync(0xffffffffu, v, 0);
+        if (v == 0) {
+            if (lane == 0) atomicOr(err, 8);
+            break;
+        }
+        v = ld_acquire_gpu(queue + 4 + s);  // every lane acquires the published ray
+        const int b = v - 1;
+        const int cnt = __ldcg(counts + b);
+        if (cnt == -2) {
+            if ((MODE & kBackward) && lane == 0) losses[b] = 0.;
+            continue;
+        }
+        const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
+        shade_ray<NSH, MODE, PREC>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber, tab,
+                                   touched, lane);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Batch MSE of the per-ray losses (getMSEError, Utils.cu:311-320), one block.
 // ---------------------------------------------------------------------------
 __global__ void k_mse(const double* losses, int len, double* out)
@@ -790,7 +968,8 @@ static int max_samples_per_ray(const cpx_grid* g)
     const double ey = (double)g->bbox[3] - g->bbox[2];
     const double ez = (double)g->bbox[5] - g->bbox[4];
     const double diag = sqrt(ex * ex + ey * ey + ez * ez);
-    return (int)ceil((diag + 2.0) / g->step) + 8;
+    // a multiple of 4, so every ray's sample records start on a 128-byte line (the fused march)
+    return (((int)ceil((diag + 2.0) / g->step) + 8) + 3) & ~3;
 }
 
 static cpx_status ensure_scratch(cpx_grid* g, int len)
@@ -810,17 +989,20 @@ static cpx_status ensure_scratch(cpx_grid* g, int len)
     cudaFree(s.colours);
     cudaFree(s.counts);
     cudaFree(s.acc);
+    cudaFree(s.queue);
     s.samples = nullptr;
     s.colours = nullptr;
     s.counts = nullptr;
     s.acc = nullptr;
+    s.queue = nullptr;
     s.cap_rays = 0;
     const int cap = len > 0 ? len : 1;
     const size_t ns = (size_t)cap * maxs;
     if (cudaMalloc((void**)&s.samples, ns * sizeof(SampleRec)) != cudaSuccess ||
         cudaMalloc((void**)&s.colours, ns * sizeof(float4)) != cudaSuccess ||
         cudaMalloc((void**)&s.counts, (size_t)cap * sizeof(int)) != cudaSuccess ||
-        cudaMalloc((void**)&s.acc, (size_t)cap * sizeof(double)) != cudaSuccess) {
+        cudaMalloc((void**)&s.acc, (size_t)cap * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&s.queue, ((size_t)cap + 4) * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         set_error("march scratch of %zu samples could not be allocated", ns);
         return CPX_ERR_OUT_OF_MEMORY;
@@ -836,14 +1018,55 @@ struct Guide {
     float* seg_w = nullptr;
     Skip skip;
     bool march32 = false;  // the FP32 march of the mixed forms (else the reference's sequence)
+    bool two_stage = false;  // placement and shading as two launches (CPX_OPT_TWO_STAGE_MARCH)
     bool on() const { return masks != nullptr || seg_w != nullptr; }
 };
+
+// Blocks of the fused march: what the GPU holds at once, at most one block per 32 rays.
+template <int NSH, int MODE, int PREC, typename Real, bool PROP>
+static int fused_blocks(int len)
+{
+    static int resident = 0;  // per kernel instance
+    if (resident == 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_march<NSH, MODE, PREC, Real, PROP>, kFusedThreads, 0);
+        resident = sms * (per > 0 ? per : 1);
+    }
+    const int want = (len + 31) / 32;
+    return want < resident ? want : resident;
+}
+
+template <int MODE, int NSH, int PREC, typename Real, bool PROP>
+static void launch_fused(cudaStream_t st, const GridView& gv, const RaysView& rv, const int32_t* sidx, int start,
+                         int len, int64_t n_rays, const MarchScratch& s, double* losses, double mask_coef,
+                         float huber, uint32_t* touched, const Guide& guide)
+{
+    cudaMemsetAsync(s.queue, 0, ((size_t)len + 4) * sizeof(int), st);
+    k_march<NSH, MODE, PREC, Real, PROP><<<fused_blocks<NSH, MODE, PREC, Real, PROP>(len), kFusedThreads, 0, st>>>(
+        gv, rv, sidx, start, len, n_rays, s.samples, s.colours, s.maxs, s.counts, s.acc, s.err,
+        PROP ? guide.masks : nullptr, PROP ? guide.seg_w : nullptr, guide.skip, losses, mask_coef, huber, touched,
+        s.queue);
+}
 
 template <int MODE, int NSH, int PREC>
 static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv, const int32_t* sidx,
                         int start, int len, int64_t n_rays, const MarchScratch& s, double* losses,
                         double mask_coef, float huber, uint32_t* touched, const Guide& guide)
 {
+    if (!guide.two_stage) {
+        if (guide.march32 && guide.on())
+            launch_fused<MODE, NSH, PREC, float, true>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef,
+                                                       huber, touched, guide);
+        else if (guide.march32)
+            launch_fused<MODE, NSH, PREC, float, false>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef,
+                                                        huber, touched, guide);
+        else
+            launch_fused<MODE, NSH, PREC, double, false>(st, gv, rv, sidx, start, len, n_rays, s, losses, mask_coef,
+                                                         huber, touched, guide);
+        return;
+    }
     const dim3 pgrid((unsigned)((len + 31) / 32));
     const dim3 sgrid((unsigned)((len + kShadeWarps - 1) / kShadeWarps));
     const dim3 sblock(kShadeWarps * 32);
@@ -936,6 +1159,7 @@ static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32
     if (rc != CPX_OK || len == 0) return rc;
     Guide gd = guide;
     gd.march32 = g->prec != kPrecFP32 || (g->options & CPX_OPT_FP32_MARCH);
+    gd.two_stage = (g->options & CPX_OPT_TWO_STAGE_MARCH) != 0 || s.queue == nullptr;
     if (guide.on() && !gd.march32) {
         set_error("the proposal-guided march runs on the FP32 march of the mixed forms only");
         return CPX_ERR_UNSUPPORTED;

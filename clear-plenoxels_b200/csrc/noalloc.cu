@@ -29,7 +29,8 @@ constexpr size_t kColoursBytes = (size_t)kNoAllocSamples * sizeof(float4);
 constexpr size_t kCountsBytes = (size_t)kNoAllocRays * sizeof(int);
 constexpr size_t kAccBytes = (size_t)kNoAllocRays * sizeof(double);
 constexpr size_t kErrBytes = 256;
-constexpr size_t kNoAllocBytes = kSamplesBytes + kColoursBytes + kCountsBytes + kAccBytes + kErrBytes;
+constexpr size_t kQueueBytes = ((size_t)kNoAllocRays + 4) * sizeof(int);  // the fused march's work queue
+constexpr size_t kNoAllocBytes = kSamplesBytes + kColoursBytes + kCountsBytes + kAccBytes + kErrBytes + kQueueBytes;
 
 // Shared by every call on a device: it keeps the last call's contents, and two calls that
 // overlap on the GPU (different streams, or different host threads) race on it.
@@ -91,9 +92,11 @@ extern "C" cpx_status cpx_render_forward_backward_noalloc(cpx_grid* g, cpx_rays*
     s.counts = reinterpret_cast<int*>(base + kSamplesBytes + kColoursBytes);
     s.acc = reinterpret_cast<double*>(base + kSamplesBytes + kColoursBytes + kCountsBytes);
     s.err = reinterpret_cast<int*>(base + kSamplesBytes + kColoursBytes + kCountsBytes + kAccBytes);
+    s.queue = reinterpret_cast<int*>(base + kSamplesBytes + kColoursBytes + kCountsBytes + kAccBytes + kErrBytes);
     s.mse = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
-    // the flags must start at zero; samples, colours, counts and sums are written before use
+    // the flags must start at zero (the march zeroes its own queue); samples, colours, counts and
+    // sums are written before use
     cudaError_t e = cudaMemsetAsync(s.err, 0, kErrBytes, st);
     if (e != cudaSuccess) return cuda_status(e, "noalloc flags");
     rc = march_launch_with(g, r, sample_index_dev, start, len, kForwardBackward, losses_dev, mask_coef,
@@ -111,6 +114,10 @@ extern "C" cpx_status cpx_render_forward_backward_noalloc(cpx_grid* g, cpx_rays*
     if (flags[0] & 1) {
         set_error("a ray's march exceeded its sample bound (near/far beyond the grid box?)");
         return CPX_ERR_ITERATION_CAP;
+    }
+    if (flags[0] & 8) {
+        set_error("a shading warp of the fused march gave up waiting for a ray's placement");
+        return CPX_ERR_NOT_READY;
     }
     return CPX_OK;
 }

@@ -97,6 +97,69 @@ const char* cpx_last_error(void);
 /* Library version as major*10000 + minor*100 + patch. */
 int cpx_version(void);
 
+/* ------------------------------------------------------------------ configuration */
+/* The reference's positional config.txt (readConfig, SVRF/Utils.cu:765-932; Configuration,
+ * SVRF/Utils.cuh): every key in the reference's order, one per line ("SceneSize:512 512 512").
+ * Flags are 0/1 as the reference's bools hold them; strings are at most 511 bytes. */
+#define CPX_CONFIG_MAX_SKIPS 256
+typedef struct cpx_config {
+    int width, height, depth;                 /* SceneSize */
+    int render_width, render_height;          /* RenderSize */
+    int graylized;                            /* Graylized */
+    int sh_band;                              /* SphericalHarmonicsBand */
+    int hierarchy_band_strategy;              /* HierarchyBandStrategy */
+    int shs_for_target_resolution_only;       /* SHsForTargetResolutionOnly */
+    int hierarchy, minimum_hierarchy;         /* Hierarchy, MinimumHierarchy */
+    int to_sparse_hierarchy;                  /* ToSparseHierarchy */
+    int silhouette_bound, silhouette_initial; /* SilhouetteBound, SilhouetteInitial */
+    int silhouette_radius;                    /* SilhouetteRadius */
+    int mask_area_only;                       /* MaskAreaOnly */
+    int initial_from_file;                    /* InitialFromFile */
+    char initial_file_dir_base[512];          /* InitialFileDirBase */
+    int available_sh_bands;                   /* AvailableSHBands */
+    int render_only;                          /* RenderOnly */
+    char views_directory[512];                /* ViewDirectory */
+    char camera_pose_file[512];               /* CameraPoseFile */
+    char validation_pose_file[512];           /* ValidationPoseFile */
+    char novel_view_pose_file[512];           /* NovelViewPoseFile */
+    double camera_distance;                   /* CameraDistance */
+    int view_count, validation_count;         /* ViewCount, ValidationCount */
+    int test_count;                           /* TestCount */
+    int train_process_view_index;             /* TrainProcessViewIndex */
+    int white_bg;                             /* WhiteBG */
+    int test_skip, repeat_layers;             /* TestSkip, RepeatLayers */
+    int random_seed;                          /* RandomSeed */
+    double learning_rate, sh_learning_rate;   /* LearningRate, SHLearningRate */
+    int density_optimizer;                    /* DensityOptimizer */
+    int color_channel_optimizer;              /* ColorChannelOptimizer */
+    double momentum;                          /* Momentum */
+    int epochs, validation_interval;          /* Epochs, ValidationInterval */
+    int batch_size, fix_batch_size;           /* BatchSize, FixBatchSize */
+    char base_dir[512];                       /* BaseDir */
+    int save_intervals, half_lr_intervals;    /* SaveIntervals, HalfLR */
+    double lowest_lr;                         /* LowestLR */
+    int prune_epoch;                          /* PruneEpoch */
+    float prune_threshold;                    /* PruneThreshold */
+    int skips;                                /* Skips */
+    int skip_index[CPX_CONFIG_MAX_SKIPS];     /* SkipIndex (the first `skips`) */
+    float step_size;                          /* StepSize */
+    int solid_strategy;                       /* SolidStrategy */
+    float initial_density, initial_color;     /* InitialDensity, InitialColor */
+    int variance_loss_interval;               /* VarianceLossInterval */
+    double variance_coefficient;              /* VarianceCoefficient (TV lambda, density) */
+    double sh_coefficient;                    /* ColorDisparityCoefficient (TV lambda, SH) */
+    double mask_ray_coefficient;              /* MaskRayCoefficient */
+    int variance_type, neighbour_nums;        /* VarianceType, NeighboorNumsForTVLoss */
+    double diffuse_ratio;                     /* DiffuseRatio */
+    int export_model, shuffle_rays;           /* ExportModel, ShuffleRays */
+    int just_model;                           /* JustModel */
+    float huber_delta;                        /* HuberDelta */
+} cpx_config;
+/* Parses `path` as readConfig does, without its side effects (no directories created, no
+ * files copied, rand() not seeded).  CPX_ERR_INVALID_ARGUMENT names the first line that is
+ * missing or out of order (where the reference reads on with fields unset). */
+cpx_status cpx_config_read(const char* path, cpx_config* out);
+
 /* ------------------------------------------------------------------ grid */
 /* Dense grid, every parameter zero, Adam moments zero, adaptive LR one, no jitter.
  * Replaces objectScene::initSelf(solid) + optimizer::initialSelf/initialAll. */
@@ -120,6 +183,18 @@ cpx_status cpx_grid_set_adaptive_lr(cpx_grid* g, const float* lr_mult, int64_t n
  * SVRF/SceneUtils.cu:792); entries past n read as zero.  n = 0 clears them. */
 cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const double* oy,
                                        const double* oz, int n);
+/* objectScene::setSelfSampleOffset(radius) (SVRF/SceneUtils.cu:792-798, randGPU at
+ * SVRF/Utils.cu:1002-1044): fills the grid's three offset arrays (maxSamplePoint =
+ * (int)(sqrt(W^2+H^2+D^2)/step + 1.5) entries, zero when first created) with
+ * N(0,1)/4 * radius from cuRAND's scrambled Sobol64 generator, exactly as the reference
+ * does.  seeds[3] are the three host rand() values the reference's three randGPU calls
+ * would draw (each axis's generator starts at point state + seed).  The reference calls it
+ * before every batch with radius = stepSize/2 when SolidStrategy is 0.  Asynchronous on
+ * `stream` after the first call (which fetches cuRAND's direction numbers). */
+cpx_status cpx_grid_fill_sample_offsets(cpx_grid* g, float radius, const uint32_t* seeds, cpx_stream stream);
+/* Host copy of the first n jitter offsets per axis (n at most the grid's offset count).
+ * Synchronous.  No reference counterpart beyond reading offset{X,Y,Z}Device. */
+cpx_status cpx_grid_download_sample_offsets(const cpx_grid* g, double* ox, double* oy, double* oz, int n);
 /* ObjectScene::optimizeStep (hierarchy level); gates SH in the type-1 TV term. */
 cpx_status cpx_grid_set_optimize_step(cpx_grid* g, int optimize_step);
 
@@ -131,6 +206,12 @@ cpx_status cpx_grid_set_optimize_step(cpx_grid* g, int optimize_step);
 cpx_status cpx_occupancy_build(cpx_grid* g, float threshold, uint8_t* occupancy_out,
                                uint8_t* in_cage_out, uint32_t* index_offsets_out,
                                uint32_t* in_cage_count_out);
+/* Host copies of the grid's current occupancy tables (those of the last cpx_occupancy_build,
+ * or of a loaded sparse checkpoint); any output may be NULL.  CPX_ERR_NOT_READY without
+ * tables.  Synchronous.  (The reference keeps them as occupancyHost / inCageInfoHost /
+ * indexOffsetsHost, SVRF/SceneUtils.cuh:4-98.) */
+cpx_status cpx_grid_download_occupancy(const cpx_grid* g, uint8_t* occupancy_out, uint8_t* in_cage_out,
+                                       uint32_t* index_offsets_out, uint32_t* in_cage_count_out);
 /* Switch to the sparse layout of the last cpx_occupancy_build: parameters compacted in
  * z-y-x order of the in-cage flags, optimizer state reset to zero. */
 cpx_status cpx_grid_make_sparse(cpx_grid* g);
@@ -274,6 +355,17 @@ cpx_status cpx_grid_save_text(const cpx_grid* g, const char* dir, int band, int 
  * file_sh_dim SH coefficients per channel from `dir` into a dense grid of at least that many
  * (the rest zero); values parsed as the reference's fscanf("%f ").  Synchronous. */
 cpx_status cpx_grid_load_text(cpx_grid* g, const char* dir, int file_sh_dim);
+/* objectScene::initFromFile (SVRF/SceneUtils.cu:703-790), sparse with occupancy: a sparse
+ * checkpoint of cpx_grid_save_text or the reference's saveSelf into a fresh dense grid of its
+ * dimensions, which becomes sparse.  The in-cage count comes from
+ * sparse_inCageInfo_band<b>.txt, where the reference's saveSelf writes it (over the in-cage
+ * flags, SVRF/SceneUtils.cu:1280-1283); the flags are rebuilt from occupancy.txt by the rule
+ * pruneScene made them with, and must give sparse_indexOffset.txt and the count exactly
+ * (else CPX_ERR_INVALID_ARGUMENT: an inconsistent checkpoint).  Compact density and the first
+ * file_sh_dim SH coefficients per channel come from the *_sparse.txt files.  (The reference's
+ * loader reads its in-cage flags from the file that then holds only the count, so every flag
+ * it loads is the count's low byte; the flags here are the saved grid's.)  Synchronous. */
+cpx_status cpx_grid_load_text_sparse(cpx_grid* g, const char* dir, int file_sh_dim);
 /* Image::initSelfFromFile (SVRF/ImageUtils.cu:84-128): <prefix>_mask.txt and
  * <prefix>_{red,green,blue}.txt (or <prefix>.txt when gray_only) into host planes of
  * width*height bytes; bbox[4] = the rows and columns bounding the nonzero mask pixels
@@ -292,10 +384,14 @@ cpx_status cpx_image_mask_pixels(const int* bbox, int width, int32_t* index_out,
  *                        sequence;
  * CPX_OPT_NO_EARLY_STOP  the FP32 march runs every ray to its far bound, instead of ending it
  *                        once its transmittance is below 1e-4 (what the rest of the ray could
- *                        add to its colour and weight). */
+ *                        add to its colour and weight);
+ * CPX_OPT_TWO_STAGE_MARCH  the march runs as two launches -- placement of every ray, then
+ *                        shading -- instead of one launch that shades rays while others are
+ *                        still being placed.  Results are the same; for comparison. */
 #define CPX_OPT_NO_EMPTY_SKIP 1
 #define CPX_OPT_FP32_MARCH 2
 #define CPX_OPT_NO_EARLY_STOP 4
+#define CPX_OPT_TWO_STAGE_MARCH 8
 cpx_status cpx_grid_set_options(cpx_grid* g, int options);
 
 /* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,
