@@ -1362,3 +1362,62 @@ double orc_bbox(const float* lr, int W, int H, int D, int* bbox)
     for (int i = 0; i < 6; i++) bbox[i] = b[i];
     return best / W * 2.;
 }
+
+/* ---------------------------------------------------------------- jitter (R12) */
+/* Standard normal quantile from the mathematics: the root of 0.5 erfc(z / sqrt 2) = q for the
+ * upper tail (q <= 0.5, z >= 0), by Newton's method on libm's erfc, which keeps relative
+ * accuracy in the tail.  Returns z with P(Z > z) = q. */
+static double upper_quantile(double q)
+{
+    const double pi = 3.14159265358979323846, sqrt2 = 1.41421356237309504880;
+    if (q >= 0.5) return 0.;
+    /* start from the tail expansion z ~ sqrt(-2 ln q) - (ln(-2 ln q) + ln 4pi) / (2 sqrt(-2 ln q)) */
+    const double l = sqrt(-2. * log(q));
+    double z = q < 0.3 ? l - (log(l * l) + log(4. * pi)) / (2. * l) : 0.;
+    if (z < 0.) z = 0.;
+    for (int it = 0; it < 100; it++) {
+        const double f = 0.5 * erfc(z / sqrt2) - q;
+        const double pdf = exp(-0.5 * z * z) / sqrt(2. * pi);
+        const double dz = f / pdf;
+        z += dz;
+        if (fabs(dz) <= 1e-17 * (1. + fabs(z))) break;
+    }
+    return z;
+}
+
+/* randGPU(dest, len, radius, 1) (SVRF/Utils.cu:1002-1044) restated.  Generator state i < min(len,
+ * 20000) is dimension i of the scrambled Sobol sequence with direction numbers dirs[i][0..63]
+ * and scramble word scramble32[i] (the reference copies the 64-bit constants into a 32-bit
+ * array), started at point i + first.  Point n of a dimension is, in the Gray-code form of
+ * Antonov and Saleev, x_n = c XOR (XOR of v_b over the set bits b of n ^ (n >> 1)); state i's
+ * j-th draw is point i + first + j.  A 64-bit point x becomes N(0,1) through the inverse
+ * normal CDF at the centre of its cell, p = (x + 1/2) / 2^64 (mirrored as 1 - p above one
+ * half so the tail keeps its precision).  Offset k = draw k / 20000 of state k % 20000, times
+ * radius / 4; only the entries the reference's square grid of 32x32 blocks reaches are
+ * written (the rest keep their value). */
+void orc_sobol_offsets(const uint64_t* dirs, const uint32_t* scramble32, int len, uint64_t first, double radius,
+                       double* out)
+{
+    const int n_states = len < 20000 ? len : 20000;
+    const int square = (int)(sqrt(len * 1.0) + 0.5);
+    const int64_t side = (square + 31) / 32;
+    const int64_t reach = side * side * 1024;
+    const int n_write = reach < len ? (int)reach : len;
+    for (int k = 0; k < n_write; k++) {
+        const int i = k % 20000;
+        if (i >= n_states) continue;
+        const uint64_t n = (uint64_t)i + first + (uint64_t)(k / 20000);
+        const uint64_t gray = n ^ (n >> 1);
+        uint64_t x = (uint64_t)scramble32[i];
+        for (int b = 0; b < 64; b++)
+            if ((gray >> b) & 1u) x ^= dirs[(size_t)i * 64 + b];
+        double z;
+        if (x >> 63) {
+            const uint64_t m = ~x; /* 2^64 - 1 - x */
+            z = upper_quantile(((double)m + 0.5) * 0x1p-64);
+        } else {
+            z = -upper_quantile(((double)x + 0.5) * 0x1p-64);
+        }
+        out[k] = z / 4. * radius + 0.;
+    }
+}

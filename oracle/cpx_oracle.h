@@ -148,6 +148,10 @@ void orc_upsample(const orc_scene* src, int dW, int dH, int dD, int dst_sh, floa
 
 /* R11: batch MSE of the per-ray losses (Utils.cu:311-320). */
 double orc_mse(const double* losses, int n);
+/* randGPU's normal jitter offsets (SVRF/Utils.cu:1002-1044) from cuRAND's scrambled Sobol64
+ * direction numbers dirs[n_states][64] and 32-bit scramble words, for len entries. */
+void orc_sobol_offsets(const uint64_t* dirs, const uint32_t* scramble32, int len, uint64_t first, double radius,
+                       double* out);
 
 /* Compositing known-answer test: the arithmetic of testRender
  * (SVRF/VolumeFieldRender.cu:111-183), FP64. */

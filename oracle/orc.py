@@ -364,3 +364,56 @@ def bbox(lr, W, H, D):
     out = np.zeros(6, np.int32)
     sr = _lib.orc_bbox(_p(np.ascontiguousarray(lr, np.float32)), int(W), int(H), int(D), _p(out))
     return tuple(int(x) for x in out), float(sr)
+
+
+_fn("orc_sobol_offsets", [_vp, _vp, C.c_int, C.c_uint64, C.c_double, _vp])
+
+_CURAND_SCRAMBLED_DIRECTION_VECTORS_64_JOEKUO6 = 104  # curandDirectionVectorSet_t (curand.h)
+_sobol_tables = None
+
+
+def sobol_tables(n_states):
+    """cuRAND's scrambled 64-bit JOEKUO6 direction numbers [n_states][64] and the first n_states
+    32-bit words of its 64-bit scramble constants (how randGPU copies them), read through the
+    host API at run time (curandGetDirectionVectors64 / curandGetScrambleConstants64)."""
+    global _sobol_tables
+    if _sobol_tables is None:
+        import ctypes.util
+        import os
+
+        names = [os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64", "libcurand.so"),
+                 ctypes.util.find_library("curand") or "libcurand.so"]
+        lib = None
+        for nm in names:
+            try:
+                lib = C.CDLL(nm)
+                break
+            except OSError:
+                continue
+        if lib is None:
+            raise ImportError("libcurand is needed for the jitter oracle's direction numbers")
+        dirs, scr = C.c_void_p(), C.c_void_p()
+        if lib.curandGetDirectionVectors64(C.byref(dirs), _CURAND_SCRAMBLED_DIRECTION_VECTORS_64_JOEKUO6) != 0 or \
+                lib.curandGetScrambleConstants64(C.byref(scr)) != 0:
+            raise RuntimeError("cuRAND tables unavailable")
+        _sobol_tables = (lib, dirs.value, scr.value)
+    _, dp, sp = _sobol_tables
+    d = np.ctypeslib.as_array(C.cast(dp, C.POINTER(C.c_uint64)), shape=(n_states * 64,)).copy()
+    s = np.ctypeslib.as_array(C.cast(sp, C.POINTER(C.c_uint32)), shape=(n_states,)).copy()
+    return d.reshape(n_states, 64), s
+
+
+def max_sample_point(W, H, D, step):
+    """objectScene::maxSamplePoint (SceneUtils.cu:96)."""
+    return int(np.sqrt(float(W * W + H * H + D * D)) / np.float64(np.float32(step)) + 1.5)
+
+
+def sobol_offsets(length, first, radius, out=None):
+    """randGPU(dest, length, radius, 1) (Utils.cu:1002-1044): float64[length]; entries beyond
+    the reference's launch grid keep `out`'s values (zero by default)."""
+    n_states = min(length, 20000)
+    d, s = sobol_tables(n_states)
+    res = np.zeros(length, np.float64) if out is None else np.ascontiguousarray(out, np.float64).copy()
+    _lib.orc_sobol_offsets(d.ctypes.data, s.ctypes.data, int(length), int(first),
+                           float(np.float64(np.float32(radius))), res.ctypes.data)
+    return res

@@ -22,6 +22,7 @@
 #include "Rays.cuh"
 
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -170,6 +171,31 @@ int ref_set_offsets(void* h, const double* ox, const double* oy, const double* o
     cudaMemcpy(c->scene.offsetZDevice, oz, sizeof(double) * n, cudaMemcpyHostToDevice);
     return fail(cudaDeviceSynchronize());
 }
+
+// objectScene::setSelfSampleOffset(stepSize / 2) right after srand(seed), as the batch loop calls
+// it under SolidStrategy 0 (SVRF/Render.cu:402-405, SceneUtils.cu:792-798): the three offset
+// arrays (maxSamplePoint entries each, x then y then z) to host memory.
+int ref_sample_offsets(void* h, unsigned seed, double* out, int* n_out)
+{
+    RefCtx* c = (RefCtx*)h;
+    srand(seed);
+    c->scene.setSelfSampleOffset(c->scene.stepSize / 2.);
+    const int n = c->scene.maxSamplePoint;
+    cudaMemcpy(out, c->scene.offsetXDevice, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(out + n, c->scene.offsetYDevice, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(out + 2 * n, c->scene.offsetZDevice, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    *n_out = n;
+    return fail(cudaDeviceSynchronize());
+}
+
+// The values the host's rand() returns after srand(seed): the seeds randGPU's calls draw.
+void ref_rand_values(unsigned seed, unsigned* out, int n)
+{
+    srand(seed);
+    for (int i = 0; i < n; i++) out[i] = (unsigned)rand();
+}
+
+int ref_max_sample_point(void* h) { return ((RefCtx*)h)->scene.maxSamplePoint; }
 
 // Optimizer over the scene's parameter table (Optimizer.cu:81-187, Render.cu:63, 300-305).
 int ref_optimizer_init(void* h, int hierarchy)

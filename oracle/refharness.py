@@ -68,6 +68,10 @@ def _setup(L):
     s("ref_train_step", [_vp, C.c_int, C.c_int, C.c_double, C.c_float, C.c_double, C.c_double, C.c_int,
                          C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _vp, _vp])
     s("ref_n_active", [_vp], C.c_int64)
+    s("ref_sample_offsets", [_vp, C.c_uint, _vp, C.POINTER(C.c_int)])
+    s("ref_max_sample_point", [_vp])
+    L.ref_rand_values.argtypes = [C.c_uint, _vp, C.c_int]
+    L.ref_rand_values.restype = None
     s("ref_params", [_vp, _vp, C.c_int])
     s("ref_grads", [_vp, _vp, C.c_int])
     s("ref_moments", [_vp, _vp, _vp, C.c_int])
@@ -119,6 +123,14 @@ class RefScene:
     def set_offsets(self, ox, oy, oz):
         arrs = [np.ascontiguousarray(a, np.float64) for a in (ox, oy, oz)]
         _ck(lib().ref_set_offsets(self.h, *[_p(a) for a in arrs], len(arrs[0])), "set_offsets")
+
+    def sample_offsets(self, seed):
+        """setSelfSampleOffset(stepSize / 2) after srand(seed): (x, y, z) float64 arrays."""
+        n = int(lib().ref_max_sample_point(self.h))
+        out = np.zeros(3 * n, np.float64)
+        got = C.c_int()
+        _ck(lib().ref_sample_offsets(self.h, int(seed), _p(out), C.byref(got)), "sample_offsets")
+        return out[:n].copy(), out[n:2 * n].copy(), out[2 * n:].copy()
 
     def optimizer_init(self, hierarchy=False):
         _ck(lib().ref_optimizer_init(self.h, 1 if hierarchy else 0), "optimizer_init")
@@ -260,6 +272,13 @@ class RefScene:
             self.close()
         except Exception:
             pass
+
+
+def rand_values(seed, n=3):
+    """What the host's rand() returns after srand(seed) (the reference draws its jitter seeds so)."""
+    out = np.zeros(n, np.uint32)
+    lib().ref_rand_values(int(seed), _p(out), int(n))
+    return out
 
 
 def load_text(directory, W, H, D, step, sh_dim, target_sh):
