@@ -23,9 +23,10 @@ __device__ __forceinline__ int64_t grid_index_upper(int x, int y, int z, int W, 
     return (int64_t)z * W * H + (int64_t)y * W + x;
 }
 
-// occupiedVoxel + pruneScene; one thread per cell, cells in z-y-x order.
-__global__ void k_prune(const float* __restrict__ dens, int W, int H, int D, float thr,
-                        uint8_t* occ, uint32_t* occ_bits, uint8_t* in_cage, int64_t n_cells,
+// occupiedVoxel + pruneScene; one thread per cell, cells in z-y-x order.  With occ_in set the
+// cells' occupancy is given (a loaded occupancy.txt) and only the in-cage rule runs.
+__global__ void k_prune(const float* __restrict__ dens, const uint8_t* __restrict__ occ_in, int W, int H, int D,
+                        float thr, uint8_t* occ, uint32_t* occ_bits, uint8_t* in_cage, int64_t n_cells,
                         unsigned long long* dropped)
 {
     const int64_t ci = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -35,10 +36,14 @@ __global__ void k_prune(const float* __restrict__ dens, int W, int H, int D, flo
         const int x = (int)(ci % Wc);
         const int y = (int)((ci / Wc) % Hc);
         const int z = (int)(ci / ((int64_t)Wc * Hc));
-        for (int dz = 0; dz <= 1 && !occupied; dz++)
-            for (int dy = 0; dy <= 1 && !occupied; dy++)
-                for (int dx = 0; dx <= 1 && !occupied; dx++)
-                    if (dens[grid_index_upper(x + dx, y + dy, z + dz, W, H, D)] > thr) occupied = true;
+        if (occ_in) {
+            occupied = occ_in[ci] != 0;
+        } else {
+            for (int dz = 0; dz <= 1 && !occupied; dz++)
+                for (int dy = 0; dy <= 1 && !occupied; dy++)
+                    for (int dx = 0; dx <= 1 && !occupied; dx++)
+                        if (dens[grid_index_upper(x + dx, y + dy, z + dz, W, H, D)] > thr) occupied = true;
+        }
         occ[ci] = occupied ? 1 : 0;
         if (occupied) {
             const int64_t N = (int64_t)W * H * D;
@@ -173,7 +178,9 @@ __global__ void k_bricks(const uint32_t* __restrict__ occ_bits, int cw, int ch, 
     if ((threadIdx.x & 31) == 0 && k < nb) brick_bits[k >> 5] = word;
 }
 
-cpx_status occupancy_launch(cpx_grid* g, float threshold)
+cpx_status occupancy_launch(cpx_grid* g, float threshold) { return occupancy_build(g, threshold, nullptr); }
+
+cpx_status occupancy_build(cpx_grid* g, float threshold, const uint8_t* occ_in_dev)
 {
     const int64_t N = g->n_dense;
     const int64_t C = (int64_t)(g->W - 1) * (g->H - 1) * (g->D - 1);
@@ -210,7 +217,7 @@ cpx_status occupancy_launch(cpx_grid* g, float threshold)
     const int64_t words = (C + 31) / 32;
     cudaMemset(g->occ_bits, 0, (words + 1) * sizeof(uint32_t));
     const int64_t prune_threads = words * 32;
-    k_prune<<<(unsigned)((prune_threads + 255) / 256), 256>>>(g->density, g->W, g->H, g->D,
+    k_prune<<<(unsigned)((prune_threads + 255) / 256), 256>>>(g->density, occ_in_dev, g->W, g->H, g->D,
                                                                threshold, g->occ_bytes,
                                                                g->occ_bits, g->in_cage, C,
                                                                dropped);

@@ -69,6 +69,20 @@ bool read_bytes(const std::string& path, uint8_t* a, int64_t n)
     return ok;
 }
 
+bool read_u32(const std::string& path, uint32_t* a, int64_t n)
+{
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    bool ok = true;
+    for (int64_t i = 0; i < n && ok; i++) {
+        int v = 0;
+        ok = std::fscanf(f, "%d ", &v) == 1;
+        a[i] = (uint32_t)v;
+    }
+    std::fclose(f);
+    return ok;
+}
+
 cpx_status io_error(const std::string& path, const char* what)
 {
     set_error("%s %s failed", what, path.c_str());
@@ -168,6 +182,101 @@ cpx_status cpx_grid_load_text(cpx_grid* g, const char* dir, int file_sh_dim)
             if (!read_floats(join(dir, name), planar.data() + (size_t)(1 + c * g->sh_dim + k) * n, n))
                 return io_error(join(dir, name), "reading");
         }
+    return cpx_grid_upload_params(g, planar.data(), n);
+}
+
+cpx_status cpx_grid_download_occupancy(const cpx_grid* g, uint8_t* occupancy_out, uint8_t* in_cage_out,
+                                       uint32_t* index_offsets_out, uint32_t* in_cage_count_out)
+{
+    if (!g) {
+        set_error("null grid");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (!g->have_occupancy) {
+        set_error("the grid has no occupancy tables");
+        return CPX_ERR_NOT_READY;
+    }
+    const int64_t C = (int64_t)(g->W - 1) * (g->H - 1) * (g->D - 1);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && occupancy_out) e = cudaMemcpy(occupancy_out, g->occ_bytes, (size_t)C, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && in_cage_out) e = cudaMemcpy(in_cage_out, g->in_cage, (size_t)g->n_dense, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && index_offsets_out)
+        e = cudaMemcpy(index_offsets_out, g->index_offsets, (size_t)g->n_dense * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (in_cage_count_out) *in_cage_count_out = g->in_cage_count;
+    return cuda_status(e, "download occupancy");
+}
+
+cpx_status cpx_grid_load_text_sparse(cpx_grid* g, const char* dir, int file_sh_dim)
+{
+    if (!g || !dir) {
+        set_error("null argument");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (g->sparse) {
+        set_error("a sparse checkpoint loads into a fresh dense grid of its dimensions");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    const int band = (int)(std::sqrt((double)file_sh_dim) - 1);
+    if (file_sh_dim < 1 || (band + 1) * (band + 1) != file_sh_dim || file_sh_dim > g->sh_dim) {
+        set_error("files of %d SH coefficients do not fit a grid of %d", file_sh_dim, g->sh_dim);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    if (g->W < 2 || g->H < 2 || g->D < 2) {
+        set_error("a sparse grid needs at least 2 vertices per axis");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    char name[256];
+    // the in-cage count, from the file initFromFile reads it from (SceneUtils.cu:725-733)
+    std::snprintf(name, sizeof(name), "sparse_inCageInfo_band%d.txt", band);
+    int count = -1;
+    {
+        FILE* f = std::fopen(join(dir, name).c_str(), "r");
+        if (!f) return io_error(join(dir, name), "reading");
+        const int got = std::fscanf(f, "%d", &count);
+        std::fclose(f);
+        if (got != 1 || count < 0 || count > g->n_dense) return io_error(join(dir, name), "reading the in-cage count of");
+    }
+    const int64_t N = g->n_dense;
+    const int64_t C = (int64_t)(g->W - 1) * (g->H - 1) * (g->D - 1);
+    std::vector<uint8_t> occ((size_t)C);
+    if (!read_bytes(join(dir, "occupancy.txt"), occ.data(), C)) return io_error(join(dir, "occupancy.txt"), "reading");
+    std::vector<uint32_t> idx((size_t)N);
+    if (!read_u32(join(dir, "sparse_indexOffset.txt"), idx.data(), N))
+        return io_error(join(dir, "sparse_indexOffset.txt"), "reading");
+    const int64_t n = count;
+    std::vector<float> planar((size_t)g->n_arrays * (n > 0 ? n : 1), 0.f);
+    std::snprintf(name, sizeof(name), "sparse_opacity_band%d.txt", band);
+    if (!read_floats(join(dir, name), planar.data(), n)) return io_error(join(dir, name), "reading");
+    const char* ch[3] = {"red", "green", "blue"};
+    for (int c = 0; c < 3; c++)
+        for (int k = 0; k < file_sh_dim; k++) {
+            std::snprintf(name, sizeof(name), "%s_%d_sparse.txt", ch[c], k);
+            if (!read_floats(join(dir, name), planar.data() + (size_t)(1 + c * g->sh_dim + k) * n, n))
+                return io_error(join(dir, name), "reading");
+        }
+    // occupancy tables from the saved cells: the in-cage flags by pruneScene's rule
+    // (SceneUtils.cu:850-873), their prefix index, the brick map
+    uint8_t* occ_dev = nullptr;
+    cudaError_t e = cudaMalloc((void**)&occ_dev, (size_t)C);
+    if (e == cudaSuccess) e = cudaMemcpy(occ_dev, occ.data(), (size_t)C, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(occ_dev);
+        return cuda_status(e, "occupancy upload");
+    }
+    cpx_status rc = occupancy_build(g, 0.f, occ_dev);
+    cudaFree(occ_dev);
+    if (rc != CPX_OK) return rc;
+    std::vector<uint32_t> built((size_t)N);
+    e = cudaMemcpy(built.data(), g->index_offsets, (size_t)N * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "index offsets");
+    if ((int64_t)g->in_cage_count != n || built != idx) {
+        g->have_occupancy = 0;
+        set_error("checkpoint %s is inconsistent: its occupancy gives %u in-cage vertices and %s index offsets, "
+                  "the files say %d", dir, g->in_cage_count, built == idx ? "the same" : "other", count);
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    rc = make_sparse_launch(g);
+    if (rc != CPX_OK) return rc;
     return cpx_grid_upload_params(g, planar.data(), n);
 }
 

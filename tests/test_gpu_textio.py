@@ -113,3 +113,99 @@ def test_image_text_reads_as_the_reference_reads(cuda, tmp_path):
     for a, b in zip(img, rimg):
         assert np.array_equal(a, b)
     assert box == rbox and np.array_equal(pix, rpix)
+
+
+def _sparse_scene(n, seed, thr=1.0):
+    import cpx
+
+    params = _params(n, seed)
+    sc = cpx.ObjectScene(n, n, n, 9)
+    sc.upload_params(params)
+    occ, cage, idx, cnt = sc.prune_self(thr)
+    sc.make_sparse()
+    return sc, params, occ, cage, idx, cnt
+
+
+def test_sparse_checkpoint_round_trip(cuda, tmp_path):
+    """cpx_grid_save_text then cpx_grid_load_text_sparse: the same occupancy tables, the same
+    compact parameters (as their 6-decimal text), and the same march."""
+    import cpx
+
+    n = 24
+    sc, params, occ, cage, idx, cnt = _sparse_scene(n, 12)
+    d = tmp_path / "ckpt"
+    d.mkdir()
+    cpx.save_text(sc, d, 2)
+    want = sc.download_params()
+    back = cpx.ObjectScene(n, n, n, 9)
+    cpx.load_text_sparse(back, d, 9)
+    assert back.sparse and back.actual_grid_nums == cnt
+    occ2, cage2, idx2 = back.occupancy_tables()
+    assert np.array_equal(occ2, occ) and np.array_equal(cage2, cage) and np.array_equal(idx2, idx)
+    got = back.download_params()
+    assert np.abs(got - want).max() <= 5e-7 * max(1.0, np.abs(want).max())
+    # reloading the files of the reloaded grid gives identical bits
+    d2 = tmp_path / "ckpt2"
+    d2.mkdir()
+    cpx.save_text(back, d2, 2)
+    _same_files(d, d2)
+    # both grids march the same (the loaded values are the text's)
+    import cpx_scenes as S
+    import torch
+
+    cams = [S.look_at_camera(p, n, 48, 48) for p in S.fibonacci_sphere(4, 4.0)]
+    rng = np.random.default_rng(1)
+    pix = S.sample_pixels(rng, 4, 48, 48, 256)
+    imgs = [tuple(rng.integers(0, 256, 48 * 48, dtype=np.uint8) for _ in range(3)) + (None,) for _ in range(4)]
+    outs = []
+    for g in (sc, back):
+        g.upload_params(got)
+        r = cpx.Rays(256)
+        r.initial_self(g, [cpx.Camera.make(**c) for c in cams], imgs, pix, 48, 48)
+        cpx.RenderUtils.renderRays(r, g)
+        outs.append(r.download(fields=cpx.RAY_OUTPUTS))
+        r.close()
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+    del torch
+
+
+def test_sparse_checkpoint_of_the_reference_loads(cuda, tmp_path):
+    """A sparse checkpoint written by the reference's own saveSelf loads into the grid the
+    reference saved: occupancy, in-cage count and index offsets bit-exact, compact parameters
+    as their text."""
+    import cpx
+    import refharness as R
+
+    n = 20
+    params = _params(n, 14)
+    d = tmp_path / "ref"
+    d.mkdir()
+    ref = R.RefScene(n, n, n, 9, 2, 0.5, params, sparse_threshold=1.0)
+    ref.save_text(d, 2)
+    rocc, rcage, ridx = ref.occupancy()
+    rparams = ref.params()
+    cnt = ref.in_cage_count
+    ref.close()
+    sc = cpx.ObjectScene(n, n, n, 9)
+    cpx.load_text_sparse(sc, d, 9)
+    assert sc.sparse and sc.actual_grid_nums == cnt
+    got = sc.download_params()
+    assert np.abs(got - rparams).max() <= 5e-7 * max(1.0, np.abs(rparams).max())
+    occ, cage, idx = sc.occupancy_tables()
+    assert np.array_equal(occ, rocc) and np.array_equal(idx, ridx) and np.array_equal(cage, rcage)
+
+
+def test_inconsistent_sparse_checkpoint_is_refused(cuda, tmp_path):
+    import cpx
+
+    n = 20
+    sc, *_ = _sparse_scene(n, 15)
+    d = tmp_path / "ckpt"
+    d.mkdir()
+    cpx.save_text(sc, d, 2)
+    with open(d / "sparse_inCageInfo_band2.txt", "w") as f:
+        f.write("%d" % (sc.actual_grid_nums + 1))
+    with pytest.raises(cpx.CpxError) as ei:
+        cpx.load_text_sparse(cpx.ObjectScene(n, n, n, 9), d, 9)
+    assert ei.value.name == "CPX_ERR_INVALID_ARGUMENT"
