@@ -222,14 +222,21 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic_per_vertex():
-    """DRAM bytes per vertex of the fused sweep from the committed ncu summary, if any."""
-    p = REPO / "profiles" / "sweep_tv_adam_256.md"
+def profiled_sweep_traffic(kernel_prefix, n_vertices):
+    """DRAM bytes per launch of the fused sweep from the committed ncu capture of the same
+    workload (profiles/sweep_traffic.json: one launch captured inside this bench's 256^3 run),
+    or None when no capture of this kernel at this size exists."""
+    p = REPO / "profiles" / "sweep_traffic.json"
     if not p.exists():
         return None
-    for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_vertex:"):
-            return float(line.split(":", 1)[1].split()[0])
+    try:
+        d = json.loads(p.read_text())
+    except ValueError:
+        return None
+    for row in d.get("captures", []):
+        if row.get("kernel", "").startswith(kernel_prefix) and int(row.get("vertices", -1)) == int(n_vertices):
+            return {"bytes": int(row["dram_read_bytes"]) + int(row["dram_write_bytes"]),
+                    "touched_vertices": row.get("touched_vertices"), "source": "profiles/sweep_traffic.json"}
     return None
 
 
@@ -332,6 +339,8 @@ def run_ours(args, wl, world, rank, local):
     scene = build_training_grid(wl, dev, args.precision, field)
     del field
     n_act = scene.actual_grid_nums
+    if args.march_options:
+        scene.set_options(args.march_options)
     pool, packed = build_pool(scene, wl, eyes, pix, order, gt, P)
     host_pool = torch.from_numpy(packed).pin_memory()
     batch_rays = cpx.Rays(R, white_bg=True)
@@ -476,12 +485,29 @@ def run_ours(args, wl, world, rank, local):
             "sparse" if thr is not None else "dense")
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
-    tpv = profiled_traffic_per_vertex() if args.precision == "fp32" else None
+    prof = profiled_sweep_traffic("k_sweep_dense" if thr is None else "k_sweep_sparse", N) \
+        if args.precision == "fp32" else None
+    # the whole step and the march, on the algorithmic bytes of the step: R * 100 B of ray
+    # records (read o/d/near/far forward and backward, ground truth, forward outputs written and
+    # read back) + U * (2P + 2G) for the touched vertices (parameter gather forward and backward,
+    # gradient read + write by the scatter), P = 112 B (FP32) or 4 + 27 * 2 B (16-bit SH), G = 112
+    p_rec = rec if args.precision == "fp32" else 4 + 27 * 2
+    march_bytes = R * 100 + touched * (2 * p_rec + 2 * rec)
+    step_ms = ms / K
+    march_gbs = march_bytes / (march_ms / 1e3) / 1e9
+    step_gbs = (march_bytes + alg_bytes) / (step_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": sweep_kernel, "achieved": round(achieved, 1),
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "alg_bytes_per_launch": int(alg_bytes), "touched_vertices_per_launch": int(touched),
-                "traffic": None if tpv is None else int(tpv * N),
-                "launch_ms": round(sweep_ms, 4)}
+                "traffic": None if prof is None else prof["bytes"],
+                "traffic_source": None if prof is None else prof["source"],
+                "launch_ms": round(sweep_ms, 4),
+                "step": {"alg_bytes": int(march_bytes + alg_bytes), "ms": round(step_ms, 4),
+                         "achieved": round(step_gbs, 1), "frac": round(step_gbs / peak, 4),
+                         "what": "whole step: R*100 + U*(2P+2G) + the sweep's bytes, over ms_per_step"},
+                "march": {"alg_bytes": int(march_bytes), "ms": round(march_ms, 4),
+                          "achieved": round(march_gbs, 1), "frac": round(march_gbs / peak, 4),
+                          "what": "march (placement + shading): R*100 + U*(2P+2G), over its device time"}}
 
     result = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -497,7 +523,7 @@ def run_ours(args, wl, world, rank, local):
                             "dense" if thr is None else "sparse (blob field > %.1f, %d active vertices)" % (thr, N),
                             R, wl["cams"], wl["img"], wl["img"], wl["gt_n"], wl["n_blobs"])),
             "grid": n, "sh_dim": SH_DIM, "batch_rays": R, "pool_rays": P, "step_constants": STEP,
-            "precision": args.precision, "form": args.form,
+            "precision": args.precision, "form": args.form, "march_options": args.march_options,
             "proposal_schedule": PROPOSAL if prop is not None else None,
             "start_batch": W, "lr_decay": "reference per batch (Render.cu:499-500)" if decay else "none",
             "l2": "inputs larger than L2: the sweep streams %.1f GB of grid state per step" % (alg_bytes / 1e9),
@@ -755,45 +781,66 @@ def render_view_march(scene, cam, img, prec, prop):
     return torch.from_numpy(rgb).cuda()
 
 
-def quality_run(args, wl, local):
-    """Trains args.quality batches in the plain FP32 form and in the --precision/--form form
-    from the same initial grid and ray pool (with the reference's per-batch learning-rate decay),
-    renders held-out views of each (through the image path -- the reference's renderer, full
-    march -- and through the form's own training march) and of the hidden grid, and reports
-    the PSNR of each against the hidden grid's views and their difference."""
+# largest per-pixel colour difference between a view rendered by the guided march and by the
+# full march of the same grid above which that view's guided render is replaced by the full march
+GUIDED_FALLBACK_MAX_DIFF = 0.05
+
+
+def held_out_views(wl):
+    """Two disjoint sets of 8 views on the upper hemisphere, neither among the training views
+    (other seeds): validation views choose the proposal's settings, test views report."""
+    import cpx_scenes as S
+
+    return {"validation": S.upper_hemisphere(8, 4.0, np.random.default_rng(wl["seed"] + 77)),
+            "test": S.upper_hemisphere(8, 4.0, np.random.default_rng(wl["seed"] + 99))}
+
+
+def quality_run(args, wl, local, prec=None, form=None, n_batches=None, repeat=None):
+    """Trains n_batches in the plain FP32 form and in the prec/form form from the same initial
+    grid and ray pool (with the reference's per-batch learning-rate decay), renders the
+    held-out views of each (through the image path -- the reference's renderer, full march --
+    and through the form's own training march) and of the hidden grid, and reports the PSNR of
+    each against the hidden grid's views, per view and on average, on the validation and the
+    test views.  A view whose guided render differs from the full march of the same grid by
+    more than GUIDED_FALLBACK_MAX_DIFF on some pixel falls back to the full march."""
     import torch
 
     import cpx
     import cpx_scenes as S
 
+    prec = args.precision if prec is None else prec
+    form = args.form if form is None else form
+    N = args.quality if n_batches is None else n_batches
+    repeat = (not args.no_repeat) if repeat is None else repeat
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    N, R = args.quality, wl["batch"]
+    R = wl["batch"]
     wlq = dict(wl, pool_batches=min(N, 256))  # distinct batches of the run's ray pool
     P = R * wlq["pool_batches"]
     eyes, pix, order = camera_set(wlq)
     gt, field, gt_scene = build_ground_truth(wlq, dev, eyes, pix, P, keep_grid=True)
     img = wl["img"]
-    held = S.upper_hemisphere(8, 4.0, np.random.default_rng(wl["seed"] + 99))  # not among the training views
-    refs = [cpx.RenderUtils.renderImage(gt_scene, cpx.Camera.make(**S.look_at_camera(e, wl["gt_n"], img, img)), img,
-                                        img, outputs=("rgb",))["rgb"].clone() for e in held]
+    view_sets = held_out_views(wl)
+    refs = {k: [cpx.RenderUtils.renderImage(gt_scene, cpx.Camera.make(**S.look_at_camera(e, wl["gt_n"], img, img)),
+                                            img, img, outputs=("rgb",))["rgb"].clone() for e in v]
+            for k, v in view_sets.items()}
     gt_scene.close()
     torch.cuda.empty_cache()
     forms = {}
     net = proposal_net(args)
     # the plain FP32 form twice: two runs differ only through the float atomics of the scatter,
     # which sets the noise floor of the comparison
-    runs = [(0, "fp32", "plain"), (1, "fp32", "plain"), (2, args.precision, args.form)]
-    if args.no_repeat:
+    runs = [(0, "fp32", "plain"), (1, "fp32", "plain"), (2, prec, form)]
+    if not repeat:
         runs.pop(1)
-    for run, prec, form in runs:
+    for run, rprec, rform in runs:
         lr = [STEP["lr"], STEP["sh_lr"]]
-        scene = build_training_grid(wl, dev, prec, field)
+        scene = build_training_grid(wl, dev, rprec, field)
         if run == 2 and args.march_options:
             scene.set_options(args.march_options)
         pool, _ = build_pool(scene, wlq, eyes, pix, order, gt, P)
         losses = torch.zeros(R, dtype=torch.float64, device=dev)
-        prop = cpx.Proposal(seed=wl["seed"] + 11, **net) if form == "proposal" else None
+        prop = cpx.Proposal(seed=wl["seed"] + 11, **net) if rform == "proposal" else None
         batches = wlq["pool_batches"]
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
@@ -814,47 +861,91 @@ def quality_run(args, wl, local):
         torch.cuda.synchronize()
         scene.check()
         ms = t0.elapsed_time(t1)
-        psnr, psnr_march, psnr_full, maxdiff = [], [], [], []
-        for e, ref in zip(held, refs):
-            cam = cpx.Camera.make(**S.look_at_camera(e, wl["n"], img, img))
-            im = cpx.RenderUtils.renderImage(scene, cam, img, img, outputs=("rgb",))["rgb"]
-            psnr.append(round(cpx.image_psnr(im, ref), 4))
-            own = render_view_march(scene, cam, img, prec, prop)
-            psnr_march.append(round(cpx.image_psnr(own, ref), 4))
-            if prop is not None:
-                full = render_view_march(scene, cam, img, prec, None)
-                psnr_full.append(round(cpx.image_psnr(full, ref), 4))
-                maxdiff.append(round(float((own - full).abs().max()), 5))
-        forms[form_key(prec, form, run, args)] = {
-            "march_options": args.march_options if run == 2 else 0,
-            "psnr_db": round(float(np.mean(psnr)), 4), "psnr_per_view": psnr,
-            "psnr_own_march_db": round(float(np.mean(psnr_march)), 4),
-            "psnr_full_march_db": round(float(np.mean(psnr_full)), 4) if psnr_full else None,
-            "max_pixel_diff_guided_vs_full": max(maxdiff) if maxdiff else None,
-            "train_ms": round(ms, 1), "train_rays_per_s": round(N * R / (ms / 1e3), 1),
-            "proposal": None if prop is None else prop.stats(),
-        }
+        entry = {"march_options": args.march_options if run == 2 else 0, "train_ms": round(ms, 1),
+                 "train_rays_per_s": round(N * R / (ms / 1e3), 1),
+                 "proposal": None if prop is None else prop.stats()}
+        for vs, views in view_sets.items():
+            psnr, psnr_march, psnr_full, maxdiff, fell_back = [], [], [], [], []
+            for e, ref in zip(views, refs[vs]):
+                cam = cpx.Camera.make(**S.look_at_camera(e, wl["n"], img, img))
+                im = cpx.RenderUtils.renderImage(scene, cam, img, img, outputs=("rgb",))["rgb"]
+                psnr.append(round(cpx.image_psnr(im, ref), 4))
+                own = render_view_march(scene, cam, img, rprec, prop)
+                if prop is not None:
+                    full = render_view_march(scene, cam, img, rprec, None)
+                    d = float((own - full).abs().max())
+                    maxdiff.append(round(d, 5))
+                    psnr_full.append(round(cpx.image_psnr(full, ref), 4))
+                    if d > GUIDED_FALLBACK_MAX_DIFF:
+                        own = full
+                        fell_back.append(len(psnr) - 1)
+                psnr_march.append(round(cpx.image_psnr(own, ref), 4))
+            entry[vs] = {"psnr_db": round(float(np.mean(psnr)), 4), "psnr_per_view": psnr,
+                         "psnr_own_march_db": round(float(np.mean(psnr_march)), 4),
+                         "psnr_own_march_per_view": psnr_march,
+                         "psnr_full_march_db": round(float(np.mean(psnr_full)), 4) if psnr_full else None,
+                         "max_pixel_diff_guided_vs_full_per_view": maxdiff or None,
+                         "guided_views_falling_back_to_full_march": fell_back if prop is not None else None}
+        forms[form_key(rprec, rform, run, args)] = entry
         if prop is not None:
             prop.close()
         pool.close()
         scene.close()
         torch.cuda.empty_cache()
     base, rep = forms["fp32/plain"], forms.get("fp32/plain (repeat)")
-    other = forms[form_key(args.precision, args.form, 2, args)]
+    other = forms[form_key(prec, form, 2, args)]
+
+    def deltas(vs):
+        per = [round(a - b, 4) for a, b in zip(base[vs]["psnr_per_view"], other[vs]["psnr_per_view"])]
+        own = [round(a - b, 4) for a, b in zip(base[vs]["psnr_own_march_per_view"],
+                                               other[vs]["psnr_own_march_per_view"])]
+        return {"delta_psnr_db": round(base[vs]["psnr_db"] - other[vs]["psnr_db"], 4), "delta_per_view_db": per,
+                "delta_per_view_range_db": [min(per), max(per)],
+                "delta_own_march_db": round(base[vs]["psnr_own_march_db"] - other[vs]["psnr_own_march_db"], 4),
+                "delta_own_march_per_view_db": own,
+                "run_to_run_fp32_db": None if rep is None else round(base[vs]["psnr_db"] - rep[vs]["psnr_db"], 4),
+                "run_to_run_fp32_per_view_db": None if rep is None else
+                [round(a - b, 4) for a, b in zip(base[vs]["psnr_per_view"], rep[vs]["psnr_per_view"])]}
+
+    test, val = deltas("test"), deltas("validation")
     return {
-        "metric": "held-out view PSNR, plain FP32 minus %s/%s after %d batches" % (args.precision, args.form, N),
-        "value": round(base["psnr_db"] - other["psnr_db"], 4), "unit": "dB", "higher_is_better": False,
-        "delta_own_march_db": round(base["psnr_own_march_db"] - other["psnr_own_march_db"], 4),
-        "run_to_run_fp32_db": None if rep is None else round(base["psnr_db"] - rep["psnr_db"], 4),
+        "metric": "held-out view PSNR, plain FP32 minus %s/%s after %d batches" % (prec, form, N),
+        "value": test["delta_psnr_db"], "unit": "dB", "higher_is_better": False,
+        "test_views": test, "validation_views": val,
         "speedup_of_training": round(other["train_rays_per_s"] / base["train_rays_per_s"], 3),
-        "proposal_net": net if args.form == "proposal" else None,
-        "forms": forms, "held_out_views": len(held), "image": [img, img],
+        "plain_rays_per_s": base["train_rays_per_s"], "form_rays_per_s": other["train_rays_per_s"],
+        "proposal_net": net if form == "proposal" else None,
+        "guided_fallback_max_diff": GUIDED_FALLBACK_MAX_DIFF if form == "proposal" else None,
+        "forms": forms, "held_out_views": {k: len(v) for k, v in view_sets.items()}, "image": [img, img],
         "config": {"workload": args.workload, "batch_rays": R, "pool_rays": P, "iterations": N,
                    "step_constants": STEP, "lr_decay": "reference per batch (Render.cu:499-500)",
-                   "proposal_schedule": PROPOSAL if args.form == "proposal" else None},
-        "data": "synthetic: seeded %d-blob %d^3 hidden grid; held-out views on the upper hemisphere (another seed)"
-                % (wl["n_blobs"], wl["gt_n"]),
+                   "proposal_schedule": PROPOSAL if form == "proposal" else None},
+        "data": "synthetic: seeded %d-blob %d^3 hidden grid; held-out validation and test views on the upper "
+                "hemisphere (two other seeds)" % (wl["n_blobs"], wl["gt_n"]),
     }
+
+
+def proposal_leg(args, wl, local, n_batches):
+    """The metric's second half on the same workload: a whole training run of n_batches in the
+    mixed BF16 + learned-proposal form against the plain FP32 form, device-timed, and the
+    held-out PSNR difference on the test views."""
+    q = quality_run(args, wl, local, prec="bf16", form="proposal", n_batches=n_batches, repeat=False)
+    t = q["test_views"]
+    other = q["forms"][form_key("bf16", "proposal", 2, args)]
+    return {"form": "mixed BF16 + learned proposal", "batches": n_batches,
+            "value": q["form_rays_per_s"], "unit": UNIT, "plain_fp32_value": q["plain_rays_per_s"],
+            "ratio_vs_plain_fp32": q["speedup_of_training"],
+            "timing": "whole training run of both forms, CUDA events, proposal warm-up, label batches and "
+                      "training rounds included",
+            "delta_psnr_db": t["delta_psnr_db"], "delta_per_view_db": t["delta_per_view_db"],
+            "delta_per_view_range_db": t["delta_per_view_range_db"],
+            "delta_own_march_db": t["delta_own_march_db"],
+            "max_pixel_diff_guided_vs_full_per_view": other["test"]["max_pixel_diff_guided_vs_full_per_view"],
+            "guided_views_falling_back_to_full_march": other["test"]["guided_views_falling_back_to_full_march"],
+            "guided_fallback_max_diff": GUIDED_FALLBACK_MAX_DIFF,
+            "settings": q["proposal_net"], "settings_chosen_on": "validation views (another seed)",
+            "validation_delta_psnr_db": q["validation_views"]["delta_psnr_db"],
+            "proposal": other["proposal"]}
 
 
 def cpu_baseline(wl, scene, pool, R, args):
@@ -1032,8 +1123,13 @@ def main():
                     help="time the window after N untimed training batches with the reference's learning-rate "
                          "decay (a mid-run step; the proposal form otherwise times batches 110-130)")
     ap.add_argument("--no-repeat", action="store_true", help="quality run: skip the second plain FP32 run")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the mixed + proposal leg of the default line (forms.proposal)")
+    ap.add_argument("--forms-batches", type=int, default=2000,
+                    help="training batches of each form in the mixed + proposal leg")
     ap.add_argument("--march-options", type=int, default=0,
-                    help="cpx_grid_set_options flags of the compared form's grid (quality run)")
+                    help="cpx_grid_set_options flags of the training grid (quality run: of the compared form's "
+                         "grid)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
@@ -1084,6 +1180,17 @@ def main():
             result["cpu_baseline"] = cpu_baseline(wl, *state[:3], args)
         else:
             result["cpu_baseline"] = None
+        # the metric's second half: mixed + proposal against plain FP32 on the same workload
+        # (single GPU; the replicas of a multi-GPU run report the plain form only)
+        if world == 1 and not args.no_forms and args.form == "plain" and args.precision == "fp32" \
+                and not args.march_options and "sparse_threshold" not in wl:
+            for obj in state[:2]:
+                obj.close()
+            state = None
+            import torch
+
+            torch.cuda.empty_cache()
+            result["forms"] = {"proposal": proposal_leg(args, wl, local, args.forms_batches)}
         print(json.dumps(result), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -9,13 +9,16 @@ the printed values and writes both into the fixture.  It needs the reference
 tree, so it runs in the build container only; the fixture is committed.
 """
 import json
+import os
 import pathlib
 import re
 import subprocess
 import sys
 
 REPO = pathlib.Path(__file__).resolve().parents[2]
-REF_SRC = pathlib.Path("/root/reference/SparseVolumeRadianceField/VolumeFieldRender.cu")
+# the reference's source tree (SparseVolumeRadianceField/); CPX_REF_DIR overrides the default
+REF_DIR = pathlib.Path(os.environ.get("CPX_REF_DIR", "/root/reference/SparseVolumeRadianceField"))
+REF_SRC = REF_DIR / "VolumeFieldRender.cu"
 KAT_BIN = REPO / "oracle" / "_ref" / "ref_kat"
 OUT = REPO / "tests" / "golden" / "kat_test_render.json"
 
