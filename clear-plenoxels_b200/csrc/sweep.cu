@@ -68,25 +68,16 @@ __device__ __forceinline__ float tv6(float self, const float* nb, float lam)
     return __fdividef(lam * disp, sd + 1.e-6f);
 }
 
-// One 16-byte slot: optional TV term from six neighbour slots, then Adam; writes the slot.
-// touched_bit is shared with the mixed-form sweep (cpx_internal.cuh).
+// The arithmetic of one 16-byte slot: optional TV term from the six neighbour slots nbv (the
+// reference's order z-1, y-1, x-1, x+1, y+1, z+1), then Adam.  g, m, vv are updated in place
+// (g to zero where Adam ran); returns the new parameters.
 template <bool TV>
-__device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint32_t v, int j,
-                                           bool tv_on, const uint32_t* nb_slot, const bool* nb_self,
-                                           float inv_bc1, float inv_bc2, float lr_density)
+__device__ __forceinline__ float4 slot_update(const SweepArgs& a, int j, bool tv_on, const float4& p,
+                                              const float4* nbv, float4& g, float4& m, float4& vv, float inv_bc1,
+                                              float inv_bc2, float lr_density)
 {
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
-    const float4 p = a.p_in[sl];
-    // untouched vertices have zero gradients: their records are neither read nor written
-    const bool tch = touched_bit(a.touched, v);
-    if (a.clear && j == 0 && (v & 31u) == 0) a.clear[v >> 5] = 0u;
-    float4 g = tch ? a.grad[sl] : make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 m = a.m[sl];
-    float4 vv = a.v[sl];
     if (TV && tv_on) {
-        float4 nbv[6];
-#pragma unroll
-        for (int k = 0; k < 6; k++) nbv[k] = nb_self[k] ? p : a.p_in[nb_slot[k]];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const int e = 4 * j + c;
@@ -113,6 +104,29 @@ __device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint
         f4set(pn, c, np);
         f4set(g, c, 0.f);
     }
+    return pn;
+}
+
+// One 16-byte slot: optional TV term from six neighbour slots, then Adam; writes the slot.
+// touched_bit is shared with the mixed-form sweep (cpx_internal.cuh).
+template <bool TV>
+__device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint32_t v, int j,
+                                           bool tv_on, const uint32_t* nb_slot, const bool* nb_self,
+                                           float inv_bc1, float inv_bc2, float lr_density)
+{
+    const float4 p = a.p_in[sl];
+    // untouched vertices have zero gradients: their records are neither read nor written
+    const bool tch = touched_bit(a.touched, v);
+    if (a.clear && j == 0 && (v & 31u) == 0) a.clear[v >> 5] = 0u;
+    float4 g = tch ? a.grad[sl] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 m = a.m[sl];
+    float4 vv = a.v[sl];
+    float4 nbv[6];
+    if (TV && tv_on) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) nbv[k] = nb_self[k] ? p : a.p_in[nb_slot[k]];
+    }
+    const float4 pn = slot_update<TV>(a, j, tv_on, p, nbv, g, m, vv, inv_bc1, inv_bc2, lr_density);
     a.p_out[sl] = pn;
     a.m[sl] = m;
     a.v[sl] = vv;
@@ -166,6 +180,96 @@ __global__ void __launch_bounds__(256) k_sweep_dense(SweepArgs a)
     }
 }
 
+// Dense grid, TV on: the 2.5-D form.  A block owns a kZTX x kZTY tile of vertex columns and
+// walks a chunk of kZChunk planes in z.  A thread owns one 16-byte slot of one column and keeps
+// the column's z-1, z and z+1 slots in registers; the tile's current plane (with a one-vertex
+// halo in x and y, loaded by the edge threads) is staged in shared memory, where the x- and
+// y-neighbours are read.  Every parameter slot then leaves L2 once per block (plus the halo),
+// instead of once for itself and once for each neighbour that needs it.  The arithmetic is
+// slot_update's, so the results equal k_sweep_dense's bit for bit.
+constexpr int kZTX = 16, kZTY = 8, kZChunk = 32;
+static_assert(kZTX > 1 && kZTY > 1, "a column is at most one of left/right and of top/bottom");
+
+template <int S>
+__global__ void __launch_bounds__(kZTX * kZTY * S, 1) k_sweep_dense_z(SweepArgs a)
+{
+    __shared__ float s_bc[2];
+    __shared__ float4 plane[kZTY + 2][kZTX + 2][S];
+    bias_corrections(a.timestep, a.t_dev, s_bc);
+    const int t = threadIdx.x;
+    const int col = t / S;
+    const int j = t - col * S;
+    const int tx = col % kZTX, ty = col / kZTX;
+    const int x = blockIdx.x * kZTX + tx, y = blockIdx.y * kZTY + ty;
+    const int z0 = blockIdx.z * kZChunk;
+    const int z1 = z0 + kZChunk < a.D ? z0 + kZChunk : a.D;
+    const bool in = x < a.W && y < a.H;
+    const uint32_t W = (uint32_t)a.W, WH = W * (uint32_t)a.H;
+    const uint32_t cv = (uint32_t)y * W + (uint32_t)x;  // the column's vertex in a plane
+    const bool xy_interior = x >= 1 && x + 2 <= a.W && y >= 1 && y <= a.H - 2;
+    const bool left = in && tx == 0 && x >= 1;
+    const bool right = in && tx == kZTX - 1 && x + 1 < a.W;
+    const bool top = in && ty == 0 && y >= 1;
+    const bool bottom = in && ty == kZTY - 1 && y + 1 < a.H;
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 p_prev = zero, p_cur = zero;
+    if (in) {
+        if (z0 >= 1) p_prev = a.p_in[((uint32_t)(z0 - 1) * WH + cv) * S + j];
+        p_cur = a.p_in[((uint32_t)z0 * WH + cv) * S + j];
+    }
+    for (int z = z0; z < z1; z++) {
+        const uint32_t v = (uint32_t)z * WH + cv;
+        const uint32_t sl = v * S + j;
+        // every load of this plane first: the next plane's slot, the halo, the optimizer state
+        // (a column is at most one of left/right and one of top/bottom: the tile is wider and
+        // taller than one vertex)
+        float4 p_next = zero, hx = zero, hy = zero;
+        float4 g = zero, m = zero, vv = zero;
+        bool tch = false;
+        float lr = a.lr;
+        if (in) {
+            if (z + 1 < a.D) p_next = a.p_in[sl + WH * S];
+            if (left) hx = a.p_in[sl - S];
+            else if (right) hx = a.p_in[sl + S];
+            if (top) hy = a.p_in[sl - W * S];
+            else if (bottom) hy = a.p_in[sl + W * S];
+            tch = touched_bit(a.touched, v);
+            if (tch) g = a.grad[sl];
+            m = a.m[sl];
+            vv = a.v[sl];
+            if (a.adaptive_lr) lr = a.lr * a.adaptive_lr[v];
+        }
+        plane[ty + 1][tx + 1][j] = p_cur;
+        if (left) plane[ty + 1][0][j] = hx;
+        else if (right) plane[ty + 1][kZTX + 1][j] = hx;
+        if (top) plane[0][tx + 1][j] = hy;
+        else if (bottom) plane[kZTY + 1][tx + 1][j] = hy;
+        __syncthreads();
+        if (in) {
+            if (a.clear && j == 0 && (v & 31u) == 0) a.clear[v >> 5] = 0u;
+            const bool tv_on = xy_interior && z >= 1 && z <= a.D - 2;
+            float4 nbv[6];
+            if (tv_on) {
+                nbv[0] = p_prev;
+                nbv[1] = plane[ty][tx + 1][j];
+                nbv[2] = plane[ty + 1][tx][j];
+                nbv[3] = plane[ty + 1][tx + 2][j];
+                nbv[4] = plane[ty + 2][tx + 1][j];
+                nbv[5] = p_next;
+            }
+            const float4 pn = slot_update<true>(a, j, tv_on, p_cur, nbv, g, m, vv, s_bc[0], s_bc[1], lr);
+            a.p_out[sl] = pn;
+            a.m[sl] = m;
+            a.v[sl] = vv;
+            if (tch) a.grad[sl] = g;
+            if (j == 0) a.density_out[v] = pn.x;
+        }
+        __syncthreads();
+        p_prev = p_cur;
+        p_cur = p_next;
+    }
+}
+
 // Sparse grid: blocks tile the compact slots; positions from the compact->dense table.
 template <int S, bool TV>
 __global__ void __launch_bounds__(256) k_sweep_sparse(SweepArgs a)
@@ -209,10 +313,15 @@ static void launch_sweep(const cpx_grid* g, const SweepArgs& a, bool tv, cudaStr
 {
     if (!g->sparse) {
         const unsigned rows = (unsigned)((int64_t)g->H * g->D);
-        if (tv)
+        if (tv && S == 7 && !(g->options & CPX_OPT_ROW_SWEEP) && !g->sparse) {
+            const dim3 grid((unsigned)((g->W + kZTX - 1) / kZTX), (unsigned)((g->H + kZTY - 1) / kZTY),
+                            (unsigned)((g->D + kZChunk - 1) / kZChunk));
+            k_sweep_dense_z<S><<<grid, kZTX * kZTY * S, 0, st>>>(a);
+        } else if (tv) {
             k_sweep_dense<S, true><<<rows, 256, 0, st>>>(a);
-        else
+        } else {
             k_sweep_dense<S, false><<<rows, 256, 0, st>>>(a);
+        }
     } else {
         const unsigned blocks = (unsigned)(((int64_t)g->n_act + 255) / 256);  // a warp per 32 vertices
         if (tv)

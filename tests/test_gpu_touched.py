@@ -74,3 +74,40 @@ def test_standalone_tv_marks_every_vertex(cuda):
     assert g.any()
     cpx.Optimizer.updateRGBScene(scene, 0.1, 0.01, 1)
     assert not scene.download_grads().any()
+
+
+@pytest.mark.parametrize("dims", [(37, 45, 70), (16, 8, 33), (64, 64, 64)])
+def test_plane_window_sweep_equals_row_sweep(cuda, dims):
+    """The FP32 dense sweep that walks z with a tile's x-y plane on chip and the sweep that runs a
+    block per row give the same parameters, moments and gradients bit for bit, two steps in a
+    row, on grids whose sides are not multiples of the 16 x 8 tile or of the 32-plane z chunk,
+    with an adaptive learning rate.  (Sweeps that read gradients through the touched maps equal
+    sweeps that read every record: test_touched_maps_equal_full_sweeps.)"""
+    import cpx
+    import cpx_scenes as S
+
+    W, H, D = dims
+    rng = np.random.default_rng(W * 131 + D)
+    params = S.make_params(rng.uniform(0.0, 30.0, W * H * D).astype(np.float32), 9, rng, 0.3)
+    grads = [rng.normal(0, 1e-2, params.shape).astype(np.float32) for _ in range(2)]
+    m0 = rng.normal(0, 1e-3, params.shape).astype(np.float32)
+    v0 = rng.uniform(0, 1e-4, params.shape).astype(np.float32)
+    alr = (rng.random(W * H * D) > 0.2).astype(np.float32)
+    outs = []
+    for opt in (0, cpx.OPT_ROW_SWEEP):
+        sc = cpx.ObjectScene(W, H, D, 9)
+        sc.set_options(opt)
+        sc.upload_params(params)
+        sc.set_adaptive_lr(alr)
+        sc.upload_moments(m0, v0)
+        res = []
+        for t, g in enumerate(grads):
+            sc.upload_grads(g)
+            cpx.Optimizer.varianceAndUpdate(sc, 1e-3, 2e-3, 0.3, 1.0, 4 + t)
+            res += [sc.download_params(), *sc.download_moments(), sc.download_grads()]
+        sc.check()
+        outs.append(res)
+        sc.close()
+    assert not np.array_equal(outs[0][0], params)
+    for a, b in zip(*outs):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
