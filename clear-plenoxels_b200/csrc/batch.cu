@@ -98,6 +98,11 @@ struct cpx_batch {
     double* d_mse = nullptr;
     BatchScene* etab = nullptr;    // scene table of eager steps
     BatchScene* gtab[2] = {nullptr, nullptr};  // scene tables of the two graphs
+    // the FP32 dense grids' sweeps run as one launch over a device table of their arguments:
+    // the eager steps' table and the two graphs' tables
+    void* stab_eager = nullptr;
+    void* stab[2] = {nullptr, nullptr};
+    std::vector<unsigned char> stab_host;
     int iteration = 0;             // host mirror of *iter
     // graphs
     cudaStream_t cap = nullptr;
@@ -126,7 +131,30 @@ static void batch_free(cpx_batch* b)
     cudaFree(b->d_len);
     cudaFree(b->d_mse);
     cudaFree(b->etab);
+    cudaFree(b->stab_eager);
+    cudaFree(b->stab[0]);
+    cudaFree(b->stab[1]);
     delete b;
+}
+
+// The grids whose sweeps run in the one batched launch, in batch order.
+static std::vector<cpx_grid*> batch_sweep_grids(const cpx_batch* b)
+{
+    std::vector<cpx_grid*> out;
+    for (cpx_grid* g : b->grids)
+        if (sweep_batchable(g, b->fuse)) out.push_back(g);
+    return out;
+}
+
+// The host image of the batched sweep's table for the grids' current buffers; returns its
+// work items (0: no grid qualifies).
+static int batch_sweep_table(cpx_batch* b, const std::vector<cpx_grid*>& sg)
+{
+    if (sg.empty()) return 0;
+    b->stab_host.resize(sweep_table_bytes((int)sg.size()));
+    const cpx_step_args& g = b->args;
+    return sweep_table_fill(sg.data(), (int)sg.size(), g.lam_density, g.lam_sh, g.lr, g.sh_lr, b->iter,
+                            b->stab_host.data());
 }
 
 static std::vector<BatchScene> batch_table(const cpx_batch* b)
@@ -150,8 +178,10 @@ static bool valid_tuning(const BatchTuning& t)
            (t.shade_warps == 2 || t.shade_warps == 4 || t.shade_warps == 8) && t.grab >= 1 && t.grab <= 8;
 }
 
-// Enqueue one iteration on st with the scene table at tab (already on the device).
-static cpx_status batch_enqueue(cpx_batch* b, const BatchScene* tab, const BatchTuning& tn, cudaStream_t st)
+// Enqueue one iteration on st with the scene table at tab and the batched sweep's table at stab
+// (items work items; both already on the device).
+static cpx_status batch_enqueue(cpx_batch* b, const BatchScene* tab, const void* stab, int items,
+                                const BatchTuning& tn, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(b->queue, 0, 2 * sizeof(int), st);
     if (e != cudaSuccess) return cuda_status(e, "batch queue");
@@ -174,14 +204,21 @@ static cpx_status batch_enqueue(cpx_batch* b, const BatchScene* tab, const Batch
     if (s != CPX_OK) return s;
     int launches = 2;
     const cpx_step_args& g = b->args;
+    const std::vector<cpx_grid*> sg = batch_sweep_grids(b);
     for (int i = 0; i < b->n; i++) {
         cpx_grid* gr = b->grids[i];
+        if (sweep_batchable(gr, b->fuse)) continue;  // in the batched sweep below
         if (g.do_tv && !b->fuse) {
             s = tv_launch(gr, g.lam_density, g.lam_sh, g.tv_type, g.tv_neighbours, st);
             if (s != CPX_OK) return s;
             launches++;
         }
         s = sweep_adam(gr, b->fuse, g.lam_density, g.lam_sh, g.lr, g.sh_lr, 1, st, b->iter);
+        if (s != CPX_OK) return s;
+        launches++;
+    }
+    if (!sg.empty()) {
+        s = sweep_batched_launch(sg.data(), (int)sg.size(), stab, items, st);
         if (s != CPX_OK) return s;
         launches++;
     }
@@ -195,10 +232,16 @@ static cpx_status batch_enqueue(cpx_batch* b, const BatchScene* tab, const Batch
 static cpx_status batch_eager(cpx_batch* b, cudaStream_t st)
 {
     const std::vector<BatchScene> t = batch_table(b);
-    // the table is copied from pageable memory: the call returns once the source is read
+    // the tables are copied from pageable memory: the call returns once the source is read
     cudaError_t e = cudaMemcpyAsync(b->etab, t.data(), sizeof(BatchScene) * b->n, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_status(e, "batch table");
-    return batch_enqueue(b, b->etab, b->tuning, st);
+    const std::vector<cpx_grid*> sg = batch_sweep_grids(b);
+    const int items = batch_sweep_table(b, sg);
+    if (items > 0) {
+        e = cudaMemcpyAsync(b->stab_eager, b->stab_host.data(), b->stab_host.size(), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_status(e, "batch sweep table");
+    }
+    return batch_enqueue(b, b->etab, b->stab_eager, items, b->tuning, st);
 }
 
 // Capture the iteration of the grids' current parity into graph p.  The capture runs the
@@ -212,6 +255,12 @@ static cpx_status batch_capture(cpx_batch* b, int p)
     const std::vector<BatchScene> t = batch_table(b);
     cudaError_t e = cudaMemcpy(b->gtab[p], t.data(), sizeof(BatchScene) * b->n, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_status(e, "batch table");
+    const std::vector<cpx_grid*> sg = batch_sweep_grids(b);
+    const int items = batch_sweep_table(b, sg);
+    if (items > 0) {
+        e = cudaMemcpy(b->stab[p], b->stab_host.data(), b->stab_host.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_status(e, "batch sweep table");
+    }
     b->sig[p] = batch_sig(b);
     std::vector<int> cur(b->n), tcur(b->n), all(b->n);
     for (int i = 0; i < b->n; i++) {
@@ -221,7 +270,7 @@ static cpx_status batch_capture(cpx_batch* b, int p)
     }
     e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_status(e, "batch capture");
-    cpx_status s = batch_enqueue(b, b->gtab[p], b->tuning, b->cap);
+    cpx_status s = batch_enqueue(b, b->gtab[p], b->stab[p], items, b->tuning, b->cap);
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(b->cap, &graph);
     for (int i = 0; i < b->n; i++) {  // nothing ran: the grids keep their buffers
@@ -380,6 +429,9 @@ cpx_status cpx_batch_create(const cpx_batch_scene* scenes, int n_scenes, const c
     grab((void**)&b->etab, sizeof(BatchScene) * n_scenes);
     grab((void**)&b->gtab[0], sizeof(BatchScene) * n_scenes);
     grab((void**)&b->gtab[1], sizeof(BatchScene) * n_scenes);
+    grab(&b->stab_eager, sweep_table_bytes(n_scenes));
+    grab(&b->stab[0], sweep_table_bytes(n_scenes));
+    grab(&b->stab[1], sweep_table_bytes(n_scenes));
     if (e != cudaSuccess) {
         cudaGetLastError();
         batch_free(b);

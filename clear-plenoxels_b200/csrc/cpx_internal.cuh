@@ -388,6 +388,15 @@ cpx_status proposal_train(cpx_proposal* p, const cpx_grid* g, cpx_rays* r, const
                           const float* seg_w, int steps, int rays_per_step, bool adam, cudaStream_t st);
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
                       double sh_lr, int timestep, cudaStream_t s, const int* t_dev = nullptr);
+// The batched form's FP32 sweeps in one launch (sweep.cu): grids that qualify (dense FP32, SH
+// band 2, fused TV), a device table of sweep_table_bytes(n) filled from the host image that
+// sweep_table_fill writes (it returns the launch's work items), then the launch, which flips
+// the grids' buffers as sweep_adam does.
+bool sweep_batchable(const cpx_grid* g, bool fused_tv);
+size_t sweep_table_bytes(int n);
+int sweep_table_fill(cpx_grid* const* grids, int n, double lam_d, double lam_sh, double lr, double sh_lr,
+                     const int* t_dev, void* host_image);
+cpx_status sweep_batched_launch(cpx_grid* const* grids, int n, const void* dev_table, int items, cudaStream_t st);
 // Once per process, before any graph capture (grid creation of a mixed form calls it): the
 // shared-memory opt-in of the mixed forms' pipelined dense sweep.
 cpx_status lowp_prepare();

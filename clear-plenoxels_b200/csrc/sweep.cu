@@ -191,17 +191,22 @@ constexpr int kZTX = 16, kZTY = 8, kZChunk = 32;
 static_assert(kZTX > 1 && kZTY > 1, "a column is at most one of left/right and of top/bottom");
 
 template <int S>
-__global__ void __launch_bounds__(kZTX * kZTY * S, 1) k_sweep_dense_z(SweepArgs a)
+struct ZPlane {
+    float4 v[kZTY + 2][kZTX + 2][S];
+};
+
+// One block's work: tile (bx, by), chunk bz of grid a; s_bc holds a's bias corrections.
+template <int S>
+__device__ __forceinline__ void sweep_dense_z_tile(const SweepArgs& a, int bx, int by, int bz, const float* s_bc,
+                                                   ZPlane<S>& pl)
 {
-    __shared__ float s_bc[2];
-    __shared__ float4 plane[kZTY + 2][kZTX + 2][S];
-    bias_corrections(a.timestep, a.t_dev, s_bc);
+    auto& plane = pl.v;
     const int t = threadIdx.x;
     const int col = t / S;
     const int j = t - col * S;
     const int tx = col % kZTX, ty = col / kZTX;
-    const int x = blockIdx.x * kZTX + tx, y = blockIdx.y * kZTY + ty;
-    const int z0 = blockIdx.z * kZChunk;
+    const int x = bx * kZTX + tx, y = by * kZTY + ty;
+    const int z0 = bz * kZChunk;
     const int z1 = z0 + kZChunk < a.D ? z0 + kZChunk : a.D;
     const bool in = x < a.W && y < a.H;
     const uint32_t W = (uint32_t)a.W, WH = W * (uint32_t)a.H;
@@ -270,6 +275,59 @@ __global__ void __launch_bounds__(kZTX * kZTY * S, 1) k_sweep_dense_z(SweepArgs 
     }
 }
 
+template <int S>
+__global__ void __launch_bounds__(kZTX * kZTY * S, 1) k_sweep_dense_z(SweepArgs a)
+{
+    __shared__ float s_bc[2];
+    __shared__ ZPlane<S> plane;
+    bias_corrections(a.timestep, a.t_dev, s_bc);
+    sweep_dense_z_tile<S>(a, blockIdx.x, blockIdx.y, blockIdx.z, s_bc, plane);
+}
+
+// Tiles of a dense grid for k_sweep_dense_z: (x tiles, y tiles, z chunks).
+__host__ __device__ __forceinline__ dim3 z_tiles(int W, int H, int D)
+{
+    return dim3((unsigned)((W + kZTX - 1) / kZTX), (unsigned)((H + kZTY - 1) / kZTY),
+                (unsigned)((D + kZChunk - 1) / kZChunk));
+}
+
+// The sweeps of many dense FP32 grids (the batched form) in one launch: block b takes work item
+// b of the concatenated tile lists, its grid found by binary search over the first items.
+struct SweepBatch {
+    const SweepArgs* args;  // [n]
+    const int* first;       // [n + 1]: first work item of each grid, then the total
+    int n;
+};
+
+template <int S>
+__global__ void __launch_bounds__(kZTX * kZTY * S, 1) k_sweep_dense_z_batched(SweepBatch sb)
+{
+    __shared__ float s_bc[2];
+    __shared__ ZPlane<S> plane;
+    __shared__ SweepArgs s_args;
+    __shared__ int s_local;
+    const int item = blockIdx.x;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = sb.n - 1;  // the last grid whose first item is <= item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sb.first[mid] <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        s_args = sb.args[lo];
+        s_local = item - sb.first[lo];
+    }
+    __syncthreads();
+    const SweepArgs& a = s_args;
+    bias_corrections(a.timestep, a.t_dev, s_bc);
+    const dim3 tiles = z_tiles(a.W, a.H, a.D);
+    const int local = s_local;
+    const int bx = local % (int)tiles.x;
+    const int by = (local / (int)tiles.x) % (int)tiles.y;
+    const int bz = local / (int)(tiles.x * tiles.y);
+    sweep_dense_z_tile<S>(a, bx, by, bz, s_bc, plane);
+}
+
 // Sparse grid: blocks tile the compact slots; positions from the compact->dense table.
 template <int S, bool TV>
 __global__ void __launch_bounds__(256) k_sweep_sparse(SweepArgs a)
@@ -314,9 +372,7 @@ static void launch_sweep(const cpx_grid* g, const SweepArgs& a, bool tv, cudaStr
     if (!g->sparse) {
         const unsigned rows = (unsigned)((int64_t)g->H * g->D);
         if (tv && S == 7 && !(g->options & CPX_OPT_ROW_SWEEP) && !g->sparse) {
-            const dim3 grid((unsigned)((g->W + kZTX - 1) / kZTX), (unsigned)((g->H + kZTY - 1) / kZTY),
-                            (unsigned)((g->D + kZChunk - 1) / kZChunk));
-            k_sweep_dense_z<S><<<grid, kZTX * kZTY * S, 0, st>>>(a);
+            k_sweep_dense_z<S><<<z_tiles(g->W, g->H, g->D), kZTX * kZTY * S, 0, st>>>(a);
         } else if (tv) {
             k_sweep_dense<S, true><<<rows, 256, 0, st>>>(a);
         } else {
@@ -353,6 +409,9 @@ static void element_masks(const cpx_grid* g, uint32_t* tv_mask, uint32_t* adam_m
     *adam_mask = am;
 }
 
+static SweepArgs sweep_args(const cpx_grid* g, double lam_d, double lam_sh, double lr, double sh_lr, int timestep,
+                            const int* t_dev);
+
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
                       double sh_lr, int timestep, cudaStream_t st, const int* t_dev)
 {
@@ -368,6 +427,27 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
         set_error("grid too large for 32-bit slot indices");
         return CPX_ERR_UNSUPPORTED;
     }
+    const SweepArgs a = sweep_args(g, lam_d, lam_sh, lr, sh_lr, timestep, t_dev);
+    switch (S) {
+    case 1: launch_sweep<1>(g, a, fused_tv, st); break;
+    case 4: launch_sweep<4>(g, a, fused_tv, st); break;
+    case 7: launch_sweep<7>(g, a, fused_tv, st); break;
+    default:
+        set_error("record of %d slots unsupported", S);
+        return CPX_ERR_UNSUPPORTED;
+    }
+    count_launch();
+    g->cur ^= 1;
+    g->tcur ^= 1;
+    g->all_touched = 0;
+    cpx_status rc = cuda_status(cudaGetLastError(), "adam sweep");
+    return rc == CPX_OK ? refresh_dense_skip(g, st) : rc;
+}
+
+// The arguments of a grid's FP32 sweep in its current state.
+static SweepArgs sweep_args(const cpx_grid* g, double lam_d, double lam_sh, double lr, double sh_lr, int timestep,
+                            const int* t_dev)
+{
     SweepArgs a;
     a.W = g->W;
     a.H = g->H;
@@ -393,20 +473,51 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
     a.sh_lr = (float)sh_lr;
     a.timestep = timestep;
     a.t_dev = t_dev;
-    switch (S) {
-    case 1: launch_sweep<1>(g, a, fused_tv, st); break;
-    case 4: launch_sweep<4>(g, a, fused_tv, st); break;
-    case 7: launch_sweep<7>(g, a, fused_tv, st); break;
-    default:
-        set_error("record of %d slots unsupported", S);
-        return CPX_ERR_UNSUPPORTED;
+    return a;
+}
+
+bool sweep_batchable(const cpx_grid* g, bool fused_tv)
+{
+    return fused_tv && g->prec == kPrecFP32 && !g->sparse && g->rec == 28 && !(g->options & CPX_OPT_ROW_SWEEP) &&
+           g->n_act > 0 && g->n_act * 7 < ((int64_t)1 << 32);
+}
+
+size_t sweep_table_bytes(int n) { return (size_t)n * sizeof(SweepArgs) + ((size_t)n + 1) * sizeof(int); }
+
+int sweep_table_fill(cpx_grid* const* grids, int n, double lam_d, double lam_sh, double lr, double sh_lr,
+                     const int* t_dev, void* host_image)
+{
+    SweepArgs* args = static_cast<SweepArgs*>(host_image);
+    int* first = reinterpret_cast<int*>(args + n);
+    int items = 0;
+    for (int i = 0; i < n; i++) {
+        args[i] = sweep_args(grids[i], lam_d, lam_sh, lr, sh_lr, 1, t_dev);
+        const dim3 t = z_tiles(grids[i]->W, grids[i]->H, grids[i]->D);
+        first[i] = items;
+        items += (int)(t.x * t.y * t.z);
     }
+    first[n] = items;
+    return items;
+}
+
+cpx_status sweep_batched_launch(cpx_grid* const* grids, int n, const void* dev_table, int items, cudaStream_t st)
+{
+    if (n == 0) return CPX_OK;
+    SweepBatch sb;
+    sb.args = static_cast<const SweepArgs*>(dev_table);
+    sb.first = reinterpret_cast<const int*>(sb.args + n);
+    sb.n = n;
+    k_sweep_dense_z_batched<7><<<(unsigned)items, kZTX * kZTY * 7, 0, st>>>(sb);
     count_launch();
-    g->cur ^= 1;
-    g->tcur ^= 1;
-    g->all_touched = 0;
-    cpx_status rc = cuda_status(cudaGetLastError(), "adam sweep");
-    return rc == CPX_OK ? refresh_dense_skip(g, st) : rc;
+    for (int i = 0; i < n; i++) {
+        cpx_grid* g = grids[i];
+        g->cur ^= 1;
+        g->tcur ^= 1;
+        g->all_touched = 0;
+        cpx_status rc = refresh_dense_skip(g, st);
+        if (rc != CPX_OK) return rc;
+    }
+    return cuda_status(cudaGetLastError(), "batched sweep");
 }
 
 // ---------------------------------------------------------------------------
