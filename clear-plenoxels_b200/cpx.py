@@ -211,7 +211,7 @@ class BatchScene(C.Structure):
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("place_block", C.c_int), ("shade_warps", C.c_int), ("grab", C.c_int)]
+    _fields_ = [("place_block", C.c_int), ("shade_warps", C.c_int), ("grab", C.c_int), ("samples_per_step", C.c_int)]
 
 
 _sig("cpx_ray_source_create", [C.c_void_p, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int,
@@ -1074,18 +1074,21 @@ class Batch:
     def tuning(self) -> dict:
         t = BatchTuning()
         _check(_lib.cpx_batch_get_tuning(self._h, C.byref(t)), "cpx_batch_get_tuning")
-        return {"place_block": t.place_block, "shade_warps": t.shade_warps, "grab": t.grab}
+        return {"place_block": t.place_block, "shade_warps": t.shade_warps, "grab": t.grab,
+                "samples_per_step": t.samples_per_step}
 
-    def set_tuning(self, place_block: int, shade_warps: int, grab: int):
+    def set_tuning(self, place_block: int, shade_warps: int, grab: int, samples_per_step: int = 1):
         t = BatchTuning()
         t.place_block, t.shade_warps, t.grab = int(place_block), int(shade_warps), int(grab)
+        t.samples_per_step = int(samples_per_step)
         _check(_lib.cpx_batch_set_tuning(self._h, C.byref(t)), "cpx_batch_set_tuning")
 
     def autotune(self, steps_per_trial: int = 3, stream=None) -> dict:
         t = BatchTuning()
         _check(_lib.cpx_batch_autotune(self._h, int(steps_per_trial), C.byref(t), _stream(stream)),
                "cpx_batch_autotune")
-        return {"place_block": t.place_block, "shade_warps": t.shade_warps, "grab": t.grab}
+        return {"place_block": t.place_block, "shade_warps": t.shade_warps, "grab": t.grab,
+                "samples_per_step": t.samples_per_step}
 
 
 def image_mse(a, b, stream=None) -> float:

@@ -175,7 +175,8 @@ static std::vector<SceneSig> batch_sig(const cpx_batch* b)
 static bool valid_tuning(const BatchTuning& t)
 {
     return t.place_block >= 32 && t.place_block <= 512 && t.place_block % 32 == 0 &&
-           (t.shade_warps == 2 || t.shade_warps == 4 || t.shade_warps == 8) && t.grab >= 1 && t.grab <= 8;
+           (t.shade_warps == 2 || t.shade_warps == 4 || t.shade_warps == 8) && t.grab >= 1 && t.grab <= 8 &&
+           (t.spl == 1 || t.spl == 2 || t.spl == 4) && t.shade_warps * t.spl <= 8;
 }
 
 // Enqueue one iteration on st with the scene table at tab and the batched sweep's table at stab
@@ -322,7 +323,8 @@ static cpx_status batch_step(cpx_batch* b, bool graphs, cudaStream_t st)
     int p = -1;
     for (int q = 0; q < 2; q++)
         if (b->graph[q] && b->sig[q] == now && b->graph_tuning[q].place_block == b->tuning.place_block &&
-            b->graph_tuning[q].shade_warps == b->tuning.shade_warps && b->graph_tuning[q].grab == b->tuning.grab)
+            b->graph_tuning[q].shade_warps == b->tuning.shade_warps && b->graph_tuning[q].grab == b->tuning.grab &&
+            b->graph_tuning[q].spl == b->tuning.spl)
             p = q;
     if (p < 0) {
         // capture this parity into a free slot; with none free both graphs are stale (a grid
@@ -526,8 +528,10 @@ cpx_status cpx_batch_set_tuning(cpx_batch* b, const cpx_batch_tuning* t)
     n.place_block = t->place_block;
     n.shade_warps = t->shade_warps;
     n.grab = t->grab;
+    n.spl = t->samples_per_step;
     if (!valid_tuning(n)) {
-        set_error("tuning outside place_block 32..512 (multiple of 32), shade_warps 2/4/8, grab 1..8");
+        set_error("tuning outside place_block 32..512 (multiple of 32), shade_warps 2/4/8, grab 1..8, "
+                  "samples_per_step 1/2/4 with shade_warps * samples_per_step <= 8");
         return CPX_ERR_INVALID_ARGUMENT;
     }
     b->tuning = n;
@@ -543,6 +547,7 @@ cpx_status cpx_batch_get_tuning(const cpx_batch* b, cpx_batch_tuning* t)
     t->place_block = b->tuning.place_block;
     t->shade_warps = b->tuning.shade_warps;
     t->grab = b->tuning.grab;
+    t->samples_per_step = b->tuning.spl;
     return CPX_OK;
 }
 
@@ -575,18 +580,20 @@ cpx_status cpx_batch_autotune(cpx_batch* b, int steps_per_trial, cpx_batch_tunin
     const int places[] = {64, 128, 256, 512};
     const int warps[] = {2, 4, 8};
     const int grabs[] = {1, 2, 4, 8};
+    const int spls[] = {1, 2, 4};
     BatchTuning cur = b->tuning;
     float best_ms = 0.f;
     cpx_status s = trial(cur, &best_ms);
     for (int round = 0; round < 2 && s == CPX_OK; round++) {
-        for (int dim = 0; dim < 3 && s == CPX_OK; dim++) {
-            const int* vals = dim == 0 ? places : dim == 1 ? warps : grabs;
-            const int nv = dim == 1 ? 3 : 4;
+        for (int dim = 0; dim < 4 && s == CPX_OK; dim++) {
+            const int* vals = dim == 0 ? places : dim == 1 ? warps : dim == 2 ? grabs : spls;
+            const int nv = dim == 1 || dim == 3 ? 3 : 4;
             for (int k = 0; k < nv && s == CPX_OK; k++) {
                 BatchTuning t = cur;
-                int& field = dim == 0 ? t.place_block : dim == 1 ? t.shade_warps : t.grab;
+                int& field = dim == 0 ? t.place_block : dim == 1 ? t.shade_warps : dim == 2 ? t.grab : t.spl;
                 if (field == vals[k]) continue;
                 field = vals[k];
+                if (!valid_tuning(t)) continue;  // tables of shade_warps * samples_per_step > 8 warps
                 float ms = 0.f;
                 s = trial(t, &ms);
                 if (s == CPX_OK && ms < best_ms) {
@@ -604,6 +611,7 @@ cpx_status cpx_batch_autotune(cpx_batch* b, int steps_per_trial, cpx_batch_tunin
         best->place_block = cur.place_block;
         best->shade_warps = cur.shade_warps;
         best->grab = cur.grab;
+        best->samples_per_step = cur.spl;
     }
     return CPX_OK;
 }

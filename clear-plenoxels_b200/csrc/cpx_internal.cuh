@@ -360,6 +360,7 @@ struct BatchTuning {
     int place_block = 64;  // threads per block of the placement launch
     int shade_warps = 4;   // warps per block of the shading launch
     int grab = 1;          // rays per warp per work-counter access in shading
+    int spl = 1;           // samples a shading lane takes per chunk (shade_warps * spl <= 8)
 };
 
 cpx_status batch_launch_march(int prec, const BatchArgs& a, const BatchTuning& tn, cudaStream_t st);

@@ -471,28 +471,42 @@ constexpr int kHashSlots = 256;
 constexpr uint32_t kEmpty = 0xffffffffu;
 
 struct WarpTable {
-    uint32_t* keys;  // [kHashSlots]
-    float* va;       // [kHashSlots] x4
+    uint32_t* keys;  // [n]
+    float* va;       // [n] x4
     float* vb0;
     float* vb1;
     float* vb2;
+    int n = kHashSlots;       // slots: kHashSlots per sample a lane takes per chunk (a power of 2)
+    uint32_t shift = 24;      // 32 - log2(n): the hash's top bits index the table
 };
 
 __device__ __forceinline__ int table_slot(const WarpTable& t, uint32_t key)
 {
-    uint32_t h = (key * 0x9E3779B1u) >> 24;  // 8 bits
-    for (int probe = 0; probe < kHashSlots; probe++) {
+    uint32_t h = (key * 0x9E3779B1u) >> t.shift;
+    for (int probe = 0; probe < t.n; probe++) {
         const uint32_t old = atomicCAS(&t.keys[h], kEmpty, key);
         if (old == kEmpty || old == key) return (int)h;
-        h = (h + 1) & (kHashSlots - 1);
+        h = (h + 1) & (uint32_t)(t.n - 1);
     }
-    return -1;  // unreachable: a chunk references at most 256 vertices
+    return -1;  // unreachable: a chunk references at most 8 vertices per sample
+}
+
+// The slot of a key already in the table (read-only probe).
+__device__ __forceinline__ int table_find(const WarpTable& t, uint32_t key)
+{
+    uint32_t h = (key * 0x9E3779B1u) >> t.shift;
+    for (int probe = 0; probe < t.n; probe++) {
+        const uint32_t k = t.keys[h];
+        if (k == key) return (int)h;
+        h = (h + 1) & (uint32_t)(t.n - 1);
+    }
+    return 0;  // unreachable: every key looked up was inserted
 }
 
 __device__ __forceinline__ void table_clear(const WarpTable& t, int lane)
 {
     __syncwarp();
-    for (int s = lane; s < kHashSlots; s += 32) {
+    for (int s = lane; s < t.n; s += 32) {
         if (t.keys[s] == kEmpty) continue;
         t.keys[s] = kEmpty;
         t.va[s] = 0.f;
@@ -511,7 +525,7 @@ __device__ __forceinline__ void table_colours(const WarpTable& t, const GridView
 {
     using RS = RecShape<NSH>;
     __syncwarp();
-    for (int s = lane; s < kHashSlots; s += 32) {
+    for (int s = lane; s < t.n; s += 32) {
         const uint32_t key = t.keys[s];
         if (key == kEmpty) continue;
         float col[3] = {0.f, 0.f, 0.f};
@@ -563,7 +577,7 @@ __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& 
 {
     using RS = RecShape<NSH>;
     __syncwarp();
-    for (int s = lane; s < kHashSlots; s += 32) {
+    for (int s = lane; s < t.n; s += 32) {
         const uint32_t key = t.keys[s];
         if (key == kEmpty) continue;
         const float va = t.va[s];
@@ -602,7 +616,10 @@ __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& 
 // Shade one ray with a whole warp: forward colour (lane per sample, warp reduction), then
 // the backward of renderRays_withGradients_RGBGPU (RenderUtils.cu:2145-2256) with warp prefix
 // scans for the running weight/colour sums and the merged gradient scatter.
-template <int NSH, int MODE, int PREC>
+// SPL: samples a lane takes per chunk.  A chunk of 32 * SPL consecutive samples shares one
+// table (of kHashSlots * SPL slots), so its distinct vertices are gathered and scattered once;
+// the scans still run over 32 samples at a time, in sample order.
+template <int NSH, int MODE, int PREC, int SPL = 1>
 __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
                                           int cnt, const SampleRec* samples, float4* colours,
                                           int maxs, const double* acc_in, double* losses,
@@ -618,33 +635,45 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
 
     // ---- forward colour ----
     double s0 = 0., s1 = 0., s2 = 0.;
-    for (int base = 0; base < n; base += 32) {
-        const int i = base + lane;
-        const bool valid = i < n;
+    for (int base = 0; base < n; base += 32 * SPL) {
         SampleRec s;
         Corners cr;
         int slot[8];
-        if (valid) {
-            s = S[i];
-            sample_corners(g, s, cr);
 #pragma unroll
-            for (int q = 0; q < 8; q++) slot[q] = table_slot(tab, cr.idx[q]);
+        for (int k = 0; k < SPL; k++) {
+            const int i = base + 32 * k + lane;
+            if (i < n) {
+                s = S[i];
+                sample_corners(g, s, cr);
+#pragma unroll
+                for (int q = 0; q < 8; q++) slot[q] = table_slot(tab, cr.idx[q]);
+            }
         }
         table_colours<NSH, PREC>(tab, g, shs, lane);
-        if (valid) {
-            float raw[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-                raw[0] = fmaf(cr.w[q], tab.vb0[slot[q]], raw[0]);
-                raw[1] = fmaf(cr.w[q], tab.vb1[slot[q]], raw[1]);
-                raw[2] = fmaf(cr.w[q], tab.vb2[slot[q]], raw[2]);
+        for (int k = 0; k < SPL; k++) {
+            const int i = base + 32 * k + lane;
+            if (i < n) {
+                if (SPL > 1) {  // with more than one sample per lane, the corners are looked up again
+                    s = S[i];
+                    sample_corners(g, s, cr);
+#pragma unroll
+                    for (int q = 0; q < 8; q++) slot[q] = table_find(tab, cr.idx[q]);
+                }
+                float raw[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    raw[0] = fmaf(cr.w[q], tab.vb0[slot[q]], raw[0]);
+                    raw[1] = fmaf(cr.w[q], tab.vb1[slot[q]], raw[1]);
+                    raw[2] = fmaf(cr.w[q], tab.vb2[slot[q]], raw[2]);
+                }
+                const float col[3] = {colour_act(raw[0]), colour_act(raw[1]), colour_act(raw[2])};
+                C[i] = make_float4(col[0], col[1], col[2], 0.f);
+                const double w = (double)s.w;
+                s0 += w * col[0];
+                s1 += w * col[1];
+                s2 += w * col[2];
             }
-            const float col[3] = {colour_act(raw[0]), colour_act(raw[1]), colour_act(raw[2])};
-            C[i] = make_float4(col[0], col[1], col[2], 0.f);
-            const double w = (double)s.w;
-            s0 += w * col[0];
-            s1 += w * col[1];
-            s2 += w * col[2];
         }
         table_clear(tab, lane);
     }
@@ -708,53 +737,57 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
     const float step = g.step;
 
     double carry_w = 0., carry_c0 = 0., carry_c1 = 0., carry_c2 = 0.;
-    for (int base = 0; base < n; base += 32) {
-        const int i = base + lane;
-        const bool valid = i < n;
-        SampleRec s;
-        float4 col = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (valid) {
-            s = S[i];
-            col = C[i];
-        } else {
-            s.w = 0.f;
-        }
-        const double w = valid ? (double)s.w : 0.;
-        const double aw = warp_inclusive_scan(w, lane);
-        const double a0 = warp_inclusive_scan(w * col.x, lane);
-        const double a1 = warp_inclusive_scan(w * col.y, lane);
-        const double a2 = warp_inclusive_scan(w * col.z, lane);
-        const double acc_i = carry_w + aw;
-        const double acc_rgb0 = carry_c0 + a0;
-        const double acc_rgb1 = carry_c1 + a1;
-        const double acc_rgb2 = carry_c2 + a2;
-        carry_w += __shfl_sync(0xffffffffu, aw, 31);
-        carry_c0 += __shfl_sync(0xffffffffu, a0, 31);
-        carry_c1 += __shfl_sync(0xffffffffu, a1, 31);
-        carry_c2 += __shfl_sync(0xffffffffu, a2, 31);
-        if (valid) {
-            float grad[4];
-            grad[1] = 0.6667f * w * res[0] * colour_deriv_from_act(col.x);
-            grad[2] = 0.6667f * w * res[1] * colour_deriv_from_act(col.y);
-            grad[3] = 0.6667f * w * res[2] * colour_deriv_from_act(col.z);
-            const double Ti = (double)s.tn;
-            grad[0] = res[0] * (Ti * col.x - (pred[0] - acc_rgb0));
-            grad[0] += res[1] * (Ti * col.y - (pred[1] - acc_rgb1));
-            grad[0] += res[2] * (Ti * col.z - (pred[2] - acc_rgb2));
-            const float dd = 1.f / (1.f + expf(13.f - s.raw));  // density_derivation (RenderUtils.cu:497)
-            grad[0] *= 0.6667 * step * dd;
-            grad[0] += step * dd * (accw_f - acc_i - Ti) * mask_loss;
-            // corner q receives grad[0]*w_q and grad[1+ch]*w_q*basis[k]: merge per vertex first
-            Corners cr;
-            sample_corners(g, s, cr);
+    for (int base0 = 0; base0 < n; base0 += 32 * SPL) {
+        for (int k = 0; k < SPL; k++) {
+            const int base = base0 + 32 * k;
+            if (base >= n) break;  // warp-uniform
+            const int i = base + lane;
+            const bool valid = i < n;
+            SampleRec s;
+            float4 col = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (valid) {
+                s = S[i];
+                col = C[i];
+            } else {
+                s.w = 0.f;
+            }
+            const double w = valid ? (double)s.w : 0.;
+            const double aw = warp_inclusive_scan(w, lane);
+            const double a0 = warp_inclusive_scan(w * col.x, lane);
+            const double a1 = warp_inclusive_scan(w * col.y, lane);
+            const double a2 = warp_inclusive_scan(w * col.z, lane);
+            const double acc_i = carry_w + aw;
+            const double acc_rgb0 = carry_c0 + a0;
+            const double acc_rgb1 = carry_c1 + a1;
+            const double acc_rgb2 = carry_c2 + a2;
+            carry_w += __shfl_sync(0xffffffffu, aw, 31);
+            carry_c0 += __shfl_sync(0xffffffffu, a0, 31);
+            carry_c1 += __shfl_sync(0xffffffffu, a1, 31);
+            carry_c2 += __shfl_sync(0xffffffffu, a2, 31);
+            if (valid) {
+                float grad[4];
+                grad[1] = 0.6667f * w * res[0] * colour_deriv_from_act(col.x);
+                grad[2] = 0.6667f * w * res[1] * colour_deriv_from_act(col.y);
+                grad[3] = 0.6667f * w * res[2] * colour_deriv_from_act(col.z);
+                const double Ti = (double)s.tn;
+                grad[0] = res[0] * (Ti * col.x - (pred[0] - acc_rgb0));
+                grad[0] += res[1] * (Ti * col.y - (pred[1] - acc_rgb1));
+                grad[0] += res[2] * (Ti * col.z - (pred[2] - acc_rgb2));
+                const float dd = 1.f / (1.f + expf(13.f - s.raw));  // density_derivation (RenderUtils.cu:497)
+                grad[0] *= 0.6667 * step * dd;
+                grad[0] += step * dd * (accw_f - acc_i - Ti) * mask_loss;
+                // corner q receives grad[0]*w_q and grad[1+ch]*w_q*basis[k]: merge per vertex first
+                Corners cr;
+                sample_corners(g, s, cr);
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const float wq = cr.w[q];
-                const int sl = table_slot(tab, cr.idx[q]);
-                atomicAdd(&tab.va[sl], grad[0] * wq);
-                atomicAdd(&tab.vb0[sl], grad[1] * wq);
-                atomicAdd(&tab.vb1[sl], grad[2] * wq);
-                atomicAdd(&tab.vb2[sl], grad[3] * wq);
+                for (int q = 0; q < 8; q++) {
+                    const float wq = cr.w[q];
+                    const int sl = table_slot(tab, cr.idx[q]);
+                    atomicAdd(&tab.va[sl], grad[0] * wq);
+                    atomicAdd(&tab.vb0[sl], grad[1] * wq);
+                    atomicAdd(&tab.vb1[sl], grad[2] * wq);
+                    atomicAdd(&tab.vb2[sl], grad[3] * wq);
+                }
             }
         }
         table_flush<NSH>(tab, g, shs, touched, lane);
@@ -1271,21 +1304,27 @@ __global__ void k_place_batched(BatchArgs a)
     }
 }
 
-template <int NSH, int PREC, int WARPS>
+// SPL: samples a lane takes per chunk (the autotuner's samples-per-step), tables of
+// kHashSlots * SPL slots per warp.
+template <int NSH, int PREC, int WARPS, int SPL>
 __global__ void __launch_bounds__(WARPS * 32, 20 / WARPS) k_shade_batched(BatchArgs a)
 {
-    __shared__ uint32_t h_keys[WARPS][kHashSlots];
-    __shared__ float h_vals[WARPS][4][kHashSlots];
+    constexpr int kSlots = kHashSlots * SPL;
+    static_assert(WARPS * SPL * kHashSlots * 5 * 4 <= 48 * 1024, "static shared memory of the tables");
+    __shared__ uint32_t h_keys[WARPS][kSlots];
+    __shared__ float h_vals[WARPS][4][kSlots];
     __shared__ int s_base[kMaxBatchScenes];
     for (int i = threadIdx.x; i < a.n_scenes; i += blockDim.x) s_base[i] = a.scenes[i].ray_base;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    for (int s = lane; s < kHashSlots; s += 32) {
+    for (int s = lane; s < kSlots; s += 32) {
         h_keys[warp][s] = kEmpty;
         h_vals[warp][0][s] = h_vals[warp][1][s] = h_vals[warp][2][s] = h_vals[warp][3][s] = 0.f;
     }
     __syncthreads();
-    const WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
+    WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
+    tab.n = kSlots;
+    tab.shift = SPL == 1 ? 24u : (SPL == 2 ? 23u : 22u);
     const int iter = *a.iter;
     while (true) {
         int first = 0;
@@ -1304,7 +1343,7 @@ __global__ void __launch_bounds__(WARPS * 32, 20 / WARPS) k_shade_batched(BatchA
                 continue;
             }
             const int64_t ri = (int64_t)(iter % sc.pool_batches) * sc.len + b;
-            shade_ray<NSH, kForwardBackward, PREC>(sc.g, sc.r, b, ri, cnt, a.samples + sc.sample_base,
+            shade_ray<NSH, kForwardBackward, PREC, SPL>(sc.g, sc.r, b, ri, cnt, a.samples + sc.sample_base,
                                                    a.colours + sc.sample_base, sc.maxs, a.acc + sc.ray_base,
                                                    a.losses + sc.ray_base, a.mask_coef, a.huber, tab, sc.touched,
                                                    lane);
@@ -1327,14 +1366,18 @@ static cpx_status batch_launch_prec(const BatchArgs& a, const BatchTuning& tn, c
     using Real = typename std::conditional<PREC == kPrecFP32, double, float>::type;
     const int pb = batch_blocks((const void*)k_place_batched<Real>, tn.place_block, 0);
     k_place_batched<Real><<<pb, tn.place_block, 0, st>>>(a);
-#define CPX_SHADE_B(W)                                                                              \
+#define CPX_SHADE_B(W, SPL)                                                                         \
     {                                                                                               \
-        const int sb = batch_blocks((const void*)k_shade_batched<9, PREC, W>, W * 32, 0);           \
-        k_shade_batched<9, PREC, W><<<sb, W * 32, 0, st>>>(a);                                      \
+        const int sb = batch_blocks((const void*)k_shade_batched<9, PREC, W, SPL>, W * 32, 0);      \
+        k_shade_batched<9, PREC, W, SPL><<<sb, W * 32, 0, st>>>(a);                                 \
     }
-    if (tn.shade_warps == 2) CPX_SHADE_B(2)
-    else if (tn.shade_warps == 8) CPX_SHADE_B(8)
-    else CPX_SHADE_B(4)
+    // shading warps per block x samples per lane: the combinations whose tables fit in a block
+    if (tn.shade_warps == 2 && tn.spl == 4) CPX_SHADE_B(2, 4)
+    else if (tn.shade_warps == 2 && tn.spl == 2) CPX_SHADE_B(2, 2)
+    else if (tn.shade_warps == 2) CPX_SHADE_B(2, 1)
+    else if (tn.shade_warps == 4 && tn.spl == 2) CPX_SHADE_B(4, 2)
+    else if (tn.shade_warps == 8) CPX_SHADE_B(8, 1)
+    else CPX_SHADE_B(4, 1)
 #undef CPX_SHADE_B
     count_launch(2);
     return cuda_status(cudaGetLastError(), "batched march");

@@ -542,12 +542,15 @@ typedef struct cpx_batch_scene {
     int rays_per_batch;
 } cpx_batch_scene;
 /* Launch shapes of the batched march: threads per placement block (32..512, a multiple of
- * 32), warps per shading block (2, 4 or 8) and rays a shading warp takes per work-counter
- * access (1..8). */
+ * 32), warps per shading block (2, 4 or 8), rays a shading warp takes per work-counter
+ * access (1..8), and samples a shading lane takes per chunk (1, 2 or 4; a chunk of
+ * 32 * samples_per_step samples shares one vertex table, so its corners are gathered and its
+ * gradients scattered once; shade_warps * samples_per_step <= 8, the tables' shared memory). */
 typedef struct cpx_batch_tuning {
     int place_block;
     int shade_warps;
     int grab;
+    int samples_per_step;
 } cpx_batch_tuning;
 /* args->timestep is the first iteration's timestep; losses of every step stay on the device
  * ([sum of rays_per_batch], scene after scene). */
@@ -568,7 +571,8 @@ cpx_status cpx_batch_info(const cpx_batch* b, int* iteration, int* total_rays, i
 cpx_status cpx_batch_set_tuning(cpx_batch* b, const cpx_batch_tuning* t);
 cpx_status cpx_batch_get_tuning(const cpx_batch* b, cpx_batch_tuning* t);
 /* Coordinate-descent search of the launch shapes (placement blocks of 64/128/256/512 threads,
- * shading blocks of 2/4/8 warps, 1/2/4/8 rays per access): every candidate runs steps_per_trial real
+ * shading blocks of 2/4/8 warps, 1/2/4/8 rays per access, 1/2/4 samples per lane and chunk,
+ * where the tables fit): every candidate runs steps_per_trial real
  * training iterations (they advance training like cpx_batch_step), timed with CUDA events;
  * the fastest shapes are kept and written to best (may be NULL). */
 cpx_status cpx_batch_autotune(cpx_batch* b, int steps_per_trial, cpx_batch_tuning* best, cpx_stream stream);

@@ -187,3 +187,30 @@ def test_batch_rejects_mixed_forms(cuda):
         cpx.Batch([(a[0], a[1], 512)], **STEP_KW)  # more rays per batch than the table holds
     with pytest.raises(cpx.CpxError):
         cpx.Batch([(a[0], a[1], 128), (a[0], a[1], 128)], **STEP_KW)
+
+
+@pytest.mark.parametrize("warps,spl", [(2, 2), (2, 4), (4, 2)])
+def test_samples_per_step_equals_one_sample_per_lane(cuda, warps, spl):
+    """Shading chunks of 32 * samples_per_step samples (one vertex table per chunk) give the
+    forward of one sample per lane exactly (first-step MSE to 1e-12) and the same training
+    within float-atomics noise after three steps."""
+    import cpx
+
+    lens = [sp[3] for sp in SPECS]
+    runs = []
+    for tuning in ((64, warps, 1, 1), (64, warps, 1, spl)):
+        sc = [_scene(s, n, nr, "fp32", sp) for s, n, nr, _, sp in SPECS]
+        batch = cpx.Batch([(s, r, n) for (s, r), n in zip(sc, lens)], **STEP_KW)
+        batch.set_tuning(*tuning)
+        assert batch.tuning["samples_per_step"] == tuning[3]
+        mses = []
+        for _ in range(3):
+            batch.step(graphs=False)
+            mses.append(batch.mse())
+        batch.check()
+        runs.append((mses, [s.download_params() for s, _ in sc]))
+        batch.close()
+    (m1, p1), (m2, p2) = runs
+    assert np.all(np.abs(m1[0] - m2[0]) <= 1e-12 * np.abs(m1[0]))
+    for a, b in zip(p1, p2):
+        _close(a, b, "params")
