@@ -506,8 +506,8 @@ cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const doub
 
 cpx_status cpx_grid_set_options(cpx_grid* g, int options)
 {
-    if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH | CPX_OPT_NO_EARLY_STOP | CPX_OPT_TWO_STAGE_MARCH |
-                                   CPX_OPT_ROW_SWEEP))) return CPX_ERR_INVALID_ARGUMENT;
+    if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH | CPX_OPT_NO_EARLY_STOP | CPX_OPT_FUSED_MARCH |
+                                   CPX_OPT_PLANE_SWEEP))) return CPX_ERR_INVALID_ARGUMENT;
     g->options = options;
     cpx_status rc = refresh_dense_skip(g, 0);  // the maps of a grid now marched with jumps
     if (rc != CPX_OK) return rc;

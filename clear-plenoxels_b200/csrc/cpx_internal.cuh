@@ -391,7 +391,7 @@ cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, d
                       double sh_lr, int timestep, cudaStream_t s, const int* t_dev = nullptr);
 // The batched form's FP32 sweeps in one launch (sweep.cu): grids that qualify (dense FP32, SH
 // band 2, fused TV), a device table of sweep_table_bytes(n) filled from the host image that
-// sweep_table_fill writes (it returns the launch's work items), then the launch, which flips
+// sweep_table_fill writes (it returns the launch's rows), then the launch, which flips
 // the grids' buffers as sweep_adam does.
 bool sweep_batchable(const cpx_grid* g, bool fused_tv);
 size_t sweep_table_bytes(int n);

@@ -1051,7 +1051,7 @@ struct Guide {
     float* seg_w = nullptr;
     Skip skip;
     bool march32 = false;  // the FP32 march of the mixed forms (else the reference's sequence)
-    bool two_stage = false;  // placement and shading as two launches (CPX_OPT_TWO_STAGE_MARCH)
+    bool two_stage = true;  // placement and shading as two launches (else the fused march, CPX_OPT_FUSED_MARCH)
     bool on() const { return masks != nullptr || seg_w != nullptr; }
 };
 
@@ -1192,7 +1192,7 @@ static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32
     if (rc != CPX_OK || len == 0) return rc;
     Guide gd = guide;
     gd.march32 = g->prec != kPrecFP32 || (g->options & CPX_OPT_FP32_MARCH);
-    gd.two_stage = (g->options & CPX_OPT_TWO_STAGE_MARCH) != 0 || s.queue == nullptr;
+    gd.two_stage = !(g->options & CPX_OPT_FUSED_MARCH) || s.queue == nullptr;
     if (guide.on() && !gd.march32) {
         set_error("the proposal-guided march runs on the FP32 march of the mixed forms only");
         return CPX_ERR_UNSUPPORTED;

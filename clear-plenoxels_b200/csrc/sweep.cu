@@ -149,12 +149,10 @@ __device__ __forceinline__ void bias_corrections(int t, const int* t_dev, float*
 }
 
 // Dense grid: one block per (y, z) row of W vertices, S slots each.
+// One (y, z) row of W vertices, S slots each, by a block (s_bc: the bias corrections).
 template <int S, bool TV>
-__global__ void __launch_bounds__(256) k_sweep_dense(SweepArgs a)
+__device__ __forceinline__ void sweep_dense_row(const SweepArgs& a, int row, const float* s_bc)
 {
-    __shared__ float s_bc[2];
-    bias_corrections(a.timestep, a.t_dev, s_bc);
-    const int row = blockIdx.x;
     const int y = row % a.H;
     const int z = row / a.H;
     const uint32_t WH = (uint32_t)a.W * a.H;
@@ -178,6 +176,45 @@ __global__ void __launch_bounds__(256) k_sweep_dense(SweepArgs a)
         const float lr_d = a.adaptive_lr ? a.lr * a.adaptive_lr[v] : a.lr;
         sweep_slot<TV>(a, sl, v, j, tv_on, nb_slot, nb_self, s_bc[0], s_bc[1], lr_d);
     }
+}
+
+// Dense grid: one block per (y, z) row of W vertices, S slots each.
+template <int S, bool TV>
+__global__ void __launch_bounds__(256) k_sweep_dense(SweepArgs a)
+{
+    __shared__ float s_bc[2];
+    bias_corrections(a.timestep, a.t_dev, s_bc);
+    sweep_dense_row<S, TV>(a, blockIdx.x, s_bc);
+}
+
+// The row sweeps of many dense FP32 grids (the batched form) in one launch: block b takes row b
+// of the concatenated row lists, its grid found by binary search over the first rows.
+struct SweepBatch {
+    const SweepArgs* args;  // [n]
+    const int* first;       // [n + 1]: first row of each grid, then the total
+    int n;
+};
+
+template <int S>
+__global__ void __launch_bounds__(256) k_sweep_dense_batched(SweepBatch sb)
+{
+    __shared__ float s_bc[2];
+    __shared__ SweepArgs s_args;
+    __shared__ int s_row;
+    const int item = blockIdx.x;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = sb.n - 1;  // the last grid whose first row is <= item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sb.first[mid] <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        s_args = sb.args[lo];
+        s_row = item - sb.first[lo];
+    }
+    __syncthreads();
+    bias_corrections(s_args.timestep, s_args.t_dev, s_bc);
+    sweep_dense_row<S, true>(s_args, s_row, s_bc);
 }
 
 // Dense grid, TV on: the 2.5-D form.  A block owns a kZTX x kZTY tile of vertex columns and
@@ -291,43 +328,6 @@ __host__ __device__ __forceinline__ dim3 z_tiles(int W, int H, int D)
                 (unsigned)((D + kZChunk - 1) / kZChunk));
 }
 
-// The sweeps of many dense FP32 grids (the batched form) in one launch: block b takes work item
-// b of the concatenated tile lists, its grid found by binary search over the first items.
-struct SweepBatch {
-    const SweepArgs* args;  // [n]
-    const int* first;       // [n + 1]: first work item of each grid, then the total
-    int n;
-};
-
-template <int S>
-__global__ void __launch_bounds__(kZTX * kZTY * S, 1) k_sweep_dense_z_batched(SweepBatch sb)
-{
-    __shared__ float s_bc[2];
-    __shared__ ZPlane<S> plane;
-    __shared__ SweepArgs s_args;
-    __shared__ int s_local;
-    const int item = blockIdx.x;
-    if (threadIdx.x == 0) {
-        int lo = 0, hi = sb.n - 1;  // the last grid whose first item is <= item
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (sb.first[mid] <= item) lo = mid;
-            else hi = mid - 1;
-        }
-        s_args = sb.args[lo];
-        s_local = item - sb.first[lo];
-    }
-    __syncthreads();
-    const SweepArgs& a = s_args;
-    bias_corrections(a.timestep, a.t_dev, s_bc);
-    const dim3 tiles = z_tiles(a.W, a.H, a.D);
-    const int local = s_local;
-    const int bx = local % (int)tiles.x;
-    const int by = (local / (int)tiles.x) % (int)tiles.y;
-    const int bz = local / (int)(tiles.x * tiles.y);
-    sweep_dense_z_tile<S>(a, bx, by, bz, s_bc, plane);
-}
-
 // Sparse grid: blocks tile the compact slots; positions from the compact->dense table.
 template <int S, bool TV>
 __global__ void __launch_bounds__(256) k_sweep_sparse(SweepArgs a)
@@ -371,7 +371,7 @@ static void launch_sweep(const cpx_grid* g, const SweepArgs& a, bool tv, cudaStr
 {
     if (!g->sparse) {
         const unsigned rows = (unsigned)((int64_t)g->H * g->D);
-        if (tv && S == 7 && !(g->options & CPX_OPT_ROW_SWEEP) && !g->sparse) {
+        if (tv && S == 7 && (g->options & CPX_OPT_PLANE_SWEEP) && !g->sparse) {
             k_sweep_dense_z<S><<<z_tiles(g->W, g->H, g->D), kZTX * kZTY * S, 0, st>>>(a);
         } else if (tv) {
             k_sweep_dense<S, true><<<rows, 256, 0, st>>>(a);
@@ -478,8 +478,8 @@ static SweepArgs sweep_args(const cpx_grid* g, double lam_d, double lam_sh, doub
 
 bool sweep_batchable(const cpx_grid* g, bool fused_tv)
 {
-    return fused_tv && g->prec == kPrecFP32 && !g->sparse && g->rec == 28 && !(g->options & CPX_OPT_ROW_SWEEP) &&
-           g->n_act > 0 && g->n_act * 7 < ((int64_t)1 << 32);
+    return fused_tv && g->prec == kPrecFP32 && !g->sparse && g->rec == 28 && g->n_act > 0 &&
+           g->n_act * 7 < ((int64_t)1 << 32);
 }
 
 size_t sweep_table_bytes(int n) { return (size_t)n * sizeof(SweepArgs) + ((size_t)n + 1) * sizeof(int); }
@@ -492,9 +492,8 @@ int sweep_table_fill(cpx_grid* const* grids, int n, double lam_d, double lam_sh,
     int items = 0;
     for (int i = 0; i < n; i++) {
         args[i] = sweep_args(grids[i], lam_d, lam_sh, lr, sh_lr, 1, t_dev);
-        const dim3 t = z_tiles(grids[i]->W, grids[i]->H, grids[i]->D);
         first[i] = items;
-        items += (int)(t.x * t.y * t.z);
+        items += grids[i]->H * grids[i]->D;  // rows
     }
     first[n] = items;
     return items;
@@ -507,7 +506,7 @@ cpx_status sweep_batched_launch(cpx_grid* const* grids, int n, const void* dev_t
     sb.args = static_cast<const SweepArgs*>(dev_table);
     sb.first = reinterpret_cast<const int*>(sb.args + n);
     sb.n = n;
-    k_sweep_dense_z_batched<7><<<(unsigned)items, kZTX * kZTY * 7, 0, st>>>(sb);
+    k_sweep_dense_batched<7><<<(unsigned)items, 256, 0, st>>>(sb);
     count_launch();
     for (int i = 0; i < n; i++) {
         cpx_grid* g = grids[i];

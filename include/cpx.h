@@ -385,18 +385,21 @@ cpx_status cpx_image_mask_pixels(const int* bbox, int width, int32_t* index_out,
  * CPX_OPT_NO_EARLY_STOP  the FP32 march runs every ray to its far bound, instead of ending it
  *                        once its transmittance is below 1e-4 (what the rest of the ray could
  *                        add to its colour and weight);
- * CPX_OPT_TWO_STAGE_MARCH  the march runs as two launches -- placement of every ray, then
- *                        shading -- instead of one launch that shades rays while others are
- *                        still being placed.  Results are the same; for comparison;
- * CPX_OPT_ROW_SWEEP      the FP32 form's fused TV + Adam sweep of a dense grid (SH band 2)
- *                        runs a block per row of vertices reading neighbours from L1/L2,
- *                        instead of walking z with the x-y plane of a tile on chip.  Results
- *                        are the same bit for bit; for comparison. */
+ * CPX_OPT_FUSED_MARCH    the march runs as one launch that shades rays while others are
+ *                        still being placed, instead of two launches (placement of every ray,
+ *                        then shading).  Results are the same; slower on the B200 (placement's
+ *                        dependent chains lose issue slots to the shading warps beside them);
+ *                        for comparison;
+ * CPX_OPT_PLANE_SWEEP    the FP32 form's fused TV + Adam sweep of a dense grid (SH band 2)
+ *                        walks z with the x-y plane of a tile on chip instead of running a
+ *                        block per row of vertices that reads neighbours from L1/L2.  Results
+ *                        are the same bit for bit; slower on the B200 (one z-step of loads in
+ *                        flight per SM); for comparison. */
 #define CPX_OPT_NO_EMPTY_SKIP 1
 #define CPX_OPT_FP32_MARCH 2
 #define CPX_OPT_NO_EARLY_STOP 4
-#define CPX_OPT_TWO_STAGE_MARCH 8
-#define CPX_OPT_ROW_SWEEP 16
+#define CPX_OPT_FUSED_MARCH 8
+#define CPX_OPT_PLANE_SWEEP 16
 cpx_status cpx_grid_set_options(cpx_grid* g, int options);
 
 /* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,

@@ -140,7 +140,7 @@ def test_fused_march_equals_two_stage(plain128, cuda):
     nr = rays.total_rays
     zero = np.zeros((28, scene.actual_grid_nums), np.float32)
     outs = []
-    for opt in (0, cpx.OPT_TWO_STAGE_MARCH):
+    for opt in (cpx.OPT_FUSED_MARCH, 0):
         scene.set_options(opt)
         losses = torch.zeros(nr, dtype=torch.float64, device=cuda)
         scene.upload_grads(zero)
@@ -171,7 +171,9 @@ def test_tv_matches_oracle(plain128, typ, nb):
     got = scene.download_grads()
     want = g0.copy()
     orc.tv_grad(osc, want, 1e-3, 2e-3, typ, nb)
-    assert_grads_close(got - g0, want - g0, rel=1e-5, what="TV gradient")
+    # type 0 is a deterministic per-vertex sum; types 1 and 2 add each cell's share to its corners
+    # with float atomics, whose order varies
+    assert_grads_close(got - g0, want - g0, rel=1e-5 if typ == 0 else 1e-4, what="TV gradient")
 
 
 def test_adam_matches_oracle(plain128):

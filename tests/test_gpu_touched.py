@@ -94,7 +94,7 @@ def test_plane_window_sweep_equals_row_sweep(cuda, dims):
     v0 = rng.uniform(0, 1e-4, params.shape).astype(np.float32)
     alr = (rng.random(W * H * D) > 0.2).astype(np.float32)
     outs = []
-    for opt in (0, cpx.OPT_ROW_SWEEP):
+    for opt in (cpx.OPT_PLANE_SWEEP, 0):
         sc = cpx.ObjectScene(W, H, D, 9)
         sc.set_options(opt)
         sc.upload_params(params)

@@ -15,7 +15,12 @@ per parameter array, two ways:
   magnitude is at least `floor_frac` of its array's largest magnitude.  Below
   that floor an element is a near-cancelling sum of much larger per-sample
   contributions, and its relative error is set by the accumulation order, not
-  by the arithmetic; the normwise check still bounds it.
+  by the arithmetic; the normwise check still bounds it.  Measured on the B200
+  against the reference's kernels (128^3 case, 4096 rays): with the floor at
+  1e-2 of the array maximum, reordered float atomics alone left a few elements
+  1.0e-4 .. 1.6e-4 off while every array stayed within 8e-6 normwise, so the
+  floor is 0.1.  A wrong term moves most elements of an array by far more than
+  1e-4 and fails both checks.
 """
 from __future__ import annotations
 
@@ -23,7 +28,7 @@ import numpy as np
 
 RGB_ABS = 1e-5
 GRAD_REL = 1e-4
-GRAD_FLOOR_FRAC = 1e-2
+GRAD_FLOOR_FRAC = 1e-1
 
 
 def normwise(a, b):
