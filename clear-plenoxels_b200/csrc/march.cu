@@ -160,7 +160,7 @@ __device__ __forceinline__ float real_exp(float x) { return expf(x); }
 template <typename Real>
 struct PlaceRay {
     float ox, oy, oz, dx, dy, dz, near_t, far_t;
-    Real t, Ti, acc, accD, seg_len, inv_seg;
+    Real t, acc, accD, seg_len, inv_seg;
     float accDen;
     int intT, n, it, it_cap, b;
     int64_t ri;
@@ -169,6 +169,10 @@ struct PlaceRay {
     uint32_t seg_mask;
     float* seg_w;
     SampleRec* out;
+    // The last sample's record waits here for its transmittance, exp(-accD), which is worked
+    // out with the next sample (or at the ray's end): the double exp then overlaps the next
+    // sample's trilinear chain instead of stalling the in-order issue on its own.
+    SampleRec pend;
 };
 
 // renderRaysGPU's set-up of one ray (RenderUtils.cu:1927-1946).  Returns false for a ray with
@@ -207,7 +211,6 @@ __device__ __forceinline__ bool place_begin(PlaceRay<Real>& st, const GridView& 
     st.it_cap = (bound < (double)(maxs + 16) ? (int)bound : maxs + 16) + (PROP ? 2 * kProposalSegments : 0);
     st.out = samples + (size_t)b * maxs;
     st.t = st.near_t;
-    st.Ti = 1;
     st.acc = 0;
     st.accD = 0;
     st.accDen = 0.f;
@@ -233,7 +236,8 @@ __device__ __forceinline__ bool place_iter(PlaceRay<Real>& st, const GridView& g
 {
     const float step = g.step;
     if (++st.it > st.it_cap || st.n >= maxs) {
-        atomicOr(err, 1);
+        // not an overrun when the last sample already ended the ray (the stop of the FP32 march)
+        if (!(st.n > 0 && real_exp(-st.accD) < (Real)sk.t_stop)) atomicOr(err, 1);
         return true;
     }
     Real t = st.t;
@@ -332,15 +336,22 @@ __device__ __forceinline__ bool place_iter(PlaceRay<Real>& st, const GridView& g
     tri0 += c * st.cd[6];
     c = x * y * z;
     tri0 += c * st.cd[7];
+    // the transmittance before this sample, exp(-sum sigma step) of the samples so far (the
+    // reference's T, RenderUtils.cu:1693-1704; exactly 1 before the first sample)
+    const Real Ti = real_exp(-st.accD);
+    if (st.n > 0) {
+        st.pend.tn = (float)Ti;  // the previous sample's transmittance after it
+        st.out[st.n - 1] = st.pend;
+        if (Ti < (Real)sk.t_stop) return true;  // FP32 march: nothing visible remains behind
+    }
     // density_activation (RenderUtils.cu:491) and the weight (RenderUtils.cu:1693-1704)
     const float sigma = logf(1.f + expf(tri0 - 13.f));
-    const Real w = st.Ti * (one - expf(-sigma * step));
+    const Real w = Ti * (one - expf(-sigma * step));
     st.acc += w;
     st.accDen += sigma;
     st.accD += sigma * step;
     if (PROP && st.seg_w) st.seg_w[seg] += (float)w;
-    const Real Tn = real_exp(-st.accD);
-    SampleRec rec;
+    SampleRec& rec = st.pend;
     rec.bx = (uint16_t)(b0 < 65535u ? b0 : 65535u);
     rec.by = (uint16_t)(b1 < 65535u ? b1 : 65535u);
     rec.bz = (uint16_t)(b2 < 65535u ? b2 : 65535u);
@@ -350,19 +361,20 @@ __device__ __forceinline__ bool place_iter(PlaceRay<Real>& st, const GridView& g
     rec.fz = (float)z;
     rec.raw = tri0;
     rec.w = (float)w;
-    rec.tn = (float)Tn;
-    st.out[st.n] = rec;
-    st.Ti = Tn;
     st.t = t + fabs(step - w);  // fabs(float) is the float overload
     ++st.intT;
     ++st.n;
-    return Tn < (Real)sk.t_stop;  // FP32 march: nothing visible remains behind
+    return false;
 }
 
 template <typename Real>
-__device__ __forceinline__ void place_end(const PlaceRay<Real>& st, const RaysView& r, int* counts,
+__device__ __forceinline__ void place_end(PlaceRay<Real>& st, const RaysView& r, int* counts,
                                           double* acc_out, bool write_fwd)
 {
+    if (st.n > 0) {  // the last sample's record, with its transmittance
+        st.pend.tn = (float)real_exp(-st.accD);
+        st.out[st.n - 1] = st.pend;
+    }
     if (write_fwd) {
         r.acc_den[st.ri] = st.accDen;
         r.acc_w[st.ri] = (float)st.acc;
@@ -850,6 +862,73 @@ __global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysV
                                tab, touched, lane);
 }
 
+// Shading with a work counter: the rays in order of decreasing sample count (k_order_by_count,
+// a counting sort on count / 16 in one block), taken a ray per warp from the counter by
+// persistent blocks -- the last rays the warps take are the short ones, so no SM waits on one
+// long ray at the end of the launch.
+constexpr int kOrderBuckets = 256;
+
+__device__ __forceinline__ int order_bucket(int count)
+{
+    int k = count < 0 ? 0 : count >> 4;
+    k = k < kOrderBuckets - 1 ? k : kOrderBuckets - 1;
+    return kOrderBuckets - 1 - k;  // longest first
+}
+
+__global__ void __launch_bounds__(1024) k_order_by_count(const int* __restrict__ counts, int len, int* order,
+                                                         int* ctr)
+{
+    __shared__ int hist[kOrderBuckets];
+    for (int i = threadIdx.x; i < kOrderBuckets; i += blockDim.x) hist[i] = 0;
+    if (threadIdx.x == 0) *ctr = 0;  // the shading warps' work counter
+    __syncthreads();
+    for (int b = threadIdx.x; b < len; b += blockDim.x) atomicAdd(&hist[order_bucket(counts[b])], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int k = 0; k < kOrderBuckets; k++) {
+            const int h = hist[k];
+            hist[k] = run;
+            run += h;
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < len; b += blockDim.x) order[atomicAdd(&hist[order_bucket(counts[b])], 1)] = b;
+}
+
+template <int NSH, int MODE, int PREC>
+__global__ void __launch_bounds__(kShadeWarps * 32, 6)
+    k_shade_dyn(GridView g, RaysView r, const int32_t* sidx, int start, int len, const SampleRec* samples,
+                float4* colours, int maxs, const int* counts, const double* acc, double* losses, double mask_coef,
+                float huber, uint32_t* touched, const int* order, int* ctr)
+{
+    __shared__ uint32_t h_keys[kShadeWarps][kHashSlots];
+    __shared__ float h_vals[kShadeWarps][4][kHashSlots];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for (int s = lane; s < kHashSlots; s += 32) {
+        h_keys[warp][s] = kEmpty;
+        h_vals[warp][0][s] = h_vals[warp][1][s] = h_vals[warp][2][s] = h_vals[warp][3][s] = 0.f;
+    }
+    __syncwarp();
+    const WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
+    while (true) {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(ctr, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= len) break;  // warp-uniform
+        const int b = order[k];
+        const int cnt = counts[b];
+        if (cnt == -2) {
+            if ((MODE & kBackward) && lane == 0) losses[b] = 0.;
+            continue;
+        }
+        const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
+        shade_ray<NSH, MODE, PREC>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber, tab,
+                                   touched, lane);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // The fused march: placement and shading in one launch, overlapped.  Placement is one
 // dependent chain per ray and keeps only a warp or two per SM busy; shading is a warp per ray
@@ -1112,6 +1191,24 @@ static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv,
     else
         k_place<MODE, double, false><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
                                                            s.counts, s.acc, s.err, nullptr, nullptr, guide.skip);
+    if (s.queue) {
+        // longest rays first from a work counter (the queue's first word and its ray slots)
+        static int resident = 0;  // per instance
+        if (resident == 0) {
+            int dev = 0, sms = 0, per = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade_dyn<NSH, MODE, PREC>, kShadeWarps * 32, 0);
+            resident = sms * (per > 0 ? per : 1);
+        }
+        const int blocks = (int)sgrid.x < resident ? (int)sgrid.x : resident;
+        k_order_by_count<<<1, 1024, 0, st>>>(s.counts, len, s.queue + 4, s.queue);
+        count_launch();
+        k_shade_dyn<NSH, MODE, PREC><<<blocks, sblock, 0, st>>>(gv, rv, sidx, start, len, s.samples, s.colours,
+                                                                 s.maxs, s.counts, s.acc, losses, mask_coef, huber,
+                                                                 touched, s.queue + 4, s.queue);
+        return;
+    }
     k_shade<NSH, MODE, PREC><<<sgrid, sblock, 0, st>>>(gv, rv, sidx, start, len, s.samples, s.colours, s.maxs,
                                                        s.counts, s.acc, losses, mask_coef, huber, touched);
 }
