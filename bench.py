@@ -69,6 +69,11 @@ WORKLOADS = {
                                 init_density=0.1, seed=100 + i)
                            for i, (n, b) in enumerate(zip([48, 64, 80, 96, 112, 128, 160, 192] * 3,
                                                           [512, 1024, 2048, 768, 1536, 4096] * 4))]),
+    # many tiny scenes, where an iteration's device work is short next to the host's launch work:
+    # 64 dense scenes of 24^3 .. 40^3, batches of 128 .. 512 rays from 4 64x64 views each
+    "multi64": dict(multi=[dict(n=n, gt_n=n, n_blobs=4, gt_sh_std=0.5, cams=4, img=64, batch=b, pool_batches=4,
+                                init_density=0.1, seed=300 + i)
+                           for i, (n, b) in enumerate(zip([24, 28, 32, 36, 40] * 13, [128, 256, 384, 512] * 16))][:64]),
 }
 # the reference's shipped training constants (SparseVolumeRadianceField/config_linux.txt)
 STEP = dict(mask_coef=1.0, huber=0.1, lam_density=1e-5, lam_sh=1e-6, lr=0.3, sh_lr=1.0)
@@ -389,9 +394,23 @@ def run_ours(args, wl, world, rank, local):
         if decay:  # Render.cu:499-500
             lr[:] = [cpx.lr_decay(x, wl["pool_batches"], k // wl["pool_batches"]) for x in lr]
 
+    # the plain FP32 form steps with cpx_train_step_ahead: each step places the next batch's samples
+    # beside its own optimizer sweep (the product's fastest path); the march and the sweep are then
+    # timed apart in a split leg after the timed region
+    ahead = prop is None and args.precision == "fp32" and thr is None and not args.no_ahead
+
+    def step_ahead(k):
+        b, nb = k % wl["pool_batches"], (k + 1) % wl["pool_batches"]
+        cpx.train_step_ahead(scene, pool, losses, start=b * R, length=R, next_rays=pool, next_start=nb * R,
+                             next_length=R, mask_coef=STEP["mask_coef"], huber_delta=STEP["huber"],
+                             lam_density=STEP["lam_density"], lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1],
+                             timestep=k + 1, want_mse=False, stream=stream)
+        if decay:  # Render.cu:499-500
+            lr[:] = [cpx.lr_decay(x, wl["pool_batches"], k // wl["pool_batches"]) for x in lr]
+
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
     for k in range(W):
-        step(k)
+        (step_ahead if ahead else step)(k)
     torch.cuda.synchronize()
     scene.check()
 
@@ -406,9 +425,12 @@ def run_ours(args, wl, world, rank, local):
     torch.cuda.nvtx.range_push("timed")  # lets a profiler capture the timed steps alone (--nvtx-include timed/)
     t0.record(stream)
     for k in range(K):
-        evs[k][0].record(stream)
-        step(W + k, evs[k])
-        evs[k][2].record(stream)
+        if ahead:
+            step_ahead(W + k)
+        else:
+            evs[k][0].record(stream)
+            step(W + k, evs[k])
+            evs[k][2].record(stream)
     t1.record(stream)
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
@@ -416,15 +438,32 @@ def run_ours(args, wl, world, rank, local):
     clk = clocks.stop()
     dist_barrier(world)
     scene.check()
+    split_ms = None
+    if ahead:
+        # split leg: the same steps with the march and the sweep one after the other, timed apart
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for k in range(K):
+            evs[k][0].record(stream)
+            step(W + K + k, evs[k])
+            evs[k][2].record(stream)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        scene.check()
+        split_ms = s0.elapsed_time(s1) / K
+        W_used = W + K
+    else:
+        W_used = W
     # vertices whose gradient records a sweep reads: counted on untimed batches of the pool
     tcounts = []
     for k in range(min(4, wl["pool_batches"])):
-        b = (W + K + k) % wl["pool_batches"]
+        b = (W_used + K + k) % wl["pool_batches"]
         cpx.RenderUtils.renderRays_forwardBackward(scene, pool, losses, None, b * R, R, STEP["mask_coef"],
                                                    STEP["huber"], stream=stream)
         tcounts.append(scene.touched_count())
-        cpx.Optimizer.varianceAndUpdate(scene, STEP["lam_density"], STEP["lam_sh"], lr[0], lr[1], W + K + k + 1,
-                                        stream=stream)
+        cpx.Optimizer.varianceAndUpdate(scene, STEP["lam_density"], STEP["lam_sh"], lr[0], lr[1],
+                                        W_used + K + k + 1, stream=stream)
     touched = float(np.mean(tcounts))
     ms_local = t0.elapsed_time(t1)
     ms = dist_max(ms_local, world, True)
@@ -436,7 +475,7 @@ def run_ours(args, wl, world, rank, local):
     # samples of images held on the device (cpx_ray_source), then the same training step
     src_result = None
     if prop is None:
-        src_result = ray_source_leg(args, wl, scene, eyes, pix, gt, R, K, W + K + 4, stream, world, dev)
+        src_result = ray_source_leg(args, wl, scene, eyes, pix, gt, R, K, W_used + K + 4, stream, world, dev)
 
     # ---- e2e: host buffers through the public API (H2D batch, step, MSE back)
     mses = []
@@ -445,10 +484,25 @@ def run_ours(args, wl, world, rank, local):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    bufs = [batch_rays, cpx.Rays(R, white_bg=True)] if ahead else [batch_rays]
+    if ahead:  # the first batch; each step uploads the next one, placed beside its sweep
+        bufs[0].upload_packed(host_pool[0:R], stream=stream)
     for k in range(K):
         b = k % wl["pool_batches"]
+        it = W_used + K + 4 + k
+        if ahead:
+            cur, nxt = bufs[k % 2], bufs[(k + 1) % 2]
+            last = k + 1 == K
+            if not last:
+                nb = (k + 1) % wl["pool_batches"]
+                nxt.upload_packed(host_pool[nb * R:(nb + 1) * R], stream=stream)
+            mses.append(cpx.train_step_ahead(scene, cur, losses, start=0, length=R, next_rays=None if last else nxt,
+                                             next_start=0, next_length=0 if last else R,
+                                             mask_coef=STEP["mask_coef"], huber_delta=STEP["huber"],
+                                             lam_density=STEP["lam_density"], lam_sh=STEP["lam_sh"], lr=lr[0],
+                                             sh_lr=lr[1], timestep=it + 1, want_mse=True, stream=stream))
+            continue
         batch_rays.upload_packed(host_pool[b * R:(b + 1) * R], stream=stream)
-        it = W + K + 4 + k
         if prop is not None:
             mses.append(cpx.train_step_proposal(scene, batch_rays, prop, losses, it, start=0, length=R,
                                                 mask_coef=STEP["mask_coef"], huber_delta=STEP["huber"],
@@ -463,6 +517,8 @@ def run_ours(args, wl, world, rank, local):
     e1.record(stream)
     torch.cuda.synchronize()
     scene.check()
+    for extra in bufs[1:]:
+        extra.close()
     e2e_ms = dist_max(e0.elapsed_time(e1), world, True)
     e2e_value = world * R * K / (e2e_ms / 1e3)
 
@@ -525,6 +581,7 @@ def run_ours(args, wl, world, rank, local):
                             R, wl["cams"], wl["img"], wl["img"], wl["gt_n"], wl["n_blobs"])),
             "grid": n, "sh_dim": SH_DIM, "batch_rays": R, "pool_rays": P, "step_constants": STEP,
             "precision": args.precision, "form": args.form, "march_options": args.march_options,
+            "look_ahead": ahead,
             "proposal_schedule": PROPOSAL if prop is not None else None,
             "start_batch": W, "lr_decay": "reference per batch (Render.cu:499-500)" if decay else "none",
             "l2": "inputs larger than L2: the sweep streams %.1f GB of grid state per step" % (alg_bytes / 1e9),
@@ -532,7 +589,11 @@ def run_ours(args, wl, world, rank, local):
         },
         "roofline": roofline,
         "kernels_ms": {"march_fwd_bwd" if prop is None else "proposal_and_march": round(march_ms, 4),
-                       "tv_adam_sweep": round(sweep_ms, 4)},
+                       "tv_adam_sweep": round(sweep_ms, 4),
+                       "timed_in": "split leg after the timed region (march, then sweep)" if ahead else "timed region"},
+        "step_form": ("cpx_train_step_ahead: the next batch placed beside each step's sweep; split leg (placement, "
+                      "shading, sweep one after the other) %.4f ms per step" % split_ms) if ahead else
+                     "march then sweep",
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": R * RAY_BYTES,
                 "d2h_bytes_per_step": 8, "last_mse": mses[-1]},
         "gpu_launches": int(launches),
@@ -854,6 +915,10 @@ def quality_run(args, wl, local, prec=None, form=None, n_batches=None, repeat=No
                           timestep=k + 1, want_mse=False)
             if prop is not None:
                 cpx.train_step_proposal(scene, pool, prop, losses, k, **common, **PROPOSAL)
+            elif rprec == "fp32" and not args.no_ahead and wl.get("sparse_threshold") is None:
+                # the plain form's fastest path: the next batch placed beside each sweep
+                nb = (k + 1) % batches
+                cpx.train_step_ahead(scene, pool, losses, next_rays=pool, next_start=nb * R, next_length=R, **common)
             else:
                 cpx.train_step(scene, pool, losses, **common)
             # the reference's per-batch learning-rate decay (Render.cu:499-500)
@@ -1124,6 +1189,9 @@ def main():
                     help="time the window after N untimed training batches with the reference's learning-rate "
                          "decay (a mid-run step; the proposal form otherwise times batches 110-130)")
     ap.add_argument("--no-repeat", action="store_true", help="quality run: skip the second plain FP32 run")
+    ap.add_argument("--no-ahead", action="store_true",
+                    help="step the plain FP32 form with cpx_train_step (no placement of the next batch beside "
+                         "the sweep)")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the mixed + proposal leg of the default line (forms.proposal)")
     ap.add_argument("--forms-batches", type=int, default=2000,

@@ -54,7 +54,7 @@ EXPORTED = [
     "cpx_occupancy_build", "cpx_grid_download_occupancy", "cpx_grid_make_sparse", "cpx_rays_create", "cpx_rays_destroy",
     "cpx_rays_upload", "cpx_rays_upload_packed", "cpx_rays_download", "cpx_rays_init_camera",
     "cpx_render_forward", "cpx_render_backward", "cpx_render_forward_backward", "cpx_tv_grad",
-    "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_grid_check",
+    "cpx_adam_step", "cpx_tv_adam_step", "cpx_train_step", "cpx_train_step_ahead", "cpx_grid_check",
     "cpx_last_sample_counts", "cpx_kernel_launches", "cpx_render_forward_backward_noalloc",
     "cpx_render_image", "cpx_image_mse", "cpx_grid_touched_count", "cpx_grid_download_cell_map",
     "cpx_proposal_param_count", "cpx_proposal_create", "cpx_proposal_destroy", "cpx_proposal_params",
@@ -166,6 +166,8 @@ _sig("cpx_adam_step", [_vp, C.c_double, C.c_double, C.c_int, _vp])
 _sig("cpx_tv_adam_step", [_vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _vp])
 _sig("cpx_train_step", [_vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), _vp,
                         C.POINTER(C.c_double), _vp])
+_sig("cpx_train_step_ahead", [_vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), _vp,
+                              C.POINTER(C.c_double), _vp])
 _sig("cpx_last_sample_counts", [_vp, _i32p, C.c_int])
 _sig("cpx_render_image", [_vp, C.POINTER(Camera), C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp])
 _sig("cpx_image_mse", [_vp, _vp, C.c_int64, C.POINTER(C.c_double), _vp])
@@ -879,6 +881,34 @@ def train_step(scene: ObjectScene, rays: Rays, losses, *, start: int = 0, length
     _check(_lib.cpx_train_step(scene.handle, rays.handle, _ptr(sample_index), int(start), n, C.byref(a),
                                _ptr(losses), C.byref(mse) if want_mse else None, _stream(stream)),
            "train_step")
+    return mse.value if want_mse else None
+
+
+def train_step_ahead(scene: ObjectScene, rays: Rays, losses, *, start: int = 0, length: int | None = None,
+                     sample_index=None, next_rays: Rays | None = None, next_start: int = 0, next_length: int = 0,
+                     next_sample_index=None, mask_coef: float = 1.0, huber_delta: float = 0.1, do_tv: bool = True,
+                     tv_type: int = 0, tv_neighbours: int = 6, lam_density: float = 1e-5, lam_sh: float = 1e-6,
+                     lr: float = 0.3, sh_lr: float = 1.0, timestep: int = 1, want_mse: bool = True, stream=None):
+    """train_step that also places the next batch's samples while the optimizer sweep runs (the
+    next call with that batch shades it at once); returns the batch MSE."""
+    a = StepArgs()
+    a.mask_coef = float(mask_coef)
+    a.huber_delta = float(huber_delta)
+    a.do_tv = 1 if do_tv else 0
+    a.tv_type = int(tv_type)
+    a.tv_neighbours = int(tv_neighbours)
+    a.lam_density = float(lam_density)
+    a.lam_sh = float(lam_sh)
+    a.lr = float(lr)
+    a.sh_lr = float(sh_lr)
+    a.timestep = int(timestep)
+    n = _len(rays, start, length)
+    mse = C.c_double(0.0)
+    _check(_lib.cpx_train_step_ahead(scene.handle, rays.handle, _ptr(sample_index), int(start), n,
+                                     None if next_rays is None else next_rays.handle, _ptr(next_sample_index),
+                                     int(next_start), int(next_length), C.byref(a), _ptr(losses),
+                                     C.byref(mse) if want_mse else None, _stream(stream)),
+           "train_step_ahead")
     return mse.value if want_mse else None
 
 

@@ -5,6 +5,8 @@
 // the order of launches of one training batch (SVRF/Render.cu:407-500).
 #include "cpx_internal.cuh"
 
+#include <utility>
+
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -252,6 +254,14 @@ static void free_grid(cpx_grid* g)
     cudaFree(g->scratch.queue);
     cudaFree(g->scratch.err);
     cudaFree(g->scratch.mse);
+    cudaFree(g->scratch2.samples);  // its error flags and MSE word are the first scratch's
+    cudaFree(g->scratch2.colours);
+    cudaFree(g->scratch2.counts);
+    cudaFree(g->scratch2.acc);
+    cudaFree(g->scratch2.queue);
+    if (g->aside) cudaStreamDestroy(g->aside);
+    if (g->ev_fork) cudaEventDestroy(g->ev_fork);
+    if (g->ev_join) cudaEventDestroy(g->ev_join);
 }
 
 // Zeroed per-vertex state of `n` active vertices in the grid's storage form.
@@ -415,6 +425,7 @@ cpx_status cpx_grid_info(const cpx_grid* g, int64_t* n_active, int* n_arrays, in
 
 cpx_status cpx_grid_upload_params(cpx_grid* g, const float* planar, int64_t n)
 {
+    if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (check_grid(g) || !planar) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
     return planar_to_records(g, kParams, planar, n);
@@ -422,6 +433,7 @@ cpx_status cpx_grid_upload_params(cpx_grid* g, const float* planar, int64_t n)
 
 cpx_status cpx_grid_upload_params_device(cpx_grid* g, const float* planar_dev, int64_t n)
 {
+    if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (check_grid(g) || !planar_dev) return CPX_ERR_INVALID_ARGUMENT;
     if (check_n(g, n)) return CPX_ERR_INVALID_ARGUMENT;
     for (int a = 0; a < g->n_arrays; a++) set_column(g, kParams, planar_dev + (int64_t)a * n, n, a);
@@ -486,6 +498,7 @@ cpx_status cpx_grid_set_adaptive_lr(cpx_grid* g, const float* lr_mult, int64_t n
 cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const double* oy,
                                        const double* oz, int n)
 {
+    if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (check_grid(g) || n < 0 || (n > 0 && (!ox || !oy || !oz))) return CPX_ERR_INVALID_ARGUMENT;
     cudaDeviceSynchronize();
     for (int i = 0; i < 3; i++) {
@@ -506,6 +519,7 @@ cpx_status cpx_grid_set_sample_offsets(cpx_grid* g, const double* ox, const doub
 
 cpx_status cpx_grid_set_options(cpx_grid* g, int options)
 {
+    if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH | CPX_OPT_NO_EARLY_STOP | CPX_OPT_FUSED_MARCH |
                                    CPX_OPT_PLANE_SWEEP))) return CPX_ERR_INVALID_ARGUMENT;
     g->options = options;
@@ -525,6 +539,7 @@ cpx_status cpx_occupancy_build(cpx_grid* g, float threshold, uint8_t* occupancy_
                                uint8_t* in_cage_out, uint32_t* index_offsets_out,
                                uint32_t* in_cage_count_out)
 {
+    if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
     if (g->sparse) {
         set_error("occupancy is built from a dense grid");
@@ -547,6 +562,7 @@ cpx_status cpx_occupancy_build(cpx_grid* g, float threshold, uint8_t* occupancy_
 
 cpx_status cpx_grid_make_sparse(cpx_grid* g)
 {
+    if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (check_grid(g)) return CPX_ERR_INVALID_ARGUMENT;
     return make_sparse_launch(g);
 }
@@ -612,6 +628,7 @@ cpx_status cpx_rays_upload(cpx_rays* r, int64_t offset, int64_t count, const flo
                            const uint8_t* gt_mask, const uint8_t* gt_r, const uint8_t* gt_g,
                            const uint8_t* gt_b, cpx_stream stream)
 {
+    if (r) ++r->epoch;  // the ray fields change: a placement done in advance is stale
     if (!range_ok(r, offset, count)) return CPX_ERR_INVALID_ARGUMENT;
     cudaStream_t st = (cudaStream_t)stream;
     const float* fs[8] = {ox, oy, oz, dx, dy, dz, near_t, far_t};
@@ -630,6 +647,7 @@ cpx_status cpx_rays_upload(cpx_rays* r, int64_t offset, int64_t count, const flo
 cpx_status cpx_rays_upload_packed(cpx_rays* r, int64_t offset, int64_t count,
                                   const uint32_t* packed, cpx_stream stream)
 {
+    if (r) ++r->epoch;  // the ray fields change: a placement done in advance is stale
     if (!range_ok(r, offset, count) || (!packed && count > 0)) return CPX_ERR_INVALID_ARGUMENT;
     if (count == 0) return CPX_OK;
     cudaStream_t st = (cudaStream_t)stream;
@@ -676,6 +694,7 @@ cpx_status cpx_rays_init_camera(cpx_rays* r, const cpx_grid* g, const cpx_camera
                                 const uint8_t* blue, const uint8_t* gt_mask,
                                 const int32_t* pixel_index, int64_t n_pix, int64_t offset)
 {
+    if (r) ++r->epoch;  // the ray fields change: a placement done in advance is stale
     if (check_grid(g) || !cam || !red || !green || !blue || (!pixel_index && n_pix > 0) ||
         img_w <= 0 || img_h <= 0)
         return CPX_ERR_INVALID_ARGUMENT;
@@ -793,6 +812,69 @@ cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int sta
         if (s != CPX_OK) return s;
         cudaError_t e = cudaMemcpyAsync(mse_out, g->scratch.mse, sizeof(double),
                                         cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_status(e, "mse");
+    }
+    return CPX_OK;
+}
+
+cpx_status cpx_train_step_ahead(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                                cpx_rays* next_r, const int32_t* next_sidx, int next_start, int next_len,
+                                const cpx_step_args* a, double* losses, double* mse_out, cpx_stream stream)
+{
+    if (check_grid(g) || !r || !a) return CPX_ERR_INVALID_ARGUMENT;
+    if (a->timestep < 1) {
+        set_error("timestep starts at 1");
+        return CPX_ERR_INVALID_ARGUMENT;
+    }
+    const bool fuse = a->do_tv && a->tv_type == 0 && a->tv_neighbours == 6;
+    const bool ahead_ok = g->prec == kPrecFP32 && !g->sparse && g->rec == 28 && (fuse || !a->do_tv) &&
+                          !(g->options & (CPX_OPT_FUSED_MARCH | CPX_OPT_FP32_MARCH)) && next_r && next_len > 0 &&
+                          len > 0;
+    if (!ahead_ok) {  // the plain step: nothing is placed in advance
+        g->ahead.valid = 0;
+        return cpx_train_step(g, r, sidx, start, len, a, losses, mse_out, stream);
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // this batch: only its shading when the last step placed it on the current densities
+    const bool placed = g->ahead.valid && g->ahead.r == r && g->ahead.rays_epoch == r->epoch && g->ahead.sidx == sidx &&
+                        g->ahead.start == start && g->ahead.len == len && g->ahead.epoch == g->epoch;
+    g->ahead.valid = 0;
+    if (placed) std::swap(g->scratch, g->scratch2);  // the placed batch becomes the grid's own scratch
+    g->last_len = len;
+    cpx_status s = march_launch_stages(g, r, sidx, start, len, losses, a->mask_coef, a->huber_delta, 0,
+                                       placed ? 2 : 3, st);
+    if (s != CPX_OK) return s;
+    // the densities the sweep will write, then the next batch's placement on them beside the sweep
+    s = density_preview(g, fuse, a->lam_density, a->lam_sh, a->lr, a->sh_lr, a->timestep, st);
+    if (s != CPX_OK) return s;
+    cudaError_t e = cudaSuccess;
+    if (!g->aside) e = cudaStreamCreateWithFlags(&g->aside, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !g->ev_fork) e = cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !g->ev_join) e = cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(g->ev_fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(g->aside, g->ev_fork, 0);
+    if (e != cudaSuccess) return cuda_status(e, "look-ahead stream");
+    s = march_launch_stages(g, next_r, next_sidx, next_start, next_len, losses, a->mask_coef, a->huber_delta, 1, 1,
+                            g->aside);
+    if (s != CPX_OK) return s;
+    e = cudaEventRecord(g->ev_join, g->aside);
+    if (e != cudaSuccess) return cuda_status(e, "look-ahead join");
+    s = sweep_adam(g, fuse, a->lam_density, a->lam_sh, a->lr, a->sh_lr, a->timestep, st);
+    if (s != CPX_OK) return s;
+    e = cudaStreamWaitEvent(st, g->ev_join, 0);  // work after this step sees the placement done
+    if (e != cudaSuccess) return cuda_status(e, "look-ahead join");
+    g->ahead.valid = 1;
+    g->ahead.r = next_r;
+    g->ahead.rays_epoch = next_r->epoch;
+    g->ahead.sidx = next_sidx;
+    g->ahead.start = next_start;
+    g->ahead.len = next_len;
+    g->ahead.epoch = g->epoch;
+    if (mse_out) {
+        s = mse_launch(losses, len, g->scratch.mse, st);
+        if (s != CPX_OK) return s;
+        e = cudaMemcpyAsync(mse_out, g->scratch.mse, sizeof(double), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_status(e, "mse");
     }

@@ -117,6 +117,7 @@ extern "C" cpx_status cpx_carve_silhouette(cpx_grid* g, const double* projection
                                            const uint8_t* red, const uint8_t* green, const uint8_t* blue,
                                            const uint8_t* mask, int radius, cpx_stream stream)
 {
+    if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (!g || !projection || !red || !green || !blue || img_w < 1 || img_h < 1 || radius < 0) {
         set_error("carving needs a grid, a projection, three colour planes and a radius >= 0");
         return CPX_ERR_INVALID_ARGUMENT;

@@ -156,6 +156,22 @@ struct cpx_grid {
     int sobol_n = 0;
     cpx::MarchScratch scratch;
     int last_len = 0;
+    // The look-ahead step (cpx_train_step_ahead): a second sample scratch, the batch it holds
+    // placed in advance, and the side stream that placed it.  `epoch` counts every change of
+    // what placement reads (densities, jitter offsets, occupancy, march options); a placement
+    // done in advance is used only while the epoch and its rays' epoch are unchanged.
+    cpx::MarchScratch scratch2;
+    uint64_t epoch = 0;
+    struct {
+        int valid = 0;
+        const cpx_rays* r = nullptr;
+        uint64_t rays_epoch = 0;
+        const int32_t* sidx = nullptr;
+        int start = 0, len = 0;
+        uint64_t epoch = 0;
+    } ahead;
+    cudaStream_t aside = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 struct cpx_rays {
@@ -167,6 +183,7 @@ struct cpx_rays {
     float *acc_den, *acc_w, *acc_r, *acc_g, *acc_b;
     uint32_t* staging = nullptr;  // device copy of the last packed upload
     int64_t staging_cap = 0;
+    uint64_t epoch = 0;  // counts every change of the ray fields (a placement done in advance checks it)
 };
 
 namespace cpx {
@@ -374,6 +391,14 @@ void free_state(cpx_grid* g);
 cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                         int mode, double* losses, double mask_coef, float huber,
                         cudaStream_t s);
+// The forward+backward march in stages (bit 0: placement, bit 1: shading) on scratch `which`
+// (0: the grid's own, 1: the look-ahead step's second one).
+cpx_status march_launch_stages(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len, double* losses,
+                               double mask_coef, float huber, int which, int stages, cudaStream_t st);
+// sweep.cu: the densities the next FP32 dense sweep will write (TV type 0/6 fused when
+// fused_tv, else none), written to the density mirror ahead of the sweep, bit for bit.
+cpx_status density_preview(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
+                           int timestep, cudaStream_t st);
 cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                              int mode, double* losses, double mask_coef, float huber,
                              const MarchScratch& s, cudaStream_t st);

@@ -85,6 +85,7 @@ using namespace cpx;
 extern "C" cpx_status cpx_grid_fill_sample_offsets(cpx_grid* g, float radius, const uint32_t* seeds,
                                                    cpx_stream stream)
 {
+    if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (!g || !seeds || !(radius >= 0.f)) {
         set_error("fill_sample_offsets: null grid or seeds, or negative radius");
         return CPX_ERR_INVALID_ARGUMENT;

@@ -1084,18 +1084,23 @@ static int max_samples_per_ray(const cpx_grid* g)
     return (((int)ceil((diag + 2.0) / g->step) + 8) + 3) & ~3;
 }
 
-static cpx_status ensure_scratch(cpx_grid* g, int len)
+// The grid's march scratch `which` (0: the march's own; 1: the look-ahead step's second one,
+// which shares the error flags and the MSE word of the first) with room for len rays.
+static cpx_status ensure_scratch(cpx_grid* g, int len, int which = 0)
 {
-    MarchScratch& s = g->scratch;
     const int maxs = max_samples_per_ray(g);
-    if (s.err == nullptr) {
-        if (cudaMalloc((void**)&s.err, sizeof(int) * 4) != cudaSuccess ||
-            cudaMalloc((void**)&s.mse, sizeof(double)) != cudaSuccess) {
+    MarchScratch& s0 = g->scratch;
+    if (s0.err == nullptr) {
+        if (cudaMalloc((void**)&s0.err, sizeof(int) * 4) != cudaSuccess ||
+            cudaMalloc((void**)&s0.mse, sizeof(double)) != cudaSuccess) {
             set_error("scratch allocation failed");
             return CPX_ERR_OUT_OF_MEMORY;
         }
-        cudaMemset(s.err, 0, sizeof(int) * 4);
+        cudaMemset(s0.err, 0, sizeof(int) * 4);
     }
+    MarchScratch& s = which ? g->scratch2 : g->scratch;
+    s.err = s0.err;
+    s.mse = s0.mse;
     if (s.cap_rays >= len && s.maxs == maxs) return CPX_OK;
     cudaFree(s.samples);
     cudaFree(s.colours);
@@ -1131,6 +1136,7 @@ struct Guide {
     Skip skip;
     bool march32 = false;  // the FP32 march of the mixed forms (else the reference's sequence)
     bool two_stage = true;  // placement and shading as two launches (else the fused march, CPX_OPT_FUSED_MARCH)
+    int stages = 3;         // bit 0: placement, bit 1: shading (a look-ahead step runs them apart)
     bool on() const { return masks != nullptr || seg_w != nullptr; }
 };
 
@@ -1182,7 +1188,9 @@ static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv,
     const dim3 pgrid((unsigned)((len + 31) / 32));
     const dim3 sgrid((unsigned)((len + kShadeWarps - 1) / kShadeWarps));
     const dim3 sblock(kShadeWarps * 32);
-    if (guide.march32 && guide.on())
+    if (!(guide.stages & 1)) {
+        // placement already done (a look-ahead step placed this batch under the last sweep)
+    } else if (guide.march32 && guide.on())
         k_place<MODE, float, true><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
                                                          s.counts, s.acc, s.err, guide.masks, guide.seg_w, guide.skip);
     else if (guide.march32)
@@ -1191,6 +1199,7 @@ static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv,
     else
         k_place<MODE, double, false><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
                                                            s.counts, s.acc, s.err, nullptr, nullptr, guide.skip);
+    if (!(guide.stages & 2)) return;
     if (s.queue) {
         // longest rays first from a work counter (the queue's first word and its ray slots)
         static int resident = 0;  // per instance
@@ -1289,7 +1298,7 @@ static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32
     if (rc != CPX_OK || len == 0) return rc;
     Guide gd = guide;
     gd.march32 = g->prec != kPrecFP32 || (g->options & CPX_OPT_FP32_MARCH);
-    gd.two_stage = !(g->options & CPX_OPT_FUSED_MARCH) || s.queue == nullptr;
+    gd.two_stage = !(g->options & CPX_OPT_FUSED_MARCH) || s.queue == nullptr || guide.stages != 3;
     if (guide.on() && !gd.march32) {
         set_error("the proposal-guided march runs on the FP32 march of the mixed forms only");
         return CPX_ERR_UNSUPPORTED;
@@ -1323,8 +1332,22 @@ static cpx_status march_launch_guided_with(cpx_grid* g, cpx_rays* r, const int32
         rc = launch_prec<kPrecFP16>(g->sh_dim, mode, st, gv, rv, sidx, start, len, r->n, s, losses, mask_coef, huber,
                                     touched, gd);
     if (rc != CPX_OK) return rc;
-    count_launch(2);
+    count_launch((gd.stages & 1) + ((gd.stages >> 1) & 1));
     return cuda_status(cudaGetLastError(), "march");
+}
+
+cpx_status march_launch_stages(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len, double* losses,
+                               double mask_coef, float huber, int which, int stages, cudaStream_t st)
+{
+    cpx_status rc = march_check_args(g, r, sidx, start, len, kForwardBackward, losses);
+    if (rc != CPX_OK) return rc;
+    if (len == 0) return CPX_OK;
+    rc = ensure_scratch(g, len, which);
+    if (rc != CPX_OK) return rc;
+    Guide guide;
+    guide.stages = stages;
+    return march_launch_guided_with(g, r, sidx, start, len, kForwardBackward, losses, mask_coef, huber,
+                                    which ? g->scratch2 : g->scratch, guide, st);
 }
 
 cpx_status march_launch(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,

@@ -377,6 +377,7 @@ cpx_status cpx_ray_source_keys(const cpx_ray_source* s, uint32_t* keys, int* hal
 cpx_status cpx_ray_source_generate(cpx_ray_source* s, const cpx_grid* g, int64_t start, int len, cpx_rays* batch,
                                    cpx_stream stream)
 {
+    if (batch) ++batch->epoch;  // new ray fields: a placement done in advance is stale
     if (!s || !g || !batch || len < 0 || start < 0 || start + len > s->a.n || len > batch->n) {
         set_error("batch [%lld, +%d) outside the source's %lld samples or the ray buffer", (long long)start, len,
                   s ? (long long)s->a.n : 0ll);

@@ -187,6 +187,43 @@ __global__ void __launch_bounds__(256) k_sweep_dense(SweepArgs a)
     sweep_dense_row<S, TV>(a, blockIdx.x, s_bc);
 }
 
+// The density each vertex of a dense FP32 grid will have after the next sweep, written to the
+// density mirror ahead of that sweep: slot 0's TV + Adam (slot_update on the same operands, so
+// the same bits the sweep writes), nothing else stored.  A look-ahead step places the next
+// batch's samples on these densities while the sweep itself runs.
+template <int S, bool TV>
+__global__ void __launch_bounds__(256) k_density_preview(SweepArgs a)
+{
+    __shared__ float s_bc[2];
+    bias_corrections(a.timestep, a.t_dev, s_bc);
+    const uint32_t WH = (uint32_t)a.W * a.H;
+    const uint32_t n = WH * (uint32_t)a.D;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t x = v % (uint32_t)a.W;
+        const uint32_t y = (v / (uint32_t)a.W) % (uint32_t)a.H;
+        const uint32_t z = v / WH;
+        const bool tv_on = y >= 1 && y + 2 <= (uint32_t)a.H && z >= 1 && z + 2 <= (uint32_t)a.D && x >= 1 &&
+                           x + 2 <= (uint32_t)a.W;
+        const uint32_t sl = v * S;
+        const float4 p = a.p_in[sl];
+        float4 g = touched_bit(a.touched, v) ? a.grad[sl] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 m = a.m[sl];
+        float4 vv = a.v[sl];
+        float4 nbv[6];
+        if (TV && tv_on) {
+            nbv[0] = a.p_in[sl - WH * S];
+            nbv[1] = a.p_in[sl - (uint32_t)a.W * S];
+            nbv[2] = a.p_in[sl - S];
+            nbv[3] = a.p_in[sl + S];
+            nbv[4] = a.p_in[sl + (uint32_t)a.W * S];
+            nbv[5] = a.p_in[sl + WH * S];
+        }
+        const float lr_d = a.adaptive_lr ? a.lr * a.adaptive_lr[v] : a.lr;
+        const float4 pn = slot_update<TV>(a, 0, tv_on, p, nbv, g, m, vv, s_bc[0], s_bc[1], lr_d);
+        a.density_out[v] = pn.x;
+    }
+}
+
 // The row sweeps of many dense FP32 grids (the batched form) in one launch: block b takes row b
 // of the concatenated row lists, its grid found by binary search over the first rows.
 struct SweepBatch {
@@ -415,6 +452,7 @@ static SweepArgs sweep_args(const cpx_grid* g, double lam_d, double lam_sh, doub
 cpx_status sweep_adam(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr,
                       double sh_lr, int timestep, cudaStream_t st, const int* t_dev)
 {
+    ++g->epoch;  // new densities: a placement done in advance on the old ones is stale
     if (g->n_act == 0) return CPX_OK;
     if (g->prec != kPrecFP32) {
         uint32_t tvm, am;
@@ -476,6 +514,27 @@ static SweepArgs sweep_args(const cpx_grid* g, double lam_d, double lam_sh, doub
     return a;
 }
 
+cpx_status density_preview(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
+                           int timestep, cudaStream_t st)
+{
+    if (g->prec != kPrecFP32 || g->sparse || g->rec != 28 || g->n_act * 7 >= ((int64_t)1 << 32)) {
+        set_error("the density preview runs on dense FP32 grids of SH band 2");
+        return CPX_ERR_UNSUPPORTED;
+    }
+    const SweepArgs a = sweep_args(g, lam_d, lam_sh, lr, sh_lr, timestep, nullptr);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t want = (g->n_act + 255) / 256;
+    const unsigned blocks = (unsigned)(want < (int64_t)sms * 8 ? want : (int64_t)sms * 8);
+    if (fused_tv)
+        k_density_preview<7, true><<<blocks, 256, 0, st>>>(a);
+    else
+        k_density_preview<7, false><<<blocks, 256, 0, st>>>(a);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "density preview");
+}
+
 bool sweep_batchable(const cpx_grid* g, bool fused_tv)
 {
     return fused_tv && g->prec == kPrecFP32 && !g->sparse && g->rec == 28 && g->n_act > 0 &&
@@ -510,6 +569,7 @@ cpx_status sweep_batched_launch(cpx_grid* const* grids, int n, const void* dev_t
     count_launch();
     for (int i = 0; i < n; i++) {
         cpx_grid* g = grids[i];
+        ++g->epoch;
         g->cur ^= 1;
         g->tcur ^= 1;
         g->all_touched = 0;

@@ -111,6 +111,7 @@ using namespace cpx;
 extern "C" cpx_status cpx_grid_upsample(const cpx_grid* src, cpx_grid* dst, float threshold, int low_band_only,
                                         cpx_stream stream)
 {
+    if (dst) ++dst->epoch;  // new densities: a placement done in advance is stale
     if (!src || !dst) {
         set_error("null grid handle");
         return CPX_ERR_INVALID_ARGUMENT;

@@ -434,6 +434,23 @@ typedef struct cpx_step_args {
 cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev, int start,
                           int len, const cpx_step_args* args, double* losses_dev,
                           double* mse_out, cpx_stream stream);
+/* cpx_train_step (the reference's batch, SVRF/Render.cu:407-500) that also places the NEXT
+ * batch's samples while this batch's optimizer sweep runs: after this batch's march, the
+ * densities the sweep will write are worked out first (bit-identical to the sweep's), and a
+ * second stream places next_r's rays [next_start, next_start + next_len) on them beside the
+ * sweep.  The next call with that batch then only shades it.  Results are those of
+ * cpx_train_step bit for bit in every placed sample; placement, which is one dependent chain per
+ * ray and keeps the GPU mostly idle, no longer adds to the step.  The placement done in advance
+ * is used only if nothing it read has changed: any call that changes the grid's densities,
+ * jitter offsets, occupancy or march options, or the next batch's ray fields, makes the next
+ * call place the batch itself.  It applies to dense FP32 grids of SH band 2 with TV type 0/6 (or
+ * none) in the reference's march; elsewhere (or with next_r NULL) the call is cpx_train_step.
+ * The next batch's sample index and ray buffers must stay valid until the next call.  No
+ * reference counterpart beyond the batch it replaces. */
+cpx_status cpx_train_step_ahead(cpx_grid* g, cpx_rays* r, const int32_t* sample_index_dev, int start, int len,
+                                cpx_rays* next_r, const int32_t* next_sample_index_dev, int next_start,
+                                int next_len, const cpx_step_args* args, double* losses_dev, double* mse_out,
+                                cpx_stream stream);
 
 /* Synchronise the grid's work and report (then clear) the sticky device-side errors of
  * earlier asynchronous calls: CPX_ERR_ITERATION_CAP when a ray's march exceeded its
