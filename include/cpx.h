@@ -293,8 +293,10 @@ cpx_status cpx_render_forward_backward(cpx_grid* g, cpx_rays* r, double* losses_
  * bound), larger batches return CPX_ERR_INVALID_ARGUMENT.  The first call on a device looks
  * up the array's device address; make that first call before any stream capture.  Every
  * call on a device shares the array and overwrites it, so calls that overlap on the GPU
- * race.  The call returns once the batch has run, with the status of its device-side
- * checks; cpx_last_sample_counts does not see its counts. */
+ * race.  The call synchronises its stream: it reads its device-side check flags back and
+ * returns once the batch has run, with their status; cpx_last_sample_counts does not see its
+ * counts.  The array's address is looked up once per device and kept for the life of the
+ * process, so the library is not for use across a cudaDeviceReset. */
 cpx_status cpx_render_forward_backward_noalloc(cpx_grid* g, cpx_rays* r, double* losses_dev,
                                                const int32_t* sample_index_dev, int start,
                                                int len, double mask_coef, float huber_delta,
