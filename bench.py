@@ -394,10 +394,11 @@ def run_ours(args, wl, world, rank, local):
         if decay:  # Render.cu:499-500
             lr[:] = [cpx.lr_decay(x, wl["pool_batches"], k // wl["pool_batches"]) for x in lr]
 
-    # the plain FP32 form steps with cpx_train_step_ahead: each step places the next batch's samples
-    # beside its own optimizer sweep (the product's fastest path); the march and the sweep are then
-    # timed apart in a split leg after the timed region
-    ahead = prop is None and args.precision == "fp32" and thr is None and not args.no_ahead
+    # --ahead: the plain FP32 form steps with cpx_train_step_ahead, each step placing the next batch's
+    # samples beside its own optimizer sweep; the march and the sweep are then timed apart in a split
+    # leg after the timed region.  Measured slower than march-then-sweep on the 256^3 workload (the
+    # density preview it needs costs more than the placement it hides), so it is not the default.
+    ahead = prop is None and args.precision == "fp32" and thr is None and args.ahead
 
     def step_ahead(k):
         b, nb = k % wl["pool_batches"], (k + 1) % wl["pool_batches"]
@@ -915,8 +916,8 @@ def quality_run(args, wl, local, prec=None, form=None, n_batches=None, repeat=No
                           timestep=k + 1, want_mse=False)
             if prop is not None:
                 cpx.train_step_proposal(scene, pool, prop, losses, k, **common, **PROPOSAL)
-            elif rprec == "fp32" and not args.no_ahead and wl.get("sparse_threshold") is None:
-                # the plain form's fastest path: the next batch placed beside each sweep
+            elif rprec == "fp32" and args.ahead and wl.get("sparse_threshold") is None:
+                # --ahead: the next batch placed beside each sweep
                 nb = (k + 1) % batches
                 cpx.train_step_ahead(scene, pool, losses, next_rays=pool, next_start=nb * R, next_length=R, **common)
             else:
@@ -1189,9 +1190,9 @@ def main():
                     help="time the window after N untimed training batches with the reference's learning-rate "
                          "decay (a mid-run step; the proposal form otherwise times batches 110-130)")
     ap.add_argument("--no-repeat", action="store_true", help="quality run: skip the second plain FP32 run")
-    ap.add_argument("--no-ahead", action="store_true",
-                    help="step the plain FP32 form with cpx_train_step (no placement of the next batch beside "
-                         "the sweep)")
+    ap.add_argument("--ahead", action="store_true",
+                    help="step the plain FP32 form with cpx_train_step_ahead (the next batch's placement beside "
+                         "each sweep) instead of cpx_train_step")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the mixed + proposal leg of the default line (forms.proposal)")
     ap.add_argument("--forms-batches", type=int, default=2000,

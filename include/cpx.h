@@ -441,8 +441,11 @@ cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sample_index_
  * densities the sweep will write are worked out first (bit-identical to the sweep's), and a
  * second stream places next_r's rays [next_start, next_start + next_len) on them beside the
  * sweep.  The next call with that batch then only shades it.  Results are those of
- * cpx_train_step bit for bit in every placed sample; placement, which is one dependent chain per
- * ray and keeps the GPU mostly idle, no longer adds to the step.  The placement done in advance
+ * cpx_train_step bit for bit in every placed sample.  A comparison form: on the B200 at 256^3
+ * with 8192-ray batches it is slower than cpx_train_step (7.7 against 4.7 ms a step) -- working
+ * out the densities ahead reads a sector of every parameter, gradient and moment record and
+ * costs more than the placement it hides, and placement beside the bandwidth-bound sweep waits
+ * behind the sweep's traffic.  The placement done in advance
  * is used only if nothing it read has changed: any call that changes the grid's densities,
  * jitter offsets, occupancy or march options, or the next batch's ray fields, makes the next
  * call place the batch itself.  It applies to dense FP32 grids of SH band 2 with TV type 0/6 (or
