@@ -87,7 +87,7 @@ class GridDesc(C.Structure):
 
 
 # storage forms (cpx_precision)
-PRECISIONS = {"fp32": 0, "bf16": 1, "fp16": 2}
+PRECISIONS = {"fp32": 0, "bf16": 1, "fp16": 2, "fp16full": 3}
 
 
 class Camera(C.Structure):
@@ -282,8 +282,9 @@ class ObjectScene:
 
     def __init__(self, width, height, depth, sh_dim=9, optimizing_band=None, step_size=0.5,
                  hierarchy_strategy=False, bbox=None, precision="fp32", sr_seed=0):
-        """precision: "fp32" (the reference's form) or the mixed forms "bf16" / "fp16"
-        (16-bit SH and moments, FP32 density, gradients and march, stochastic rounding)."""
+        """precision: "fp32" (the reference's form) or the mixed forms "bf16" / "fp16" /
+        "fp16full" (16-bit SH and moments -- bfloat16 moments in "bf16" and "fp16", half moments
+        in "fp16full" -- FP32 density, gradients and march, stochastic rounding)."""
         if optimizing_band is None:
             optimizing_band = int(round(sh_dim ** 0.5)) - 1
         if bbox is None:  # initSelf: bbox spans the grid (SceneUtils.cu:107-112)

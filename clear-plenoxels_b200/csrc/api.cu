@@ -70,6 +70,27 @@ __global__ void k_get_column16(float* col, const uint16_t* recs, int64_t n, int 
     col[i] = sh_to_f<PREC>(recs[i * slots + e]);
 }
 
+// Moment column e of the half-moment form: m as m * 2^8, v through its root (sqrt(v) * 2^8),
+// rounded to nearest and saturating as the sweep's stores do.
+__global__ void k_set_moment16h(uint16_t* recs, const float* col, int64_t n, int slots, int e, int second)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float x = col[i];
+    if (second) x = sqrtf(x > 0.f ? x : 0.f);
+    x *= kMomScale;
+    x = x > 65504.f ? 65504.f : (x < -65504.f ? -65504.f : x);
+    recs[i * slots + e] = f_to_h16_rn(x);
+}
+
+__global__ void k_get_moment16h(float* col, const uint16_t* recs, int64_t n, int slots, int e, int second)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float x = h16_to_f(recs[i * slots + e]) * (1.f / kMomScale);
+    col[i] = second ? x * x : x;
+}
+
 // Number of set bits of a word array (block reduction, one atomic per block).
 __global__ void k_popcount(const uint32_t* __restrict__ w, int64_t n, unsigned long long* out)
 {
@@ -137,6 +158,8 @@ static void set_column(cpx_grid* g, Field f, const float* col, int64_t n, int a)
         return;
     } else if (f == kParams && g->prec == kPrecFP16) {
         k_set_column16<kPrecFP16><<<nb, 256>>>(g->sh16[g->cur], col, n, g->slots, a);
+    } else if (g->mom_h) {
+        k_set_moment16h<<<nb, 256>>>(f == kMoment1 ? g->m16 : g->v16, col, n, g->slots, a, f == kMoment2);
     } else {
         uint16_t* dst = f == kParams ? g->sh16[g->cur] : (f == kMoment1 ? g->m16 : g->v16);
         k_set_column16<kPrecBF16><<<nb, 256>>>(dst, col, n, g->slots, a);
@@ -157,6 +180,8 @@ static void get_column(const cpx_grid* g, Field f, float* col, int64_t n, int a)
         k_get_column<<<nb, 256>>>(col, g->dens[g->cur], n, 1, 0);
     } else if (f == kParams && g->prec == kPrecFP16) {
         k_get_column16<kPrecFP16><<<nb, 256>>>(col, g->sh16[g->cur], n, g->slots, a);
+    } else if (g->mom_h) {
+        k_get_moment16h<<<nb, 256>>>(col, f == kMoment1 ? g->m16 : g->v16, n, g->slots, a, f == kMoment2);
     } else {
         const uint16_t* src = f == kParams ? g->sh16[g->cur] : (f == kMoment1 ? g->m16 : g->v16);
         k_get_column16<kPrecBF16><<<nb, 256>>>(col, src, n, g->slots, a);
@@ -357,7 +382,7 @@ cpx_status cpx_grid_create(const cpx_grid_desc* d, cpx_grid** out)
         return CPX_ERR_INVALID_ARGUMENT;
     }
     if (d->precision != CPX_PRECISION_FP32 && d->precision != CPX_PRECISION_BF16 &&
-        d->precision != CPX_PRECISION_FP16) {
+        d->precision != CPX_PRECISION_FP16 && d->precision != CPX_PRECISION_FP16_FULL) {
         set_error("unknown precision %d", d->precision);
         return CPX_ERR_INVALID_ARGUMENT;
     }
@@ -376,7 +401,8 @@ cpx_status cpx_grid_create(const cpx_grid_desc* d, cpx_grid** out)
     for (int i = 0; i < 6; i++) g->bbox[i] = d->bbox[i];
     g->n_dense = n;
     g->n_act = n;
-    g->prec = d->precision;
+    g->prec = d->precision == CPX_PRECISION_FP16_FULL ? kPrecFP16 : d->precision;
+    g->mom_h = d->precision == CPX_PRECISION_FP16_FULL ? 1 : 0;
     g->sr_seed = d->sr_seed;
     g->slots = lowp_slots(g->n_arrays);
     cudaError_t e = alloc_state(g, n);
@@ -1022,6 +1048,10 @@ cpx_status cpx_grid_check(cpx_grid* g)
     }
     if (flags[0] & 8) {
         set_error("a shading warp of the fused march gave up waiting for a ray's placement");
+        return CPX_ERR_NOT_READY;
+    }
+    if (flags[0] & 32) {
+        set_error("a shading warp gave up waiting for a vertex record copy");
         return CPX_ERR_NOT_READY;
     }
     return CPX_OK;

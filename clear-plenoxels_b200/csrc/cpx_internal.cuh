@@ -101,7 +101,8 @@ struct cpx_grid {
     int bbox[6];
     int64_t n_dense, n_act;
     int sparse = 0;
-    int prec = 0;          // cpx_precision
+    int prec = 0;          // storage form: kPrecFP32, kPrecBF16 or kPrecFP16 (the SH storage)
+    int mom_h = 0;         // kPrecFP16 with both Adam moments in half (CPX_PRECISION_FP16_FULL)
     uint32_t sr_seed = 0;
     int slots = 0;         // 16-bit slots per record of the mixed forms
     float* params[2] = {nullptr, nullptr};  // FP32 form: parameter records, ping-pong

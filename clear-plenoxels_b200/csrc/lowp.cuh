@@ -110,6 +110,83 @@ __device__ __forceinline__ void unpack2(uint32_t w, float& lo, float& hi)
     }
 }
 
+// Stochastic rounding as sr_pack2, saturating: a value beyond the largest finite 16-bit number
+// lands on that number instead of infinity.
+template <int PREC>
+__device__ __forceinline__ uint32_t sr_pack2_sat(float lo, float hi, uint32_t rbits)
+{
+    uint32_t d;
+    if (PREC == kPrecFP16)
+        asm("cvt.rs.satfinite.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    else
+        asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+
+// The optimizer sweep's form "FP16 with half moments" (grid precision CPX_PRECISION_FP16_FULL):
+// SH in half as the FP16 form, and both Adam moments in half too.  Half spans about 12
+// decades (subnormals included) and the second moment v = E[g^2] of gradients between 1e-8
+// and 1 spans 16, so v is kept through its root: the records hold m * 2^8 and sqrt(v) * 2^8
+// (exact power-of-two scalings), with room for |m| and sqrt(v) from about 2.3e-10 (subnormal)
+// and 2.4e-7 (normal) up to 255.9, where the store saturates.  Internal to the sweeps; grids
+// carry it as precision FP16 with mom_h set.
+constexpr int kPrecFP16M = 3;
+constexpr float kMomScale = 256.f;
+
+// The SH storage of a sweep form.
+template <int PREC>
+__host__ __device__ constexpr int sh_prec()
+{
+    return PREC == kPrecFP16M ? kPrecFP16 : PREC;
+}
+
+__device__ __forceinline__ float sqrt_approx(float x)
+{
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// One 32-bit word of two first-moment values of sweep form PREC <-> floats.
+template <int PREC>
+__device__ __forceinline__ void mom1_unpack2(uint32_t w, float& lo, float& hi)
+{
+    if (PREC == kPrecFP16M) {
+        unpack2<kPrecFP16>(w, lo, hi);
+        lo *= 1.f / kMomScale;
+        hi *= 1.f / kMomScale;
+    } else {
+        unpack2<kPrecBF16>(w, lo, hi);
+    }
+}
+template <int PREC>
+__device__ __forceinline__ uint32_t mom1_pack2(float lo, float hi, uint32_t rbits)
+{
+    if (PREC == kPrecFP16M) return sr_pack2_sat<kPrecFP16>(lo * kMomScale, hi * kMomScale, rbits);
+    return sr_pack2<kPrecBF16>(lo, hi, rbits);
+}
+// ... and of two second-moment values (stored through their roots in the half form).
+template <int PREC>
+__device__ __forceinline__ void mom2_unpack2(uint32_t w, float& lo, float& hi)
+{
+    if (PREC == kPrecFP16M) {
+        unpack2<kPrecFP16>(w, lo, hi);
+        lo *= 1.f / kMomScale;
+        hi *= 1.f / kMomScale;
+        lo *= lo;
+        hi *= hi;
+    } else {
+        unpack2<kPrecBF16>(w, lo, hi);
+    }
+}
+template <int PREC>
+__device__ __forceinline__ uint32_t mom2_pack2(float lo, float hi, uint32_t rbits)
+{
+    if (PREC == kPrecFP16M)
+        return sr_pack2_sat<kPrecFP16>(sqrt_approx(lo) * kMomScale, sqrt_approx(hi) * kMomScale, rbits);
+    return sr_pack2<kPrecBF16>(lo, hi, rbits);
+}
+
 __device__ __forceinline__ uint2 pack4(const uint16_t* h)
 {
     return make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));

@@ -625,18 +625,231 @@ __device__ __forceinline__ void table_flush(const WarpTable& t, const GridView& 
     __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// Record passes through the copy engine (k_shade / k_shade_dyn).  A lane that gathers a
+// 112-byte vertex record with seven 16-byte loads costs the L1 one wavefront per load, and the
+// 32 lanes of a warp touch 32 different records, so the record passes dominated the shading's
+// L1 traffic.  Here each lane moves a whole record with one bulk copy instead: the forward
+// pulls the record into the lane's slot of a per-warp shared-memory stage (cp.async.bulk,
+// completing on the warp's mbarrier) and reads it back with conflict-free 16-byte shared loads
+// (records 112 B apart: the 8 lanes of a quarter-warp hit 8 distinct 4-bank groups); the flush
+// writes the gradient record into the slot and adds it to global memory with one bulk
+// reduction (cp.reduce.async.bulk .add.f32, element-wise atomic adds in L2) in place of seven
+// vector atomics.  The occupied table slots are listed first, so a pass moves up to 32 records
+// and a chunk's ~100 distinct vertices take about four passes.  Addresses and sizes are
+// multiples of 16 bytes.
+// ---------------------------------------------------------------------------
+struct Stage {
+    uint32_t smem;   // shared-window address of lane 0's record slot (lane l's at smem + l * record bytes)
+    uint32_t mbar;   // the warp's mbarrier (arrival count 1)
+    uint32_t phase;  // parity of the mbarrier phase the next pass waits for
+    int* err;        // error word: 32 = a record copy did not complete within the wait's limit
+    uint8_t* list;   // the warp's list of occupied table slots (tables of at most 256 slots)
+    bool ok;
+};
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_reduce_add(float* dst, uint32_t src, uint32_t bytes)
+{
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f32 [%0], [%1], %2;" ::"l"(dst), "r"(src),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// This thread's bulk reductions have read their shared-memory sources (the slot is free).
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// ... and have completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void proxy_fence_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect(uint32_t mbar, uint32_t bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(mbar),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// Waits for phase `parity` of the mbarrier, for about a second at most.  Each try suspends the
+// thread until the phase completes or for up to the hint (about 0.1 ms), so a wait costs a try
+// or two instead of a polling loop.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity), "r"(100000u)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1ll << 31)) return false;
+    }
+}
+
+__device__ __forceinline__ float4 lds128(uint32_t addr)
+{
+    float4 r;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w) : "r"(addr));
+    return r;
+}
+
+__device__ __forceinline__ void sts128(uint32_t addr, float a, float b, float c, float d)
+{
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+
+// The occupied slots of a table of at most 256 slots, in slot order, into list[0..nd); returns
+// nd (every lane).
+__device__ __forceinline__ int table_compact(const WarpTable& t, uint8_t* list, int lane)
+{
+    __syncwarp();
+    int nd = 0;
+    for (int base = 0; base < t.n; base += 32) {
+        const int s = base + lane;
+        const bool occ = t.keys[s] != kEmpty;
+        const uint32_t m = __ballot_sync(0xffffffffu, occ);
+        if (occ) list[nd + __popc(m & ((1u << lane) - 1u))] = (uint8_t)s;
+        nd += __popc(m);
+    }
+    __syncwarp();
+    return nd;
+}
+
+// The forward record pass of table_colours (FP32 records) through the stage: per pass of up to
+// 32 listed vertices, lane 0 announces the bytes of the pass's records, each vertex's lane
+// copies its record, the warp waits for the mbarrier's phase and forms the colours from shared
+// memory in the same order as table_colours.  Returns false (error word set) when a copy did
+// not complete within the wait's limit; the warp then stops shading.
+template <int NSH>
+__device__ __forceinline__ bool table_colours_bulk(const WarpTable& t, const GridView& g, const float* shs, int lane,
+                                                   Stage& st)
+{
+    using RS = RecShape<NSH>;
+    constexpr uint32_t kRecBytes = RS::REC * 4;
+    const uint32_t mine = st.smem + (uint32_t)lane * kRecBytes;
+    bulk_wait_read();  // the slot's last bulk reduction has read it
+    proxy_fence_smem();
+    const int nd = table_compact(t, st.list, lane);
+    for (int p0 = 0; p0 < nd; p0 += 32) {  // passes of up to 32 listed vertices
+        const int i = p0 + lane;
+        const bool occ = i < nd;
+        int s = 0;
+        uint32_t key = 0u;
+        if (occ) {
+            s = st.list[i];
+            key = t.keys[s];
+        }
+        if (lane == 0) mbar_expect(st.mbar, (uint32_t)(nd - p0 < 32 ? nd - p0 : 32) * kRecBytes);
+        if (occ) bulk_load(mine, g.params + (size_t)key * RS::REC, kRecBytes, st.mbar);
+        const bool done = __all_sync(0xffffffffu, mbar_wait_bounded(st.mbar, st.phase));
+        if (!done) {
+            if (lane == 0) atomicOr(st.err, 32);
+            mbar_wait_bounded(st.mbar, st.phase);  // one more bounded wait for the copies in flight
+            st.ok = false;
+            return false;
+        }
+        st.phase ^= 1u;
+        if (occ) {
+            float col[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int v = 0; v < RS::NV4; v++) {
+                const float4 p = lds128(mine + 16u * v);
+                const float pv[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int e = 4 * v + k;
+                    if (e >= 1 && e < RS::NA) {
+                        const int ch = (e - 1) / NSH;
+                        const int kk = (e - 1) % NSH;
+                        if (kk < g.n_sh_fwd) col[ch] = fmaf(pv[k], shs[kk], col[ch]);
+                    }
+                }
+            }
+            t.vb0[s] = col[0];
+            t.vb1[s] = col[1];
+            t.vb2[s] = col[2];
+        }
+        __syncwarp();
+        proxy_fence_smem();  // the shared reads above before the next pass's copies overwrite the slots
+    }
+    __syncwarp();
+    return true;
+}
+
+// The flush of table_flush through the stage: the lane of each listed vertex writes the
+// vertex's gradient record into its stage slot and adds it to the grid's gradient record with
+// one bulk reduction.
+template <int NSH>
+__device__ __forceinline__ void table_flush_bulk(const WarpTable& t, const GridView& g, const float* shs,
+                                                 uint32_t* touched, int lane, const Stage& st)
+{
+    using RS = RecShape<NSH>;
+    constexpr uint32_t kRecBytes = RS::REC * 4;
+    const uint32_t mine = st.smem + (uint32_t)lane * kRecBytes;
+    const int nd = table_compact(t, st.list, lane);
+    for (int i = lane; i < nd; i += 32) {
+        const int s = st.list[i];
+        const uint32_t key = t.keys[s];
+        const float va = t.va[s];
+        const float bch[3] = {t.vb0[s], t.vb1[s], t.vb2[s]};
+        bulk_wait_read();  // the slot's previous reduction has read it
+#pragma unroll
+        for (int q = 0; q < RS::NV4; q++) {
+            float e4[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int e = 4 * q + k;
+                float val = 0.f;
+                if (e == 0) {
+                    val = va;
+                } else if (e < RS::NA) {
+                    const int ch = (e - 1) / NSH;
+                    const int kk = (e - 1) % NSH;
+                    bool on = true;
+                    if (g.hierarchy) on = kk >= g.band * g.band && kk < g.n_sh_fwd;
+                    val = on ? bch[ch] * shs[kk] : 0.f;
+                }
+                e4[k] = val;
+            }
+            sts128(mine + 16u * q, e4[0], e4[1], e4[2], e4[3]);
+        }
+        proxy_fence_smem();  // the record's shared stores before the copy engine reads them
+        bulk_reduce_add(g.grad + (size_t)key * RS::REC, mine, kRecBytes);
+        atomicOr(touched + (key >> 5), 1u << (key & 31u));
+        t.keys[s] = kEmpty;
+        t.va[s] = 0.f;
+        t.vb0[s] = 0.f;
+        t.vb1[s] = 0.f;
+        t.vb2[s] = 0.f;
+    }
+    __syncwarp();
+}
+
 // Shade one ray with a whole warp: forward colour (lane per sample, warp reduction), then
 // the backward of renderRays_withGradients_RGBGPU (RenderUtils.cu:2145-2256) with warp prefix
 // scans for the running weight/colour sums and the merged gradient scatter.
 // SPL: samples a lane takes per chunk.  A chunk of 32 * SPL consecutive samples shares one
 // table (of kHashSlots * SPL slots), so its distinct vertices are gathered and scattered once;
 // the scans still run over 32 samples at a time, in sample order.
-template <int NSH, int MODE, int PREC, int SPL = 1>
+// BULK: the record passes go through the copy engine (table_colours_bulk for FP32 records,
+// table_flush_bulk), staged in *stg.
+template <int NSH, int MODE, int PREC, int SPL = 1, bool BULK = false>
 __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
                                           int cnt, const SampleRec* samples, float4* colours,
                                           int maxs, const double* acc_in, double* losses,
                                           double mask_coef, float huber, const WarpTable& tab,
-                                          uint32_t* touched, int lane)
+                                          uint32_t* touched, int lane, Stage* stg = nullptr)
 {
     const bool miss = cnt < 0;
     const int n = miss ? 0 : cnt;
@@ -661,7 +874,11 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
                 for (int q = 0; q < 8; q++) slot[q] = table_slot(tab, cr.idx[q]);
             }
         }
-        table_colours<NSH, PREC>(tab, g, shs, lane);
+        if constexpr (BULK && PREC == kPrecFP32) {
+            if (!table_colours_bulk<NSH>(tab, g, shs, lane, *stg)) return;
+        } else {
+            table_colours<NSH, PREC>(tab, g, shs, lane);
+        }
 #pragma unroll
         for (int k = 0; k < SPL; k++) {
             const int i = base + 32 * k + lane;
@@ -802,7 +1019,10 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
                 }
             }
         }
-        table_flush<NSH>(tab, g, shs, touched, lane);
+        if constexpr (BULK)
+            table_flush_bulk<NSH>(tab, g, shs, touched, lane, *stg);
+        else
+            table_flush<NSH>(tab, g, shs, touched, lane);
     }
 }
 
@@ -831,6 +1051,35 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
 
 constexpr int kShadeWarps = 4;
 
+static_assert(kHashSlots <= 256, "the stage's slot lists hold 8-bit slot indices");
+
+// The stages of a block's shading warps: a record slot of RecShape<NSH>::REC floats (16-byte
+// aligned) per lane, the warp's mbarrier and its list of occupied table slots.
+template <int NSH>
+struct ShadeStage {
+    float4 slots[kShadeWarps][32][RecShape<NSH>::NV4];
+    unsigned long long mbar[kShadeWarps];
+    uint8_t list[kShadeWarps][kHashSlots];
+};
+
+template <int NSH>
+__device__ __forceinline__ Stage stage_init(ShadeStage<NSH>& ss, int warp, int lane, int* err)
+{
+    Stage st;
+    st.smem = (uint32_t)__cvta_generic_to_shared(&ss.slots[warp][0][0]);
+    st.mbar = (uint32_t)__cvta_generic_to_shared(&ss.mbar[warp]);
+    st.phase = 0u;
+    st.err = err;
+    st.list = ss.list[warp];
+    st.ok = true;
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st.mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    return st;
+}
+
 template <int NSH, int MODE, int PREC>
 __global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysView r,
                                                              const int32_t* sidx, int start,
@@ -838,17 +1087,18 @@ __global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysV
                                                              float4* colours, int maxs,
                                                              const int* counts, const double* acc,
                                                              double* losses, double mask_coef,
-                                                             float huber, uint32_t* touched)
+                                                             float huber, uint32_t* touched, int* err)
 {
     __shared__ uint32_t h_keys[kShadeWarps][kHashSlots];
     __shared__ float h_vals[kShadeWarps][4][kHashSlots];
+    __shared__ ShadeStage<NSH> stage;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     for (int s = lane; s < kHashSlots; s += 32) {
         h_keys[warp][s] = kEmpty;
         h_vals[warp][0][s] = h_vals[warp][1][s] = h_vals[warp][2][s] = h_vals[warp][3][s] = 0.f;
     }
-    __syncwarp();
+    Stage stg = stage_init<NSH>(stage, warp, lane, err);
     const int b = blockIdx.x * kShadeWarps + warp;
     if (b >= len) return;  // warp-uniform
     const int cnt = counts[b];
@@ -858,8 +1108,9 @@ __global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysV
     }
     const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
     const WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
-    shade_ray<NSH, MODE, PREC>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber,
-                               tab, touched, lane);
+    shade_ray<NSH, MODE, PREC, 1, true>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber,
+                                        tab, touched, lane, &stg);
+    bulk_wait_all();  // the bulk reductions are complete before the warp exits
 }
 
 // Shading with a work counter: the rays in order of decreasing sample count (k_order_by_count,
@@ -900,17 +1151,18 @@ template <int NSH, int MODE, int PREC>
 __global__ void __launch_bounds__(kShadeWarps * 32, 6)
     k_shade_dyn(GridView g, RaysView r, const int32_t* sidx, int start, int len, const SampleRec* samples,
                 float4* colours, int maxs, const int* counts, const double* acc, double* losses, double mask_coef,
-                float huber, uint32_t* touched, const int* order, int* ctr)
+                float huber, uint32_t* touched, const int* order, int* ctr, int* err)
 {
     __shared__ uint32_t h_keys[kShadeWarps][kHashSlots];
     __shared__ float h_vals[kShadeWarps][4][kHashSlots];
+    __shared__ ShadeStage<NSH> stage;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     for (int s = lane; s < kHashSlots; s += 32) {
         h_keys[warp][s] = kEmpty;
         h_vals[warp][0][s] = h_vals[warp][1][s] = h_vals[warp][2][s] = h_vals[warp][3][s] = 0.f;
     }
-    __syncwarp();
+    Stage stg = stage_init<NSH>(stage, warp, lane, err);
     const WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
     while (true) {
         int k = 0;
@@ -924,9 +1176,11 @@ __global__ void __launch_bounds__(kShadeWarps * 32, 6)
             continue;
         }
         const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
-        shade_ray<NSH, MODE, PREC>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber, tab,
-                                   touched, lane);
+        shade_ray<NSH, MODE, PREC, 1, true>(g, r, b, ri, cnt, samples, colours, maxs, acc, losses, mask_coef, huber,
+                                            tab, touched, lane, &stg);
+        if (!stg.ok) break;  // a record copy timed out (error word set)
     }
+    bulk_wait_all();  // the bulk reductions are complete before the warp exits
 }
 
 // ---------------------------------------------------------------------------
@@ -1215,11 +1469,11 @@ static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv,
         count_launch();
         k_shade_dyn<NSH, MODE, PREC><<<blocks, sblock, 0, st>>>(gv, rv, sidx, start, len, s.samples, s.colours,
                                                                  s.maxs, s.counts, s.acc, losses, mask_coef, huber,
-                                                                 touched, s.queue + 4, s.queue);
+                                                                 touched, s.queue + 4, s.queue, s.err);
         return;
     }
     k_shade<NSH, MODE, PREC><<<sgrid, sblock, 0, st>>>(gv, rv, sidx, start, len, s.samples, s.colours, s.maxs,
-                                                       s.counts, s.acc, losses, mask_coef, huber, touched);
+                                                       s.counts, s.acc, losses, mask_coef, huber, touched, s.err);
 }
 
 template <int NSH, int PREC>

@@ -119,5 +119,9 @@ extern "C" cpx_status cpx_render_forward_backward_noalloc(cpx_grid* g, cpx_rays*
         set_error("a shading warp of the fused march gave up waiting for a ray's placement");
         return CPX_ERR_NOT_READY;
     }
+    if (flags[0] & 32) {
+        set_error("a shading warp gave up waiting for a vertex record copy");
+        return CPX_ERR_NOT_READY;
+    }
     return CPX_OK;
 }

@@ -106,6 +106,10 @@ template <> struct Unit<4> {
     }
     __device__ static void floats(const F& g, float* f) { f[0] = g.x; f[1] = g.y; f[2] = g.z; f[3] = g.w; }
     __device__ static F make(const float* f) { return make_float4(f[0], f[1], f[2], f[3]); }
+    template <int PREC> __device__ static void unpack_m(const H& w, float* f) { mom1_unpack2<PREC>(w.x, f[0], f[1]); mom1_unpack2<PREC>(w.y, f[2], f[3]); }
+    template <int PREC> __device__ static void unpack_v(const H& w, float* f) { mom2_unpack2<PREC>(w.x, f[0], f[1]); mom2_unpack2<PREC>(w.y, f[2], f[3]); }
+    template <int PREC> __device__ static H pack_m(const float* f, uint32_t r0, uint32_t r1) { return make_uint2(mom1_pack2<PREC>(f[0], f[1], r0), mom1_pack2<PREC>(f[2], f[3], r1)); }
+    template <int PREC> __device__ static H pack_v(const float* f, uint32_t r0, uint32_t r1) { return make_uint2(mom2_pack2<PREC>(f[0], f[1], r0), mom2_pack2<PREC>(f[2], f[3], r1)); }
 };
 template <> struct Unit<2> {
     using H = uint32_t;
@@ -115,6 +119,10 @@ template <> struct Unit<2> {
     template <int PREC> __device__ static H pack(const float* f, uint32_t r0, uint32_t) { return sr_pack2<PREC>(f[0], f[1], r0); }
     __device__ static void floats(const F& g, float* f) { f[0] = g.x; f[1] = g.y; }
     __device__ static F make(const float* f) { return make_float2(f[0], f[1]); }
+    template <int PREC> __device__ static void unpack_m(const H& w, float* f) { mom1_unpack2<PREC>(w, f[0], f[1]); }
+    template <int PREC> __device__ static void unpack_v(const H& w, float* f) { mom2_unpack2<PREC>(w, f[0], f[1]); }
+    template <int PREC> __device__ static H pack_m(const float* f, uint32_t r0, uint32_t) { return mom1_pack2<PREC>(f[0], f[1], r0); }
+    template <int PREC> __device__ static H pack_v(const float* f, uint32_t r0, uint32_t) { return mom2_pack2<PREC>(f[0], f[1], r0); }
 };
 
 // Unit u (record slots E*u .. E*u+E-1) of vertex v, unit index q = v * U + u; nbq: the same
@@ -136,7 +144,8 @@ __device__ __forceinline__ void lowp_unit(const LowpArgs& a, uint32_t v, uint32_
     // every record a unit reads is written only by the same thread after the read (or not at
     // all), so all of them load through the non-coherent path
     float p[E];
-    UT::template unpack<PREC>(__ldg(sh_in + q), p);
+    constexpr int SHP = sh_prec<PREC>();
+    UT::template unpack<SHP>(__ldg(sh_in + q), p);
     if (u == 0) p[0] = vx.dens;  // slot 0 of an SH record is unused: density is FP32
     // untouched vertices have zero gradients: their records are neither read nor written
     const bool tch = vx.bits & 1u;
@@ -148,8 +157,8 @@ __device__ __forceinline__ void lowp_unit(const LowpArgs& a, uint32_t v, uint32_
         for (int c = 0; c < E; c++) g[c] = 0.f;
     }
     float mo[E], vo[E];
-    UT::unpack_bf16(__ldg(mrec + q), mo);
-    UT::unpack_bf16(__ldg(vrec + q), vo);
+    UT::template unpack_m<PREC>(__ldg(mrec + q), mo);
+    UT::template unpack_v<PREC>(__ldg(vrec + q), vo);
     if (TV && (vx.bits & 2u)) {
         float sum[E], disp[E];
 #pragma unroll
@@ -159,7 +168,7 @@ __device__ __forceinline__ void lowp_unit(const LowpArgs& a, uint32_t v, uint32_
 #pragma unroll
                 for (int c = 0; c < E; c++) nb[c] = p[c];
             } else {
-                UT::template unpack<PREC>(__ldg(sh_in + nbq[k]), nb);
+                UT::template unpack<SHP>(__ldg(sh_in + nbq[k]), nb);
             }
 #pragma unroll
             for (int c = 0; c < E; c++) {
@@ -203,9 +212,9 @@ __device__ __forceinline__ void lowp_unit(const LowpArgs& a, uint32_t v, uint32_
     // and the two moments take them in rotated forms
     const uint32_t r0 = fmix32(step_key ^ (v * 0x632BE5ABu) ^ ((uint32_t)u << 27));
     const uint32_t r1 = draw32(r0, 0x85EBCA6Bu);
-    sh_out[q] = UT::template pack<PREC>(np, r0, r1);
-    mrec[q] = UT::template pack<kPrecBF16>(mn, __funnelshift_l(r0, r0, 11), __funnelshift_l(r1, r1, 11));
-    vrec[q] = UT::template pack<kPrecBF16>(vn, __funnelshift_l(r0, r0, 22), __funnelshift_l(r1, r1, 22));
+    sh_out[q] = UT::template pack<SHP>(np, r0, r1);
+    mrec[q] = UT::template pack_m<PREC>(mn, __funnelshift_l(r0, r0, 11), __funnelshift_l(r1, r1, 11));
+    vrec[q] = UT::template pack_v<PREC>(vn, __funnelshift_l(r0, r0, 22), __funnelshift_l(r1, r1, 22));
     if (tch) grad[q] = UT::make(g);
 }
 
@@ -290,10 +299,11 @@ __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint
 {
     const float beta1 = 0.9f, beta2 = 0.999f, eps = 1.e-6f;
     const float2 neg1 = make_float2(-1.f, -1.f);
+    constexpr int SHP = sh_prec<PREC>();
     const uint2 sh_raw = src.self();
     float2 p01, p23;
-    unpack2<PREC>(sh_raw.x, p01.x, p01.y);
-    unpack2<PREC>(sh_raw.y, p23.x, p23.y);
+    unpack2<SHP>(sh_raw.x, p01.x, p01.y);
+    unpack2<SHP>(sh_raw.y, p23.x, p23.y);
     if (u == 0) p01.x = vx.dens;  // slot 0 of an SH record is unused: density is FP32
     const bool tch = vx.bits & 1u;
     float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -301,10 +311,10 @@ __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint
     float2 g01 = make_float2(g4.x, g4.y), g23 = make_float2(g4.z, g4.w);
     const uint2 m_raw = src.m(), v_raw = src.v();
     float2 mo01, mo23, vo01, vo23;
-    unpack2<kPrecBF16>(m_raw.x, mo01.x, mo01.y);
-    unpack2<kPrecBF16>(m_raw.y, mo23.x, mo23.y);
-    unpack2<kPrecBF16>(v_raw.x, vo01.x, vo01.y);
-    unpack2<kPrecBF16>(v_raw.y, vo23.x, vo23.y);
+    mom1_unpack2<PREC>(m_raw.x, mo01.x, mo01.y);
+    mom1_unpack2<PREC>(m_raw.y, mo23.x, mo23.y);
+    mom2_unpack2<PREC>(v_raw.x, vo01.x, vo01.y);
+    mom2_unpack2<PREC>(v_raw.y, vo23.x, vo23.y);
     if (TV && (vx.bits & 2u)) {
         float2 s01, s23, d01s, d23s;
         const float2 mp01 = __fmul2_rn(p01, neg1), mp23 = __fmul2_rn(p23, neg1);
@@ -315,8 +325,8 @@ __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint
             float2 d01 = make_float2(0.f, 0.f), d23 = make_float2(0.f, 0.f);
             if (!NB_SELF || !((vx.bits >> (2 + k)) & 1u)) {
                 const uint2 w = src.nb(k);
-                d01 = add2_h16<PREC>(w.x, mp01);
-                d23 = add2_h16<PREC>(w.y, mp23);
+                d01 = add2_h16<SHP>(w.x, mp01);
+                d23 = add2_h16<SHP>(w.y, mp23);
             }
             s01 = k == 0 ? __fmul2_rn(d01, d01) : __ffma2_rn(d01, d01, s01);
             s23 = k == 0 ? __fmul2_rn(d23, d23) : __ffma2_rn(d23, d23, s23);
@@ -353,11 +363,11 @@ __device__ __forceinline__ void lowp_quad_x2(const LowpArgs& a, uint32_t v, uint
     }
     const uint32_t r0 = fmix32(step_key ^ (v * 0x632BE5ABu) ^ ((uint32_t)u << 27));
     const uint32_t r1 = draw32(r0, 0x85EBCA6Bu);
-    a.sh_out[q] = make_uint2(sr_pack2<PREC>(np01.x, np01.y, r0), sr_pack2<PREC>(np23.x, np23.y, r1));
-    a.m[q] = make_uint2(sr_pack2<kPrecBF16>(mn01.x, mn01.y, __funnelshift_l(r0, r0, 11)),
-                        sr_pack2<kPrecBF16>(mn23.x, mn23.y, __funnelshift_l(r1, r1, 11)));
-    a.v[q] = make_uint2(sr_pack2<kPrecBF16>(vn01.x, vn01.y, __funnelshift_l(r0, r0, 22)),
-                        sr_pack2<kPrecBF16>(vn23.x, vn23.y, __funnelshift_l(r1, r1, 22)));
+    a.sh_out[q] = make_uint2(sr_pack2<SHP>(np01.x, np01.y, r0), sr_pack2<SHP>(np23.x, np23.y, r1));
+    a.m[q] = make_uint2(mom1_pack2<PREC>(mn01.x, mn01.y, __funnelshift_l(r0, r0, 11)),
+                        mom1_pack2<PREC>(mn23.x, mn23.y, __funnelshift_l(r1, r1, 11)));
+    a.v[q] = make_uint2(mom2_pack2<PREC>(vn01.x, vn01.y, __funnelshift_l(r0, r0, 22)),
+                        mom2_pack2<PREC>(vn23.x, vn23.y, __funnelshift_l(r1, r1, 22)));
     if (tch) a.grad[q] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
@@ -681,7 +691,8 @@ cpx_status lowp_prepare()
 {
     if (g_async_ready >= 0) return CPX_OK;
     const bool ok = async_opt_in<kPrecBF16, 1>() && async_opt_in<kPrecBF16, 4>() && async_opt_in<kPrecBF16, 7>() &&
-                    async_opt_in<kPrecFP16, 1>() && async_opt_in<kPrecFP16, 4>() && async_opt_in<kPrecFP16, 7>();
+                    async_opt_in<kPrecFP16, 1>() && async_opt_in<kPrecFP16, 4>() && async_opt_in<kPrecFP16, 7>() &&
+                    async_opt_in<kPrecFP16M, 1>() && async_opt_in<kPrecFP16M, 4>() && async_opt_in<kPrecFP16M, 7>();
     if (!ok) cudaGetLastError();
     g_async_ready = ok ? 1 : 0;
     return CPX_OK;
@@ -775,8 +786,9 @@ cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_
     a.seed = g->sr_seed;
     const uint32_t all = (g->rec >= 32) ? 0xffffffffu : ((1u << g->rec) - 1u);
     a.full_masks = (tv_mask & all) == all && (adam_mask & all) == all ? 1 : 0;
-    cpx_status rc = g->prec == kPrecFP16 ? launch_lowp_shape<kPrecFP16>(g, a, fused_tv, st)
-                                         : launch_lowp_shape<kPrecBF16>(g, a, fused_tv, st);
+    cpx_status rc = g->prec != kPrecFP16 ? launch_lowp_shape<kPrecBF16>(g, a, fused_tv, st)
+                    : g->mom_h           ? launch_lowp_shape<kPrecFP16M>(g, a, fused_tv, st)
+                                         : launch_lowp_shape<kPrecFP16>(g, a, fused_tv, st);
     if (rc != CPX_OK) return rc;
     count_launch();
     g->cur ^= 1;

@@ -71,14 +71,17 @@ typedef struct cpx_grid_desc {
 
 /* Storage forms.  FP32 is the reference's (every parameter and moment in float, the march
  * in the reference's FP64/FP32 mix, bit-compatible with it).  The mixed forms store the SH
- * coefficients in bfloat16 (BF16) or half (FP16) and both Adam moments in bfloat16, keep
- * density, gradients and all accumulation in FP32, march in FP32, and write the optimizer
- * results back with stochastic rounding.  They support TV type 0 with 6 neighbours, fused
- * into the optimizer sweep (cpx_tv_adam_step / cpx_train_step), or no TV. */
+ * coefficients in bfloat16 (BF16) or half (FP16 and FP16_FULL) and both Adam moments in
+ * bfloat16 (BF16, FP16) or half (FP16_FULL: the first moment as m * 2^8, the second through
+ * its root, sqrt(v) * 2^8, since v spans more decades than half holds; stores saturate at
+ * 255.9), keep density, gradients and all accumulation in FP32, march in FP32, and write the
+ * optimizer results back with stochastic rounding.  They support TV type 0 with 6 neighbours,
+ * fused into the optimizer sweep (cpx_tv_adam_step / cpx_train_step), or no TV. */
 typedef enum cpx_precision {
     CPX_PRECISION_FP32 = 0,
     CPX_PRECISION_BF16 = 1,
-    CPX_PRECISION_FP16 = 2
+    CPX_PRECISION_FP16 = 2,
+    CPX_PRECISION_FP16_FULL = 3
 } cpx_precision;
 
 /* Pinhole camera as the reference's getBound reads it (SVRF/CameraUtils.cuh:16-26):
@@ -459,7 +462,9 @@ cpx_status cpx_train_step_ahead(cpx_grid* g, cpx_rays* r, const int32_t* sample_
 
 /* Synchronise the grid's work and report (then clear) the sticky device-side errors of
  * earlier asynchronous calls: CPX_ERR_ITERATION_CAP when a ray's march exceeded its
- * sample bound, CPX_ERR_INVALID_ARGUMENT when a sample index was out of range. */
+ * sample bound, CPX_ERR_INVALID_ARGUMENT when a sample index was out of range,
+ * CPX_ERR_NOT_READY when a shading warp gave up one of its bounded waits (a ray's placement in
+ * the fused march, or a vertex record copy) and stopped. */
 cpx_status cpx_grid_check(cpx_grid* g);
 /* No reference counterpart (a diagnostic): the number of vertices marked in the touched map
  * the next optimizer sweep will read.  The backward marks every vertex it scatters gradients
