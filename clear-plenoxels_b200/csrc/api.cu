@@ -313,8 +313,10 @@ cudaError_t alloc_state(cpx_grid* g, int64_t n)
         get((void**)&g->density, (size_t)nn * sizeof(float));
     } else {
         const size_t hb = (size_t)nn * g->slots * sizeof(uint16_t);
-        get((void**)&g->sh16[0], hb);
-        get((void**)&g->sh16[1], hb);
+        // SH records with 16 bytes to spare: the shading's bulk copies move a record's 16-byte
+        // aligned window, which for the last record reaches up to 8 bytes past it
+        get((void**)&g->sh16[0], hb + 16);
+        get((void**)&g->sh16[1], hb + 16);
         get((void**)&g->m16, hb);
         get((void**)&g->v16, hb);
         get((void**)&g->dens[0], (size_t)nn * sizeof(float));

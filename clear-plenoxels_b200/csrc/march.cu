@@ -704,6 +704,13 @@ __device__ __forceinline__ float4 lds128(uint32_t addr)
     return r;
 }
 
+__device__ __forceinline__ uint2 lds64(uint32_t addr)
+{
+    uint2 r;
+    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(r.x), "=r"(r.y) : "r"(addr));
+    return r;
+}
+
 __device__ __forceinline__ void sts128(uint32_t addr, float a, float b, float c, float d)
 {
     asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
@@ -726,17 +733,24 @@ __device__ __forceinline__ int table_compact(const WarpTable& t, uint8_t* list, 
     return nd;
 }
 
-// The forward record pass of table_colours (FP32 records) through the stage: per pass of up to
-// 32 listed vertices, lane 0 announces the bytes of the pass's records, each vertex's lane
-// copies its record, the warp waits for the mbarrier's phase and forms the colours from shared
-// memory in the same order as table_colours.  Returns false (error word set) when a copy did
-// not complete within the wait's limit; the warp then stops shading.
-template <int NSH>
+// The forward record pass of table_colours through the stage: per pass of up to 32 listed
+// vertices, lane 0 announces the bytes of the pass's copies, each vertex's lane copies its
+// record, the warp waits for the mbarrier's phase and forms the colours from shared memory in
+// the same order as table_colours.  FP32 records (112 B at SH band 2) are 16-byte aligned and
+// copied as they are; a 16-bit record of the mixed forms (56 B) starts on an 8-byte boundary,
+// so the lane copies the 16-byte aligned window around it (64 B; the SH buffers carry 16
+// spare bytes for the last record's window) and reads from the record's offset in it.
+// Returns false (error word set) when a copy did not complete within the wait's limit; the
+// warp then stops shading.
+template <int NSH, int PREC>
 __device__ __forceinline__ bool table_colours_bulk(const WarpTable& t, const GridView& g, const float* shs, int lane,
                                                    Stage& st)
 {
     using RS = RecShape<NSH>;
-    constexpr uint32_t kRecBytes = RS::REC * 4;
+    constexpr uint32_t kRecBytes = RS::REC * 4;  // the lane's stage slot
+    constexpr uint32_t kSrcBytes = PREC == kPrecFP32 ? RS::REC * 4 : RS::REC * 2;
+    constexpr uint32_t kCopyBytes = kSrcBytes % 16 == 0 ? kSrcBytes : ((kSrcBytes + 8 + 15) & ~15u);
+    static_assert(kCopyBytes <= kRecBytes, "a copy window fits the lane's stage slot");
     const uint32_t mine = st.smem + (uint32_t)lane * kRecBytes;
     bulk_wait_read();  // the slot's last bulk reduction has read it
     proxy_fence_smem();
@@ -746,12 +760,17 @@ __device__ __forceinline__ bool table_colours_bulk(const WarpTable& t, const Gri
         const bool occ = i < nd;
         int s = 0;
         uint32_t key = 0u;
+        uint32_t off = 0u;  // the record's offset in its copy window
         if (occ) {
             s = st.list[i];
             key = t.keys[s];
+            const char* src = PREC == kPrecFP32
+                                  ? reinterpret_cast<const char*>(g.params + (size_t)key * RS::REC)
+                                  : reinterpret_cast<const char*>(sh16_records(g) + (size_t)key * RS::REC);
+            off = (uint32_t)(reinterpret_cast<uintptr_t>(src) & 15u);
+            bulk_load(mine, src - off, kCopyBytes, st.mbar);
         }
-        if (lane == 0) mbar_expect(st.mbar, (uint32_t)(nd - p0 < 32 ? nd - p0 : 32) * kRecBytes);
-        if (occ) bulk_load(mine, g.params + (size_t)key * RS::REC, kRecBytes, st.mbar);
+        if (lane == 0) mbar_expect(st.mbar, (uint32_t)(nd - p0 < 32 ? nd - p0 : 32) * kCopyBytes);
         const bool done = __all_sync(0xffffffffu, mbar_wait_bounded(st.mbar, st.phase));
         if (!done) {
             if (lane == 0) atomicOr(st.err, 32);
@@ -764,8 +783,16 @@ __device__ __forceinline__ bool table_colours_bulk(const WarpTable& t, const Gri
             float col[3] = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int v = 0; v < RS::NV4; v++) {
-                const float4 p = lds128(mine + 16u * v);
-                const float pv[4] = {p.x, p.y, p.z, p.w};
+                float pv[4];
+                if (PREC == kPrecFP32) {
+                    const float4 p = lds128(mine + 16u * v);
+                    pv[0] = p.x;
+                    pv[1] = p.y;
+                    pv[2] = p.z;
+                    pv[3] = p.w;
+                } else {
+                    unpack4<PREC>(lds64(mine + off + 8u * v), pv);
+                }
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const int e = 4 * v + k;
@@ -842,8 +869,8 @@ __device__ __forceinline__ void table_flush_bulk(const WarpTable& t, const GridV
 // SPL: samples a lane takes per chunk.  A chunk of 32 * SPL consecutive samples shares one
 // table (of kHashSlots * SPL slots), so its distinct vertices are gathered and scattered once;
 // the scans still run over 32 samples at a time, in sample order.
-// BULK: the record passes go through the copy engine (table_colours_bulk for FP32 records,
-// table_flush_bulk), staged in *stg.
+// BULK: the record passes go through the copy engine (table_colours_bulk, table_flush_bulk),
+// staged in *stg.
 template <int NSH, int MODE, int PREC, int SPL = 1, bool BULK = false>
 __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, int b, int64_t ri,
                                           int cnt, const SampleRec* samples, float4* colours,
@@ -874,8 +901,8 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
                 for (int q = 0; q < 8; q++) slot[q] = table_slot(tab, cr.idx[q]);
             }
         }
-        if constexpr (BULK && PREC == kPrecFP32) {
-            if (!table_colours_bulk<NSH>(tab, g, shs, lane, *stg)) return;
+        if constexpr (BULK) {
+            if (!table_colours_bulk<NSH, PREC>(tab, g, shs, lane, *stg)) return;
         } else {
             table_colours<NSH, PREC>(tab, g, shs, lane);
         }
