@@ -408,19 +408,27 @@ def run_ours(args, wl, world, rank, local):
     # leg after the timed region.  Measured slower than march-then-sweep on the 256^3 workload (the
     # density preview it needs costs more than the placement it hides), so it is not the default.
     ahead = prop is None and args.precision == "fp32" and thr is None and args.ahead
+    # march option OPT_SPLIT_SWEEP: the whole step is one cpx_train_step call (its sweep of the
+    # untouched vertices runs beside the shading), so it too is timed whole, with a split leg after
+    split = (prop is None and args.precision == "fp32" and thr is None and not ahead
+             and bool(args.march_options & cpx.OPT_SPLIT_SWEEP))
+    whole = ahead or split
 
     def step_ahead(k):
         b, nb = k % wl["pool_batches"], (k + 1) % wl["pool_batches"]
-        cpx.train_step_ahead(scene, pool, losses, start=b * R, length=R, next_rays=pool, next_start=nb * R,
-                             next_length=R, mask_coef=STEP["mask_coef"], huber_delta=STEP["huber"],
-                             lam_density=STEP["lam_density"], lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1],
-                             timestep=k + 1, want_mse=False, stream=stream)
+        common = dict(mask_coef=STEP["mask_coef"], huber_delta=STEP["huber"], lam_density=STEP["lam_density"],
+                      lam_sh=STEP["lam_sh"], lr=lr[0], sh_lr=lr[1], timestep=k + 1, want_mse=False, stream=stream)
+        if ahead:
+            cpx.train_step_ahead(scene, pool, losses, start=b * R, length=R, next_rays=pool, next_start=nb * R,
+                                 next_length=R, **common)
+        else:
+            cpx.train_step(scene, pool, losses, start=b * R, length=R, **common)
         if decay:  # Render.cu:499-500
             lr[:] = [cpx.lr_decay(x, wl["pool_batches"], k // wl["pool_batches"]) for x in lr]
 
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
     for k in range(W):
-        (step_ahead if ahead else step)(k)
+        (step_ahead if whole else step)(k)
     torch.cuda.synchronize()
     scene.check()
 
@@ -435,7 +443,7 @@ def run_ours(args, wl, world, rank, local):
     torch.cuda.nvtx.range_push("timed")  # lets a profiler capture the timed steps alone (--nvtx-include timed/)
     t0.record(stream)
     for k in range(K):
-        if ahead:
+        if whole:
             step_ahead(W + k)
         else:
             evs[k][0].record(stream)
@@ -449,7 +457,7 @@ def run_ours(args, wl, world, rank, local):
     dist_barrier(world)
     scene.check()
     split_ms = None
-    if ahead:
+    if whole:
         # split leg: the same steps with the march and the sweep one after the other, timed apart
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
@@ -600,9 +608,11 @@ def run_ours(args, wl, world, rank, local):
         "roofline": roofline,
         "kernels_ms": {"march_fwd_bwd" if prop is None else "proposal_and_march": round(march_ms, 4),
                        "tv_adam_sweep": round(sweep_ms, 4),
-                       "timed_in": "split leg after the timed region (march, then sweep)" if ahead else "timed region"},
+                       "timed_in": "split leg after the timed region (march, then sweep)" if whole else "timed region"},
         "step_form": ("cpx_train_step_ahead: the next batch placed beside each step's sweep; split leg (placement, "
                       "shading, sweep one after the other) %.4f ms per step" % split_ms) if ahead else
+                     ("cpx_train_step with OPT_SPLIT_SWEEP: the untouched vertices swept beside the shading; split "
+                      "leg (march, then sweep) %.4f ms per step" % split_ms) if split else
                      "march then sweep",
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": R * RAY_BYTES,
                 "d2h_bytes_per_step": 8, "last_mse": mses[-1]},

@@ -549,7 +549,7 @@ cpx_status cpx_grid_set_options(cpx_grid* g, int options)
 {
     if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH | CPX_OPT_NO_EARLY_STOP | CPX_OPT_FUSED_MARCH |
-                                   CPX_OPT_PLANE_SWEEP))) return CPX_ERR_INVALID_ARGUMENT;
+                                   CPX_OPT_PLANE_SWEEP | CPX_OPT_SPLIT_SWEEP))) return CPX_ERR_INVALID_ARGUMENT;
     g->options = options;
     cpx_status rc = refresh_dense_skip(g, 0);  // the maps of a grid now marched with jumps
     if (rc != CPX_OK) return rc;
@@ -811,6 +811,47 @@ cpx_status cpx_tv_adam_step(cpx_grid* g, double lam_d, double lam_sh, double lr,
     return sweep_adam(g, true, lam_d, lam_sh, lr, sh_lr, timestep, (cudaStream_t)stream);
 }
 
+// The step of CPX_OPT_SPLIT_SWEEP: placement; then, on the grid's second stream, the touched
+// map from the placed samples and the sweep of the untouched vertices, beside the shading on
+// the caller's stream; then the sweep of the touched vertices once both are done.  The
+// untouched vertices' update reads nothing the shading writes (their gradients are zero and
+// not read) and writes nothing it reads (the other parameter buffer, the moments, the density
+// mirror that only placement reads), so the two run side by side.
+static cpx_status train_step_split(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
+                                   const cpx_step_args* a, double* losses, double* mse_out, cudaStream_t st)
+{
+    g->last_len = len;
+    cpx_status s = march_launch_stages(g, r, sidx, start, len, losses, a->mask_coef, a->huber_delta, 0, 1, st);
+    if (s != CPX_OK) return s;
+    cudaError_t e = cudaSuccess;
+    if (!g->aside) e = cudaStreamCreateWithFlags(&g->aside, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !g->ev_fork) e = cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !g->ev_join) e = cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(g->ev_fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(g->aside, g->ev_fork, 0);
+    if (e != cudaSuccess) return cuda_status(e, "split sweep stream");
+    s = mark_touched(g, len, g->aside);
+    if (s == CPX_OK)
+        s = sweep_adam_pass(g, true, a->lam_density, a->lam_sh, a->lr, a->sh_lr, a->timestep, 1, g->aside);
+    e = cudaEventRecord(g->ev_join, g->aside);  // recorded on every path: the caller's stream joins it
+    if (s != CPX_OK) return s;
+    if (e != cudaSuccess) return cuda_status(e, "split sweep join");
+    s = march_launch_stages(g, r, sidx, start, len, losses, a->mask_coef, a->huber_delta, 0, 2, st);
+    e = cudaStreamWaitEvent(st, g->ev_join, 0);
+    if (s != CPX_OK) return s;
+    if (e != cudaSuccess) return cuda_status(e, "split sweep join");
+    s = sweep_adam_pass(g, true, a->lam_density, a->lam_sh, a->lr, a->sh_lr, a->timestep, 2, st);
+    if (s != CPX_OK) return s;
+    if (mse_out) {
+        s = mse_launch(losses, len, g->scratch.mse, st);
+        if (s != CPX_OK) return s;
+        e = cudaMemcpyAsync(mse_out, g->scratch.mse, sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_status(e, "mse");
+    }
+    return CPX_OK;
+}
+
 cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,
                           const cpx_step_args* a, double* losses, double* mse_out,
                           cpx_stream stream)
@@ -822,6 +863,10 @@ cpx_status cpx_train_step(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int sta
         set_error("the mixed forms run TV type 0 / 6 neighbours fused into the optimizer sweep only");
         return CPX_ERR_UNSUPPORTED;
     }
+    const bool split = (g->options & CPX_OPT_SPLIT_SWEEP) && fuse && g->prec == kPrecFP32 && !g->sparse &&
+                       g->rec == 28 && !g->all_touched && len > 0 && a->timestep >= 1 &&
+                       !(g->options & (CPX_OPT_FUSED_MARCH | CPX_OPT_FP32_MARCH | CPX_OPT_PLANE_SWEEP));
+    if (split) return train_step_split(g, r, sidx, start, len, a, losses, mse_out, st);
     cpx_status s = march_launch(g, r, sidx, start, len, kForwardBackward, losses, a->mask_coef,
                                 a->huber_delta, st);
     if (s != CPX_OK) return s;

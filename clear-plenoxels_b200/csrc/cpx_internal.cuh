@@ -398,6 +398,13 @@ cpx_status march_launch_stages(cpx_grid* g, cpx_rays* r, const int32_t* sidx, in
                                double mask_coef, float huber, int which, int stages, cudaStream_t st);
 // sweep.cu: the densities the next FP32 dense sweep will write (TV type 0/6 fused when
 // fused_tv, else none), written to the density mirror ahead of the sweep, bit for bit.
+// The touched map of the batch in the grid's scratch, from its placed samples (the corners of
+// every sample's cell), ahead of the shading.
+cpx_status mark_touched(cpx_grid* g, int len, cudaStream_t st);
+// One pass of the FP32 dense fused sweep: 1 = the vertices the touched map leaves out, 2 = the
+// touched ones (and the grid's buffer flips).  Together, the single sweep's results.
+cpx_status sweep_adam_pass(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
+                           int timestep, int pass, cudaStream_t st);
 cpx_status density_preview(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
                            int timestep, cudaStream_t st);
 cpx_status march_launch_with(cpx_grid* g, cpx_rays* r, const int32_t* sidx, int start, int len,

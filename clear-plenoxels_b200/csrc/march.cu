@@ -1328,6 +1328,50 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
 }
 
 // ---------------------------------------------------------------------------
+// The touched map from the placed samples: a warp per ray, a lane per sample; a sample whose
+// cell differs from the previous sample's sets its cell's 8 corner bits (the corners the
+// shading will scatter gradients to, found the same way).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mark_touched(GridView g, const SampleRec* samples, const int* counts, int len,
+                                                      int maxs, uint32_t* touched)
+{
+    const int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= len) return;  // warp-uniform
+    const int cnt = counts[b];
+    const SampleRec* S = samples + (size_t)b * maxs;
+    unsigned long long prev = ~0ull;  // the cell of the previous sample
+    for (int base = 0; base < cnt; base += 32) {
+        const int i = base + lane;
+        SampleRec s;
+        unsigned long long key = ~0ull - 1ull;
+        if (i < cnt) {
+            s = S[i];
+            key = (unsigned long long)s.bx | ((unsigned long long)s.by << 16) | ((unsigned long long)s.bz << 32);
+        }
+        unsigned long long before = __shfl_up_sync(0xffffffffu, key, 1);
+        if (lane == 0) before = prev;
+        if (i < cnt && key != before) {
+            unsigned idx[8];
+            cell_corners(g, s.bx, s.by, s.bz, idx);
+#pragma unroll
+            for (int q = 0; q < 8; q++) atomicOr(touched + (idx[q] >> 5), 1u << (idx[q] & 31u));
+        }
+        prev = __shfl_sync(0xffffffffu, key, 31);
+    }
+}
+
+cpx_status mark_touched(cpx_grid* g, int len, cudaStream_t st)
+{
+    if (len <= 0) return CPX_OK;
+    const GridView gv = grid_view(g);
+    k_mark_touched<<<(unsigned)((len + 7) / 8), 256, 0, st>>>(gv, g->scratch.samples, g->scratch.counts, len,
+                                                             g->scratch.maxs, g->touched[g->tcur]);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "touched map");
+}
+
+// ---------------------------------------------------------------------------
 // Batch MSE of the per-ray losses (getMSEError, Utils.cu:311-320), one block.
 // ---------------------------------------------------------------------------
 __global__ void k_mse(const double* losses, int len, double* out)

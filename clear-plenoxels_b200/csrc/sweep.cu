@@ -39,6 +39,7 @@ struct SweepArgs {
     float lr, sh_lr;
     int timestep;
     const int* t_dev;  // when set, the timestep is *t_dev + 1 (a replayed CUDA graph)
+    int pass;          // 0: every vertex; 1: untouched vertices only; 2: touched vertices only
 };
 
 __device__ __forceinline__ float f4get(const float4& v, int c)
@@ -114,10 +115,11 @@ __device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint
                                            bool tv_on, const uint32_t* nb_slot, const bool* nb_self,
                                            float inv_bc1, float inv_bc2, float lr_density)
 {
-    const float4 p = a.p_in[sl];
     // untouched vertices have zero gradients: their records are neither read nor written
     const bool tch = touched_bit(a.touched, v);
-    if (a.clear && j == 0 && (v & 31u) == 0) a.clear[v >> 5] = 0u;
+    if (a.clear && a.pass != 2 && j == 0 && (v & 31u) == 0) a.clear[v >> 5] = 0u;
+    if ((a.pass == 1 && tch) || (a.pass == 2 && !tch)) return;  // the other pass's vertex
+    const float4 p = a.p_in[sl];
     float4 g = tch ? a.grad[sl] : make_float4(0.f, 0.f, 0.f, 0.f);
     float4 m = a.m[sl];
     float4 vv = a.v[sl];
@@ -511,7 +513,30 @@ static SweepArgs sweep_args(const cpx_grid* g, double lam_d, double lam_sh, doub
     a.sh_lr = (float)sh_lr;
     a.timestep = timestep;
     a.t_dev = t_dev;
+    a.pass = 0;
     return a;
+}
+
+cpx_status sweep_adam_pass(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,
+                           int timestep, int pass, cudaStream_t st)
+{
+    if (g->prec != kPrecFP32 || g->sparse || g->rec != 28 || g->n_act * 7 >= ((int64_t)1 << 32) ||
+        (g->options & CPX_OPT_PLANE_SWEEP) || g->all_touched || (pass != 1 && pass != 2)) {
+        set_error("the split sweep runs on dense FP32 grids of SH band 2 with a touched map");
+        return CPX_ERR_UNSUPPORTED;
+    }
+    ++g->epoch;
+    if (g->n_act == 0) return CPX_OK;
+    SweepArgs a = sweep_args(g, lam_d, lam_sh, lr, sh_lr, timestep, nullptr);
+    a.pass = pass;
+    launch_sweep<7>(g, a, fused_tv, st);
+    count_launch();
+    cpx_status rc = cuda_status(cudaGetLastError(), "adam sweep pass");
+    if (rc != CPX_OK || pass == 1) return rc;
+    g->cur ^= 1;
+    g->tcur ^= 1;
+    g->all_touched = 0;
+    return refresh_dense_skip(g, st);
 }
 
 cpx_status density_preview(cpx_grid* g, bool fused_tv, double lam_d, double lam_sh, double lr, double sh_lr,

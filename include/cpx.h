@@ -399,12 +399,18 @@ cpx_status cpx_image_mask_pixels(const int* bbox, int width, int32_t* index_out,
  *                        walks z with the x-y plane of a tile on chip instead of running a
  *                        block per row of vertices that reads neighbours from L1/L2.  Results
  *                        are the same bit for bit; slower on the B200 (one z-step of loads in
- *                        flight per SM); for comparison. */
+ *                        flight per SM); for comparison;
+ * CPX_OPT_SPLIT_SWEEP    cpx_train_step on a dense FP32 grid of SH band 2 with the fused TV:
+ *                        once the batch is placed, the vertices its samples cannot reach (the
+ *                        corners of no sample's cell, marked from the placed samples) are swept
+ *                        on a second stream while the batch is shaded, and the rest after the
+ *                        shading.  Results are those of the single sweep bit for bit. */
 #define CPX_OPT_NO_EMPTY_SKIP 1
 #define CPX_OPT_FP32_MARCH 2
 #define CPX_OPT_NO_EARLY_STOP 4
 #define CPX_OPT_FUSED_MARCH 8
 #define CPX_OPT_PLANE_SWEEP 16
+#define CPX_OPT_SPLIT_SWEEP 32
 cpx_status cpx_grid_set_options(cpx_grid* g, int options);
 
 /* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,

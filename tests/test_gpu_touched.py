@@ -111,3 +111,40 @@ def test_plane_window_sweep_equals_row_sweep(cuda, dims):
     assert not np.array_equal(outs[0][0], params)
     for a, b in zip(*outs):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_split_sweep_trains_as_the_single_sweep(cuda):
+    """CPX_OPT_SPLIT_SWEEP: the vertices no placed sample reaches are swept beside the shading
+    and the rest after it.  Four training steps match the single sweep's: the first step's batch
+    MSE exactly (same parameters before it), the parameters and moments after the fourth within
+    float-atomics noise on 99.9% of the values."""
+    import torch
+
+    import cpx
+    import cpx_scenes as S
+
+    cfg = S.small_config(seed=43, n=48, n_cams=6, img=64, n_rays=2048)
+    n = cfg["W"]
+    step = dict(mask_coef=1.0, huber_delta=0.1, lam_density=1e-4, lam_sh=1e-5, lr=0.05, sh_lr=0.2)
+    runs = []
+    for opt in (cpx.OPT_SPLIT_SWEEP, 0):
+        scene = cpx.ObjectScene(n, n, n, 9, step_size=cfg["step"])
+        scene.set_options(opt)
+        scene.upload_params(cfg["params"])
+        rays = cpx.Rays(2048, white_bg=True)
+        rays.initial_self(scene, [cpx.Camera.make(**c) for c in cfg["cams"]], cfg["images"], cfg["pix"],
+                          cfg["img_w"], cfg["img_h"])
+        losses = torch.zeros(512, dtype=torch.float64, device=cuda)
+        mses = []
+        for k in range(4):
+            mses.append(cpx.train_step(scene, rays, losses, start=(k % 4) * 512, length=512, timestep=k + 1, **step))
+        scene.check()
+        runs.append((mses, scene.download_params(), *scene.download_moments()))
+        scene.close()
+        rays.close()
+    (ms, ps, ms1, vs), (mp, pp, mp1, vp) = runs
+    assert ms[0] == mp[0]
+    assert all(abs(a - b) <= 1e-4 * b for a, b in zip(ms, mp))
+    assert not np.array_equal(pp, cfg["params"])
+    for got, want, tol in ((ps, pp, 1e-4 * step["lr"]), (ms1, mp1, 1e-6), (vs, vp, 1e-9)):
+        assert np.mean(np.abs(got - want) <= tol + 1e-4 * np.abs(want)) >= 0.999
