@@ -404,7 +404,9 @@ cpx_status cpx_image_mask_pixels(const int* bbox, int width, int32_t* index_out,
  *                        once the batch is placed, the vertices its samples cannot reach (the
  *                        corners of no sample's cell, marked from the placed samples) are swept
  *                        on a second stream while the batch is shaded, and the rest after the
- *                        shading.  Results are those of the single sweep bit for bit. */
+ *                        shading.  Results are those of the single sweep bit for bit.  Slower on
+ *                        the B200 (6.1 against 4.5 ms a step at 256^3: the shading's gathers
+ *                        and atomics wait behind the sweep's DRAM traffic); for comparison. */
 #define CPX_OPT_NO_EMPTY_SKIP 1
 #define CPX_OPT_FP32_MARCH 2
 #define CPX_OPT_NO_EARLY_STOP 4
