@@ -205,6 +205,7 @@ OPT_NO_EARLY_STOP = 4  # the FP32 march runs every ray to its far bound (no tran
 OPT_FUSED_MARCH = 8  # placement and shading overlapped in one launch instead of two launches
 OPT_PLANE_SWEEP = 16  # the FP32 dense sweep walking z with a tile's plane on chip instead of a block per row
 OPT_SPLIT_SWEEP = 32  # the untouched vertices' sweep beside the shading, the touched ones after it
+OPT_SPARSE_ADAM = 64  # mixed forms: the sweep updates the touched vertices only, in place
 _sig("cpx_train_step_proposal", [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(StepArgs), C.POINTER(ProposalSchedule),
                                  C.c_int, _vp, C.POINTER(C.c_double), _vp])
 
@@ -462,7 +463,7 @@ class ObjectScene:
 
     def set_options(self, options: int):
         """March and sweep options (OPT_NO_EMPTY_SKIP, OPT_FP32_MARCH, OPT_NO_EARLY_STOP, OPT_FUSED_MARCH,
-        OPT_PLANE_SWEEP, OPT_SPLIT_SWEEP)."""
+        OPT_PLANE_SWEEP, OPT_SPLIT_SWEEP, OPT_SPARSE_ADAM)."""
         _check(_lib.cpx_grid_set_options(self._h, int(options)), "cpx_grid_set_options")
 
     def touched_count(self) -> int:

@@ -549,7 +549,8 @@ cpx_status cpx_grid_set_options(cpx_grid* g, int options)
 {
     if (g) ++g->epoch;  // what placement reads changes: a placement done in advance is stale
     if (check_grid(g) || (options & ~(CPX_OPT_NO_EMPTY_SKIP | CPX_OPT_FP32_MARCH | CPX_OPT_NO_EARLY_STOP | CPX_OPT_FUSED_MARCH |
-                                   CPX_OPT_PLANE_SWEEP | CPX_OPT_SPLIT_SWEEP))) return CPX_ERR_INVALID_ARGUMENT;
+                                   CPX_OPT_PLANE_SWEEP | CPX_OPT_SPLIT_SWEEP | CPX_OPT_SPARSE_ADAM)))
+        return CPX_ERR_INVALID_ARGUMENT;
     g->options = options;
     cpx_status rc = refresh_dense_skip(g, 0);  // the maps of a grid now marched with jumps
     if (rc != CPX_OK) return rc;

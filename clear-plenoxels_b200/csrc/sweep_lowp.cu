@@ -41,6 +41,7 @@ struct LowpArgs {
     const int* t_dev;   // when set, the timestep is *t_dev + 1 (a replayed CUDA graph)
     uint32_t seed;
     int full_masks;     // TV and Adam apply to every slot of every quad (no padding, no hierarchy)
+    int sparse_adam;    // CPX_OPT_SPARSE_ADAM: untouched vertices are skipped, the rest updated in place
 };
 
 // Square root through the hardware reciprocal square root (about 2 ulp; the results are
@@ -55,18 +56,27 @@ struct LowpVertex {
     float dens;     // FP32 density
     float tv0;      // TV term of the density (0 when it does not apply)
     float lr_d;     // density learning rate (adaptive multiplier included)
-    uint32_t bits;  // bit 0: touched; bit 1: TV applies; bits 2..7: neighbour k reads the vertex itself
+    uint32_t bits;  // bit 0: touched; bit 1: TV applies; bits 2..7: neighbour k reads the vertex itself;
+                    // bit 8: skipped (sparse Adam, untouched)
 };
+
+constexpr uint32_t kSkipBit = 1u << 8;
 
 template <bool TV>
 __device__ __forceinline__ LowpVertex lowp_vertex(const LowpArgs& a, uint32_t v, bool tv_on, const uint32_t* nb_v,
                                                   uint32_t self_bits, float lr_d)
 {
     LowpVertex r;
-    r.dens = __ldg(a.d_in + v);
-    r.lr_d = lr_d;
     r.tv0 = 0.f;
-    r.bits = (touched_bit(a.touched, v) ? 1u : 0u) | (tv_on ? 2u : 0u) | (self_bits << 2);
+    r.lr_d = lr_d;
+    const bool tch = touched_bit(a.touched, v);
+    if (a.sparse_adam && !tch) {  // sparse Adam: a zero gradient leaves the vertex as it is
+        r.dens = 0.f;
+        r.bits = kSkipBit;
+        return r;
+    }
+    r.dens = __ldg(a.d_in + v);
+    r.bits = (tch ? 1u : 0u) | (tv_on ? 2u : 0u) | (self_bits << 2);
     if (TV && tv_on && (a.tv_mask & 1u)) {
         float sum = 0.f, disp = 0.f;
 #pragma unroll
@@ -434,7 +444,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep_lowp_dense(LowpArgs a)
             const uint32_t vl = i / U;
             const int u = (int)(i - vl * U);
             const LowpVertex vx = shfl_vertex(mine, (int)vl);
-            if (vl >= nx) continue;
+            if (vl >= nx || (vx.bits & kSkipBit)) continue;
             const uint32_t vv = v0 + x0 + vl;
             const uint32_t q = vv * U + u;
             const uint32_t nbq[6] = {q + off[0], q + off[1], q + off[2], q + off[3], q + off[4], q + off[5]};
@@ -477,7 +487,7 @@ __global__ void __launch_bounds__(256) k_sweep_lowp_sparse(LowpArgs a)
         const SparseTv t = TV ? shfl_tv(mine, (int)vl) : mine;
         const LowpVertex vx = shfl_vertex(mv, (int)vl);
         const uint32_t v = v0 + vl;
-        if (v >= a.n_act) continue;
+        if (v >= a.n_act || (vx.bits & kSkipBit)) continue;
         uint32_t nbq[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) nbq[k] = t.nb[k] * U + u;
@@ -565,7 +575,7 @@ __global__ void __launch_bounds__(kAsyncThreads, kAsyncBlocks) k_sweep_lowp_dens
             const uint32_t i = it * 32u + lane;
             const uint32_t vl = i / U;
             const LowpVertex vx = shfl_vertex(mine, (int)vl);
-            if (vl < nx) {
+            if (vl < nx && !(vx.bits & kSkipBit)) {
                 const uint32_t q = (v0 + x0 + vl) * U + (i - vl * U);
                 const uint32_t d = slot0 + (it % NS) * kAsyncStageBytes;
                 cp_async8(d, a.sh_in + q);
@@ -590,7 +600,7 @@ __global__ void __launch_bounds__(kAsyncThreads, kAsyncBlocks) k_sweep_lowp_dens
             const uint32_t vl = i / U;
             const int u = (int)(i - vl * U);
             const LowpVertex vx = shfl_vertex(mine, (int)vl);
-            if (vl >= nx) continue;
+            if (vl >= nx || (vx.bits & kSkipBit)) continue;
             const uint32_t vv = v0 + x0 + vl;
             const uint32_t q = vv * U + u;
             const QuadStaged src{slot0 + (it % NS) * kAsyncStageBytes, stride, g0 + (it % NS) * kAsyncStageBytes};
@@ -639,7 +649,7 @@ __global__ void __launch_bounds__(kAsyncThreads, kAsyncBlocks) k_sweep_lowp_spar
         const SparseTv t = TV ? shfl_tv(mine, (int)vl) : mine;
         const LowpVertex vx = shfl_vertex(mv, (int)vl);
         const uint32_t v = v0 + vl;
-        if (v < a.n_act) {
+        if (v < a.n_act && !(vx.bits & kSkipBit)) {
             const uint32_t q = v * U + u;
             const uint32_t d = slot0 + (it % NS) * kAsyncStageBytes;
             cp_async8(d, a.sh_in + q);
@@ -665,7 +675,7 @@ __global__ void __launch_bounds__(kAsyncThreads, kAsyncBlocks) k_sweep_lowp_spar
         const int u = (int)(i - vl * U);
         const LowpVertex vx = shfl_vertex(mv, (int)vl);
         const uint32_t v = v0 + vl;
-        if (v >= a.n_act) continue;
+        if (v >= a.n_act || (vx.bits & kSkipBit)) continue;
         const QuadStaged src{slot0 + (it % NS) * kAsyncStageBytes, stride, g0 + (it % NS) * kAsyncStageBytes};
         lowp_quad_x2<PREC, TV>(a, v, v * U + u, u, vx, src, s_bc[0], s_bc[1], s_key);
     }
@@ -765,6 +775,11 @@ cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_
     a.dense_mirror = g->sparse ? g->dense_mirror : nullptr;
     a.sh_in = reinterpret_cast<const uint2*>(g->sh16[g->cur]);
     a.sh_out = reinterpret_cast<uint2*>(g->sh16[g->cur ^ 1]);
+    a.sparse_adam = (g->options & CPX_OPT_SPARSE_ADAM) && !g->all_touched ? 1 : 0;
+    if (a.sparse_adam) {  // in place: the skipped vertices' values stay where they are
+        a.d_out = g->dens[g->cur];
+        a.sh_out = reinterpret_cast<uint2*>(g->sh16[g->cur]);
+    }
     a.grad = reinterpret_cast<float4*>(g->grad);
     a.m = reinterpret_cast<uint2*>(g->m16);
     a.v = reinterpret_cast<uint2*>(g->v16);
@@ -791,7 +806,7 @@ cpx_status sweep_adam_lowp(cpx_grid* g, bool fused_tv, double lam_d, double lam_
                                          : launch_lowp_shape<kPrecFP16>(g, a, fused_tv, st);
     if (rc != CPX_OK) return rc;
     count_launch();
-    g->cur ^= 1;
+    if (!a.sparse_adam) g->cur ^= 1;
     g->density = g->dens[g->cur];
     g->tcur ^= 1;
     g->all_touched = 0;

@@ -406,13 +406,21 @@ cpx_status cpx_image_mask_pixels(const int* bbox, int width, int32_t* index_out,
  *                        on a second stream while the batch is shaded, and the rest after the
  *                        shading.  Results are those of the single sweep bit for bit.  Slower on
  *                        the B200 (6.1 against 4.5 ms a step at 256^3: the shading's gathers
- *                        and atomics wait behind the sweep's DRAM traffic); for comparison. */
+ *                        and atomics wait behind the sweep's DRAM traffic); for comparison;
+ * CPX_OPT_SPARSE_ADAM    mixed forms only (no reference counterpart): the optimizer sweep
+ *                        updates only the vertices the batch touched -- a vertex whose gradient
+ *                        is zero keeps its parameters and moments, as sparse Adam skips zero
+ *                        gradients -- in place, so it neither reads nor writes the others; the
+ *                        TV term applies at the updated vertices, from neighbour values that
+ *                        may already be this step's.  The grid then trains differently from the
+ *                        reference's dense Adam; bench.py --quality measures by how much. */
 #define CPX_OPT_NO_EMPTY_SKIP 1
 #define CPX_OPT_FP32_MARCH 2
 #define CPX_OPT_NO_EARLY_STOP 4
 #define CPX_OPT_FUSED_MARCH 8
 #define CPX_OPT_PLANE_SWEEP 16
 #define CPX_OPT_SPLIT_SWEEP 32
+#define CPX_OPT_SPARSE_ADAM 64
 cpx_status cpx_grid_set_options(cpx_grid* g, int options);
 
 /* TV ("variance") gradient: type 0 with 3/6/26 neighbours, type 1 voxel disparity,

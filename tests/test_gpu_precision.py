@@ -390,3 +390,36 @@ def test_dense_cell_map_is_bit_exact(cuda, dims):
     fp32.upload_params(params)
     with pytest.raises(cpx.CpxError):
         fp32.cell_map()
+
+
+def test_sparse_adam_updates_touched_vertices_only(cuda, case):
+    """CPX_OPT_SPARSE_ADAM on a BF16 grid with non-zero moments everywhere: after one batch of
+    512 rays and the fused TV + Adam sweep, every vertex the batch gave a gradient has new
+    moments, every vertex whose moments did not change kept its parameters bit for bit (dense
+    Adam would move them through their moments), and most of the 64^3 grid is such a vertex."""
+    import torch
+
+    import cpx
+
+    scene, rays = make(case, "bf16")
+    scene.set_options(cpx.OPT_SPARSE_ADAM)
+    rng = np.random.default_rng(2)
+    shape = (28, scene.actual_grid_nums)
+    scene.upload_moments(rng.normal(0, 1e-3, shape).astype(np.float32),
+                         rng.uniform(1e-8, 1e-6, shape).astype(np.float32))
+    p0 = scene.download_params()
+    m0, v0 = scene.download_moments()
+    losses = torch.zeros(512, dtype=torch.float64, device=cuda)
+    cpx.RenderUtils.renderRays_forwardBackward(scene, rays, losses, None, 0, 512, MASK_COEF, HUBER)
+    scene.check()
+    hit = np.any(scene.download_grads() != 0, axis=0)
+    cpx.Optimizer.varianceAndUpdate(scene, 1e-3, 1e-3, 0.1, 0.01, 1)
+    scene.check()
+    p1 = scene.download_params()
+    m1, v1 = scene.download_moments()
+    moved = np.any(m1 != m0, axis=0) | np.any(v1 != v0, axis=0)
+    assert hit.sum() > 0 and np.all(moved[hit])
+    assert np.array_equal(p1[:, ~moved].view(np.uint32), p0[:, ~moved].view(np.uint32))
+    assert (~moved).mean() > 0.5
+    scene.close()
+    rays.close()
