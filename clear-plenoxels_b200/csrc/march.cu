@@ -1108,7 +1108,7 @@ __device__ __forceinline__ Stage stage_init(ShadeStage<NSH>& ss, int warp, int l
 }
 
 template <int NSH, int MODE, int PREC>
-__global__ void __launch_bounds__(kShadeWarps * 32, 6) k_shade(GridView g, RaysView r,
+__global__ void __launch_bounds__(kShadeWarps * 32, 5) k_shade(GridView g, RaysView r,
                                                              const int32_t* sidx, int start,
                                                              int len, const SampleRec* samples,
                                                              float4* colours, int maxs,
@@ -1175,7 +1175,7 @@ __global__ void __launch_bounds__(1024) k_order_by_count(const int* __restrict__
 }
 
 template <int NSH, int MODE, int PREC>
-__global__ void __launch_bounds__(kShadeWarps * 32, 6)
+__global__ void __launch_bounds__(kShadeWarps * 32, 5)
     k_shade_dyn(GridView g, RaysView r, const int32_t* sidx, int start, int len, const SampleRec* samples,
                 float4* colours, int maxs, const int* counts, const double* acc, double* losses, double mask_coef,
                 float huber, uint32_t* touched, const int* order, int* ctr, int* err)
