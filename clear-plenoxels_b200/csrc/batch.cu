@@ -499,6 +499,10 @@ cpx_status cpx_batch_check(cpx_batch* b)
         set_error("a ray's march exceeded its sample bound (near/far beyond the grid box?)");
         return CPX_ERR_ITERATION_CAP;
     }
+    if (flags[0] & 32) {
+        set_error("a shading warp gave up waiting for a vertex record copy");
+        return CPX_ERR_NOT_READY;
+    }
     return CPX_OK;
 }
 

@@ -1082,15 +1082,15 @@ static_assert(kHashSlots <= 256, "the stage's slot lists hold 8-bit slot indices
 
 // The stages of a block's shading warps: a record slot of RecShape<NSH>::REC floats (16-byte
 // aligned) per lane, the warp's mbarrier and its list of occupied table slots.
-template <int NSH>
+template <int NSH, int W = kShadeWarps>
 struct ShadeStage {
-    float4 slots[kShadeWarps][32][RecShape<NSH>::NV4];
-    unsigned long long mbar[kShadeWarps];
-    uint8_t list[kShadeWarps][kHashSlots];
+    float4 slots[W][32][RecShape<NSH>::NV4];
+    unsigned long long mbar[W];
+    uint8_t list[W][kHashSlots];
 };
 
-template <int NSH>
-__device__ __forceinline__ Stage stage_init(ShadeStage<NSH>& ss, int warp, int lane, int* err)
+template <int NSH, int W = kShadeWarps>
+__device__ __forceinline__ Stage stage_init(ShadeStage<NSH, W>& ss, int warp, int lane, int* err)
 {
     Stage st;
     st.smem = (uint32_t)__cvta_generic_to_shared(&ss.slots[warp][0][0]);
@@ -1755,9 +1755,15 @@ template <int NSH, int PREC, int WARPS, int SPL>
 __global__ void __launch_bounds__(WARPS * 32, 20 / WARPS) k_shade_batched(BatchArgs a)
 {
     constexpr int kSlots = kHashSlots * SPL;
-    static_assert(WARPS * SPL * kHashSlots * 5 * 4 <= 48 * 1024, "static shared memory of the tables");
+    // the bulk record passes where the stage fits beside the tables (one sample per lane, up to
+    // four warps: the autotuner's usual shapes); the other shapes keep per-lane loads and atomics
+    constexpr bool kBulk = SPL == 1 && WARPS <= 4;
+    using StageMem = ShadeStage<NSH, kBulk ? WARPS : 1>;
+    static_assert(WARPS * SPL * kHashSlots * 5 * 4 + sizeof(StageMem) + kMaxBatchScenes * 4 <= 48 * 1024,
+                  "static shared memory of the tables and the stage");
     __shared__ uint32_t h_keys[WARPS][kSlots];
     __shared__ float h_vals[WARPS][4][kSlots];
+    __shared__ StageMem stage;
     __shared__ int s_base[kMaxBatchScenes];
     for (int i = threadIdx.x; i < a.n_scenes; i += blockDim.x) s_base[i] = a.scenes[i].ray_base;
     const int lane = threadIdx.x & 31;
@@ -1766,6 +1772,9 @@ __global__ void __launch_bounds__(WARPS * 32, 20 / WARPS) k_shade_batched(BatchA
         h_keys[warp][s] = kEmpty;
         h_vals[warp][0][s] = h_vals[warp][1][s] = h_vals[warp][2][s] = h_vals[warp][3][s] = 0.f;
     }
+    Stage stg;
+    stg.ok = true;
+    if constexpr (kBulk) stg = stage_init<NSH, WARPS>(stage, warp, lane, a.err);
     __syncthreads();
     WarpTable tab{h_keys[warp], h_vals[warp][0], h_vals[warp][1], h_vals[warp][2], h_vals[warp][3]};
     tab.n = kSlots;
@@ -1788,12 +1797,15 @@ __global__ void __launch_bounds__(WARPS * 32, 20 / WARPS) k_shade_batched(BatchA
                 continue;
             }
             const int64_t ri = (int64_t)(iter % sc.pool_batches) * sc.len + b;
-            shade_ray<NSH, kForwardBackward, PREC, SPL>(sc.g, sc.r, b, ri, cnt, a.samples + sc.sample_base,
-                                                   a.colours + sc.sample_base, sc.maxs, a.acc + sc.ray_base,
-                                                   a.losses + sc.ray_base, a.mask_coef, a.huber, tab, sc.touched,
-                                                   lane);
+            shade_ray<NSH, kForwardBackward, PREC, SPL, kBulk>(sc.g, sc.r, b, ri, cnt, a.samples + sc.sample_base,
+                                                          a.colours + sc.sample_base, sc.maxs, a.acc + sc.ray_base,
+                                                          a.losses + sc.ray_base, a.mask_coef, a.huber, tab,
+                                                          sc.touched, lane, kBulk ? &stg : nullptr);
+            if (!stg.ok) break;  // a record copy timed out (error word set)
         }
+        if (!stg.ok) break;
     }
+    if constexpr (kBulk) bulk_wait_all();  // the bulk reductions are complete before the warp exits
 }
 
 static int batch_blocks(const void* fn, int threads, int smem)
