@@ -139,9 +139,16 @@ __device__ __forceinline__ int empty_steps(const Skip& sk, const Real* bc, unsig
     return n < (Real)1 ? 1 : (n > (Real)1.0e6f ? 1000000 : (int)n);
 }
 
-// exp in the march's precision
+// exp in the march's precision.  The FP32 march of the mixed forms (not bound to the reference's
+// bits) takes the hardware approximations (__expf, __logf: a few ulp), which shorten its
+// per-sample dependent chain; the FP64/FP32 placement of the FP32 form keeps the reference's
+// exp / expf / logf.
 __device__ __forceinline__ double real_exp(double x) { return exp(x); }
-__device__ __forceinline__ float real_exp(float x) { return expf(x); }
+__device__ __forceinline__ float real_exp(float x) { return __expf(x); }
+__device__ __forceinline__ float march_expf(double, float x) { return expf(x); }
+__device__ __forceinline__ float march_expf(float, float x) { return __expf(x); }
+__device__ __forceinline__ float march_logf(double, float x) { return logf(x); }
+__device__ __forceinline__ float march_logf(float, float x) { return __logf(x); }
 
 // ---------------------------------------------------------------------------
 // Sample placement: one thread per ray.  With Real = double this is the reference's
@@ -345,8 +352,8 @@ __device__ __forceinline__ bool place_iter(PlaceRay<Real>& st, const GridView& g
         if (Ti < (Real)sk.t_stop) return true;  // FP32 march: nothing visible remains behind
     }
     // density_activation (RenderUtils.cu:491) and the weight (RenderUtils.cu:1693-1704)
-    const float sigma = logf(1.f + expf(tri0 - 13.f));
-    const Real w = Ti * (one - expf(-sigma * step));
+    const float sigma = march_logf(one, 1.f + march_expf(one, tri0 - 13.f));
+    const Real w = Ti * (one - march_expf(one, -sigma * step));
     st.acc += w;
     st.accDen += sigma;
     st.accD += sigma * step;
