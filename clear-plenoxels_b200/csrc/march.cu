@@ -23,6 +23,8 @@
 // Reference citations: file:line in SparseVolumeRadianceField/.
 #include "cpx_internal.cuh"
 
+#include <cstdlib>
+#include <mutex>
 #include <type_traits>
 
 namespace cpx {
@@ -1064,13 +1066,19 @@ __device__ __forceinline__ void shade_ray(const GridView& g, const RaysView& r, 
 // The two stages as kernels.  Placement is latency-bound per ray and needs only one thread
 // per ray, all resident in one wave; shading is throughput-bound and takes a warp per ray.
 // ---------------------------------------------------------------------------
+// A placement block is one warp that marches `lanes` rays (lanes 0 .. lanes-1; the others exit
+// at once).  Each ray is a dependent chain, and the lanes of a warp run in lock step: with 32
+// rays a warp, nearly every iteration takes some lane into a new cell, so every lane pays for
+// the cell's corner loads and waits on the slowest of them.  Fewer rays a warp spread the same
+// chains over more warps, which the SM's schedulers interleave.
 template <int MODE, typename Real, bool PROP>
 __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int32_t* sidx, int start,
                                                int len, int64_t n_rays, SampleRec* samples, int maxs,
                                                int* counts, double* acc, int* err, const uint32_t* seg_masks,
-                                               float* seg_w, Skip sk)
+                                               float* seg_w, Skip sk, int lanes)
 {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((int)threadIdx.x >= lanes) return;
+    const int b = blockIdx.x * lanes + threadIdx.x;
     if (b >= len) return;
     const int64_t ri = sidx ? (int64_t)sidx[start + b] : (int64_t)start + b;
     if (ri < 0 || ri >= n_rays) {
@@ -1081,6 +1089,46 @@ __global__ void __launch_bounds__(32) k_place(GridView g, RaysView r, const int3
     const uint32_t mask = PROP && seg_masks ? seg_masks[b] : 0xffffffffu;
     float* sw = PROP && seg_w ? seg_w + (size_t)b * kProposalSegments : nullptr;
     place_ray<Real, PROP>(g, r, b, ri, samples, maxs, counts, acc, err, (MODE & kForward) != 0, mask, sw, sk);
+}
+
+// Rays a placement warp marches: the fewest (down to a floor, kPlaceLanesFloor or the
+// CPX_PLACE_LANES environment variable) that still keep every warp of the batch resident at
+// once, since a second wave would add a whole chain's length to the launch.
+constexpr int kPlaceLanesFloor = 8;
+
+static int place_lanes(const void* kernel, int len)
+{
+    struct Entry {
+        const void* fn;
+        int dev, resident;
+    };
+    static Entry cache[32];
+    static int n_cache = 0;
+    static std::mutex mu;
+    static int floor_lanes = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int resident = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (floor_lanes == 0) {
+            const char* e = getenv("CPX_PLACE_LANES");
+            const int v = e ? atoi(e) : kPlaceLanesFloor;
+            floor_lanes = (v == 1 || v == 2 || v == 4 || v == 8 || v == 16 || v == 32) ? v : kPlaceLanesFloor;
+        }
+        for (int i = 0; i < n_cache; i++)
+            if (cache[i].fn == kernel && cache[i].dev == dev) resident = cache[i].resident;
+        if (resident == 0) {
+            int sms = 0, per = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 32, 0);
+            resident = sms * (per > 0 ? per : 1);
+            if (n_cache < 32) cache[n_cache++] = Entry{kernel, dev, resident};
+        }
+    }
+    int lanes = 32;
+    while (lanes > floor_lanes && (len + lanes / 2 - 1) / (lanes / 2) <= resident) lanes /= 2;
+    return lanes;
 }
 
 constexpr int kShadeWarps = 4;
@@ -1517,20 +1565,26 @@ static void launch_mode(cudaStream_t st, const GridView& gv, const RaysView& rv,
                                                          huber, touched, guide);
         return;
     }
-    const dim3 pgrid((unsigned)((len + 31) / 32));
     const dim3 sgrid((unsigned)((len + kShadeWarps - 1) / kShadeWarps));
     const dim3 sblock(kShadeWarps * 32);
     if (!(guide.stages & 1)) {
         // placement already done (a look-ahead step placed this batch under the last sweep)
-    } else if (guide.march32 && guide.on())
-        k_place<MODE, float, true><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
-                                                         s.counts, s.acc, s.err, guide.masks, guide.seg_w, guide.skip);
-    else if (guide.march32)
-        k_place<MODE, float, false><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
-                                                          s.counts, s.acc, s.err, nullptr, nullptr, guide.skip);
-    else
-        k_place<MODE, double, false><<<pgrid, 32, 0, st>>>(gv, rv, sidx, start, len, n_rays, s.samples, s.maxs,
-                                                           s.counts, s.acc, s.err, nullptr, nullptr, guide.skip);
+    } else if (guide.march32 && guide.on()) {
+        const int lanes = place_lanes((const void*)k_place<MODE, float, true>, len);
+        k_place<MODE, float, true><<<(len + lanes - 1) / lanes, 32, 0, st>>>(
+            gv, rv, sidx, start, len, n_rays, s.samples, s.maxs, s.counts, s.acc, s.err, guide.masks, guide.seg_w,
+            guide.skip, lanes);
+    } else if (guide.march32) {
+        const int lanes = place_lanes((const void*)k_place<MODE, float, false>, len);
+        k_place<MODE, float, false><<<(len + lanes - 1) / lanes, 32, 0, st>>>(
+            gv, rv, sidx, start, len, n_rays, s.samples, s.maxs, s.counts, s.acc, s.err, nullptr, nullptr, guide.skip,
+            lanes);
+    } else {
+        const int lanes = place_lanes((const void*)k_place<MODE, double, false>, len);
+        k_place<MODE, double, false><<<(len + lanes - 1) / lanes, 32, 0, st>>>(
+            gv, rv, sidx, start, len, n_rays, s.samples, s.maxs, s.counts, s.acc, s.err, nullptr, nullptr, guide.skip,
+            lanes);
+    }
     if (!(guide.stages & 2)) return;
     if (s.queue) {
         // longest rays first from a work counter (the queue's first word and its ray slots)
