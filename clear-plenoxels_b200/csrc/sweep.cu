@@ -13,6 +13,9 @@
 //
 // TV and Adam arithmetic is FP32 (the reference mixes double into the TV
 // division and the Adam update; the FP32 results differ from it by a few ulp).
+// The fused sweep takes its square roots from the hardware approximation
+// (sqrt.approx, about an ulp); the standalone TV kernels keep sqrtf and the
+// division by the neighbour count as the reference writes them.
 #include "cpx_internal.cuh"
 
 namespace cpx {
@@ -65,7 +68,10 @@ __device__ __forceinline__ float tv6(float self, const float* nb, float lam)
         sum += d * d;
         disp = (j == 0) ? d : disp + d;
     }
-    const float sd = sqrtf(sum) / 6.f;
+    // sqrt(sum) / 6 (RenderUtils.cu:2708) by the hardware square root and a multiply: the IEEE
+    // square root and division take a dozen instructions each with their special-case checks,
+    // in a sweep that issues about 450 instructions per slot; the result differs by an ulp or two
+    const float sd = sqrt_approx(sum) * (1.f / 6.f);
     return __fdividef(lam * disp, sd + 1.e-6f);
 }
 
@@ -100,7 +106,7 @@ __device__ __forceinline__ float4 slot_update(const SweepArgs& a, int j, bool tv
         f4set(m, c, mc);
         f4set(vv, c, vc);
         const float lr = e == 0 ? lr_density : a.sh_lr;
-        float np = f4get(p, c) - __fdividef(lr * (mc * inv_bc1), sqrtf(vc * inv_bc2) + eps);
+        float np = f4get(p, c) - __fdividef(lr * (mc * inv_bc1), sqrt_approx(vc * inv_bc2) + eps);
         if (e == 0) np = np < 0.f ? 0.f : np;  // density clamp (Optimizer.cu:384)
         f4set(pn, c, np);
         f4set(g, c, 0.f);
