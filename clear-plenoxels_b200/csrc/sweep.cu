@@ -43,6 +43,7 @@ struct SweepArgs {
     int timestep;
     const int* t_dev;  // when set, the timestep is *t_dev + 1 (a replayed CUDA graph)
     int pass;          // 0: every vertex; 1: untouched vertices only; 2: touched vertices only
+    int full_masks;    // every element of a record takes TV and Adam (no padding, no hierarchy)
 };
 
 __device__ __forceinline__ float f4get(const float4& v, int c)
@@ -77,8 +78,9 @@ __device__ __forceinline__ float tv6(float self, const float* nb, float lam)
 
 // The arithmetic of one 16-byte slot: optional TV term from the six neighbour slots nbv (the
 // reference's order z-1, y-1, x-1, x+1, y+1, z+1), then Adam.  g, m, vv are updated in place
-// (g to zero where Adam ran); returns the new parameters.
-template <bool TV>
+// (g to zero where Adam ran); returns the new parameters.  FULL: every element takes TV and
+// Adam (SweepArgs::full_masks), so the per-element mask tests drop out.
+template <bool TV, bool FULL = false>
 __device__ __forceinline__ float4 slot_update(const SweepArgs& a, int j, bool tv_on, const float4& p,
                                               const float4* nbv, float4& g, float4& m, float4& vv, float inv_bc1,
                                               float inv_bc2, float lr_density)
@@ -88,7 +90,7 @@ __device__ __forceinline__ float4 slot_update(const SweepArgs& a, int j, bool tv
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const int e = 4 * j + c;
-            if (!((a.tv_mask >> e) & 1u)) continue;
+            if (!FULL && !((a.tv_mask >> e) & 1u)) continue;
             float nb[6];
 #pragma unroll
             for (int k = 0; k < 6; k++) nb[k] = f4get(nbv[k], c);
@@ -99,7 +101,7 @@ __device__ __forceinline__ float4 slot_update(const SweepArgs& a, int j, bool tv
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const int e = 4 * j + c;
-        if (!((a.adam_mask >> e) & 1u)) continue;
+        if (!FULL && !((a.adam_mask >> e) & 1u)) continue;
         const float gc = f4get(g, c);
         const float mc = fmaf(1.f - beta1, gc, beta1 * f4get(m, c));
         const float vc = fmaf((1.f - beta2) * gc, gc, beta2 * f4get(vv, c));
@@ -134,7 +136,8 @@ __device__ __forceinline__ void sweep_slot(const SweepArgs& a, uint32_t sl, uint
 #pragma unroll
         for (int k = 0; k < 6; k++) nbv[k] = nb_self[k] ? p : a.p_in[nb_slot[k]];
     }
-    const float4 pn = slot_update<TV>(a, j, tv_on, p, nbv, g, m, vv, inv_bc1, inv_bc2, lr_density);
+    const float4 pn = a.full_masks ? slot_update<TV, true>(a, j, tv_on, p, nbv, g, m, vv, inv_bc1, inv_bc2, lr_density)
+                                   : slot_update<TV>(a, j, tv_on, p, nbv, g, m, vv, inv_bc1, inv_bc2, lr_density);
     a.p_out[sl] = pn;
     a.m[sl] = m;
     a.v[sl] = vv;
@@ -513,6 +516,8 @@ static SweepArgs sweep_args(const cpx_grid* g, double lam_d, double lam_sh, doub
     a.touched = g->all_touched ? nullptr : g->touched[g->tcur];
     a.clear = g->touched[g->tcur ^ 1];
     element_masks(g, &a.tv_mask, &a.adam_mask);
+    const uint32_t all = g->rec >= 32 ? 0xffffffffu : (1u << g->rec) - 1u;
+    a.full_masks = (a.tv_mask & all) == all && (a.adam_mask & all) == all ? 1 : 0;
     a.lam_d = (float)lam_d;
     a.lam_sh = (float)lam_sh;
     a.lr = (float)lr;
