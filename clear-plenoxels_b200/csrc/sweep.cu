@@ -14,7 +14,7 @@
 // TV and Adam arithmetic is FP32 (the reference mixes double into the TV
 // division and the Adam update; the FP32 results differ from it by a few ulp).
 // The fused sweep takes its square roots from the hardware approximation
-// (sqrt.approx, about an ulp); the standalone TV kernels keep sqrtf and the
+// (sqrt.approx.ftz, about an ulp); the standalone TV kernels keep sqrtf and the
 // division by the neighbour count as the reference writes them.
 #include "cpx_internal.cuh"
 
@@ -58,6 +58,15 @@ __device__ __forceinline__ void f4set(float4& v, int c, float x)
     else v.w = x;
 }
 
+// Hardware square root (about an ulp), a denormal argument flushed to zero: a TV sum or an Adam
+// second moment below 1.2e-38 changes no FP32 result the sweep writes.
+__device__ __forceinline__ float sqrt_ftz(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // The six-neighbour TV term for one parameter (RenderUtils.cu:2672-2757); neighbours in
 // the reference's order z-1, y-1, x-1, x+1, y+1, z+1.
 __device__ __forceinline__ float tv6(float self, const float* nb, float lam)
@@ -72,7 +81,7 @@ __device__ __forceinline__ float tv6(float self, const float* nb, float lam)
     // sqrt(sum) / 6 (RenderUtils.cu:2708) by the hardware square root and a multiply: the IEEE
     // square root and division take a dozen instructions each with their special-case checks,
     // in a sweep that issues about 450 instructions per slot; the result differs by an ulp or two
-    const float sd = sqrt_approx(sum) * (1.f / 6.f);
+    const float sd = sqrt_ftz(sum) * (1.f / 6.f);
     return __fdividef(lam * disp, sd + 1.e-6f);
 }
 
@@ -108,7 +117,7 @@ __device__ __forceinline__ float4 slot_update(const SweepArgs& a, int j, bool tv
         f4set(m, c, mc);
         f4set(vv, c, vc);
         const float lr = e == 0 ? lr_density : a.sh_lr;
-        float np = f4get(p, c) - __fdividef(lr * (mc * inv_bc1), sqrt_approx(vc * inv_bc2) + eps);
+        float np = f4get(p, c) - __fdividef(lr * (mc * inv_bc1), sqrt_ftz(vc * inv_bc2) + eps);
         if (e == 0) np = np < 0.f ? 0.f : np;  // density clamp (Optimizer.cu:384)
         f4set(pn, c, np);
         f4set(g, c, 0.f);

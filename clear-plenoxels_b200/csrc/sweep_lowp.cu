@@ -229,12 +229,13 @@ __device__ __forceinline__ void lowp_unit(const LowpArgs& a, uint32_t v, uint32_
 }
 
 // Hardware approximations (about 1 ulp) of the square root and of the reciprocal of each half
-// of a pair; the reciprocal takes arguments of at least 1e-6 here (no denormals to flush).
+// of a pair, denormal arguments flushed to zero (a TV sum or second moment that small adds
+// nothing a 16-bit value can hold); the reciprocal takes arguments of at least 1e-6 here.
 __device__ __forceinline__ float2 sqrt2_approx(float2 x)
 {
     float2 r;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(r.x) : "f"(x.x));
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(r.y) : "f"(x.y));
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(x.x));
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(x.y));
     return r;
 }
 __device__ __forceinline__ float2 rcp2_approx(float2 x)
